@@ -1,0 +1,234 @@
+/*
+ * ptb200.h -- C ABI of libptb200.so, the B200 (sm_100a) implementation of the
+ * trajectory and transport-statistics hot path of particle_transport.
+ *
+ * The reference has no FFI layer: its hot path sits behind Julia functions.
+ * Each entry point below names the reference function (file:line, paths in
+ * the reference project) whose body it replaces; the Julia host keeps the
+ * function's signature, its HDF5 I/O and its config handling and calls the
+ * library through ccall (see INTEGRATION.md for the bindings).
+ *
+ * Conventions
+ *  - Every function returns PT_OK (0) or a negative PT_ERR_* code; the
+ *    message of the last failure on the calling thread is pt_last_error().
+ *  - Host arrays are owned by the caller and use the reference's Julia
+ *    (column-major) layouts, spelled out per argument below.  The library
+ *    never frees caller memory.  Device memory lives behind opaque handles.
+ *  - Statistics accumulators are add-into, like the reference's `+=` across
+ *    particle chunks; per-lag Welford triples are merged with the reference's
+ *    combine_welford_stats! formula (Chan et al.).
+ *  - NaN marks dead or invalid samples, exactly as in the reference.
+ *  - A pt_ctx is not re-entrant: use one per host thread / Julia task.
+ *    Calls are synchronous unless their name ends in _device (those enqueue
+ *    on the context stream and take device pointers).
+ */
+#ifndef PTB200_H
+#define PTB200_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define PTB200_VERSION 1
+
+enum {
+    PT_OK = 0,
+    PT_ERR_ARG = -1,      /* invalid argument (null, size, range)                 */
+    PT_ERR_CUDA = -2,     /* CUDA runtime failure                                 */
+    PT_ERR_OOM = -3,      /* device allocation failed / over the device budget    */
+    PT_ERR_TIMEOUT = -4,  /* a bounded device-side wait gave up                    */
+    PT_ERR_CALLBACK = -5, /* the caller's save callback returned non-zero          */
+    PT_ERR_STATE = -6     /* object used in the wrong state                        */
+};
+
+/* field storage on the device */
+enum {
+    PT_FIELD_REF_F64 = 0, /* six column-major Float64 arrays, SI units (parity form)        */
+    PT_FIELD_BRICK_F32 = 1, /* Morton 8^3 bricks, 6 comps interleaved per node, Float32      */
+    PT_FIELD_BRICK_BF16 = 2 /* Morton 8^3 bricks, 6 comps interleaved per node, bfloat16     */
+};
+
+/* cache written at every save step (pre-push state) */
+enum { PT_CACHE_NONE = 0, PT_CACHE_MU = 1, PT_CACHE_PHASE_SPACE = 2 };
+
+/* push arithmetic */
+enum { PT_PUSH_F64 = 0, PT_PUSH_F32 = 1 };
+
+/* D_mumu estimator (dmumu_start_mode) */
+enum { PT_START_SLIDING = 0, PT_START_INJECTION = 1 };
+
+typedef struct pt_ctx pt_ctx;
+typedef struct pt_field pt_field;
+
+/* Node grid: nodes at xmin + i*dx, i = 0..nx-1 (reference build_uniform_coords,
+ * src/phase_space_gpu_runner.jl:125-130: xmin = x[1], xmax = x[end],
+ * dx = x[2] - x[1]). */
+typedef struct {
+    int64_t nx, ny, nz;
+    double xmin, ymin, zmin;
+    double xmax, ymax, zmax;
+    double dx, dy, dz;
+} pt_grid;
+
+typedef struct {
+    double dt;                /* integration step [s] (trajectory_time.dt_s)            */
+    int64_t nsteps;           /* integration samples; nsteps-1 pushes                   */
+    int64_t stride;           /* save stride; saves at steps 0, stride, ... (0-based)   */
+    int32_t periodic;         /* 1: wrap positions, 0: open boundary (kill on exit)     */
+    int32_t cache_mode;       /* PT_CACHE_*                                             */
+    int32_t cache_f64;        /* 0: Float32 cache (reference default), 1: Float64       */
+    int32_t precision;        /* PT_PUSH_F64 (REF_F64 field) or PT_PUSH_F32 (bricks)    */
+    int32_t steps_per_launch; /* steps kept in registers per launch; 0 = auto           */
+    int32_t sort_every;       /* F32 form: re-sort particles by brick every N steps; 0 off */
+} pt_push_params;
+
+/* Save sink for pt_push_run: called on the calling thread once per save row,
+ * in save order.  data holds the row in the cache layout of the reference
+ * writers: mu: n values (src/multimode_multienergy_cache_pipeline.jl:1318-1321);
+ * phase space: positions[3][n] then momenta[3][n]
+ * (src/phase_space_gpu_runner.jl:413-421).  Return non-zero to abort. */
+typedef int (*pt_save_fn)(void* user, int64_t save_index, const void* data, int64_t nbytes);
+
+const char* pt_last_error(void);
+int pt_version(void);
+
+int pt_ctx_create(int device, pt_ctx** out);
+int pt_ctx_destroy(pt_ctx* ctx);
+/* Use the given cudaStream_t for all *_device entry points (NULL = library stream). */
+int pt_ctx_set_stream(pt_ctx* ctx, void* cuda_stream);
+int pt_ctx_synchronize(pt_ctx* ctx);
+
+/* Upload a static field library (load_static_fields output,
+ * src/phase_space_gpu_runner.jl:95-123; SI units: B in T, u in m/s).
+ * comps = {Bx, By, Bz, ux, uy, uz}, each nx*ny*nz doubles, x fastest.
+ * storage = PT_FIELD_*; B_ref_T scales the nondimensional brick forms
+ * (B stored as B/B_ref_T, u as u/c); it is ignored for REF_F64. */
+int pt_field_upload(pt_ctx* ctx, const double* const comps[6], const pt_grid* grid, int storage,
+                    double B_ref_T, pt_field** out);
+/* Same, from device pointers (e.g. fields generated on the GPU). */
+int pt_field_upload_device(pt_ctx* ctx, const double* const d_comps[6], const pt_grid* grid, int storage,
+                           double B_ref_T, pt_field** out);
+int pt_field_destroy(pt_field* field);
+int64_t pt_field_device_bytes(const pt_field* field);
+
+/*
+ * Whole-ensemble push with host state: replaces the body of
+ *   run_gpu_ensemble       src/phase_space_gpu_runner.jl:476 (lines 506-592)
+ *   run_mu_cache_ensemble  src/multimode_multienergy_cache_pipeline.jl:1380 (lines 1410-1500)
+ * x1..p3: n doubles each (SI), updated in place to the final state; alive: n
+ * bytes (1 live), updated in place.  Each save row is handed to `save` on the
+ * calling thread while the next steps run on the GPU.  alive_count[nsteps]
+ * receives sum(dalive) after each step (src/phase_space_gpu_runner.jl:576).
+ */
+int pt_push_run(pt_ctx* ctx, const pt_field* field, double* x1, double* x2, double* x3, double* p1, double* p2,
+                double* p3, uint8_t* alive, int64_t n, const pt_push_params* params, pt_save_fn save, void* user,
+                int64_t* alive_count);
+
+/*
+ * Device-resident push of steps [step_begin, step_begin + step_count) on the
+ * context stream (advance_particles_kernel!, src/phase_space_gpu_runner.jl:330-391,
+ * fused with reconstruct_mu_step_kernel!, pipeline:1349-1374).
+ * PT_PUSH_F64: d_x1..d_p3 are the SI Float64 state (n each).
+ * PT_PUSH_F32: the state is a pt_fast_state created by pt_fast_state_create
+ *   and d_x1..d_p3 must be NULL (pass the state via pt_push_advance_fast).
+ * Save rows r in [cache_row_base, cache_row_base + cache_rows) are written to
+ * d_cache + (r - cache_row_base) * row_elems (mu: n elements; phase space:
+ * 6n, positions then momenta).  d_deaths[nsteps] (int64, may be NULL)
+ * counts particles killed at each step (open boundary).
+ */
+int pt_push_advance_device(pt_ctx* ctx, const pt_field* field, double* d_x1, double* d_x2, double* d_x3,
+                           double* d_p1, double* d_p2, double* d_p3, uint8_t* d_alive, int64_t n,
+                           const pt_push_params* params, int64_t step_begin, int64_t step_count, void* d_cache,
+                           int64_t cache_row_base, int64_t cache_rows, int64_t* d_deaths);
+
+/* Mixed-precision state (FP32 momentum, FP64 positions in cell units, FP64
+ * |p|^2 per particle, particle ids and optional brick sort).  Converts from /
+ * to the SI Float64 state. */
+typedef struct pt_fast_state pt_fast_state;
+int pt_fast_state_create(pt_ctx* ctx, const pt_field* field, const double* d_x1, const double* d_x2,
+                         const double* d_x3, const double* d_p1, const double* d_p2, const double* d_p3,
+                         const uint8_t* d_alive, int64_t n, pt_fast_state** out);
+int pt_fast_state_export(pt_ctx* ctx, const pt_fast_state* st, double* d_x1, double* d_x2, double* d_x3,
+                         double* d_p1, double* d_p2, double* d_p3, uint8_t* d_alive);
+int pt_fast_state_destroy(pt_fast_state* st);
+/* Re-sort the particle slots by the brick holding their cell (one-digit
+ * radix / counting sort); results do not depend on the slot order.  Runs on
+ * the context stream.  No reference counterpart (the reference keeps the
+ * particles in index order). */
+int pt_fast_state_sort(pt_ctx* ctx, pt_fast_state* st);
+int pt_push_advance_fast(pt_ctx* ctx, const pt_field* field, pt_fast_state* st, const pt_push_params* params,
+                         int64_t step_begin, int64_t step_count, void* d_cache, int64_t cache_row_base,
+                         int64_t cache_rows, int64_t* d_deaths);
+
+/*
+ * D_mumu / <dmu^2> lag-pair accumulation: replaces process_mu_chunk_dmumu_cpu!
+ *   src/compute_delta_mu2_dmumu_full.jl:656 (sliding :457-560, injection :562-654),
+ * called from pipeline:1718 and dmumu:1150.
+ * mu: Float32, element (particle p, save s) at mu[p*sp + s*ss]; the Julia
+ *   mu_chunk (nsave, chunk) is sp = nsave, ss = 1; the device mu cache
+ *   [nsave][n] is sp = 1, ss = n.
+ * lag_steps[n_lags]: save offsets (same in 0- and 1-based indexing).
+ * mu_edges[n_bins+1]: the Float64 edges of build_mu_edges_full (dmumu:289-302).
+ * counts/sum_d/sum_d2: Julia (n_bins, n_lags) = [lag][bin], add-into.
+ * w_count/w_mean/w_m2/pair_ss/pair_n: [n_lags], merged / added into.
+ * Host pointers (synchronous).
+ */
+int pt_dmumu_accumulate(pt_ctx* ctx, const float* mu, int64_t n, int64_t nsave, int64_t sp, int64_t ss,
+                        const int64_t* lag_steps, int n_lags, const double* mu_edges, int n_bins, int start_mode,
+                        int bin_abs, int64_t* counts, double* sum_d, double* sum_d2, int64_t* w_count,
+                        double* w_mean, double* w_m2, double* pair_ss, int64_t* pair_n);
+/* Same with device pointers for mu, lag_steps, mu_edges and all accumulators
+ * (enqueued on the context stream). */
+int pt_dmumu_accumulate_device(pt_ctx* ctx, const float* d_mu, int64_t n, int64_t nsave, int64_t sp, int64_t ss,
+                               const int64_t* d_lag_steps, int n_lags, const double* d_mu_edges, int n_bins,
+                               int start_mode, int bin_abs, int64_t* d_counts, double* d_sum_d, double* d_sum_d2,
+                               int64_t* d_w_count, double* d_w_mean, double* d_w_m2, double* d_pair_ss,
+                               int64_t* d_pair_n);
+
+/*
+ * D_pp lag statistics: replaces process_momenta_chunk_dpp_cpu!
+ *   src/compute_dpp_full.jl:247-288.
+ * mom: Float32 phase-space momenta, Julia (chunk, 3, nsave): element
+ *   (p, c, s) at mom[(s*3 + c)*chunk + p].
+ * counts/sdp/sdp2/sdn/sdn2: [n_lags], add-into.
+ */
+int pt_dpp_accumulate(pt_ctx* ctx, const float* mom, int64_t chunk, int64_t nsave, const int64_t* lag_steps,
+                      int n_lags, double p0, int64_t* counts, double* sdp, double* sdp2, double* sdn, double* sdn2);
+int pt_dpp_accumulate_device(pt_ctx* ctx, const float* d_mom, int64_t chunk, int64_t nsave,
+                             const int64_t* d_lag_steps, int n_lags, double p0, int64_t* d_counts, double* d_sdp,
+                             double* d_sdp2, double* d_sdn, double* d_sdn2);
+
+/*
+ * Kinetic-energy snapshots: replaces fill_energy_snapshots!
+ *   src/compute_dpp_full.jl:290-299 (kinetic_energy_gev_from_pmag :236-240).
+ * snap_steps[n_snap]: 0-based save indices.  out: Julia (n_snap, n_total)
+ * Float64, written for columns particle_offset .. particle_offset+chunk-1.
+ */
+int pt_energy_snapshots(pt_ctx* ctx, const float* mom, int64_t chunk, int64_t nsave, const int64_t* snap_steps,
+                        int n_snap, int64_t particle_offset, double* out);
+/* On-device histogram of the snapshot energies into n_hist log-spaced bins on
+ * [e_min, e_max] GeV (counts[n_snap][n_hist], add-into; out-of-range and NaN
+ * energies are not counted).  No reference counterpart: the reference stores
+ * the raw energies and bins them in Python (scripts/plot_energy_distribution.py:167-174). */
+int pt_energy_histogram_device(pt_ctx* ctx, const float* d_mom, int64_t chunk, int64_t nsave,
+                               const int64_t* d_snap_steps, int n_snap, double e_min, double e_max, int n_hist,
+                               int64_t* d_counts);
+
+/*
+ * Phase-space mu reconstruction: replaces reconstruct_mu_chunk_gpu
+ *   src/compute_delta_mu2_curve.jl:186-225 (kernel :151-184).
+ * pos/mom: Julia (chunk, 3, nsave) in the compute precision (f32: float,
+ * f64: double); bfield = {Bx, By, Bz} host column-major in the compute
+ * precision; grid scalars already in that precision.
+ * mu_out: Julia (nsave, chunk) = [p][s] (time fastest).
+ */
+int pt_reconstruct_mu(pt_ctx* ctx, const void* pos, const void* mom, int64_t chunk, int64_t nsave,
+                      const void* const bfield[3], const pt_grid* grid, int f64, void* mu_out);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* PTB200_H */

@@ -1,0 +1,632 @@
+// Lag-pair statistics on the device.
+//
+// D_mumu / <dmu^2> (process_mu_chunk_dmumu_cpu!, src/compute_delta_mu2_dmumu_full.jl:457-704)
+// -----------------------------------------------------------------------------------------
+// Work unit = (particle, lag).  A warp owns one particle and 32 lags (lane =
+// lag); all lanes therefore visit the same start save s at the same time, and
+// the bin of a pair depends only on mu(s).  Each particle's mu series is
+// staged on chip together with the list of its valid start saves sorted
+// (stably) by start bin, so the pair loop runs bin by bin: every lane keeps
+// (count, sum dmu, sum dmu^2) for the current bin in registers and flushes
+// once per bin per particle into the CTA's shared (bin, lag) accumulators.
+// Per-particle <dmu^2> values feed per-lane Welford triples in registers.
+// CTA results go to per-CTA partials and a finalize kernel reduces them in
+// CTA order, merging Welford triples with the reference formula
+// (combine_welford_stats!, :439-455).  Integer counts are exact; FP64 sums
+// differ from the reference only by summation order.
+//
+// D_pp (process_momenta_chunk_dpp_cpu!, src/compute_dpp_full.jl:247-288)
+// ---------------------------------------------------------------------
+// Same layout without bins: |p| is computed once per (particle, save) in FP64
+// and every lane keeps its lag's five sums in registers for the whole launch.
+#include "pt_internal.cuh"
+
+#include <algorithm>
+
+namespace pt {
+namespace {
+
+constexpr int kWarp = 32;
+
+struct WelfordPart {
+    long long count;
+    double mean, m2, pair_ss;
+    long long pair_n;
+};
+
+// combine_welford_stats! (src/compute_delta_mu2_dmumu_full.jl:439-455)
+__device__ __forceinline__ void welford_merge(long long& gc, double& gm, double& gm2, long long lc, double lm,
+                                              double lm2)
+{
+    if (lc <= 0) return;
+    if (gc == 0) {
+        gc = lc; gm = lm; gm2 = lm2;
+        return;
+    }
+    long long cc = gc + lc;
+    double delta = lm - gm;
+    gm += delta * (double)lc / (double)cc;
+    gm2 += lm2 + delta * delta * (double)gc * (double)lc / (double)cc;
+    gc = cc;
+}
+
+// mu_bin_value + mu_bin_index_full (dmumu:304-318): 0-based bin, n_bins for a
+// finite value outside [edges[0], edges[n_bins]], -1 for a non-finite value.
+__device__ __forceinline__ int bin_of(float mu, const double* __restrict__ edges, int n_bins, int bin_abs)
+{
+    double v = (double)mu;
+    if (!isfinite(v)) return -1;
+    if (bin_abs) v = fabs(v);
+    if (v < edges[0] || v > edges[n_bins]) return n_bins;
+    int lo = 0, hi = n_bins + 1;
+    while (lo < hi) {
+        int mid = (lo + hi) >> 1;
+        if (edges[mid] <= v) lo = mid + 1;
+        else hi = mid;
+    }
+    if (lo == n_bins + 1) return n_bins - 1;
+    return lo < 1 ? n_bins : lo - 1;
+}
+
+struct DmumuLaunch {
+    const float* mu;
+    int64_t n, nsave, sp, ss;
+    int64_t start_cap;         // 1 for the injection estimator, nsave for sliding
+    const int64_t* lags;       // this batch's lags
+    int nl;                    // lags in this batch
+    const double* edges;
+    int n_bins, bin_abs;
+    int ppc, groups;           // particle slots per CTA, 32-lag groups per slot
+    size_t slot_bytes;
+    char* gslots;              // global staging when the slots do not fit on chip
+    // per-CTA outputs
+    unsigned long long* part_cnt;  // [grid][nl][n_bins]
+    double* part_sd;
+    double* part_sd2;
+    WelfordPart* part_w;           // [grid][nl]
+};
+
+template <typename IdxT, bool SMEM_SLOTS>
+__global__ void __launch_bounds__(1024) dmumu_kernel(DmumuLaunch a)
+{
+    extern __shared__ __align__(16) unsigned char smem[];
+    const int nb = a.n_bins, nl = a.nl;
+    // shared layout: edges | acc_cnt | acc_sd | acc_sd2 | slots
+    double* s_edges = (double*)smem;
+    size_t off = ((size_t)(nb + 1) * sizeof(double) + 15) & ~(size_t)15;
+    unsigned long long* acc_cnt = (unsigned long long*)(smem + off);
+    off += (size_t)nl * nb * sizeof(unsigned long long);
+    double* acc_sd = (double*)(smem + off);
+    off += (size_t)nl * nb * sizeof(double);
+    double* acc_sd2 = (double*)(smem + off);
+    off += (size_t)nl * nb * sizeof(double);
+    unsigned char* slot_base = SMEM_SLOTS ? (smem + off) : (unsigned char*)(a.gslots + (size_t)blockIdx.x * a.ppc * a.slot_bytes);
+
+    for (int i = threadIdx.x; i <= nb; i += blockDim.x) s_edges[i] = a.edges[i];
+    for (int i = threadIdx.x; i < nl * nb; i += blockDim.x) {
+        acc_cnt[i] = 0ull;
+        acc_sd[i] = 0.0;
+        acc_sd2[i] = 0.0;
+    }
+
+    const int warp = threadIdx.x / kWarp, lane = threadIdx.x % kWarp;
+    const int slot = warp / a.groups, group = warp % a.groups;
+    const int li = group * kWarp + lane;
+    const bool lane_on = li < nl;
+    int64_t L = lane_on ? a.lags[li] : 0;
+    if (L < 1 || L >= a.nsave) L = a.nsave;  // reference: lag >= nsteps -> skipped
+    const int64_t lim = a.nsave - L;         // valid starts: s < lim
+
+    // slot layout: series[nsave] float | list[nsave] IdxT | hist[nb+1] int | cur[nb+2] int
+    unsigned char* sb = slot_base + (size_t)slot * a.slot_bytes;
+    float* series = (float*)sb;
+    IdxT* list = (IdxT*)(sb + ((a.nsave * sizeof(float) + 15) & ~(size_t)15));
+    int* hist = (int*)((unsigned char*)list + ((a.nsave * sizeof(IdxT) + 15) & ~(size_t)15));
+    int* cur = hist + (nb + 1);
+
+    long long wc = 0, pn = 0;
+    double wm = 0.0, wm2 = 0.0, pss = 0.0;
+    const int64_t scap = min(a.start_cap, a.nsave);
+    const unsigned lt_mask = (1u << lane) - 1u;
+
+    __syncthreads();
+    const int64_t tiles = (a.n + a.ppc - 1) / a.ppc;
+    for (int64_t tile = blockIdx.x; tile < tiles; tile += gridDim.x) {
+        const int64_t p = tile * a.ppc + slot;
+        const bool have = p < a.n;
+        // ---- stage (group-0 warp of each slot)
+        if (group == 0 && have) {
+            for (int b = lane; b <= nb; b += kWarp) hist[b] = 0;
+            __syncwarp();
+            const float* src = a.mu + p * a.sp;
+            for (int64_t s0 = 0; s0 < a.nsave; s0 += kWarp) {
+                const int64_t s = s0 + lane;
+                float v = NAN;
+                int b = -1;
+                if (s < a.nsave) {
+                    v = src[s * a.ss];
+                    series[s] = v;
+                    if (s < scap) b = bin_of(v, s_edges, nb, a.bin_abs);
+                }
+                const unsigned active = __ballot_sync(0xffffffffu, b >= 0);
+                if (b >= 0) {
+                    const unsigned same = __match_any_sync(active, b);
+                    if ((same & lt_mask) == 0) hist[b] += __popc(same);
+                }
+                __syncwarp();
+            }
+            // exclusive scan of hist[0..nb] into cur[0..nb+1]
+            if (lane == 0) {
+                int run = 0;
+                for (int b = 0; b <= nb; ++b) {
+                    cur[b] = run;
+                    run += hist[b];
+                }
+                cur[nb + 1] = run;
+            }
+            __syncwarp();
+            for (int b = lane; b <= nb; b += kWarp) hist[b] = cur[b];  // hist becomes the scatter cursor
+            __syncwarp();
+            for (int64_t s0 = 0; s0 < scap; s0 += kWarp) {
+                const int64_t s = s0 + lane;
+                int b = -1;
+                if (s < scap) b = bin_of(series[s], s_edges, nb, a.bin_abs);
+                const unsigned active = __ballot_sync(0xffffffffu, b >= 0);
+                if (b >= 0) {
+                    const unsigned same = __match_any_sync(active, b);
+                    const int rank = __popc(same & lt_mask);
+                    list[hist[b] + rank] = (IdxT)s;
+                    __syncwarp(active);
+                    if (rank == 0) hist[b] += __popc(same);
+                }
+                __syncwarp();
+            }
+        }
+        __syncthreads();
+        // ---- pairs: bin by bin
+        if (have) {
+            long long tot_c = 0;
+            double tot_sd2 = 0.0;
+            for (int b = 0; b <= nb; ++b) {
+                const int e0 = cur[b], e1 = cur[b + 1];
+                long long c = 0;
+                double sd = 0.0, sd2 = 0.0;
+                int e = e0;
+                for (; e + 4 <= e1; e += 4) {
+                    int64_t s_[4];
+                    float a_[4], v_[4];
+#pragma unroll
+                    for (int k = 0; k < 4; ++k) {
+                        s_[k] = (int64_t)list[e + k];
+                        a_[k] = series[s_[k]];
+                        v_[k] = s_[k] < lim ? series[s_[k] + L] : NAN;
+                    }
+#pragma unroll
+                    for (int k = 0; k < 4; ++k) {
+                        const double d = (double)v_[k] - (double)a_[k];
+                        if (isfinite(d)) {
+                            c += 1;
+                            sd += d;
+                            sd2 = fma(d, d, sd2);
+                        }
+                    }
+                }
+                for (; e < e1; ++e) {
+                    const int64_t s = (int64_t)list[e];
+                    const float av = series[s];
+                    const float vv = s < lim ? series[s + L] : NAN;
+                    const double d = (double)vv - (double)av;
+                    if (isfinite(d)) {
+                        c += 1;
+                        sd += d;
+                        sd2 = fma(d, d, sd2);
+                    }
+                }
+                if (b < nb && c > 0 && lane_on) {
+                    const int ai = li * nb + b;
+                    atomicAdd(&acc_cnt[ai], (unsigned long long)c);
+                    atomicAdd(&acc_sd[ai], sd);
+                    atomicAdd(&acc_sd2[ai], sd2);
+                }
+                tot_c += c;
+                tot_sd2 += sd2;
+            }
+            if (tot_c > 0) {
+                // per-particle value: mean dmu^2 over its valid pairs (dmumu:528-537);
+                // for the injection estimator tot_c == 1 and the value is dmu^2 (:625-631)
+                const double value = tot_sd2 / (double)tot_c;
+                wc += 1;
+                const double delta = value - wm;
+                wm += delta / (double)wc;
+                wm2 += delta * (value - wm);
+                pss += tot_sd2;
+                pn += tot_c;
+            }
+        }
+        __syncthreads();
+    }
+
+    // ---- CTA epilogue: (bin, lag) accumulators and Welford triples
+    const int64_t cta = blockIdx.x;
+    for (int i = threadIdx.x; i < nl * nb; i += blockDim.x) {
+        a.part_cnt[cta * nl * nb + i] = acc_cnt[i];
+        a.part_sd[cta * nl * nb + i] = acc_sd[i];
+        a.part_sd2[cta * nl * nb + i] = acc_sd2[i];
+    }
+    __syncthreads();
+    // reuse the accumulator region to gather per-warp Welford triples
+    WelfordPart* wp = (WelfordPart*)(smem + (((size_t)(nb + 1) * sizeof(double) + 15) & ~(size_t)15));
+    const int nwarps = blockDim.x / kWarp;
+    wp[warp * kWarp + lane] = WelfordPart{wc, wm, wm2, pss, pn};
+    __syncthreads();
+    for (int l = threadIdx.x; l < nl; l += blockDim.x) {
+        const int g = l / kWarp, ln = l % kWarp;
+        long long c = 0, n2 = 0;
+        double m = 0.0, m2 = 0.0, ss = 0.0;
+        for (int sl = 0; sl < a.ppc; ++sl) {
+            const int w = sl * a.groups + g;
+            if (w >= nwarps) break;
+            const WelfordPart q = wp[w * kWarp + ln];
+            welford_merge(c, m, m2, q.count, q.mean, q.m2);
+            ss += q.pair_ss;
+            n2 += q.pair_n;
+        }
+        a.part_w[cta * nl + l] = WelfordPart{c, m, m2, ss, n2};
+    }
+}
+
+// Reduce per-CTA partials in CTA order and add / merge into the outputs.
+__global__ void dmumu_finalize_kernel(const unsigned long long* __restrict__ part_cnt,
+                                      const double* __restrict__ part_sd, const double* __restrict__ part_sd2,
+                                      const WelfordPart* __restrict__ part_w, int grid, int nl, int nb, int lag0,
+                                      int n_lags_total, int64_t* counts, double* sum_d, double* sum_d2,
+                                      int64_t* w_count, double* w_mean, double* w_m2, double* pair_ss,
+                                      int64_t* pair_n)
+{
+    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t < nl * nb) {
+        unsigned long long c = 0;
+        double sd = 0.0, sd2 = 0.0;
+        for (int g = 0; g < grid; ++g) {
+            c += part_cnt[(int64_t)g * nl * nb + t];
+            sd += part_sd[(int64_t)g * nl * nb + t];
+            sd2 += part_sd2[(int64_t)g * nl * nb + t];
+        }
+        const int l = t / nb, b = t % nb;
+        const int64_t o = (int64_t)(lag0 + l) * nb + b;  // Julia (n_bins, n_lags)
+        counts[o] += (int64_t)c;
+        sum_d[o] += sd;
+        sum_d2[o] += sd2;
+    }
+    if (t < nl) {
+        long long c = 0, n2 = 0;
+        double m = 0.0, m2 = 0.0, ss = 0.0;
+        for (int g = 0; g < grid; ++g) {
+            const WelfordPart q = part_w[(int64_t)g * nl + t];
+            welford_merge(c, m, m2, q.count, q.mean, q.m2);
+            ss += q.pair_ss;
+            n2 += q.pair_n;
+        }
+        const int l = lag0 + t;
+        long long gc = w_count[l];
+        double gm = w_mean[l], gm2 = w_m2[l];
+        welford_merge(gc, gm, gm2, c, m, m2);
+        w_count[l] = gc;
+        w_mean[l] = gm;
+        w_m2[l] = gm2;
+        pair_ss[l] += ss;
+        pair_n[l] += n2;
+    }
+    (void)n_lags_total;
+}
+
+// ------------------------------------------------------------------ D_pp
+// momentum_magnitude (src/compute_dpp_full.jl:232-234) with the reference's
+// rounding: explicitly rounded products and sums are never contracted into
+// FMA, so |p| is bit-identical to the reference's and dp = p_end - p_start
+// keeps its last bits.
+__device__ __forceinline__ double pmag_exact(float px, float py, float pz)
+{
+    const double x = (double)px, y = (double)py, z = (double)pz;
+    return __dsqrt_rn(__dadd_rn(__dadd_rn(__dmul_rn(x, x), __dmul_rn(y, y)), __dmul_rn(z, z)));
+}
+
+struct DppPart {
+    long long count;
+    double sdp, sdp2, sdn, sdn2;
+};
+
+struct DppLaunch {
+    const float* mom;
+    int64_t chunk, nsave;
+    const int64_t* lags;
+    int nl;
+    double p0;
+    int ppc, groups;
+    size_t slot_bytes;
+    char* gslots;
+    DppPart* part;  // [grid][nl]
+};
+
+template <bool SMEM_SLOTS>
+__global__ void __launch_bounds__(1024) dpp_kernel(DppLaunch a)
+{
+    extern __shared__ __align__(16) unsigned char smem[];
+    unsigned char* slot_base = SMEM_SLOTS ? smem : (unsigned char*)(a.gslots + (size_t)blockIdx.x * a.ppc * a.slot_bytes);
+    const int warp = threadIdx.x / kWarp, lane = threadIdx.x % kWarp;
+    const int slot = warp / a.groups, group = warp % a.groups;
+    const int li = group * kWarp + lane;
+    const bool lane_on = li < a.nl;
+    int64_t L = lane_on ? a.lags[li] : 0;
+    if (L < 1 || L >= a.nsave) L = a.nsave;
+    const int64_t lim = a.nsave - L;
+    double* series = (double*)(slot_base + (size_t)slot * a.slot_bytes);
+    long long c = 0;
+    double sdp = 0, sdp2 = 0, sdn = 0, sdn2 = 0;
+    const int64_t tiles = (a.chunk + a.ppc - 1) / a.ppc;
+    for (int64_t tile = blockIdx.x; tile < tiles; tile += gridDim.x) {
+        // cooperative staging: thread t -> (save, particle slot)
+        const int64_t p0i = tile * a.ppc;
+        const int np = (int)(a.chunk - p0i < (int64_t)a.ppc ? a.chunk - p0i : (int64_t)a.ppc);
+        for (int64_t t = threadIdx.x; t < (int64_t)np * a.nsave; t += blockDim.x) {
+            const int sl = (int)(t % np);
+            const int64_t s = t / np;
+            const float* m = a.mom + s * 3 * a.chunk + p0i + sl;
+            ((double*)(slot_base + (size_t)sl * a.slot_bytes))[s] = pmag_exact(m[0], m[a.chunk], m[2 * a.chunk]);
+        }
+        __syncthreads();
+        if (slot < np) {
+            for (int64_t s = 0; s < lim; ++s) {
+                const double ps = series[s];
+                const double pe = series[s + L];
+                if (!(isfinite(ps) && isfinite(pe))) continue;
+                const double d = pe - ps;
+                const double dn = d / a.p0;
+                c += 1;
+                sdp += d;
+                sdp2 = fma(d, d, sdp2);
+                sdn += dn;
+                sdn2 = fma(dn, dn, sdn2);
+            }
+        }
+        __syncthreads();
+    }
+    // CTA epilogue in fixed warp order
+    DppPart* wp = (DppPart*)(SMEM_SLOTS ? smem : smem);
+    __syncthreads();
+    wp[warp * kWarp + lane] = DppPart{c, sdp, sdp2, sdn, sdn2};
+    __syncthreads();
+    const int nwarps = blockDim.x / kWarp;
+    for (int l = threadIdx.x; l < a.nl; l += blockDim.x) {
+        const int g = l / kWarp, ln = l % kWarp;
+        DppPart r{0, 0, 0, 0, 0};
+        for (int sl = 0; sl < a.ppc; ++sl) {
+            const int w = sl * a.groups + g;
+            if (w >= nwarps) break;
+            const DppPart q = wp[w * kWarp + ln];
+            r.count += q.count; r.sdp += q.sdp; r.sdp2 += q.sdp2; r.sdn += q.sdn; r.sdn2 += q.sdn2;
+        }
+        a.part[(int64_t)blockIdx.x * a.nl + l] = r;
+    }
+}
+
+__global__ void dpp_finalize_kernel(const DppPart* __restrict__ part, int grid, int nl, int lag0, int64_t* counts,
+                                    double* sdp, double* sdp2, double* sdn, double* sdn2)
+{
+    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= nl) return;
+    DppPart r{0, 0, 0, 0, 0};
+    for (int g = 0; g < grid; ++g) {
+        const DppPart q = part[(int64_t)g * nl + t];
+        r.count += q.count; r.sdp += q.sdp; r.sdp2 += q.sdp2; r.sdn += q.sdn; r.sdn2 += q.sdn2;
+    }
+    const int l = lag0 + t;
+    counts[l] += r.count;
+    sdp[l] += r.sdp;
+    sdp2[l] += r.sdp2;
+    sdn[l] += r.sdn;
+    sdn2[l] += r.sdn2;
+}
+
+// ------------------------------------------------------------------ energies
+// kinetic_energy_gev_from_pmag (dpp:236-240)
+__device__ __forceinline__ double kinetic_gev(double pmag)
+{
+    if (!isfinite(pmag)) return NAN;
+    const double gev_to_j = 1.0e9 * 1.602176634e-19;
+    const double r = __ddiv_rn(pmag, M_P * C_LIGHT);
+    const double gamma = __dsqrt_rn(__dadd_rn(1.0, __dmul_rn(r, r)));
+    return __ddiv_rn(__dmul_rn(__dmul_rn(__dadd_rn(gamma, -1.0), M_P), C_LIGHT * C_LIGHT), gev_to_j);
+}
+
+__global__ void energy_snap_kernel(const float* __restrict__ mom, int64_t chunk, const int64_t* __restrict__ snaps,
+                                   int n_snap, int64_t offset, double* __restrict__ out)
+{
+    const int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= chunk * n_snap) return;
+    const int64_t p = t % chunk;
+    const int j = (int)(t / chunk);
+    const float* m = mom + snaps[j] * 3 * chunk + p;
+    out[(offset + p) * n_snap + j] = kinetic_gev(pmag_exact(m[0], m[chunk], m[2 * chunk]));
+}
+
+__global__ void energy_hist_kernel(const float* __restrict__ mom, int64_t chunk, const int64_t* __restrict__ snaps,
+                                   int n_snap, double log_emin, double inv_dlog, int n_hist,
+                                   unsigned long long* __restrict__ counts)
+{
+    extern __shared__ unsigned long long h[];
+    for (int i = threadIdx.x; i < n_snap * n_hist; i += blockDim.x) h[i] = 0ull;
+    __syncthreads();
+    for (int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; t < chunk * n_snap;
+         t += (int64_t)gridDim.x * blockDim.x) {
+        const int64_t p = t % chunk;
+        const int j = (int)(t / chunk);
+        const float* m = mom + snaps[j] * 3 * chunk + p;
+        const double e = kinetic_gev(pmag_exact(m[0], m[chunk], m[2 * chunk]));
+        if (!(e > 0.0) || !isfinite(e)) continue;
+        const double f = (log(e) - log_emin) * inv_dlog;
+        if (!(f >= 0.0) || f >= (double)n_hist) continue;
+        atomicAdd(&h[j * n_hist + (int)f], 1ull);
+    }
+    __syncthreads();
+    for (int i = threadIdx.x; i < n_snap * n_hist; i += blockDim.x)
+        if (h[i]) atomicAdd(&counts[i], h[i]);
+}
+
+size_t align16(size_t b) { return (b + 15) & ~(size_t)15; }
+
+}  // namespace
+
+// ------------------------------------------------------------------ host side
+int run_dmumu(pt_ctx* ctx, const DmumuArgs& a, cudaStream_t s)
+{
+    if (a.n <= 0 || a.n_lags <= 0) return PT_OK;
+    if (a.n_bins < 1 || a.n_bins > 4096) return fail(PT_ERR_ARG, "n_bins must be in [1, 4096]");
+    if (a.nsave < 1) return fail(PT_ERR_ARG, "nsave must be positive");
+    int dev = ctx->device;
+    int max_smem = 0;
+    cudaDeviceGetAttribute(&max_smem, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev);
+    const size_t budget = (size_t)std::min(max_smem, 200 * 1024);
+    const bool small_idx = a.nsave <= 65535;
+    const size_t idx_bytes = small_idx ? 2 : 4;
+    const size_t slot_bytes = align16(a.nsave * sizeof(float)) + align16(a.nsave * idx_bytes) +
+                              align16(sizeof(int) * (size_t)(2 * a.n_bins + 3));
+    const size_t edge_bytes = align16(sizeof(double) * (size_t)(a.n_bins + 1));
+    // lags per launch: multiple of 32 with the accumulators taking <= ~half the budget
+    int nl_cap = (int)std::max<size_t>(32, ((budget / 2) / ((size_t)a.n_bins * 24)) / 32 * 32);
+    nl_cap = std::min(nl_cap, 32 * 8);
+    const int lag_batches = (a.n_lags + nl_cap - 1) / nl_cap;
+    for (int lb = 0; lb < lag_batches; ++lb) {
+        const int lag0 = lb * nl_cap;
+        const int nl = std::min(nl_cap, a.n_lags - lag0);
+        const int groups = (nl + kWarp - 1) / kWarp;
+        const size_t acc_bytes = (size_t)nl * a.n_bins * 24;
+        size_t fixed = edge_bytes + std::max(acc_bytes, sizeof(WelfordPart) * 1024);
+        bool smem_slots = fixed + slot_bytes <= budget;
+        int ppc;
+        if (smem_slots) ppc = (int)std::min<size_t>((budget - fixed) / slot_bytes, (size_t)(32 / groups));
+        else ppc = std::max(1, std::min(8, 32 / groups));
+        ppc = std::max(1, ppc);
+        const int threads = ppc * groups * kWarp;
+        size_t smem = fixed + (smem_slots ? (size_t)ppc * slot_bytes : 0);
+        const int64_t tiles = (a.n + ppc - 1) / ppc;
+        int per_sm = 1;
+        void* kfn = small_idx ? (smem_slots ? (void*)dmumu_kernel<uint16_t, true> : (void*)dmumu_kernel<uint16_t, false>)
+                              : (smem_slots ? (void*)dmumu_kernel<uint32_t, true> : (void*)dmumu_kernel<uint32_t, false>);
+        PT_CUDA(cudaFuncSetAttribute(kfn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kfn, threads, smem);
+        per_sm = std::max(1, per_sm);
+        const int grid = (int)std::max<int64_t>(1, std::min<int64_t>(tiles, (int64_t)ctx->num_sms * per_sm));
+        // scratch: per-CTA partials (+ global staging slots when needed)
+        const size_t part_acc = (size_t)grid * nl * a.n_bins;
+        const size_t bytes = align16(part_acc * 8) * 3 + align16(sizeof(WelfordPart) * (size_t)grid * nl) +
+                             (smem_slots ? 0 : (size_t)grid * ppc * slot_bytes);
+        void* scratch = nullptr;
+        int rc = scratch_get(ctx, 0, bytes, &scratch);
+        if (rc) return rc;
+        char* base = (char*)scratch;
+        DmumuLaunch L;
+        L.mu = a.mu; L.n = a.n; L.nsave = a.nsave; L.sp = a.sp; L.ss = a.ss;
+        L.start_cap = a.injection ? 1 : a.nsave;
+        L.lags = a.lags + lag0; L.nl = nl; L.edges = a.edges; L.n_bins = a.n_bins; L.bin_abs = a.bin_abs;
+        L.ppc = ppc; L.groups = groups; L.slot_bytes = slot_bytes;
+        L.part_cnt = (unsigned long long*)base;
+        L.part_sd = (double*)(base + align16(part_acc * 8));
+        L.part_sd2 = (double*)(base + 2 * align16(part_acc * 8));
+        L.part_w = (WelfordPart*)(base + 3 * align16(part_acc * 8));
+        L.gslots = smem_slots ? nullptr : (char*)L.part_w + align16(sizeof(WelfordPart) * (size_t)grid * nl);
+        if (small_idx) {
+            if (smem_slots) dmumu_kernel<uint16_t, true><<<grid, threads, smem, s>>>(L);
+            else dmumu_kernel<uint16_t, false><<<grid, threads, smem, s>>>(L);
+        } else {
+            if (smem_slots) dmumu_kernel<uint32_t, true><<<grid, threads, smem, s>>>(L);
+            else dmumu_kernel<uint32_t, false><<<grid, threads, smem, s>>>(L);
+        }
+        PT_CHECK_LAUNCH("dmumu_kernel");
+        const int fin_threads = 256;
+        const int fin_blocks = (int)((std::max(nl * a.n_bins, nl) + fin_threads - 1) / fin_threads);
+        dmumu_finalize_kernel<<<fin_blocks, fin_threads, 0, s>>>(L.part_cnt, L.part_sd, L.part_sd2, L.part_w, grid, nl,
+                                                                 a.n_bins, lag0, a.n_lags, a.counts, a.sum_d,
+                                                                 a.sum_d2, a.w_count, a.w_mean, a.w_m2, a.pair_ss,
+                                                                 a.pair_n);
+        PT_CHECK_LAUNCH("dmumu_finalize_kernel");
+    }
+    return PT_OK;
+}
+
+int run_dpp(pt_ctx* ctx, const DppArgs& a, cudaStream_t s)
+{
+    if (a.chunk <= 0 || a.n_lags <= 0) return PT_OK;
+    int max_smem = 0;
+    cudaDeviceGetAttribute(&max_smem, cudaDevAttrMaxSharedMemoryPerBlockOptin, ctx->device);
+    const size_t budget = (size_t)std::min(max_smem, 200 * 1024);
+    const size_t slot_bytes = align16(sizeof(double) * a.nsave);
+    const int nl_cap = 32 * 8;
+    for (int lag0 = 0; lag0 < a.n_lags; lag0 += nl_cap) {
+        const int nl = std::min(nl_cap, a.n_lags - lag0);
+        const int groups = (nl + kWarp - 1) / kWarp;
+        const size_t fixed = sizeof(DppPart) * 1024;
+        bool smem_slots = slot_bytes <= budget - fixed;
+        int ppc = smem_slots ? (int)std::min<size_t>((budget - fixed) / slot_bytes, (size_t)(32 / groups))
+                             : std::max(1, std::min(8, 32 / groups));
+        ppc = std::max(1, ppc);
+        const int threads = ppc * groups * kWarp;
+        const size_t smem = std::max(fixed, smem_slots ? (size_t)ppc * slot_bytes : 0) ;
+        const int64_t tiles = (a.chunk + ppc - 1) / ppc;
+        void* kfn = smem_slots ? (void*)dpp_kernel<true> : (void*)dpp_kernel<false>;
+        PT_CUDA(cudaFuncSetAttribute(kfn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+        int per_sm = 1;
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kfn, threads, smem);
+        per_sm = std::max(1, per_sm);
+        const int grid = (int)std::max<int64_t>(1, std::min<int64_t>(tiles, (int64_t)ctx->num_sms * per_sm));
+        const size_t bytes = align16(sizeof(DppPart) * (size_t)grid * nl) +
+                             (smem_slots ? 0 : (size_t)grid * ppc * slot_bytes);
+        void* scratch = nullptr;
+        int rc = scratch_get(ctx, 1, bytes, &scratch);
+        if (rc) return rc;
+        DppLaunch L;
+        L.mom = a.mom; L.chunk = a.chunk; L.nsave = a.nsave; L.lags = a.lags + lag0; L.nl = nl; L.p0 = a.p0;
+        L.ppc = ppc; L.groups = groups; L.slot_bytes = slot_bytes;
+        L.part = (DppPart*)scratch;
+        L.gslots = smem_slots ? nullptr : (char*)scratch + align16(sizeof(DppPart) * (size_t)grid * nl);
+        if (smem_slots) dpp_kernel<true><<<grid, threads, smem, s>>>(L);
+        else dpp_kernel<false><<<grid, threads, smem, s>>>(L);
+        PT_CHECK_LAUNCH("dpp_kernel");
+        dpp_finalize_kernel<<<(nl + 255) / 256, 256, 0, s>>>(L.part, grid, nl, lag0, a.counts, a.sdp, a.sdp2, a.sdn,
+                                                             a.sdn2);
+        PT_CHECK_LAUNCH("dpp_finalize_kernel");
+    }
+    return PT_OK;
+}
+
+int launch_energy_snapshots(const float* mom, int64_t chunk, int64_t nsave, const int64_t* snaps, int n_snap,
+                            int64_t offset, double* out, cudaStream_t s)
+{
+    (void)nsave;
+    const int64_t total = chunk * n_snap;
+    if (total <= 0) return PT_OK;
+    energy_snap_kernel<<<(unsigned)((total + 255) / 256), 256, 0, s>>>(mom, chunk, snaps, n_snap, offset, out);
+    PT_CHECK_LAUNCH("energy_snap_kernel");
+    return PT_OK;
+}
+
+int launch_energy_histogram(const float* mom, int64_t chunk, int64_t nsave, const int64_t* snaps, int n_snap,
+                            double e_min, double e_max, int n_hist, int64_t* counts, cudaStream_t s)
+{
+    (void)nsave;
+    const int64_t total = chunk * n_snap;
+    if (total <= 0) return PT_OK;
+    const size_t smem = sizeof(unsigned long long) * (size_t)n_snap * n_hist;
+    if (smem > 160 * 1024) return fail(PT_ERR_ARG, "n_snap * n_hist too large for the on-chip histogram");
+    if (smem > 48 * 1024)
+        PT_CUDA(cudaFuncSetAttribute(energy_hist_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    const double log_emin = log(e_min);
+    const double inv_dlog = (double)n_hist / (log(e_max) - log_emin);
+    const int blocks = (int)std::min<int64_t>((total + 255) / 256, 148 * 4);
+    energy_hist_kernel<<<blocks, 256, smem, s>>>(mom, chunk, snaps, n_snap, log_emin, inv_dlog, n_hist,
+                                                 (unsigned long long*)counts);
+    PT_CHECK_LAUNCH("energy_hist_kernel");
+    return PT_OK;
+}
+
+}  // namespace pt

@@ -1,0 +1,179 @@
+// Internal declarations shared by the libptb200 translation units.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <cuda_bf16.h>
+#include <stdint.h>
+
+#include <algorithm>
+#include <climits>
+#include <string>
+#include <vector>
+
+#include "../../include/ptb200.h"
+
+namespace pt {
+
+// Physical constants: src/phase_space_gpu_runner.jl:8-12.
+constexpr double C_LIGHT = 2.99792458e8;
+constexpr double Q_E = 1.602176634e-19;
+constexpr double M_P = 1.67262192369e-27;
+
+// ---------------------------------------------------------------- errors
+void set_error(const std::string& msg);
+int fail(int code, const std::string& msg);
+int cuda_fail(cudaError_t e, const char* what);
+
+#define PT_CUDA(call)                                         \
+    do {                                                      \
+        cudaError_t _e = (call);                              \
+        if (_e != cudaSuccess) return ::pt::cuda_fail(_e, #call); \
+    } while (0)
+
+#define PT_CHECK_LAUNCH(what)                                  \
+    do {                                                       \
+        cudaError_t _e = cudaGetLastError();                   \
+        if (_e != cudaSuccess) return ::pt::cuda_fail(_e, what); \
+    } while (0)
+
+// ---------------------------------------------------------------- context
+struct ScratchBuf {
+    void* ptr = nullptr;
+    size_t bytes = 0;
+};
+
+}  // namespace pt
+
+struct pt_ctx {
+    int device = 0;
+    int num_sms = 148;
+    cudaStream_t own_stream = nullptr;
+    cudaStream_t stream = nullptr;      // stream used by *_device calls
+    cudaStream_t copy_stream = nullptr; // egress copies in pt_push_run
+    pt::ScratchBuf scratch[4];          // reusable device scratch, grown on demand
+};
+
+struct pt_field {
+    pt_ctx* ctx = nullptr;
+    int storage = PT_FIELD_REF_F64;
+    pt_grid grid{};
+    double B_ref = 1.0;
+    // REF_F64: six column-major arrays
+    double* comp[6] = {nullptr, nullptr, nullptr, nullptr, nullptr, nullptr};
+    // brick forms: node array + per-axis node offsets (in nodes)
+    void* nodes = nullptr;
+    int64_t n_nodes = 0;
+    uint32_t* offs = nullptr;  // [nx + ny + nz]: offx, offy, offz
+    int64_t bytes = 0;
+};
+
+struct pt_fast_state {
+    pt_ctx* ctx = nullptr;
+    int64_t n = 0;
+    double* x = nullptr;    // [3][n] positions in cell units, (x - xmin)/dx
+    float* p = nullptr;     // [3][n] momentum / (m c)
+    double* p2 = nullptr;   // [n] |p/(m c)|^2 carried in FP64
+    int32_t* pid = nullptr; // [n] particle id of each slot
+    uint8_t* alive = nullptr;
+    const pt_field* field = nullptr; // field the state was created against (grid, units)
+    int64_t last_sort = INT64_MIN;   // step of the last brick re-sort
+    // scratch for the re-sort
+    void* sort_tmp = nullptr;
+    size_t sort_tmp_bytes = 0;
+};
+
+namespace pt {
+
+// Grow-only device scratch owned by the context (slot = independent user).
+int scratch_get(pt_ctx* ctx, int slot, size_t bytes, void** out);
+
+// ---------------------------------------------------------------- launches
+struct PushArgsRef {
+    const double* f[6];
+    pt_grid g;
+    double* x[3];
+    double* p[3];
+    uint8_t* alive;
+    int64_t n;
+    double dt;
+    int64_t nsteps, stride;
+    int periodic, cache_mode, cache_f64;
+    int64_t step_begin, step_count;
+    void* cache;
+    int64_t row_base, rows;
+    int64_t* deaths;
+};
+int launch_push_ref(const PushArgsRef& a, cudaStream_t s);
+
+struct FieldArgsBrick {
+    const void* nodes;
+    const uint32_t* offs;
+    int64_t nx, ny, nz;
+    int bf16;
+};
+struct PushArgsFast {
+    FieldArgsBrick fld;
+    double wx, wy, wz;     // periodic widths in cell units ((xmax-xmin)/dx)
+    double* x;             // [3][n]
+    float* p;              // [3][n]
+    double* p2;
+    int32_t* pid;
+    uint8_t* alive;
+    int64_t n;
+    float hB;              // q B_ref dt / (2 m)
+    float vfac[3];         // c dt / dx, c dt / dy, c dt / dz
+    double xmin[3], dxs[3];
+    int64_t nsteps, stride;
+    int periodic, cache_mode, cache_f64;
+    int64_t step_begin, step_count;
+    void* cache;
+    int64_t row_base, rows;
+    int64_t* deaths;
+};
+int launch_push_fast(const PushArgsFast& a, cudaStream_t s);
+int launch_fast_import(pt_fast_state* st, const pt_field* f, const double* x1, const double* x2, const double* x3,
+                       const double* p1, const double* p2, const double* p3, const uint8_t* alive, cudaStream_t s);
+int launch_fast_export(const pt_fast_state* st, const pt_field* f, double* x1, double* x2, double* x3, double* p1,
+                       double* p2, double* p3, uint8_t* alive, cudaStream_t s);
+int fast_sort(pt_ctx* ctx, pt_fast_state* st, const pt_field* f, cudaStream_t s);
+
+int launch_brick_convert(const double* const comps[6], const pt_grid& g, double B_ref, int bf16, void* nodes,
+                         const uint32_t* offs, cudaStream_t s);
+
+struct DmumuArgs {
+    const float* mu;
+    int64_t n, nsave, sp, ss;
+    const int64_t* lags;
+    int n_lags;
+    const double* edges;
+    int n_bins;
+    int injection, bin_abs;
+    int64_t* counts;
+    double* sum_d;
+    double* sum_d2;
+    int64_t* w_count;
+    double* w_mean;
+    double* w_m2;
+    double* pair_ss;
+    int64_t* pair_n;
+};
+int run_dmumu(pt_ctx* ctx, const DmumuArgs& a, cudaStream_t s);
+
+struct DppArgs {
+    const float* mom;
+    int64_t chunk, nsave;
+    const int64_t* lags;
+    int n_lags;
+    double p0;
+    int64_t* counts;
+    double *sdp, *sdp2, *sdn, *sdn2;
+};
+int run_dpp(pt_ctx* ctx, const DppArgs& a, cudaStream_t s);
+int launch_energy_snapshots(const float* mom, int64_t chunk, int64_t nsave, const int64_t* snaps, int n_snap,
+                            int64_t offset, double* out, cudaStream_t s);
+int launch_energy_histogram(const float* mom, int64_t chunk, int64_t nsave, const int64_t* snaps, int n_snap,
+                            double e_min, double e_max, int n_hist, int64_t* counts, cudaStream_t s);
+int launch_reconstruct_mu(const void* pos, const void* mom, int64_t chunk, int64_t nsave, const void* const b[3],
+                          const pt_grid& g, int f64, void* mu_out, cudaStream_t s);
+
+}  // namespace pt

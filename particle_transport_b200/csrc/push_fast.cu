@@ -1,0 +1,468 @@
+// Mixed-precision form of the push (the reference's advance_particles_kernel!,
+// src/phase_space_gpu_runner.jl:330-391, restated in nondimensional units).
+//
+// Units: positions in cells, x~ = (x - xmin)/dx (carried in FP64);
+// momentum p~ = p/(m c) in FP32 with |p~|^2 carried in FP64; B~ = B/B_ref and
+// u~ = u/c stored in Morton-ordered 8^3 bricks with the six components of a
+// node interleaved (BF16: one 16-byte load per corner; FP32: two).
+// With h = q B_ref dt/(2m) the Boris step of boris_push (:282-323) becomes
+//   eps = -(u~ x h B~)           (= q E dt/(2 m c))
+//   p-  = p~ + eps,   g- = sqrt(1 + |p-|^2)
+//   t   = h B~ / g-,  s = 2 t/(1 + t.t)
+//   p+  = p- + (p- + p- x t) x s,  rescaled to |p+| = |p-| (the rotation is
+//         norm-preserving; the scale is taken from the FP64 |p|^2)
+//   p~' = p+ + eps,   x~ += p~' (c dt/dx) / g'
+// and |p|^2 is advanced in FP64 by the two E kicks only, so with E = 0 the
+// particle energy is conserved to FP64 rounding.
+#include "pt_internal.cuh"
+
+namespace pt {
+namespace {
+
+__device__ __forceinline__ float bf_lo(uint32_t w) { return __uint_as_float(w << 16); }
+__device__ __forceinline__ float bf_hi(uint32_t w) { return __uint_as_float(w & 0xffff0000u); }
+
+struct Corners {
+    uint32_t idx[8];
+    float w[8];
+};
+
+// Corner node indices and trilinear weights of the cell holding (x, y, z)
+// (cell units).  Cell = clamp(floor(x), 0, n-2) as in trilinear_sample
+// (src/phase_space_gpu_runner.jl:247-258, 0-based).
+__device__ __forceinline__ Corners locate_brick(double x, double y, double z, const uint32_t* ox, const uint32_t* oy,
+                                                const uint32_t* oz, int nx, int ny, int nz)
+{
+    int ix = (int)floor(x), iy = (int)floor(y), iz = (int)floor(z);
+    ix = min(max(ix, 0), nx - 2);
+    iy = min(max(iy, 0), ny - 2);
+    iz = min(max(iz, 0), nz - 2);
+    float tx = (float)(x - (double)ix), ty = (float)(y - (double)iy), tz = (float)(z - (double)iz);
+    uint32_t x0 = ox[ix], x1 = ox[ix + 1], y0 = oy[iy], y1 = oy[iy + 1], z0 = oz[iz], z1 = oz[iz + 1];
+    Corners c;
+    c.idx[0] = x0 + y0 + z0; c.idx[1] = x1 + y0 + z0; c.idx[2] = x0 + y1 + z0; c.idx[3] = x1 + y1 + z0;
+    c.idx[4] = x0 + y0 + z1; c.idx[5] = x1 + y0 + z1; c.idx[6] = x0 + y1 + z1; c.idx[7] = x1 + y1 + z1;
+    float ux = 1.0f - tx, uy = 1.0f - ty, uz = 1.0f - tz;
+    float a00 = ux * uy, a10 = tx * uy, a01 = ux * ty, a11 = tx * ty;
+    c.w[0] = a00 * uz; c.w[1] = a10 * uz; c.w[2] = a01 * uz; c.w[3] = a11 * uz;
+    c.w[4] = a00 * tz; c.w[5] = a10 * tz; c.w[6] = a01 * tz; c.w[7] = a11 * tz;
+    return c;
+}
+
+template <bool BF16>
+__device__ __forceinline__ void gather6(const void* __restrict__ nodes, const Corners& c, float f[6])
+{
+#pragma unroll
+    for (int k = 0; k < 6; ++k) f[k] = 0.0f;
+    if (BF16) {
+        const uint4* N = (const uint4*)nodes;
+        uint4 v[8];
+#pragma unroll
+        for (int q = 0; q < 8; ++q) v[q] = __ldg(N + c.idx[q]);
+#pragma unroll
+        for (int q = 0; q < 8; ++q) {
+            const float w = c.w[q];
+            f[0] = fmaf(w, bf_lo(v[q].x), f[0]);
+            f[1] = fmaf(w, bf_hi(v[q].x), f[1]);
+            f[2] = fmaf(w, bf_lo(v[q].y), f[2]);
+            f[3] = fmaf(w, bf_hi(v[q].y), f[3]);
+            f[4] = fmaf(w, bf_lo(v[q].z), f[4]);
+            f[5] = fmaf(w, bf_hi(v[q].z), f[5]);
+        }
+    } else {
+        const float4* N = (const float4*)nodes;
+        float4 va[8], vb[8];
+#pragma unroll
+        for (int q = 0; q < 8; ++q) {
+            va[q] = __ldg(N + 2 * (size_t)c.idx[q]);
+            vb[q] = __ldg(N + 2 * (size_t)c.idx[q] + 1);
+        }
+#pragma unroll
+        for (int q = 0; q < 8; ++q) {
+            const float w = c.w[q];
+            f[0] = fmaf(w, va[q].x, f[0]);
+            f[1] = fmaf(w, va[q].y, f[1]);
+            f[2] = fmaf(w, va[q].z, f[2]);
+            f[3] = fmaf(w, va[q].w, f[3]);
+            f[4] = fmaf(w, vb[q].x, f[4]);
+            f[5] = fmaf(w, vb[q].y, f[5]);
+        }
+    }
+}
+
+__device__ __forceinline__ float mu_f32(float px, float py, float pz, float bx, float by, float bz)
+{
+    // pitch_mu_from_pB, src/compute_delta_mu2_curve.jl:101-110 (FP32)
+    float pn = sqrtf(px * px + py * py + pz * pz);
+    float bn = sqrtf(bx * bx + by * by + bz * bz);
+    if (!isfinite(pn) || !isfinite(bn) || pn == 0.0f || bn == 0.0f) return NAN;
+    float mu = (px * bx + py * by + pz * bz) / (pn * bn);
+    return fminf(1.0f, fmaxf(-1.0f, mu));
+}
+
+__device__ __forceinline__ double wrap_cells(double x, double w)
+{
+    // wrap_periodic_coordinate (src/phase_space_gpu_runner.jl:325-328) in cell units
+    if (x < 0.0 || x >= w) x -= floor(x / w) * w;
+    return x;
+}
+
+template <bool BF16>
+__global__ void __launch_bounds__(256) push_fast_kernel(PushArgsFast a)
+{
+    extern __shared__ uint32_t s_offs[];
+    const int nx = (int)a.fld.nx, ny = (int)a.fld.ny, nz = (int)a.fld.nz;
+    for (int i = threadIdx.x; i < nx + ny + nz; i += blockDim.x) s_offs[i] = a.fld.offs[i];
+    __syncthreads();
+    const uint32_t* ox = s_offs;
+    const uint32_t* oy = s_offs + nx;
+    const uint32_t* oz = s_offs + nx + ny;
+    const float hB = a.hB;
+    const int64_t s_end = a.step_begin + a.step_count;
+    const int64_t n = a.n;
+
+    for (int64_t slot = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; slot < n;
+         slot += (int64_t)gridDim.x * blockDim.x) {
+        double x = a.x[slot], y = a.x[n + slot], z = a.x[2 * n + slot];
+        float px = a.p[slot], py = a.p[n + slot], pz = a.p[2 * n + slot];
+        double P2 = a.p2[slot];
+        bool al = a.alive[slot] != 0;
+        const int64_t pid = a.pid[slot];
+        int64_t next_save = ((a.step_begin + a.stride - 1) / a.stride) * a.stride;
+        for (int64_t s = a.step_begin; s < s_end; ++s) {
+            const bool do_push = s < a.nsteps - 1;
+            bool is_save = false;
+            int64_t row = 0;
+            if (s == next_save) {
+                row = s / a.stride;
+                next_save += a.stride;
+                is_save = a.cache_mode != PT_CACHE_NONE && row >= a.row_base && row < a.row_base + a.rows;
+            }
+            float f[6] = {0, 0, 0, 0, 0, 0};
+            if (al && (do_push || (is_save && a.cache_mode == PT_CACHE_MU))) {
+                Corners c = locate_brick(x, y, z, ox, oy, oz, nx, ny, nz);
+                gather6<BF16>(a.fld.nodes, c, f);
+            }
+            if (is_save) {
+                const int64_t r = row - a.row_base;
+                if (a.cache_mode == PT_CACHE_MU) {
+                    float mu = NAN;
+                    if (al && x >= 0.0 && x <= a.wx && y >= 0.0 && y <= a.wy && z >= 0.0 && z <= a.wz)
+                        mu = mu_f32(px, py, pz, f[0], f[1], f[2]);
+                    if (a.cache_f64) ((double*)a.cache)[r * n + pid] = (double)mu;
+                    else ((float*)a.cache)[r * n + pid] = mu;
+                } else {
+                    double v[6];
+                    const double pm = sqrt(P2) / sqrt((double)px * px + (double)py * py + (double)pz * pz) *
+                                      (M_P * C_LIGHT);
+                    v[0] = a.xmin[0] + x * a.dxs[0];
+                    v[1] = a.xmin[1] + y * a.dxs[1];
+                    v[2] = a.xmin[2] + z * a.dxs[2];
+                    v[3] = (double)px * pm; v[4] = (double)py * pm; v[5] = (double)pz * pm;
+                    for (int k = 0; k < 6; ++k) {
+                        double w = al ? v[k] : (double)NAN;
+                        int64_t idx = (r * 6 + k) * n + pid;
+                        if (a.cache_f64) ((double*)a.cache)[idx] = w;
+                        else ((float*)a.cache)[idx] = (float)w;
+                    }
+                }
+            }
+            if (al && do_push) {
+                const float bx = hB * f[0], by = hB * f[1], bz = hB * f[2];
+                const float ux = f[3], uy = f[4], uz = f[5];
+                // eps = -(u x hB) = q E dt / (2 m c)
+                const float ex = -(uy * bz - uz * by);
+                const float ey = -(uz * bx - ux * bz);
+                const float ez = -(ux * by - uy * bx);
+                const float pmx = px + ex, pmy = py + ey, pmz = pz + ez;
+                const float e2 = ex * ex + ey * ey + ez * ez;
+                const double P2m = P2 + (double)(2.0f * (px * ex + py * ey + pz * ez) + e2);
+                const float gm = sqrtf(1.0f + (float)P2m);
+                const float ig = 1.0f / gm;
+                const float tx = bx * ig, ty = by * ig, tz = bz * ig;
+                const float t2 = tx * tx + ty * ty + tz * tz;
+                const float sf = 2.0f / (1.0f + t2);
+                const float sx = sf * tx, sy = sf * ty, sz = sf * tz;
+                const float qx = pmx + (pmy * tz - pmz * ty);
+                const float qy = pmy + (pmz * tx - pmx * tz);
+                const float qz = pmz + (pmx * ty - pmy * tx);
+                float rx = pmx + (qy * sz - qz * sy);
+                float ry = pmy + (qz * sx - qx * sz);
+                float rz = pmz + (qx * sy - qy * sx);
+                // norm-preserving rotation: pin |p+|^2 to the FP64 |p-|^2
+                const float r2 = rx * rx + ry * ry + rz * rz;
+                const float sc = sqrtf((float)P2m) * rsqrtf(r2);
+                rx *= sc; ry *= sc; rz *= sc;
+                px = rx + ex; py = ry + ey; pz = rz + ez;
+                P2 = P2m + (double)(2.0f * (rx * ex + ry * ey + rz * ez) + e2);
+                const float ign = rsqrtf(1.0f + (float)P2);
+                x += (double)(px * (a.vfac[0] * ign));
+                y += (double)(py * (a.vfac[1] * ign));
+                z += (double)(pz * (a.vfac[2] * ign));
+                if (a.periodic) {
+                    x = wrap_cells(x, a.wx);
+                    y = wrap_cells(y, a.wy);
+                    z = wrap_cells(z, a.wz);
+                } else if (x < 0.0 || x > a.wx || y < 0.0 || y > a.wy || z < 0.0 || z > a.wz) {
+                    al = false;
+                    if (a.deaths) atomicAdd((unsigned long long*)&a.deaths[s], 1ull);
+                }
+            }
+        }
+        a.x[slot] = x; a.x[n + slot] = y; a.x[2 * n + slot] = z;
+        a.p[slot] = px; a.p[n + slot] = py; a.p[2 * n + slot] = pz;
+        a.p2[slot] = P2;
+        a.alive[slot] = al ? 1 : 0;
+    }
+}
+
+// ------------------------------------------------------------ field bricks
+__global__ void brick_convert_kernel(const double* __restrict__ bx, const double* __restrict__ by,
+                                     const double* __restrict__ bz, const double* __restrict__ ux,
+                                     const double* __restrict__ uy, const double* __restrict__ uz, int64_t nx,
+                                     int64_t ny, int64_t nz, double inv_b, double inv_c, int bf16, void* nodes,
+                                     const uint32_t* __restrict__ offs)
+{
+    const int64_t total = nx * ny * nz;
+    for (int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; t < total;
+         t += (int64_t)gridDim.x * blockDim.x) {
+        const int64_t i = t % nx, j = (t / nx) % ny, k = t / (nx * ny);
+        const uint32_t node = offs[i] + offs[nx + j] + offs[nx + ny + k];
+        float v[6] = {(float)(bx[t] * inv_b), (float)(by[t] * inv_b), (float)(bz[t] * inv_b),
+                      (float)(ux[t] * inv_c), (float)(uy[t] * inv_c), (float)(uz[t] * inv_c)};
+        if (bf16) {
+            uint32_t w[3];
+            for (int q = 0; q < 3; ++q) {
+                const uint32_t lo = __bfloat16_as_ushort(__float2bfloat16_rn(v[2 * q]));
+                const uint32_t hi = __bfloat16_as_ushort(__float2bfloat16_rn(v[2 * q + 1]));
+                w[q] = lo | (hi << 16);
+            }
+            ((uint4*)nodes)[node] = make_uint4(w[0], w[1], w[2], 0u);
+        } else {
+            float4* N = (float4*)nodes;
+            N[2 * (size_t)node] = make_float4(v[0], v[1], v[2], v[3]);
+            N[2 * (size_t)node + 1] = make_float4(v[4], v[5], 0.0f, 0.0f);
+        }
+    }
+}
+
+// ------------------------------------------------------------ state import / export
+__global__ void fast_import_kernel(const double* __restrict__ x1, const double* __restrict__ x2,
+                                   const double* __restrict__ x3, const double* __restrict__ p1,
+                                   const double* __restrict__ p2, const double* __restrict__ p3,
+                                   const uint8_t* __restrict__ alive, int64_t n, double xmin, double ymin,
+                                   double zmin, double dx, double dy, double dz, double* xo, float* po, double* p2o,
+                                   int32_t* pid, uint8_t* ao)
+{
+    const double inv_mc = 1.0 / (M_P * C_LIGHT);
+    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+        xo[i] = (x1[i] - xmin) / dx;
+        xo[n + i] = (x2[i] - ymin) / dy;
+        xo[2 * n + i] = (x3[i] - zmin) / dz;
+        const double qx = p1[i] * inv_mc, qy = p2[i] * inv_mc, qz = p3[i] * inv_mc;
+        po[i] = (float)qx; po[n + i] = (float)qy; po[2 * n + i] = (float)qz;
+        p2o[i] = qx * qx + qy * qy + qz * qz;
+        pid[i] = (int32_t)i;
+        ao[i] = alive[i];
+    }
+}
+
+__global__ void fast_export_kernel(const double* __restrict__ xs, const float* __restrict__ ps,
+                                   const double* __restrict__ p2s, const int32_t* __restrict__ pid,
+                                   const uint8_t* __restrict__ as, int64_t n, double xmin, double ymin, double zmin,
+                                   double dx, double dy, double dz, double* x1, double* x2, double* x3, double* p1,
+                                   double* p2, double* p3, uint8_t* alive)
+{
+    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+        const int64_t q = pid[i];
+        x1[q] = xmin + xs[i] * dx;
+        x2[q] = ymin + xs[n + i] * dy;
+        x3[q] = zmin + xs[2 * n + i] * dz;
+        const double px = ps[i], py = ps[n + i], pz = ps[2 * n + i];
+        const double sc = sqrt(p2s[i] / (px * px + py * py + pz * pz)) * (M_P * C_LIGHT);
+        p1[q] = px * sc; p2[q] = py * sc; p3[q] = pz * sc;
+        alive[q] = as[i];
+    }
+}
+
+// ------------------------------------------------------------ brick sort
+// One-digit radix (counting) sort of the particle slots by the brick that
+// holds their cell; dead particles go to a final bucket.
+__global__ void sort_key_kernel(const double* __restrict__ xs, const uint8_t* __restrict__ as, int64_t n,
+                                const uint32_t* __restrict__ offs, int nx, int ny, int nz, uint32_t dead_key,
+                                uint32_t* __restrict__ keys, uint32_t* __restrict__ hist)
+{
+    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+        uint32_t key = dead_key;
+        if (as[i]) {
+            int ix = min(max((int)floor(xs[i]), 0), nx - 2);
+            int iy = min(max((int)floor(xs[n + i]), 0), ny - 2);
+            int iz = min(max((int)floor(xs[2 * n + i]), 0), nz - 2);
+            key = (offs[ix] + offs[nx + iy] + offs[nx + ny + iz]) >> 9;
+        }
+        keys[i] = key;
+        atomicAdd(&hist[key], 1u);
+    }
+}
+
+// Exclusive scan of hist[0..m) into cursor[0..m) by one block of 1024 threads.
+__global__ void __launch_bounds__(1024) sort_scan_kernel(const uint32_t* __restrict__ hist, uint32_t* cursor,
+                                                         int64_t m)
+{
+    __shared__ uint32_t part[1024];
+    const int t = threadIdx.x;
+    const int64_t per = (m + 1023) / 1024;
+    const int64_t b = t * per, e = min(m, b + per);
+    uint32_t sum = 0;
+    for (int64_t i = b; i < e; ++i) sum += hist[i];
+    part[t] = sum;
+    __syncthreads();
+    for (int off = 1; off < 1024; off <<= 1) {
+        uint32_t v = t >= off ? part[t - off] : 0u;
+        __syncthreads();
+        part[t] += v;
+        __syncthreads();
+    }
+    uint32_t run = part[t] - sum;
+    for (int64_t i = b; i < e; ++i) {
+        uint32_t h = hist[i];
+        cursor[i] = run;
+        run += h;
+    }
+}
+
+__global__ void sort_scatter_kernel(const uint32_t* __restrict__ keys, uint32_t* cursor, int64_t n,
+                                    const double* __restrict__ xs, const float* __restrict__ ps,
+                                    const double* __restrict__ p2s, const int32_t* __restrict__ pids,
+                                    const uint8_t* __restrict__ as, double* xd, float* pd, double* p2d, int32_t* pidd,
+                                    uint8_t* ad)
+{
+    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+        const int64_t d = atomicAdd(&cursor[keys[i]], 1u);
+        xd[d] = xs[i]; xd[n + d] = xs[n + i]; xd[2 * n + d] = xs[2 * n + i];
+        pd[d] = ps[i]; pd[n + d] = ps[n + i]; pd[2 * n + d] = ps[2 * n + i];
+        p2d[d] = p2s[i];
+        pidd[d] = pids[i];
+        ad[d] = as[i];
+    }
+}
+
+int grid_for(int64_t n, int threads, int num_sms)
+{
+    int64_t b = (n + threads - 1) / threads;
+    int64_t cap = (int64_t)num_sms * 16;
+    return (int)std::max<int64_t>(1, std::min(b, cap));
+}
+
+}  // namespace
+
+int launch_push_fast(const PushArgsFast& a, cudaStream_t s)
+{
+    if (a.n <= 0 || a.step_count <= 0) return PT_OK;
+    const int threads = 256;
+    const size_t smem = sizeof(uint32_t) * (size_t)(a.fld.nx + a.fld.ny + a.fld.nz);
+    int dev = 0, sms = 148, per_sm = 8;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    if (a.fld.bf16) {
+        if (smem > 48 * 1024) cudaFuncSetAttribute(push_fast_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, push_fast_kernel<true>, threads, smem);
+    } else {
+        if (smem > 48 * 1024) cudaFuncSetAttribute(push_fast_kernel<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, push_fast_kernel<false>, threads, smem);
+    }
+    per_sm = std::max(per_sm, 1);
+    int64_t blocks = std::min<int64_t>((a.n + threads - 1) / threads, (int64_t)sms * per_sm);
+    if (a.fld.bf16) push_fast_kernel<true><<<(unsigned)blocks, threads, smem, s>>>(a);
+    else push_fast_kernel<false><<<(unsigned)blocks, threads, smem, s>>>(a);
+    PT_CHECK_LAUNCH("push_fast_kernel");
+    return PT_OK;
+}
+
+int launch_brick_convert(const double* const comps[6], const pt_grid& g, double B_ref, int bf16, void* nodes,
+                         const uint32_t* offs, cudaStream_t s)
+{
+    const int64_t total = g.nx * g.ny * g.nz;
+    const int threads = 256;
+    int blocks = (int)std::min<int64_t>((total + threads - 1) / threads, 148 * 32);
+    brick_convert_kernel<<<blocks, threads, 0, s>>>(comps[0], comps[1], comps[2], comps[3], comps[4], comps[5],
+                                                    g.nx, g.ny, g.nz, 1.0 / B_ref, 1.0 / C_LIGHT, bf16, nodes, offs);
+    PT_CHECK_LAUNCH("brick_convert_kernel");
+    return PT_OK;
+}
+
+int launch_fast_import(pt_fast_state* st, const pt_field* f, const double* x1, const double* x2, const double* x3,
+                       const double* p1, const double* p2, const double* p3, const uint8_t* alive, cudaStream_t s)
+{
+    const pt_grid& g = f->grid;
+    fast_import_kernel<<<grid_for(st->n, 256, st->ctx->num_sms), 256, 0, s>>>(
+        x1, x2, x3, p1, p2, p3, alive, st->n, g.xmin, g.ymin, g.zmin, g.dx, g.dy, g.dz, st->x, st->p, st->p2,
+        st->pid, st->alive);
+    PT_CHECK_LAUNCH("fast_import_kernel");
+    return PT_OK;
+}
+
+int launch_fast_export(const pt_fast_state* st, const pt_field* f, double* x1, double* x2, double* x3, double* p1,
+                       double* p2, double* p3, uint8_t* alive, cudaStream_t s)
+{
+    const pt_grid& g = f->grid;
+    fast_export_kernel<<<grid_for(st->n, 256, st->ctx->num_sms), 256, 0, s>>>(
+        st->x, st->p, st->p2, st->pid, st->alive, st->n, g.xmin, g.ymin, g.zmin, g.dx, g.dy, g.dz, x1, x2, x3, p1,
+        p2, p3, alive);
+    PT_CHECK_LAUNCH("fast_export_kernel");
+    return PT_OK;
+}
+
+int fast_sort(pt_ctx* ctx, pt_fast_state* st, const pt_field* f, cudaStream_t s)
+{
+    const int64_t n = st->n;
+    if (n <= 1) return PT_OK;
+    const uint32_t nb = (uint32_t)((f->n_nodes + 511) / 512);
+    const int64_t m = (int64_t)nb + 1;  // + dead bucket
+    // scratch: keys[n], hist[m], cursor[m], then the ping-pong state
+    size_t off = 0;
+    auto take = [&](size_t bytes) {
+        size_t o = off;
+        off += (bytes + 255) & ~(size_t)255;
+        return o;
+    };
+    const size_t o_keys = take(sizeof(uint32_t) * n), o_hist = take(sizeof(uint32_t) * m),
+                 o_cur = take(sizeof(uint32_t) * m), o_x = take(sizeof(double) * 3 * n),
+                 o_p = take(sizeof(float) * 3 * n), o_p2 = take(sizeof(double) * n), o_pid = take(sizeof(int32_t) * n),
+                 o_a = take(n);
+    if (st->sort_tmp_bytes < off) {
+        if (st->sort_tmp) cudaFree(st->sort_tmp);
+        st->sort_tmp = nullptr;
+        st->sort_tmp_bytes = 0;
+        cudaError_t e = cudaMalloc(&st->sort_tmp, off);
+        if (e != cudaSuccess) return fail(PT_ERR_OOM, "sort scratch allocation failed");
+        st->sort_tmp_bytes = off;
+    }
+    char* base = (char*)st->sort_tmp;
+    uint32_t* keys = (uint32_t*)(base + o_keys);
+    uint32_t* hist = (uint32_t*)(base + o_hist);
+    uint32_t* cur = (uint32_t*)(base + o_cur);
+    double* xd = (double*)(base + o_x);
+    float* pd = (float*)(base + o_p);
+    double* p2d = (double*)(base + o_p2);
+    int32_t* pidd = (int32_t*)(base + o_pid);
+    uint8_t* ad = (uint8_t*)(base + o_a);
+    PT_CUDA(cudaMemsetAsync(hist, 0, sizeof(uint32_t) * m, s));
+    const int gb = grid_for(n, 256, ctx->num_sms);
+    sort_key_kernel<<<gb, 256, 0, s>>>(st->x, st->alive, n, f->offs, (int)f->grid.nx, (int)f->grid.ny,
+                                       (int)f->grid.nz, nb, keys, hist);
+    PT_CHECK_LAUNCH("sort_key_kernel");
+    sort_scan_kernel<<<1, 1024, 0, s>>>(hist, cur, m);
+    PT_CHECK_LAUNCH("sort_scan_kernel");
+    sort_scatter_kernel<<<gb, 256, 0, s>>>(keys, cur, n, st->x, st->p, st->p2, st->pid, st->alive, xd, pd, p2d, pidd,
+                                           ad);
+    PT_CHECK_LAUNCH("sort_scatter_kernel");
+    PT_CUDA(cudaMemcpyAsync(st->x, xd, sizeof(double) * 3 * n, cudaMemcpyDeviceToDevice, s));
+    PT_CUDA(cudaMemcpyAsync(st->p, pd, sizeof(float) * 3 * n, cudaMemcpyDeviceToDevice, s));
+    PT_CUDA(cudaMemcpyAsync(st->p2, p2d, sizeof(double) * n, cudaMemcpyDeviceToDevice, s));
+    PT_CUDA(cudaMemcpyAsync(st->pid, pidd, sizeof(int32_t) * n, cudaMemcpyDeviceToDevice, s));
+    PT_CUDA(cudaMemcpyAsync(st->alive, ad, n, cudaMemcpyDeviceToDevice, s));
+    return PT_OK;
+}
+
+}  // namespace pt

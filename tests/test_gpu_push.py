@@ -1,0 +1,158 @@
+"""Parity of the CUDA push with the CPU oracle (needs a B200).
+
+FP64 form: bit-identical to the oracle (and so to a Float64 run of the
+reference) -- trajectories, mu cache, phase-space cache and alive counts.
+FP32 form over Morton bricks: bounded deviation over the first gyroperiod,
+exact |p| conservation with E = 0, results independent of the brick sort."""
+import math
+
+import numpy as np
+import pytest
+
+from helpers import copy_state, fortran_fields, small_problem
+from particle_transport_b200 import runner as R
+from particle_transport_b200.fields import FieldLibrary
+
+pytestmark = pytest.mark.gpu
+
+
+def run_both(pb, nsteps, stride, cache, periodic=True, f64_out=False, alive=None):
+    from oracle import oracle as o
+    n = len(pb.state["x1"])
+    alive0 = np.ones(n, np.uint8) if alive is None else alive.copy()
+    st_o = copy_state(pb.state)
+    al_o = alive0.copy()
+    out_o, ac_o = o.push_run(fortran_fields(pb.fields), pb.grid, st_o, al_o, pb.dt, nsteps, stride, periodic=periodic,
+                             cache_mode={"mu": 1, "phase_space": 2}[cache], out_f64=f64_out)
+    fl = FieldLibrary(pb.fields, pb.grid, "ref_f64")
+    st_g = copy_state(pb.state)
+    al_g = alive0.copy()
+    col = R.CacheCollector(n, R.n_saves(nsteps, stride), cache, f64_out)
+    params = R.push_params(pb.dt, nsteps, stride, periodic=periodic, cache=cache, cache_f64=f64_out)
+    ac_g = R.run_push_host(fl, st_g, al_g, params, col)
+    return (out_o, ac_o, st_o, al_o), (col, ac_g, st_g, al_g)
+
+
+def test_fp64_mu_cache_bit_exact(cuda):
+    pb = small_problem(n=16, n_particles=700, u_over_c=1e-4)
+    (mu_o, ac_o, st_o, al_o), (col, ac_g, st_g, al_g) = run_both(pb, 641, 4, "mu")
+    assert np.array_equal(col.mu, mu_o, equal_nan=True)
+    for k in R.KEYS:
+        assert np.array_equal(st_g[k], st_o[k]), k
+    assert np.array_equal(ac_g, ac_o)
+    assert np.array_equal(al_g, al_o)
+
+
+@pytest.mark.parametrize("f64_out", [False, True])
+def test_fp64_phase_space_bit_exact(cuda, f64_out):
+    pb = small_problem(n=12, n_particles=300, energy_GeV=10.0, u_over_c=1e-4)
+    ((pos_o, mom_o), ac_o, st_o, _), (col, ac_g, st_g, _) = run_both(pb, 257, 8, "phase_space", f64_out=f64_out)
+    assert np.array_equal(col.positions, pos_o, equal_nan=True)
+    assert np.array_equal(col.momenta, mom_o, equal_nan=True)
+    for k in R.KEYS:
+        assert np.array_equal(st_g[k], st_o[k]), k
+
+
+def test_fp64_open_boundary_bit_exact(cuda):
+    pb = small_problem(n=10, n_particles=400, energy_GeV=30.0, u_over_c=1e-4)
+    alive = np.ones(400, np.uint8)
+    alive[::17] = 0  # some particles dead on entry
+    (mu_o, ac_o, st_o, al_o), (col, ac_g, st_g, al_g) = run_both(pb, 400, 3, "mu", periodic=False, alive=alive)
+    assert ac_o[-1] < ac_o[0]  # particles left the box
+    assert np.array_equal(ac_g, ac_o)
+    assert np.array_equal(al_g, al_o)
+    assert np.array_equal(col.mu, mu_o, equal_nan=True)
+
+
+def test_fp64_device_api_matches_host(cuda):
+    torch = cuda
+    pb = small_problem(n=16, n_particles=512)
+    nsteps, stride = 333, 4
+    (mu_o, _, st_o, _), _ = run_both(pb, nsteps, stride, "mu")
+    fl = FieldLibrary(pb.fields, pb.grid, "ref_f64")
+    ens = R.DeviceEnsemble(fl, pb.state, np.ones(512, np.uint8))
+    nsave = R.n_saves(nsteps, stride)
+    cache = torch.full((nsave, 512), float("nan"), dtype=torch.float32, device="cuda")
+    params = R.push_params(pb.dt, nsteps, stride, cache="mu", steps_per_launch=16)
+    s = 0
+    for chunk in (5, 100, 1, 227):  # uneven chunks, each a separate call
+        ens.advance(params, s, chunk, cache, 0, nsave)
+        s += chunk
+    assert s == nsteps
+    torch.cuda.synchronize()
+    assert np.array_equal(cache.cpu().numpy(), mu_o, equal_nan=True)
+    for k in R.KEYS:
+        assert np.array_equal(ens.state[k].cpu().numpy(), st_o[k]), k
+
+
+def _fast_mu(pb, storage, nsteps, stride, sort_every=0, u=True):
+    torch = __import__("torch")
+    fl = FieldLibrary(pb.fields, pb.grid, storage)
+    ens = R.FastEnsemble(fl, pb.state, np.ones(len(pb.state["x1"]), np.uint8))
+    nsave = R.n_saves(nsteps, stride)
+    cache = torch.full((nsave, ens.n), float("nan"), dtype=torch.float32, device="cuda")
+    params = R.push_params(pb.dt, nsteps, stride, cache="mu", precision="f32", sort_every=sort_every)
+    ens.advance(params, 0, nsteps, cache, 0, nsave)
+    st, al = ens.export()
+    torch.cuda.synchronize()
+    return cache.cpu().numpy(), {k: v.cpu().numpy() for k, v in st.items()}, fl
+
+
+@pytest.mark.parametrize("storage,tol_max,tol_med", [("brick_f32", 2e-3, 1e-4), ("brick_bf16", 0.2, 0.02)])
+def test_fast_push_close_over_one_gyroperiod(cuda, storage, tol_max, tol_med):
+    pb = small_problem(n=16, n_particles=1000, u_over_c=1e-4)
+    (mu_o, _, _, _), _ = run_both(pb, 65, 4, "mu")
+    mu_f, _, _ = _fast_mu(pb, storage, 65, 4)
+    d = np.abs(mu_f - mu_o)
+    assert np.all(np.isfinite(mu_f))
+    assert d.max() < tol_max and np.median(d) < tol_med, (d.max(), np.median(d))
+
+
+def test_fast_push_energy_exact_with_E_zero(cuda):
+    pb = small_problem(n=16, n_particles=800, u_over_c=0.0, energy_GeV=10.0)
+    _, st, _ = _fast_mu(pb, "brick_bf16", 3000, 50)
+    p_in = np.sqrt(pb.state["p1"] ** 2 + pb.state["p2"] ** 2 + pb.state["p3"] ** 2)
+    p_out = np.sqrt(st["p1"] ** 2 + st["p2"] ** 2 + st["p3"] ** 2)
+    assert np.max(np.abs(p_out / p_in - 1)) < 1e-13
+
+
+def test_fast_push_sort_does_not_change_results(cuda):
+    pb = small_problem(n=16, n_particles=2000, u_over_c=1e-4, energy_GeV=10.0)
+    mu_a, st_a, _ = _fast_mu(pb, "brick_bf16", 300, 5, sort_every=0)
+    mu_b, st_b, _ = _fast_mu(pb, "brick_bf16", 300, 5, sort_every=7)
+    assert np.array_equal(mu_a, mu_b, equal_nan=True)
+    for k in R.KEYS:
+        assert np.array_equal(st_a[k], st_b[k]), k
+
+
+def test_fast_state_roundtrip(cuda):
+    pb = small_problem(n=12, n_particles=333)
+    _, st, _ = _fast_mu(pb, "brick_f32", 1, 1)  # one sample, no push
+    for k in ("x1", "x2", "x3"):
+        assert np.allclose(st[k], pb.state[k], rtol=1e-14, atol=1e-14 * pb.grid.xmax)
+    for k in ("p1", "p2", "p3"):
+        pm = np.sqrt(pb.state["p1"] ** 2 + pb.state["p2"] ** 2 + pb.state["p3"] ** 2)
+        assert np.max(np.abs(st[k] - pb.state[k]) / pm) < 2e-7
+
+
+def test_host_run_fast_matches_device(cuda):
+    """pt_push_run (host buffers, pipelined egress) with the FP32 push gives
+    the same mu cache as the device entry point."""
+    pb = small_problem(n=16, n_particles=600, u_over_c=1e-4)
+    mu_dev, _, fl = _fast_mu(pb, "brick_bf16", 500, 4)
+    st = copy_state(pb.state)
+    col = R.CacheCollector(600, R.n_saves(500, 4), "mu")
+    R.run_push_host(fl, st, np.ones(600, np.uint8), R.push_params(pb.dt, 500, 4, cache="mu", precision="f32"), col)
+    assert np.array_equal(col.mu, mu_dev, equal_nan=True)
+
+
+def test_errors_raise(cuda):
+    from particle_transport_b200._lib import PtError
+    pb = small_problem(n=8, n_particles=4)
+    fl = FieldLibrary(pb.fields, pb.grid, "ref_f64")
+    with pytest.raises(PtError, match="brick field"):
+        R.run_push_host(fl, copy_state(pb.state), np.ones(4, np.uint8), R.push_params(pb.dt, 10, 1, precision="f32"))
+    with pytest.raises(PtError, match="stride"):
+        R.run_push_host(fl, copy_state(pb.state), np.ones(4, np.uint8), R.push_params(pb.dt, 10, 0))
+    with pytest.raises(ValueError):
+        R.run_push_host(fl, copy_state(pb.state), np.ones(3, np.uint8), R.push_params(pb.dt, 10, 1))
