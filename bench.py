@@ -1,0 +1,504 @@
+#!/usr/bin/env python
+"""Benchmark of the trajectory / transport-statistics hot path on B200.
+
+Workload (the large single campaign at 512^3): anisotropic
+Goldreich-Sridhar-like turbulence, dB/B0 = 1, u_rms = v_A = 1e-4 c
+(E = -u x B), 512^3 nodes with the cell = one 1 GeV gyroradius in
+B0 = 1 uG; 16,777,216 protons at 10 GeV, uniform positions, isotropic
+momenta; 64 steps per reference gyroperiod (B0_ref = mean |B|), mu cache
+every 8 steps.  Seeded synthetic inputs stand in for the MHD snapshots,
+which do not ship with the reference.
+
+One bench step = 64 pushes (one T_g0) of every particle with the 8 mu-cache
+rows written on the device.  `value` is particle-steps/s of the FP32 push
+over BF16 Morton bricks with the state resident in HBM; beside it the plain
+FP64 push (reference layout, bit-exact with the reference arithmetic) on
+the same particles, the D_mumu lag-pair rate on a full-length (500 T_g0,
+4001 saves) campaign of 1,048,576 particles, and `e2e`: the same metric
+through pt_push_run with host buffers (state upload, per-save rows to
+pinned host memory, state download inside the timed region).
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl reference]
+Under torchrun every rank pushes its own 16,777,216 particles (weak scaling,
+no collective on the data path); timing is the max over ranks.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import math
+import os
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "particle-steps/s at 512³ (mixed vs FP64 push); D_μμ lag-pairs/s; job p50/p99"
+UNIT = "particle-steps/s"
+PEAKS_FALLBACK = {"hbm_gbs": 6650.0, "source": "fallback"}
+
+# Bytes the push must move per particle-step (BF16 bricks): 8 corners x 6
+# components x 2 B.  Per launch each particle also reads and writes its
+# state (x 24 B, p 12 B, |p|^2 8 B, id 4 B, alive 1 B) and writes one 4-byte
+# mu per save row.
+GATHER_BYTES = {"brick_bf16": 96, "brick_f32": 192, "ref_f64": 384}
+STATE_BYTES = {"brick_bf16": 49, "brick_f32": 49, "ref_f64": 49}
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--grid", type=int, default=512)
+    ap.add_argument("--particles", type=int, default=16_777_216)
+    ap.add_argument("--energy", type=float, default=10.0)
+    ap.add_argument("--storage", default="brick_bf16", choices=["brick_bf16", "brick_f32"])
+    ap.add_argument("--sort-every", type=int, default=0, help="re-sort by brick every N bench steps (0: never)")
+    ap.add_argument("--lag-particles", type=int, default=1_048_576)
+    ap.add_argument("--e2e-gyroperiods", type=int, default=8)
+    ap.add_argument("--skip", default="", help="comma list of legs to skip: fp64,lag,e2e,cpu")
+    ap.add_argument("--cpu-seconds", type=float, default=10.0)
+    return ap.parse_args()
+
+
+def dist_setup(args):
+    ws = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if ws > 1:
+        import torch.distributed as dist
+        from datetime import timedelta
+        backend = "nccl" if args.impl == "ours" else "gloo"
+        if args.impl == "ours":
+            import torch
+            torch.cuda.set_device(local)
+        dist.init_process_group(backend, timeout=timedelta(seconds=600))
+    return ws, rank, local
+
+
+def load_peaks():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        d = json.load(open(p))
+        return {"hbm_gbs": float(d["hbm_gbs"]), "source": "measured"}
+    return PEAKS_FALLBACK
+
+
+class ClockSampler:
+    """nvidia-smi clock / throttle samples during the timed region."""
+
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,clocks_event_reasons.hw_slowdown,"
+         "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+         "clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device: int):
+        self.device = device
+        self.proc = None
+        self.lines = []
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", f"--id={self.device}", f"--query-gpu={self.Q}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except Exception:
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def __exit__(self, *exc):
+        if self.proc is not None:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except Exception:
+                self.proc.kill()
+
+    def summary(self):
+        sm, mx, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            f = [x.strip() for x in ln.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                mx.append(float(f[2]))
+            except ValueError:
+                continue
+            for nm, v in zip(names, f[5:9]):
+                if v.lower() == "active":
+                    reasons.add(nm)
+        if not sm:
+            return None
+        return {"sm_mhz": float(np.median(sm)), "sm_max_mhz": float(max(mx)), "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+# ---------------------------------------------------------------------------
+# workload
+# ---------------------------------------------------------------------------
+def make_workload(args, device, rank):
+    import torch
+
+    from particle_transport_b200 import fields as F
+    from particle_transport_b200.particles import energy_to_gamma, init_particles
+    from particle_transport_b200.time_units import reference_Omega0
+
+    n = args.grid
+    f_uG = F.synthetic_mhd_fields(n, 2, n // 2, 1.0, 1.0, 1e-4, seed=20260423, spectrum="gs", device=device)
+    fields = F.to_si(f_uG)
+    del f_uG
+    rg = F.gyroradius_m(1.0, 1e-10)
+    grid = F.build_uniform_grid((n - 1) * rg, n, n, n)
+    B0 = F.reference_B0_T(*fields[:3])
+    g0 = energy_to_gamma(args.energy)
+    Om = reference_Omega0(B0, g0, F.Q_E, F.M_P)
+    dt = (2 * math.pi / 64) / Om  # 64 steps per T_g0 (resolve_trajectory_time_grid)
+    state = init_particles(args.particles, grid, args.energy, seed=42 + rank)
+    return fields, grid, B0, dt, state
+
+
+def timed(fn, K, W, torch, per_step=True):
+    for _ in range(W):
+        fn(-1)
+    torch.cuda.synchronize()
+    evs = [torch.cuda.Event(enable_timing=True) for _ in range(K + 1)]
+    evs[0].record()
+    for k in range(K):
+        fn(k)
+        evs[k + 1].record()
+    torch.cuda.synchronize()
+    steps = [evs[k].elapsed_time(evs[k + 1]) for k in range(K)]
+    return evs[0].elapsed_time(evs[K]), steps
+
+
+def cpu_push_rate(fields_host, grid, state, dt, seconds):
+    """Oracle FP64 push (restatement of the reference's push) on all host cores."""
+    from oracle import build as ob
+    from oracle import oracle as o
+
+    ob.build()
+    ff = [np.asfortranarray(f.T) for f in fields_host]
+    nthreads = o.num_threads()
+    n = 4096
+    sample = None
+    while True:
+        st = {k: np.ascontiguousarray(v[:n]).copy() for k, v in state.items()}
+        t0 = time.perf_counter()
+        o.push_run(ff, grid, st, np.ones(n, np.uint8), dt, 32001, 8, cache_mode=1, step_begin=0, step_count=64)
+        el = time.perf_counter() - t0
+        if el * 4 >= seconds or n >= len(state["x1"]):
+            sample = (n, 64, el)
+            break
+        n = min(len(state["x1"]), int(n * max(2.0, min(16.0, seconds / 4 / max(el, 1e-3)))))
+    n, steps, el = sample
+    reps = max(1, int(round(seconds / max(el, 1e-3))))
+    st = {k: np.ascontiguousarray(v[:n]).copy() for k, v in state.items()}
+    t0 = time.perf_counter()
+    for r in range(reps):
+        o.push_run(ff, grid, st, np.ones(n, np.uint8), dt, 32001, 8, cache_mode=1, step_begin=64 * r, step_count=64)
+    el = time.perf_counter() - t0
+    return {"value": n * 64 * reps / el, "unit": UNIT, "cores": nthreads, "kind": "port",
+            "sample": f"{n} particles x {64 * reps} FP64 steps (mu cache every 8) of the same workload, "
+                      f"{el:.1f} s on {nthreads} threads"}
+
+
+def cpu_lag_rate(mu_chunk, lags, edges, seconds):
+    from oracle import oracle as o
+
+    nl, nb = len(lags), len(edges) - 1
+    n = 64
+    while True:
+        acc = {"counts": np.zeros((nl, nb), np.int64), "sum_d": np.zeros((nl, nb)), "sum_d2": np.zeros((nl, nb)),
+               "w_count": np.zeros(nl, np.int64), "w_mean": np.zeros(nl), "w_m2": np.zeros(nl),
+               "pair_ss": np.zeros(nl), "pair_n": np.zeros(nl, np.int64)}
+        t0 = time.perf_counter()
+        o.dmumu_accumulate(mu_chunk[:n], lags, edges, acc)
+        el = time.perf_counter() - t0
+        if el * 2 >= seconds or n >= mu_chunk.shape[0]:
+            break
+        n = min(mu_chunk.shape[0], int(n * max(2.0, min(16.0, seconds / 2 / max(el, 1e-3)))))
+    pairs = int(acc["pair_n"].sum())
+    return {"value": pairs / el, "unit": "lag-pairs/s", "cores": o.num_threads(), "kind": "port",
+            "sample": f"{n} particles x {mu_chunk.shape[1]} saves x {len(lags)} lags ({pairs} pairs), {el:.1f} s"}
+
+
+# ---------------------------------------------------------------------------
+def run_reference(args, ws, rank):
+    """Reference arm: the reference's push has no CPU path, so its CPU
+    restatement (the oracle, FP64, reference operation order) is timed on all
+    host threads over bounded samples of the same workload."""
+    if rank != 0:
+        return
+    import torch
+
+    from oracle import build as ob
+    from oracle import oracle as o
+
+    ob.build()
+    dev = "cuda" if torch.cuda.is_available() else "cpu"
+    fields, grid, B0, dt, state = make_workload(args, dev, 0)
+    fields_host = [f.cpu().numpy() for f in fields]
+    del fields
+    ff = [np.asfortranarray(f.T) for f in fields_host]
+    nthreads = o.num_threads()
+    # size one step (a sample of the particles over 64 pushes) at ~3 s
+    n = 4096
+    while True:
+        st = {k: np.ascontiguousarray(v[:n]).copy() for k, v in state.items()}
+        t0 = time.perf_counter()
+        o.push_run(ff, grid, st, np.ones(n, np.uint8), dt, 32001, 8, cache_mode=1, step_begin=0, step_count=64)
+        el = time.perf_counter() - t0
+        if el >= 1.5 or n >= args.particles:
+            break
+        n = min(args.particles, int(n * max(2.0, min(16.0, 3.0 / max(el, 1e-3)))))
+    st = {k: np.ascontiguousarray(v[:n]).copy() for k, v in state.items()}
+    al = np.ones(n, np.uint8)
+    for w in range(args.warmup):
+        o.push_run(ff, grid, st, al, dt, 32001, 8, cache_mode=1, step_begin=64 * w, step_count=64)
+    t0 = time.perf_counter()
+    for k in range(args.steps):
+        o.push_run(ff, grid, st, al, dt, 32001, 8, cache_mode=1, step_begin=64 * (args.warmup + k), step_count=64)
+    el = time.perf_counter() - t0
+    value = n * 64 * args.steps / el
+    sample = f"{n} of {args.particles} particles per step x 64 FP64 pushes (mu cache every 8)"
+    line = {"impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": ws, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": 1e3 * el / args.steps, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded GS turbulence, seeded particles)",
+            "config": {"workload": f"{args.grid}^3 GS turbulence, 10 GeV protons, 64 steps/T_g0, mu cache every 8",
+                       "sample": sample},
+            "cpu_baseline": {"value": value, "unit": UNIT, "cores": nthreads, "kind": "port", "sample": sample},
+            "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+            "note": "the reference (Julia + CUDA.jl) cannot run here; its push exists only as a CUDA.jl kernel, so "
+                    "this arm times the CPU restatement of its Float64 push (oracle/pt_oracle.c)"}
+    print(json.dumps(line), flush=True)
+
+
+def run_ours(args, ws, rank, local):
+    import torch
+
+    from particle_transport_b200 import _lib
+    from particle_transport_b200 import runner as R
+    from particle_transport_b200 import stats as S
+    from particle_transport_b200.fields import FieldLibrary
+    from particle_transport_b200.time_units import build_mu_edges_full, log_spaced_lag_steps
+
+    skip = set(filter(None, args.skip.split(",")))
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    fields, grid, B0, dt, state = make_workload(args, dev, rank)
+    n = args.particles
+    NSTEPS = 32001  # 500 T_g0 at 64 steps per T_g0
+    STRIDE = 8
+    K, W = args.steps, args.warmup
+    launches = {"push": 0, "sort": 0}
+
+    # ---------------- FP32 push over bricks (headline)
+    fb = FieldLibrary(fields, grid, args.storage, B_ref_T=B0)
+    alive = np.ones(n, np.uint8)
+    ens = R.FastEnsemble(fb, state, alive)
+    ring = torch.empty((8, n), dtype=torch.float32, device=dev)
+    params = R.push_params(dt, NSTEPS, STRIDE, cache="mu", precision="f32")
+    step_at = [0]
+
+    def fast_step(k):
+        s0 = step_at[0]
+        if args.sort_every and (s0 // 64) % args.sort_every == 0:
+            ens.sort()
+            if k >= 0:
+                launches["sort"] += 3
+        ens.advance(params, s0, 64, ring, s0 // STRIDE, 8)
+        if k >= 0:
+            launches["push"] += 1
+        step_at[0] = s0 + 64
+
+    dist_barrier(ws)
+    with ClockSampler(local) as clk:
+        total_ms, steps_ms = timed(fast_step, K, W, torch)
+    total_ms = max_over_ranks(total_ms, ws, dev)
+    value = ws * n * 64 * K / (total_ms / 1e3)
+    clocks = clk.summary()
+
+    # roofline of the push kernel: algorithmic bytes per launch / launch time
+    peaks = load_peaks()
+    bpl = n * (64 * GATHER_BYTES[args.storage] + 2 * STATE_BYTES[args.storage] + 8 * 4)
+    launch_ms = float(np.mean(steps_ms))
+    achieved = bpl / (launch_ms / 1e3) / 1e9
+    roofline = {"kernel": "push_fast_kernel", "bound": "hbm", "achieved": achieved, "peak": peaks["hbm_gbs"],
+                "unit": "GB/s", "frac": achieved / peaks["hbm_gbs"], "peak_source": peaks["source"],
+                "traffic": TRAFFIC.get((args.storage, args.grid)),
+                "algorithmic_bytes_per_launch": bpl}
+
+    # ---------------- FP64 plain push on the same particles
+    fp64 = None
+    if "fp64" not in skip:
+        fr = FieldLibrary(fields, grid, "ref_f64")
+        dens = R.DeviceEnsemble(fr, state, alive)
+        p64 = R.push_params(dt, NSTEPS, STRIDE, cache="mu", precision="f64", steps_per_launch=64)
+        at = [0]
+
+        def f64_step(k):
+            dens.advance(p64, at[0], 64, ring, at[0] // STRIDE, 8)
+            at[0] += 64
+
+        K64 = max(2, K // 2)
+        ms64, _ = timed(f64_step, K64, max(1, min(W, 3)), torch)
+        ms64 = max_over_ranks(ms64, ws, dev)
+        v64 = ws * n * 64 * K64 / (ms64 / 1e3)
+        fp64 = {"value": v64, "unit": UNIT, "ms_per_step": ms64 / K64, "steps": K64, "dtype": "f64",
+                "field": "reference layout, six FP64 arrays", "speedup_mixed_vs_fp64": value / v64}
+        del dens, fr
+        torch.cuda.empty_cache()
+    del ens, ring
+    torch.cuda.empty_cache()
+
+    # ---------------- D_mumu lag pairs on a full-length campaign subset
+    lag = None
+    if "lag" not in skip:
+        nl = min(args.lag_particles, n)
+        sub = {k: v[:nl] for k, v in state.items()}
+        ens_l = R.FastEnsemble(fb, sub, np.ones(nl, np.uint8))
+        nsave = (NSTEPS - 1) // STRIDE + 1
+        cache = torch.empty((nsave, nl), dtype=torch.float32, device=dev)
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        ens_l.advance(params, 0, NSTEPS, cache, 0, nsave)
+        torch.cuda.synchronize()
+        push_full_s = time.perf_counter() - t0
+        lags = log_spaced_lag_steps(nsave - 1, 64)
+        edges, _ = build_mu_edges_full(0.0, 1.0, 50)
+
+        def lag_pass(_k):
+            acc = S.new_dmumu_accumulators(len(lags), 50, device=dev)
+            S.process_mu_chunk_dmumu(cache, lags, edges, acc["particle_counts"], acc["particle_means"],
+                                     acc["particle_m2s"], acc["pair_sum_squares"], acc["pair_counts"],
+                                     acc["dmumu_counts"], acc["dmumu_sum_delta"], acc["dmumu_sum_delta2"],
+                                     start_mode="sliding", bin_abs=True, layout="particle_fastest")
+            lag_pass.acc = acc
+
+        lms, _ = timed(lag_pass, 2, 1, torch)
+        pairs = int(lag_pass.acc["pair_counts"].sum().item())
+        lag_s = lms / 2 / 1e3
+        lag = {"value": ws * pairs / max_over_ranks(lag_s * 1e3, ws, dev) * 1e3, "unit": "lag-pairs/s",
+               "pairs_per_pass": pairs, "ms_per_pass": lms / 2, "particles": nl, "saves": nsave,
+               "lags": int(len(lags)), "mu_bins": 50, "estimator": "sliding, |mu| bins",
+               "compulsory_bytes_per_pass": 4 * nl * nsave,
+               "hbm_frac_of_compulsory": (4 * nl * nsave / lag_s / 1e9) / peaks["hbm_gbs"],
+               "campaign_push_s": push_full_s,
+               "campaign_push_rate": nl * (NSTEPS - 1) / push_full_s}
+        if "cpu" not in skip and rank == 0:
+            sys.path.insert(0, os.path.join(ROOT, "tests"))
+            mu_host = np.ascontiguousarray(cache[:, :4096].T.cpu().numpy())
+            lag["cpu_baseline"] = cpu_lag_rate(mu_host, lags, edges, args.cpu_seconds / 2)
+        del ens_l, cache
+        torch.cuda.empty_cache()
+
+    # ---------------- e2e through pt_push_run with host buffers
+    e2e = None
+    if "e2e" not in skip:
+        G = args.e2e_gyroperiods
+        ns = 64 * G + 1
+        host = {k: np.ascontiguousarray(v).copy() for k, v in state.items()}
+        al = np.ones(n, np.uint8)
+        pe = R.push_params(dt, ns, STRIDE, cache="mu", precision="f32")
+        rows = [0]
+
+        def sink(i, row):
+            rows[0] += 1
+
+        def e2e_call(_k):
+            R.run_push_host(fb, host, al, pe, sink)
+
+        for _ in range(1):
+            e2e_call(-1)
+        dist_barrier(ws)
+        t0 = time.perf_counter()
+        ncall = max(1, min(3, K // 3))
+        for _ in range(ncall):
+            e2e_call(0)
+        el = time.perf_counter() - t0
+        el = max_over_ranks(el * 1e3, ws, dev) / 1e3
+        nsave_e = (ns - 1) // STRIDE + 1
+        e2e = {"value": ws * n * (ns - 1) * ncall / el, "unit": UNIT,
+               "h2d_bytes_per_step": int(n * (6 * 8 + 1)),
+               "d2h_bytes_per_step": int(n * (6 * 8 + 1) + nsave_e * n * 4 + 8 * ns),
+               "call": f"pt_push_run over {G} T_g0 ({ns - 1} pushes, {nsave_e} mu rows) per call, host state",
+               "calls": ncall, "s_per_call": el / ncall}
+
+    # ---------------- CPU baseline (oracle, host cores)
+    cpu = None
+    if "cpu" not in skip and rank == 0:
+        fields_host = [f.cpu().numpy() for f in fields]
+        cpu = cpu_push_rate(fields_host, grid, state, dt, args.cpu_seconds)
+        del fields_host
+
+    if rank == 0:
+        line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": ws, "steps": K, "warmup": W,
+                "ms_per_step": total_ms / K, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+                "dtype": "f32", "data": "synthetic (seeded GS turbulence and particles; no MHD snapshot ships)",
+                "config": {"workload": f"{args.grid}^3 GS turbulence dB/B0=1, u_rms=1e-4 c, {n} protons/GPU at "
+                                       f"{args.energy:g} GeV, 64 steps/T_g0, mu cache every 8; step = 64 pushes",
+                           "field_storage": args.storage, "field_bytes": fb.device_bytes,
+                           "push": "FP32 push, FP64 positions and |p|^2", "sort_every_steps": args.sort_every * 64,
+                           "l2": "inputs larger than L2 (field and state exceed 126 MB); no flush",
+                           "parallelism": f"particle-sharded replicas x{ws}"},
+                "roofline": roofline, "fp64_push": fp64, "lag_pairs": lag, "e2e": e2e, "cpu_baseline": cpu,
+                "clocks": clocks, "gpu_launches": launches["push"] + launches["sort"], "job_latency": None}
+        print(json.dumps(line), flush=True)
+
+
+TRAFFIC = {}
+
+
+def dist_barrier(ws):
+    if ws > 1:
+        import torch.distributed as dist
+        dist.barrier()
+
+
+def max_over_ranks(x, ws, dev):
+    if ws == 1:
+        return float(x)
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([float(x)], dtype=torch.float64, device=dev)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def main():
+    args = parse()
+    if args.impl == "reference":
+        # CPU-only arm: rank 0 alone runs and prints; other ranks exit without work
+        ws = int(os.environ.get("WORLD_SIZE", "1"))
+        if int(os.environ.get("RANK", "0")) == 0:
+            run_reference(args, ws, 0)
+        return
+    ws, rank, local = dist_setup(args)
+    try:
+        if args.impl == "reference":
+            run_reference(args, ws, rank)
+        else:
+            run_ours(args, ws, rank, local)
+    finally:
+        if ws > 1:
+            import torch.distributed as dist
+            dist.barrier()
+            dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()
