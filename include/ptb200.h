@@ -96,7 +96,9 @@ int pt_version(void);
 
 int pt_ctx_create(int device, pt_ctx** out);
 int pt_ctx_destroy(pt_ctx* ctx);
-/* Use the given cudaStream_t for all *_device entry points (NULL = library stream). */
+/* Use the given cudaStream_t for all *_device entry points: NULL selects the
+ * library's own (non-blocking) stream; pass cudaStreamLegacy ((void*)0x1)
+ * for the legacy default stream. */
 int pt_ctx_set_stream(pt_ctx* ctx, void* cuda_stream);
 int pt_ctx_synchronize(pt_ctx* ctx);
 

@@ -21,6 +21,7 @@ PT_FIELD_REF_F64, PT_FIELD_BRICK_F32, PT_FIELD_BRICK_BF16 = 0, 1, 2
 PT_CACHE_NONE, PT_CACHE_MU, PT_CACHE_PHASE_SPACE = 0, 1, 2
 PT_PUSH_F64, PT_PUSH_F32 = 0, 1
 PT_START_SLIDING, PT_START_INJECTION = 0, 1
+CUDA_STREAM_LEGACY = 0x1  # cudaStreamLegacy
 
 # every exported entry point of include/ptb200.h
 EXPORTS = (
@@ -155,11 +156,14 @@ class Context:
         self.device = device
 
     def use_stream(self, stream) -> None:
-        """Enqueue device calls on ``stream`` (a torch.cuda.Stream, an int handle or None)."""
-        h = None
-        if stream is not None:
-            h = stream.cuda_stream if hasattr(stream, "cuda_stream") else int(stream)
-        call("pt_ctx_set_stream", self.handle, C.c_void_p(h) if h else None)
+        """Enqueue device calls on ``stream`` (a torch.cuda.Stream or an int
+        cudaStream_t).  Handle 0 is the legacy default stream and is passed as
+        cudaStreamLegacy; None selects the library's own stream."""
+        if stream is None:
+            call("pt_ctx_set_stream", self.handle, None)
+            return
+        h = stream.cuda_stream if hasattr(stream, "cuda_stream") else int(stream)
+        call("pt_ctx_set_stream", self.handle, C.c_void_p(h if h else CUDA_STREAM_LEGACY))
 
     def synchronize(self) -> None:
         call("pt_ctx_synchronize", self.handle)
