@@ -190,6 +190,31 @@ int pt_dmumu_accumulate_device(pt_ctx* ctx, const float* d_mu, int64_t n, int64_
                                int64_t* d_pair_n);
 
 /*
+ * Same as pt_dmumu_accumulate_device, but allocates no device memory: no
+ * cudaMalloc / cudaFree and no allocating library call.  It has no
+ * counterpart in the reference.  It is for callers that cannot let a
+ * library allocate: a host that owns every device byte through its own pool
+ * (the Julia host's CUDA.jl pool, a server admitting jobs by HBM budget)
+ * cannot account for an allocation made behind its back, and cudaFree
+ * synchronises the whole device, stalling other streams.
+ * The per-CTA partials live in one fixed 16 MiB device array that every GPU
+ * loading the library keeps until the process exits.  The first call on a
+ * device looks up that array's device address (cudaGetSymbolAddress); make
+ * the first call on each device before any stream capture.  All calls share
+ * the array and fully overwrite the part they use, so nothing carries over
+ * between calls, but calls that overlap on the GPU (two streams, two host
+ * threads) race on it: serialise them.  Limits: the (lag batch x bin)
+ * partials must fit in the 16 MiB array, and each particle's mu series must
+ * fit on chip (about 30,000 saves at 50 bins); larger requests fail with
+ * PT_ERR_ARG and a message naming the limit.
+ */
+int pt_dmumu_accumulate_device_noalloc(pt_ctx* ctx, const float* d_mu, int64_t n, int64_t nsave, int64_t sp,
+                                       int64_t ss, const int64_t* d_lag_steps, int n_lags, const double* d_mu_edges,
+                                       int n_bins, int start_mode, int bin_abs, int64_t* d_counts, double* d_sum_d,
+                                       double* d_sum_d2, int64_t* d_w_count, double* d_w_mean, double* d_w_m2,
+                                       double* d_pair_ss, int64_t* d_pair_n);
+
+/*
  * D_pp lag statistics: replaces process_momenta_chunk_dpp_cpu!
  *   src/compute_dpp_full.jl:247-288.
  * mom: Float32 phase-space momenta, Julia (chunk, 3, nsave): element

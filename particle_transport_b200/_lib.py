@@ -28,7 +28,8 @@ EXPORTS = (
     "pt_last_error", "pt_version", "pt_ctx_create", "pt_ctx_destroy", "pt_ctx_set_stream", "pt_ctx_synchronize",
     "pt_field_upload", "pt_field_upload_device", "pt_field_destroy", "pt_field_device_bytes", "pt_push_run",
     "pt_push_advance_device", "pt_fast_state_create", "pt_fast_state_export", "pt_fast_state_destroy",
-    "pt_fast_state_sort", "pt_push_advance_fast", "pt_dmumu_accumulate", "pt_dmumu_accumulate_device", "pt_dpp_accumulate",
+    "pt_fast_state_sort", "pt_push_advance_fast", "pt_dmumu_accumulate", "pt_dmumu_accumulate_device",
+    "pt_dmumu_accumulate_device_noalloc", "pt_dpp_accumulate",
     "pt_dpp_accumulate_device", "pt_energy_snapshots", "pt_energy_histogram_device", "pt_reconstruct_mu",
 )
 
@@ -100,6 +101,8 @@ def load():
                                           P]),
             "pt_dmumu_accumulate_device": (i32, [P, P, i64, i64, i64, i64, P, i32, P, i32, i32, i32, P, P, P, P, P,
                                                  P, P, P]),
+            "pt_dmumu_accumulate_device_noalloc": (i32, [P, P, i64, i64, i64, i64, P, i32, P, i32, i32, i32, P, P, P,
+                                                         P, P, P, P, P]),
             "pt_dpp_accumulate": (i32, [P, P, i64, i64, P, i32, d, P, P, P, P, P]),
             "pt_dpp_accumulate_device": (i32, [P, P, i64, i64, P, i32, d, P, P, P, P, P]),
             "pt_energy_snapshots": (i32, [P, P, i64, i64, P, i32, i64, P]),

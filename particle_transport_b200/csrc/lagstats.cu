@@ -630,3 +630,145 @@ int launch_energy_histogram(const float* mom, int64_t chunk, int64_t nsave, cons
 }
 
 }  // namespace pt
+
+// ---------------------------------------------------------------------------
+// D_mumu accumulation that allocates nothing.
+//
+// Some callers cannot let a library allocate device memory: a host that owns
+// all device memory through its own pool (the Julia host's CUDA.jl pool, or
+// the campaign server's HBM-budget admission) has no way to account for a
+// cudaMalloc made behind its back, and cudaFree synchronises the whole
+// device, stalling every other stream of a busy GPU.  For them the per-CTA
+// partials of the D_mumu kernel live in a fixed, file-scope device array of
+// kDmumuNoAllocBytes (16 MiB) that every GPU which loads the library holds
+// until the process exits.  The array's device address is looked up once per
+// device with cudaGetSymbolAddress (host code cannot use the symbol itself:
+// on the host it names a stand-in, not device memory).
+// ---------------------------------------------------------------------------
+#include <mutex>
+
+static constexpr size_t kDmumuNoAllocBytes = (size_t)16 << 20;
+static __device__ __align__(256) unsigned char g_dmumu_noalloc_scratch[kDmumuNoAllocBytes];
+
+namespace pt {
+namespace {
+
+constexpr int kMaxDevices = 64;
+std::mutex g_noalloc_mutex;
+void* g_noalloc_ptr[kMaxDevices] = {};
+
+// Device address of the fixed scratch on `device` (set up on first use).
+int noalloc_scratch(int device, void** out)
+{
+    if (device < 0 || device >= kMaxDevices) return fail(PT_ERR_ARG, "device index out of range");
+    std::lock_guard<std::mutex> lock(g_noalloc_mutex);
+    if (!g_noalloc_ptr[device]) {
+        int prev = 0;
+        cudaError_t e = cudaGetDevice(&prev);
+        if (e != cudaSuccess) return cuda_fail(e, "cudaGetDevice");
+        e = cudaSetDevice(device);
+        if (e != cudaSuccess) return cuda_fail(e, "cudaSetDevice");
+        void* p = nullptr;
+        e = cudaGetSymbolAddress(&p, g_dmumu_noalloc_scratch);
+        cudaError_t e2 = cudaSetDevice(prev);
+        if (e != cudaSuccess) return cuda_fail(e, "cudaGetSymbolAddress(g_dmumu_noalloc_scratch)");
+        if (e2 != cudaSuccess) return cuda_fail(e2, "cudaSetDevice");
+        g_noalloc_ptr[device] = p;
+    }
+    *out = g_noalloc_ptr[device];
+    return PT_OK;
+}
+
+int run_dmumu_noalloc(pt_ctx* ctx, const DmumuArgs& a, cudaStream_t s)
+{
+    if (a.n <= 0 || a.n_lags <= 0) return PT_OK;
+    if (a.n_bins < 1 || a.n_bins > 4096) return fail(PT_ERR_ARG, "n_bins must be in [1, 4096]");
+    if (a.nsave < 1) return fail(PT_ERR_ARG, "nsave must be positive");
+    void* scratch = nullptr;
+    int rc = noalloc_scratch(ctx->device, &scratch);
+    if (rc) return rc;
+    int max_smem = 0;
+    cudaDeviceGetAttribute(&max_smem, cudaDevAttrMaxSharedMemoryPerBlockOptin, ctx->device);
+    const size_t budget = (size_t)std::min(max_smem, 200 * 1024);
+    const bool small_idx = a.nsave <= 65535;
+    const size_t idx_bytes = small_idx ? 2 : 4;
+    const size_t slot_bytes = align16(a.nsave * sizeof(float)) + align16(a.nsave * idx_bytes) +
+                              align16(sizeof(int) * (size_t)(2 * a.n_bins + 3));
+    const size_t edge_bytes = align16(sizeof(double) * (size_t)(a.n_bins + 1));
+    int nl_cap = (int)std::max<size_t>(32, ((budget / 2) / ((size_t)a.n_bins * 24)) / 32 * 32);
+    nl_cap = std::min(nl_cap, 32 * 8);
+    for (int lag0 = 0; lag0 < a.n_lags; lag0 += nl_cap) {
+        const int nl = std::min(nl_cap, a.n_lags - lag0);
+        const int groups = (nl + kWarp - 1) / kWarp;
+        const size_t acc_bytes = (size_t)nl * a.n_bins * 24;
+        const size_t fixed = edge_bytes + std::max(acc_bytes, sizeof(WelfordPart) * 1024);
+        if (fixed + slot_bytes > budget)
+            return fail(PT_ERR_ARG, "pt_dmumu_accumulate_device_noalloc: nsave = " + std::to_string(a.nsave) +
+                                        " is too long for on-chip staging with " + std::to_string(a.n_bins) +
+                                        " bins; use pt_dmumu_accumulate_device");
+        int ppc = (int)std::min<size_t>((budget - fixed) / slot_bytes, (size_t)(32 / groups));
+        ppc = std::max(1, ppc);
+        const int threads = ppc * groups * kWarp;
+        const size_t smem = fixed + (size_t)ppc * slot_bytes;
+        // per-CTA partials: counts, sum, sum^2 per (lag, bin) and a Welford triple per lag
+        const size_t per_cta = (size_t)nl * a.n_bins * 24 + sizeof(WelfordPart) * (size_t)nl + 64;
+        const int64_t cap_grid = (int64_t)((kDmumuNoAllocBytes - 1024) / per_cta);
+        if (cap_grid < 1)
+            return fail(PT_ERR_ARG, "pt_dmumu_accumulate_device_noalloc: n_lags x n_bins too large for the " +
+                                        std::to_string(kDmumuNoAllocBytes >> 20) + " MiB fixed scratch");
+        void* kfn = small_idx ? (void*)dmumu_kernel<uint16_t, true> : (void*)dmumu_kernel<uint32_t, true>;
+        PT_CUDA(cudaFuncSetAttribute(kfn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+        int per_sm = 1;
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kfn, threads, smem);
+        per_sm = std::max(1, per_sm);
+        const int64_t tiles = (a.n + ppc - 1) / ppc;
+        const int grid = (int)std::max<int64_t>(
+            1, std::min<int64_t>(std::min<int64_t>(tiles, (int64_t)ctx->num_sms * per_sm), cap_grid));
+        const size_t part_acc = (size_t)grid * nl * a.n_bins;
+        char* base = (char*)scratch;
+        DmumuLaunch L;
+        L.mu = a.mu; L.n = a.n; L.nsave = a.nsave; L.sp = a.sp; L.ss = a.ss;
+        L.start_cap = a.injection ? 1 : a.nsave;
+        L.lags = a.lags + lag0; L.nl = nl; L.edges = a.edges; L.n_bins = a.n_bins; L.bin_abs = a.bin_abs;
+        L.ppc = ppc; L.groups = groups; L.slot_bytes = slot_bytes;
+        L.part_cnt = (unsigned long long*)base;
+        L.part_sd = (double*)(base + align16(part_acc * 8));
+        L.part_sd2 = (double*)(base + 2 * align16(part_acc * 8));
+        L.part_w = (WelfordPart*)(base + 3 * align16(part_acc * 8));
+        L.gslots = nullptr;
+        if (3 * align16(part_acc * 8) + sizeof(WelfordPart) * (size_t)grid * nl > kDmumuNoAllocBytes)
+            return fail(PT_ERR_ARG, "internal: no-alloc scratch overflow");
+        if (small_idx) dmumu_kernel<uint16_t, true><<<grid, threads, smem, s>>>(L);
+        else dmumu_kernel<uint32_t, true><<<grid, threads, smem, s>>>(L);
+        PT_CHECK_LAUNCH("dmumu_kernel (no-alloc)");
+        const int fin_blocks = (int)((std::max(nl * a.n_bins, nl) + 255) / 256);
+        dmumu_finalize_kernel<<<fin_blocks, 256, 0, s>>>(L.part_cnt, L.part_sd, L.part_sd2, L.part_w, grid, nl,
+                                                         a.n_bins, lag0, a.n_lags, a.counts, a.sum_d, a.sum_d2,
+                                                         a.w_count, a.w_mean, a.w_m2, a.pair_ss, a.pair_n);
+        PT_CHECK_LAUNCH("dmumu_finalize_kernel (no-alloc)");
+    }
+    return PT_OK;
+}
+
+}  // namespace
+}  // namespace pt
+
+extern "C" int pt_dmumu_accumulate_device_noalloc(pt_ctx* ctx, const float* d_mu, int64_t n, int64_t nsave, int64_t sp,
+                                                  int64_t ss, const int64_t* d_lags, int n_lags, const double* d_edges,
+                                                  int n_bins, int start_mode, int bin_abs, int64_t* d_counts,
+                                                  double* d_sum_d, double* d_sum_d2, int64_t* d_w_count,
+                                                  double* d_w_mean, double* d_w_m2, double* d_pair_ss,
+                                                  int64_t* d_pair_n)
+{
+    using namespace pt;
+    if (!ctx) return fail(PT_ERR_ARG, "ctx is null");
+    if (n < 0 || nsave < 1 || n_lags < 0 || n_bins < 1) return fail(PT_ERR_ARG, "bad sizes");
+    if (start_mode != PT_START_SLIDING && start_mode != PT_START_INJECTION) return fail(PT_ERR_ARG, "start_mode");
+    if (n == 0 || n_lags == 0) return PT_OK;
+    if (!(d_mu && d_lags && d_edges && d_counts && d_sum_d && d_sum_d2 && d_w_count && d_w_mean && d_w_m2 &&
+          d_pair_ss && d_pair_n))
+        return fail(PT_ERR_ARG, "null pointer");
+    DmumuArgs a{d_mu, n, nsave, sp, ss, d_lags, n_lags, d_edges, n_bins, start_mode == PT_START_INJECTION, bin_abs != 0,
+                d_counts, d_sum_d, d_sum_d2, d_w_count, d_w_mean, d_w_m2, d_pair_ss, d_pair_n};
+    return run_dmumu_noalloc(ctx, a, ctx->stream);
+}
