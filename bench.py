@@ -60,7 +60,8 @@ def parse():
     ap.add_argument("--particles", type=int, default=16_777_216)
     ap.add_argument("--energy", type=float, default=10.0)
     ap.add_argument("--storage", default="brick_bf16", choices=["brick_bf16", "brick_f32"])
-    ap.add_argument("--sort-every", type=int, default=0, help="re-sort by brick every N bench steps (0: never)")
+    ap.add_argument("--sort-every", type=int, default=64, help="re-sort particles by brick every N pushes (0: never)")
+    ap.add_argument("--variant", type=int, default=1, help="push launch shape (pt_push_params.kernel_variant)")
     ap.add_argument("--lag-particles", type=int, default=1_048_576)
     ap.add_argument("--e2e-gyroperiods", type=int, default=8)
     ap.add_argument("--skip", default="", help="comma list of legs to skip: fp64,lag,e2e,cpu")
@@ -311,17 +312,27 @@ def run_ours(args, ws, rank, local):
     alive = np.ones(n, np.uint8)
     ens = R.FastEnsemble(fb, state, alive)
     ring = torch.empty((8, n), dtype=torch.float32, device=dev)
-    params = R.push_params(dt, NSTEPS, STRIDE, cache="mu", precision="f32")
+    # the sort cadence is driven here (same rule as pt_push_advance_fast's
+    # sort_every) so that events can bracket the push launch alone
+    params = R.push_params(dt, NSTEPS, STRIDE, cache="mu", precision="f32", kernel_variant=args.variant)
     step_at = [0]
+    last_sort = [None]
+    push_ev = []
 
     def fast_step(k):
         s0 = step_at[0]
-        if args.sort_every and (s0 // 64) % args.sort_every == 0:
+        if args.sort_every and (last_sort[0] is None or s0 - last_sort[0] >= args.sort_every):
             ens.sort()
+            last_sort[0] = s0
             if k >= 0:
                 launches["sort"] += 3
+        if k >= 0:
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record()
         ens.advance(params, s0, 64, ring, s0 // STRIDE, 8)
         if k >= 0:
+            e1.record()
+            push_ev.append((e0, e1))
             launches["push"] += 1
         step_at[0] = s0 + 64
 
@@ -335,12 +346,13 @@ def run_ours(args, ws, rank, local):
     # roofline of the push kernel: algorithmic bytes per launch / launch time
     peaks = load_peaks()
     bpl = n * (64 * GATHER_BYTES[args.storage] + 2 * STATE_BYTES[args.storage] + 8 * 4)
-    launch_ms = float(np.mean(steps_ms))
+    launch_ms = float(np.mean([a.elapsed_time(b) for a, b in push_ev]))
     achieved = bpl / (launch_ms / 1e3) / 1e9
     roofline = {"kernel": "push_fast_kernel", "bound": "hbm", "achieved": achieved, "peak": peaks["hbm_gbs"],
                 "unit": "GB/s", "frac": achieved / peaks["hbm_gbs"], "peak_source": peaks["source"],
-                "traffic": TRAFFIC.get((args.storage, args.grid)),
-                "algorithmic_bytes_per_launch": bpl}
+                "traffic": TRAFFIC.get((args.storage, args.grid, n)),
+                "algorithmic_bytes_per_launch": bpl, "launch_ms": launch_ms,
+                "sort_ms_per_step": float(np.mean(steps_ms)) - launch_ms}
 
     # ---------------- FP64 plain push on the same particles
     fp64 = None
@@ -375,7 +387,8 @@ def run_ours(args, ws, rank, local):
         cache = torch.empty((nsave, nl), dtype=torch.float32, device=dev)
         torch.cuda.synchronize()
         t0 = time.perf_counter()
-        ens_l.advance(params, 0, NSTEPS, cache, 0, nsave)
+        ens_l.advance(R.push_params(dt, NSTEPS, STRIDE, cache="mu", precision="f32", sort_every=args.sort_every,
+                                    kernel_variant=args.variant), 0, NSTEPS, cache, 0, nsave)
         torch.cuda.synchronize()
         push_full_s = time.perf_counter() - t0
         lags = log_spaced_lag_steps(nsave - 1, 64)
@@ -413,7 +426,8 @@ def run_ours(args, ws, rank, local):
         ns = 64 * G + 1
         host = {k: np.ascontiguousarray(v).copy() for k, v in state.items()}
         al = np.ones(n, np.uint8)
-        pe = R.push_params(dt, ns, STRIDE, cache="mu", precision="f32")
+        pe = R.push_params(dt, ns, STRIDE, cache="mu", precision="f32", sort_every=args.sort_every,
+                           kernel_variant=args.variant)
         rows = [0]
 
         def sink(i, row):
@@ -452,7 +466,8 @@ def run_ours(args, ws, rank, local):
                 "config": {"workload": f"{args.grid}^3 GS turbulence dB/B0=1, u_rms=1e-4 c, {n} protons/GPU at "
                                        f"{args.energy:g} GeV, 64 steps/T_g0, mu cache every 8; step = 64 pushes",
                            "field_storage": args.storage, "field_bytes": fb.device_bytes,
-                           "push": "FP32 push, FP64 positions and |p|^2", "sort_every_steps": args.sort_every * 64,
+                           "push": "FP32 push, FP64 positions and |p|^2", "sort_every_steps": args.sort_every,
+                           "kernel_variant": args.variant,
                            "l2": "inputs larger than L2 (field and state exceed 126 MB); no flush",
                            "parallelism": f"particle-sharded replicas x{ws}"},
                 "roofline": roofline, "fp64_push": fp64, "lag_pairs": lag, "e2e": e2e, "cpu_baseline": cpu,

@@ -82,6 +82,11 @@ typedef struct {
     int32_t precision;        /* PT_PUSH_F64 (REF_F64 field) or PT_PUSH_F32 (bricks)    */
     int32_t steps_per_launch; /* steps kept in registers per launch; 0 = auto           */
     int32_t sort_every;       /* F32 form: re-sort particles by brick every N steps; 0 off */
+    int32_t kernel_variant;   /* F32 form: launch shape, threads per block x resident
+                                 blocks per SM: 0 = auto (= 1), 1 = 256 x occupancy,
+                                 2 = 256 x 4, 3 = 128 x 8, 4 = 512 x 2, 5 = 256 x 1,
+                                 6 = 512 x 1, 7 = 128 x 3, 8 = 128 x 2              */
+    int32_t reserved;
 } pt_push_params;
 
 /* Save sink for pt_push_run: called on the calling thread once per save row,

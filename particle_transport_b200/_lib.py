@@ -55,7 +55,8 @@ class PushParams(C.Structure):
     _fields_ = [
         ("dt", C.c_double), ("nsteps", C.c_int64), ("stride", C.c_int64),
         ("periodic", C.c_int32), ("cache_mode", C.c_int32), ("cache_f64", C.c_int32), ("precision", C.c_int32),
-        ("steps_per_launch", C.c_int32), ("sort_every", C.c_int32),
+        ("steps_per_launch", C.c_int32), ("sort_every", C.c_int32), ("kernel_variant", C.c_int32),
+        ("reserved", C.c_int32),
     ]
 
 

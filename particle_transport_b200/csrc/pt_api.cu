@@ -237,6 +237,7 @@ PushArgsFast fast_args(const pt_field* f, pt_fast_state* st, const pt_push_param
     a.dxs[0] = g.dx; a.dxs[1] = g.dy; a.dxs[2] = g.dz;
     a.nsteps = p->nsteps; a.stride = p->stride;
     a.periodic = p->periodic; a.cache_mode = p->cache_mode; a.cache_f64 = p->cache_f64;
+    a.variant = p->kernel_variant;
     return a;
 }
 
@@ -260,6 +261,8 @@ static int advance_fast(pt_ctx* ctx, const pt_field* f, pt_fast_state* st, const
         }
         int64_t c = std::min(K, end - s);
         if (p->sort_every > 0) c = std::min(c, st->last_sort + p->sort_every - s);
+        // the sort swaps the state buffers: take the current ones
+        a.x = st->x; a.p = st->p; a.p2 = st->p2; a.pid = st->pid; a.alive = st->alive;
         a.step_begin = s;
         a.step_count = c;
         int rc = launch_push_fast(a, ctx->stream);
@@ -441,6 +444,11 @@ int pt_fast_state_destroy(pt_fast_state* st)
     if (st->p2) cudaFree(st->p2);
     if (st->pid) cudaFree(st->pid);
     if (st->alive) cudaFree(st->alive);
+    if (st->x_alt) cudaFree(st->x_alt);
+    if (st->p_alt) cudaFree(st->p_alt);
+    if (st->p2_alt) cudaFree(st->p2_alt);
+    if (st->pid_alt) cudaFree(st->pid_alt);
+    if (st->alive_alt) cudaFree(st->alive_alt);
     if (st->sort_tmp) cudaFree(st->sort_tmp);
     delete st;
     return PT_OK;

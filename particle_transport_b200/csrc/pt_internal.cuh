@@ -75,6 +75,12 @@ struct pt_fast_state {
     double* p2 = nullptr;   // [n] |p/(m c)|^2 carried in FP64
     int32_t* pid = nullptr; // [n] particle id of each slot
     uint8_t* alive = nullptr;
+    // second copy of the state: the brick sort scatters into it and swaps
+    double* x_alt = nullptr;
+    float* p_alt = nullptr;
+    double* p2_alt = nullptr;
+    int32_t* pid_alt = nullptr;
+    uint8_t* alive_alt = nullptr;
     const pt_field* field = nullptr; // field the state was created against (grid, units)
     int64_t last_sort = INT64_MIN;   // step of the last brick re-sort
     // scratch for the re-sort
@@ -129,6 +135,7 @@ struct PushArgsFast {
     void* cache;
     int64_t row_base, rows;
     int64_t* deaths;
+    int variant;           // launch shape, see pt_push_params.kernel_variant
 };
 int launch_push_fast(const PushArgsFast& a, cudaStream_t s);
 int launch_fast_import(pt_fast_state* st, const pt_field* f, const double* x1, const double* x2, const double* x3,

@@ -107,8 +107,8 @@ __device__ __forceinline__ double wrap_cells(double x, double w)
     return x;
 }
 
-template <bool BF16>
-__global__ void __launch_bounds__(256) push_fast_kernel(PushArgsFast a)
+template <bool BF16, int BLOCK, int MINB>
+__global__ void __launch_bounds__(BLOCK, MINB) push_fast_kernel(PushArgsFast a)
 {
     extern __shared__ uint32_t s_offs[];
     const int nx = (int)a.fld.nx, ny = (int)a.fld.ny, nz = (int)a.fld.nz;
@@ -288,20 +288,33 @@ __global__ void fast_export_kernel(const double* __restrict__ xs, const float* _
 // ------------------------------------------------------------ brick sort
 // One-digit radix (counting) sort of the particle slots by the brick that
 // holds their cell; dead particles go to a final bucket.
+// Histogram and scatter aggregate equal keys within a warp (__match_any_sync)
+// so that runs of particles in one brick -- the common case once sorted --
+// cost one atomic per warp instead of one per particle.  blockDim must be a
+// multiple of 32 (every lane of a warp runs the same loop trips).
 __global__ void sort_key_kernel(const double* __restrict__ xs, const uint8_t* __restrict__ as, int64_t n,
                                 const uint32_t* __restrict__ offs, int nx, int ny, int nz, uint32_t dead_key,
                                 uint32_t* __restrict__ keys, uint32_t* __restrict__ hist)
 {
-    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+    const int lane = threadIdx.x & 31;
+    const unsigned lt = (1u << lane) - 1u;
+    const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+    for (int64_t base = (int64_t)blockIdx.x * blockDim.x + (threadIdx.x & ~31); base < n; base += stride) {
+        const int64_t i = base + lane;
+        const bool valid = i < n;
         uint32_t key = dead_key;
-        if (as[i]) {
+        if (valid && as[i]) {
             int ix = min(max((int)floor(xs[i]), 0), nx - 2);
             int iy = min(max((int)floor(xs[n + i]), 0), ny - 2);
             int iz = min(max((int)floor(xs[2 * n + i]), 0), nz - 2);
             key = (offs[ix] + offs[nx + iy] + offs[nx + ny + iz]) >> 9;
         }
-        keys[i] = key;
-        atomicAdd(&hist[key], 1u);
+        const unsigned act = __ballot_sync(0xffffffffu, valid);
+        if (valid) {
+            keys[i] = key;
+            const unsigned same = __match_any_sync(act, key);
+            if ((same & lt) == 0) atomicAdd(&hist[key], (uint32_t)__popc(same));
+        }
     }
 }
 
@@ -337,8 +350,21 @@ __global__ void sort_scatter_kernel(const uint32_t* __restrict__ keys, uint32_t*
                                     const uint8_t* __restrict__ as, double* xd, float* pd, double* p2d, int32_t* pidd,
                                     uint8_t* ad)
 {
-    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
-        const int64_t d = atomicAdd(&cursor[keys[i]], 1u);
+    const int lane = threadIdx.x & 31;
+    const unsigned lt = (1u << lane) - 1u;
+    const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+    for (int64_t base = (int64_t)blockIdx.x * blockDim.x + (threadIdx.x & ~31); base < n; base += stride) {
+        const int64_t i = base + lane;
+        const bool valid = i < n;
+        const unsigned act = __ballot_sync(0xffffffffu, valid);
+        if (!valid) continue;
+        const uint32_t key = keys[i];
+        const unsigned same = __match_any_sync(act, key);
+        const int leader = __ffs(same) - 1;
+        uint32_t first = 0;
+        if (lane == leader) first = atomicAdd(&cursor[key], (uint32_t)__popc(same));
+        first = __shfl_sync(same, first, leader);
+        const int64_t d = (int64_t)first + __popc(same & lt);
         xd[d] = xs[i]; xd[n + d] = xs[n + i]; xd[2 * n + d] = xs[2 * n + i];
         pd[d] = ps[i]; pd[n + d] = ps[n + i]; pd[2 * n + d] = ps[2 * n + i];
         p2d[d] = p2s[i];
@@ -356,27 +382,47 @@ int grid_for(int64_t n, int threads, int num_sms)
 
 }  // namespace
 
+// Persistent launch: (SM count) x (resident blocks per SM, optionally capped).
+// The gather is cache-bound, so fewer resident warps can win (less L1 churn).
+template <bool BF16, int BLOCK, int MINB>
+int launch_push_fast_shape(const PushArgsFast& a, cudaStream_t s, int cap_per_sm = 0)
+{
+    const size_t smem = sizeof(uint32_t) * (size_t)(a.fld.nx + a.fld.ny + a.fld.nz);
+    int dev = 0, sms = 148, per_sm = 1;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    auto kfn = push_fast_kernel<BF16, BLOCK, MINB>;
+    if (smem > 48 * 1024) PT_CUDA(cudaFuncSetAttribute(kfn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kfn, BLOCK, smem);
+    per_sm = std::max(per_sm, 1);
+    if (cap_per_sm > 0) per_sm = std::min(per_sm, cap_per_sm);
+    const int64_t blocks = std::min<int64_t>((a.n + BLOCK - 1) / BLOCK, (int64_t)sms * per_sm);
+    kfn<<<(unsigned)blocks, BLOCK, smem, s>>>(a);
+    PT_CHECK_LAUNCH("push_fast_kernel");
+    return PT_OK;
+}
+
+template <bool BF16>
+int launch_push_fast_t(const PushArgsFast& a, cudaStream_t s)
+{
+    switch (a.variant) {
+    case 2: return launch_push_fast_shape<BF16, 256, 4>(a, s);
+    case 3: return launch_push_fast_shape<BF16, 128, 8>(a, s);
+    case 4: return launch_push_fast_shape<BF16, 512, 2>(a, s);
+    case 5: return launch_push_fast_shape<BF16, 256, 1>(a, s, 1);
+    case 6: return launch_push_fast_shape<BF16, 512, 1>(a, s, 1);
+    case 7: return launch_push_fast_shape<BF16, 128, 1>(a, s, 3);
+    case 8: return launch_push_fast_shape<BF16, 128, 1>(a, s, 2);
+    case 0:
+    case 1:
+    default: return launch_push_fast_shape<BF16, 256, 1>(a, s);
+    }
+}
+
 int launch_push_fast(const PushArgsFast& a, cudaStream_t s)
 {
     if (a.n <= 0 || a.step_count <= 0) return PT_OK;
-    const int threads = 256;
-    const size_t smem = sizeof(uint32_t) * (size_t)(a.fld.nx + a.fld.ny + a.fld.nz);
-    int dev = 0, sms = 148, per_sm = 8;
-    cudaGetDevice(&dev);
-    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-    if (a.fld.bf16) {
-        if (smem > 48 * 1024) cudaFuncSetAttribute(push_fast_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, push_fast_kernel<true>, threads, smem);
-    } else {
-        if (smem > 48 * 1024) cudaFuncSetAttribute(push_fast_kernel<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, push_fast_kernel<false>, threads, smem);
-    }
-    per_sm = std::max(per_sm, 1);
-    int64_t blocks = std::min<int64_t>((a.n + threads - 1) / threads, (int64_t)sms * per_sm);
-    if (a.fld.bf16) push_fast_kernel<true><<<(unsigned)blocks, threads, smem, s>>>(a);
-    else push_fast_kernel<false><<<(unsigned)blocks, threads, smem, s>>>(a);
-    PT_CHECK_LAUNCH("push_fast_kernel");
-    return PT_OK;
+    return a.fld.bf16 ? launch_push_fast_t<true>(a, s) : launch_push_fast_t<false>(a, s);
 }
 
 int launch_brick_convert(const double* const comps[6], const pt_grid& g, double B_ref, int bf16, void* nodes,
@@ -419,7 +465,8 @@ int fast_sort(pt_ctx* ctx, pt_fast_state* st, const pt_field* f, cudaStream_t s)
     if (n <= 1) return PT_OK;
     const uint32_t nb = (uint32_t)((f->n_nodes + 511) / 512);
     const int64_t m = (int64_t)nb + 1;  // + dead bucket
-    // scratch: keys[n], hist[m], cursor[m], then the ping-pong state
+    // scratch: keys[n], hist[m], cursor[m]; the scatter goes to the state's
+    // second buffer set, which then becomes the current one
     size_t off = 0;
     auto take = [&](size_t bytes) {
         size_t o = off;
@@ -427,26 +474,33 @@ int fast_sort(pt_ctx* ctx, pt_fast_state* st, const pt_field* f, cudaStream_t s)
         return o;
     };
     const size_t o_keys = take(sizeof(uint32_t) * n), o_hist = take(sizeof(uint32_t) * m),
-                 o_cur = take(sizeof(uint32_t) * m), o_x = take(sizeof(double) * 3 * n),
-                 o_p = take(sizeof(float) * 3 * n), o_p2 = take(sizeof(double) * n), o_pid = take(sizeof(int32_t) * n),
-                 o_a = take(n);
+                 o_cur = take(sizeof(uint32_t) * m);
     if (st->sort_tmp_bytes < off) {
         if (st->sort_tmp) cudaFree(st->sort_tmp);
         st->sort_tmp = nullptr;
         st->sort_tmp_bytes = 0;
         cudaError_t e = cudaMalloc(&st->sort_tmp, off);
-        if (e != cudaSuccess) return fail(PT_ERR_OOM, "sort scratch allocation failed");
+        if (e != cudaSuccess) {
+            cudaGetLastError();
+            return fail(PT_ERR_OOM, "sort scratch allocation failed");
+        }
         st->sort_tmp_bytes = off;
+    }
+    if (!st->x_alt) {
+        cudaError_t e = cudaMalloc((void**)&st->x_alt, sizeof(double) * 3 * n);
+        if (e == cudaSuccess) e = cudaMalloc((void**)&st->p_alt, sizeof(float) * 3 * n);
+        if (e == cudaSuccess) e = cudaMalloc((void**)&st->p2_alt, sizeof(double) * n);
+        if (e == cudaSuccess) e = cudaMalloc((void**)&st->pid_alt, sizeof(int32_t) * n);
+        if (e == cudaSuccess) e = cudaMalloc((void**)&st->alive_alt, n);
+        if (e != cudaSuccess) {
+            cudaGetLastError();
+            return fail(PT_ERR_OOM, "sort state buffers allocation failed");
+        }
     }
     char* base = (char*)st->sort_tmp;
     uint32_t* keys = (uint32_t*)(base + o_keys);
     uint32_t* hist = (uint32_t*)(base + o_hist);
     uint32_t* cur = (uint32_t*)(base + o_cur);
-    double* xd = (double*)(base + o_x);
-    float* pd = (float*)(base + o_p);
-    double* p2d = (double*)(base + o_p2);
-    int32_t* pidd = (int32_t*)(base + o_pid);
-    uint8_t* ad = (uint8_t*)(base + o_a);
     PT_CUDA(cudaMemsetAsync(hist, 0, sizeof(uint32_t) * m, s));
     const int gb = grid_for(n, 256, ctx->num_sms);
     sort_key_kernel<<<gb, 256, 0, s>>>(st->x, st->alive, n, f->offs, (int)f->grid.nx, (int)f->grid.ny,
@@ -454,14 +508,14 @@ int fast_sort(pt_ctx* ctx, pt_fast_state* st, const pt_field* f, cudaStream_t s)
     PT_CHECK_LAUNCH("sort_key_kernel");
     sort_scan_kernel<<<1, 1024, 0, s>>>(hist, cur, m);
     PT_CHECK_LAUNCH("sort_scan_kernel");
-    sort_scatter_kernel<<<gb, 256, 0, s>>>(keys, cur, n, st->x, st->p, st->p2, st->pid, st->alive, xd, pd, p2d, pidd,
-                                           ad);
+    sort_scatter_kernel<<<gb, 256, 0, s>>>(keys, cur, n, st->x, st->p, st->p2, st->pid, st->alive, st->x_alt,
+                                           st->p_alt, st->p2_alt, st->pid_alt, st->alive_alt);
     PT_CHECK_LAUNCH("sort_scatter_kernel");
-    PT_CUDA(cudaMemcpyAsync(st->x, xd, sizeof(double) * 3 * n, cudaMemcpyDeviceToDevice, s));
-    PT_CUDA(cudaMemcpyAsync(st->p, pd, sizeof(float) * 3 * n, cudaMemcpyDeviceToDevice, s));
-    PT_CUDA(cudaMemcpyAsync(st->p2, p2d, sizeof(double) * n, cudaMemcpyDeviceToDevice, s));
-    PT_CUDA(cudaMemcpyAsync(st->pid, pidd, sizeof(int32_t) * n, cudaMemcpyDeviceToDevice, s));
-    PT_CUDA(cudaMemcpyAsync(st->alive, ad, n, cudaMemcpyDeviceToDevice, s));
+    std::swap(st->x, st->x_alt);
+    std::swap(st->p, st->p_alt);
+    std::swap(st->p2, st->p2_alt);
+    std::swap(st->pid, st->pid_alt);
+    std::swap(st->alive, st->alive_alt);
     return PT_OK;
 }
 

@@ -32,6 +32,8 @@ struct PtPushParams
     precision::Int32
     steps_per_launch::Int32
     sort_every::Int32
+    kernel_variant::Int32
+    reserved::Int32
 end
 
 function check(rc::Cint, where::AbstractString)
@@ -127,7 +129,7 @@ function push_run!(field::Field, x1, x2, x3, p1, p2, p3, dt, nsteps::Integer, st
     alive_count = zeros(Int64, nsteps)
     f64out = writer.outtype == Float64
     params = PtPushParams(Float64(dt), nsteps, stride, periodic, cache == :mu ? PT_CACHE_MU : PT_CACHE_PHASE_SPACE,
-                          f64out, precision == :f64 ? PT_PUSH_F64 : PT_PUSH_F32, 0, sort_every)
+                          f64out, precision == :f64 ? PT_PUSH_F64 : PT_PUSH_F32, 0, sort_every, 0, 0)
     sink = cache == :mu ? MuSink(writer) : PhaseSink(writer, n)
     cb = cache == :mu ? @cfunction(_mu_cb, Cint, (Ptr{Cvoid}, Int64, Ptr{Cvoid}, Int64)) :
                         @cfunction(_phase_cb, Cint, (Ptr{Cvoid}, Int64, Ptr{Cvoid}, Int64))

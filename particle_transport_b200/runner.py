@@ -30,9 +30,10 @@ PRECISION = {"f64": _lib.PT_PUSH_F64, "f32": _lib.PT_PUSH_F32}
 
 
 def push_params(dt: float, nsteps: int, stride: int, periodic: bool = True, cache: str = "mu", cache_f64=False,
-                precision: str = "f64", steps_per_launch: int = 0, sort_every: int = 0) -> _lib.PushParams:
+                precision: str = "f64", steps_per_launch: int = 0, sort_every: int = 0,
+                kernel_variant: int = 0) -> _lib.PushParams:
     return _lib.PushParams(float(dt), int(nsteps), int(stride), int(bool(periodic)), CACHE[cache], int(bool(cache_f64)),
-                           PRECISION[precision], int(steps_per_launch), int(sort_every))
+                           PRECISION[precision], int(steps_per_launch), int(sort_every), int(kernel_variant), 0)
 
 
 def n_saves(nsteps: int, stride: int) -> int:
