@@ -64,7 +64,7 @@ def parse():
     ap.add_argument("--variant", type=int, default=1, help="push launch shape (pt_push_params.kernel_variant)")
     ap.add_argument("--lag-particles", type=int, default=1_048_576)
     ap.add_argument("--e2e-gyroperiods", type=int, default=8)
-    ap.add_argument("--skip", default="", help="comma list of legs to skip: fp64,lag,e2e,cpu")
+    ap.add_argument("--skip", default="", help="comma list of legs to skip: fp64,lag,e2e,cpu,batch,serve")
     ap.add_argument("--cpu-seconds", type=float, default=10.0)
     return ap.parse_args()
 
@@ -452,6 +452,15 @@ def run_ours(args, ws, rank, local):
                "call": f"pt_push_run over {G} T_g0 ({ns - 1} pushes, {nsave_e} mu rows) per call, host state",
                "calls": ncall, "s_per_call": el / ncall}
 
+    # ---------------- batched campaigns and serving (their own field libraries)
+    field_bytes = fb.device_bytes
+    del fb
+    torch.cuda.empty_cache()
+    batched = run_batched(args, dev, rank) if "batch" not in skip else None
+    torch.cuda.empty_cache()
+    serving = run_serving(args, dev) if ("serve" not in skip and ws == 1) else None
+    torch.cuda.empty_cache()
+
     # ---------------- CPU baseline (oracle, host cores)
     cpu = None
     if "cpu" not in skip and rank == 0:
@@ -465,17 +474,149 @@ def run_ours(args, ws, rank, local):
                 "dtype": "f32", "data": "synthetic (seeded GS turbulence and particles; no MHD snapshot ships)",
                 "config": {"workload": f"{args.grid}^3 GS turbulence dB/B0=1, u_rms=1e-4 c, {n} protons/GPU at "
                                        f"{args.energy:g} GeV, 64 steps/T_g0, mu cache every 8; step = 64 pushes",
-                           "field_storage": args.storage, "field_bytes": fb.device_bytes,
+                           "field_storage": args.storage, "field_bytes": field_bytes,
                            "push": "FP32 push, FP64 positions and |p|^2", "sort_every_steps": args.sort_every,
                            "kernel_variant": args.variant,
                            "l2": "inputs larger than L2 (field and state exceed 126 MB); no flush",
                            "parallelism": f"particle-sharded replicas x{ws}"},
                 "roofline": roofline, "fp64_push": fp64, "lag_pairs": lag, "e2e": e2e, "cpu_baseline": cpu,
-                "clocks": clocks, "gpu_launches": launches["push"] + launches["sort"], "job_latency": None}
+                "clocks": clocks, "gpu_launches": launches["push"] + launches["sort"], "batched": batched,
+                "job_latency": ({"p50_s": serving["p50_s"], "p99_s": serving["p99_s"]} if serving else None),
+                "serving": serving}
         print(json.dumps(line), flush=True)
 
 
 TRAFFIC = {}
+
+
+def run_batched(args, dev, rank):
+    """Batched campaigns: 12 campaigns (4 modes x 1/10/100 GeV) on a resident
+    256^3 FP32 field library, N log-uniform in [65536, 4194304], 20-500 T_g0
+    at 64 steps per T_g0 of each energy, one persistent launch per epoch
+    (CUDA graph), launch shape picked by the autotuner; then D_mumu per
+    campaign (32 log lags x 20 |mu| bins) from its full mu cache (a save
+    every 32 steps)."""
+    import torch
+
+    from particle_transport_b200 import fields as F
+    from particle_transport_b200 import stats as S
+    from particle_transport_b200.batch import Batch, autotune
+    from particle_transport_b200.fields import FieldLibrary
+    from particle_transport_b200.particles import energy_to_gamma, init_particles
+    from particle_transport_b200.time_units import build_mu_edges_full, log_spaced_lag_steps, reference_Omega0
+
+    n = 256
+    rg = F.gyroradius_m(1.0, 1e-10)
+    grid = F.build_uniform_grid((n - 1) * rg, n, n, n)
+    libs, B0 = {}, None
+    for m in ("total", "alfven", "fast", "slow"):
+        f = F.to_si(F.synthetic_mhd_fields(n, 2, n // 2, 0.5, 1.0, 1e-4, seed=77, spectrum="isotropic", modes=m,
+                                           device=dev))
+        if m == "total":
+            B0 = F.reference_B0_T(*f[:3])
+        libs[m] = FieldLibrary(f, grid, "brick_f32", B_ref_T=B0)
+        del f
+    torch.cuda.empty_cache()
+    rng = np.random.default_rng(4 + rank)
+    camps = []
+    for m in libs:
+        for E in (1.0, 10.0, 100.0):
+            N = int(np.exp(rng.uniform(np.log(65536), np.log(4194304))))
+            dur = float(rng.uniform(20, 500))
+            g0 = energy_to_gamma(E)
+            dt = (2 * math.pi / 64) / reference_Omega0(B0, g0, F.Q_E, F.M_P)
+            camps.append(dict(field=libs[m], state=init_particles(N, grid, E, seed=len(camps) + 100 * rank), dt=dt,
+                              nsteps=int(round(64 * dur)) + 1, stride=32, mode=m, E=E))
+    ntot = sum(len(c["state"]["x1"]) for c in camps)
+    t0 = time.perf_counter()
+    best, timings = autotune(camps, "brick_f32", ntot, epochs=2, use_cache=False)
+    tune_s = time.perf_counter() - t0
+    K, bps = best
+    b = Batch(ntot, max_campaigns=len(camps), storage="brick_f32", steps_per_epoch=K, blocks_per_sm=bps)
+    caches = []
+    for c in camps:
+        nsave = (c["nsteps"] - 1) // c["stride"] + 1
+        caches.append(torch.empty((nsave, len(c["state"]["x1"])), dtype=torch.float32, device=dev))
+        c["id"] = b.add(c["field"], c["state"], c["dt"], c["nsteps"], c["stride"], cache=caches[-1])
+    epochs = max(math.ceil(c["nsteps"] / K) for c in camps)
+    b.run(1)  # graph capture + first epoch
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    b.run(epochs - 1)
+    e1.record()
+    torch.cuda.synchronize()
+    push_s = e0.elapsed_time(e1) / 1e3
+    steps_timed = sum(len(c["state"]["x1"]) * max(0, c["nsteps"] - 1 - K) for c in camps)
+    assert all(b.done(c["id"]) for c in camps)
+    b.close()
+    pairs = 0
+    e0.record()
+    for c, cache in zip(camps, caches):
+        nsave = cache.shape[0]
+        lags = log_spaced_lag_steps(nsave - 1, 32)
+        edges, _ = build_mu_edges_full(0.0, 1.0, 20)
+        acc = S.new_dmumu_accumulators(len(lags), 20, device=dev)
+        S.process_mu_chunk_dmumu(cache, lags, edges, acc["particle_counts"], acc["particle_means"],
+                                 acc["particle_m2s"], acc["pair_sum_squares"], acc["pair_counts"], acc["dmumu_counts"],
+                                 acc["dmumu_sum_delta"], acc["dmumu_sum_delta2"], layout="particle_fastest")
+        c["pairs"] = acc["pair_counts"]
+    e1.record()
+    torch.cuda.synchronize()
+    lag_s = e0.elapsed_time(e1) / 1e3
+    pairs = int(sum(int(c["pairs"].sum().item()) for c in camps))
+    return {"campaigns": len(camps), "particles": ntot, "epochs": epochs, "steps_per_epoch": K,
+            "blocks_per_sm": bps, "autotune": {"candidates": timings, "seconds": tune_s},
+            "value": steps_timed / push_s, "unit": UNIT, "push_s": push_s,
+            "lag_pairs_per_s": pairs / lag_s, "lag_s": lag_s, "field": "256^3 FP32 bricks x 4 modes",
+            "per_campaign": [{"mode": c["mode"], "E_GeV": c["E"], "n": len(c["state"]["x1"]),
+                              "T_g0": (c["nsteps"] - 1) / 64} for c in camps]}
+
+
+def run_serving(args, dev, n_jobs=16, rate=4.0):
+    """Serving: a Poisson stream (mean 4 jobs/s) of transport jobs against
+    resident 256^3 and 512^3 BF16 libraries (4 modes each), admitted against a
+    150 GB HBM budget, continuously batched; p50/p99 job latency and the
+    aggregate particle-step rate."""
+    import torch
+
+    from particle_transport_b200 import fields as F
+    from particle_transport_b200.fields import FieldLibrary
+    from particle_transport_b200.server import CampaignServer, sample_jobs
+
+    libs, B0, host = {}, {}, {}
+    for n in (256, 512):
+        rg = F.gyroradius_m(1.0, 1e-10)
+        grid = F.build_uniform_grid((n - 1) * rg, n, n, n)
+        libs[str(n)], host[str(n)] = {}, {}
+        for m in ("total", "alfven", "fast", "slow"):
+            f = F.to_si(F.synthetic_mhd_fields(n, 2, n // 2, 0.5 if n == 256 else 1.0, 1.0, 1e-4, seed=91 + n,
+                                               spectrum="isotropic" if n == 256 else "gs", modes=m, device=dev))
+            if m == "total":
+                B0[str(n)] = F.reference_B0_T(*f[:3])
+            libs[str(n)][m] = FieldLibrary(f, grid, "brick_bf16", B_ref_T=B0[str(n)])
+            host[str(n)][m] = [x.cpu().numpy() for x in f[:3]]
+            del f
+        torch.cuda.empty_cache()
+    arrivals, specs = sample_jobs(n_jobs, rate, ["256", "512"], seed=2026)
+    srv = CampaignServer(libs, B0, hbm_budget_bytes=150e9, capacity=1 << 27, max_jobs=n_jobs, host_fields=host)
+    torch.cuda.synchronize()
+    t_start = time.perf_counter()
+    nxt = 0
+    while nxt < n_jobs or not srv.idle():
+        now = time.perf_counter() - t_start
+        while nxt < n_jobs and arrivals[nxt] <= now:
+            srv.submit(specs[nxt], arrival=t_start + arrivals[nxt])
+            nxt += 1
+        srv.tick()
+    wall = time.perf_counter() - t_start
+    lat = np.array([r.latency for r in srv.results])
+    steps = sum(r.particle_steps for r in srv.results)
+    srv.close()
+    return {"jobs": n_jobs, "rate_per_s": rate, "p50_s": float(np.percentile(lat, 50)),
+            "p99_s": float(np.percentile(lat, 99)), "mean_s": float(lat.mean()), "wall_s": wall,
+            "particle_steps": int(steps), "aggregate_rate": steps / wall, "unit": UNIT, "push": "FP32 / BF16 bricks",
+            "hbm_budget_GB": 150, "epochs": srv.epochs}
 
 
 def dist_barrier(ws):

@@ -170,6 +170,58 @@ int pt_push_advance_fast(pt_ctx* ctx, const pt_field* field, pt_fast_state* st, 
                          int64_t cache_rows, int64_t* d_deaths);
 
 /*
+ * Batched campaigns.  A batch is an arena of particle slots on one device
+ * holding many campaigns (mode x energy, or jobs of a server), each with its
+ * own field, dt, step count, save stride and mu cache.  One persistent
+ * kernel advances every campaign by steps_per_epoch steps per epoch
+ * (finished campaigns idle); with sort = 1 the slots are re-sorted by brick
+ * within each campaign before every epoch.  Epochs run as CUDA graphs (one
+ * per sort buffer parity) when use_graph = 1.  Campaigns can be added and
+ * removed between epochs.  A particle's trajectory and cache rows are
+ * bit-identical to a single-campaign pt_push_advance_fast run.
+ * No reference counterpart: the reference runs campaigns one after another
+ * (run_mode_campaigns, src/multimode_multienergy_cache_pipeline.jl:2924).
+ */
+typedef struct pt_batch pt_batch;
+
+typedef struct {
+    const pt_field* field;     /* brick field (all campaigns of a batch share its storage type) */
+    double dt;                 /* integration step of this campaign [s]                      */
+    int64_t nsteps;            /* samples; nsteps - 1 pushes                                  */
+    int64_t stride;            /* save stride                                                */
+    int32_t periodic;
+    int32_t cache_f64;         /* 0: Float32 mu cache                                        */
+    int64_t n;                 /* particles                                                  */
+    const double* d_x1;        /* initial SI state on the device (n each)                    */
+    const double* d_x2;
+    const double* d_x3;
+    const double* d_p1;
+    const double* d_p2;
+    const double* d_p3;
+    const uint8_t* d_alive;
+    void* d_cache;             /* mu rows [cache_rows][n] (NULL: no cache)                   */
+    int64_t cache_rows;
+    int32_t cache_ring;        /* 1: save row r goes to row r % cache_rows                   */
+    int32_t reserved;
+    int64_t* d_deaths;         /* [nsteps] particles killed per step (open boundary), or NULL */
+} pt_campaign_desc;
+
+/* capacity: particle slots; blocks_per_sm: resident blocks of the persistent
+ * kernel per SM (0 = 2). */
+int pt_batch_create(pt_ctx* ctx, int64_t capacity, int max_campaigns, int storage, int steps_per_epoch, int sort,
+                    int blocks_per_sm, pt_batch** out);
+int pt_batch_add(pt_ctx* ctx, pt_batch* batch, const pt_campaign_desc* campaign, int* id);
+int pt_batch_remove(pt_ctx* ctx, pt_batch* batch, int id);
+/* Run `epochs` epochs on the context stream (asynchronous). */
+int pt_batch_run(pt_ctx* ctx, pt_batch* batch, int64_t epochs, int use_graph);
+/* Next step of campaign `id` (synchronises the context stream). */
+int pt_batch_step(pt_ctx* ctx, pt_batch* batch, int id, int64_t* step);
+/* Copy campaign `id`'s state back to SI device arrays (n each). */
+int pt_batch_export(pt_ctx* ctx, pt_batch* batch, int id, double* d_x1, double* d_x2, double* d_x3, double* d_p1,
+                    double* d_p2, double* d_p3, uint8_t* d_alive);
+int pt_batch_destroy(pt_batch* batch);
+
+/*
  * D_mumu / <dmu^2> lag-pair accumulation: replaces process_mu_chunk_dmumu_cpu!
  *   src/compute_delta_mu2_dmumu_full.jl:656 (sliding :457-560, injection :562-654),
  * called from pipeline:1718 and dmumu:1150.

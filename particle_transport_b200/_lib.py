@@ -28,7 +28,9 @@ EXPORTS = (
     "pt_last_error", "pt_version", "pt_ctx_create", "pt_ctx_destroy", "pt_ctx_set_stream", "pt_ctx_synchronize",
     "pt_field_upload", "pt_field_upload_device", "pt_field_destroy", "pt_field_device_bytes", "pt_push_run",
     "pt_push_advance_device", "pt_fast_state_create", "pt_fast_state_export", "pt_fast_state_destroy",
-    "pt_fast_state_sort", "pt_push_advance_fast", "pt_dmumu_accumulate", "pt_dmumu_accumulate_device",
+    "pt_fast_state_sort", "pt_push_advance_fast", "pt_batch_create", "pt_batch_add", "pt_batch_remove",
+    "pt_batch_run", "pt_batch_step", "pt_batch_export", "pt_batch_destroy", "pt_dmumu_accumulate",
+    "pt_dmumu_accumulate_device",
     "pt_dmumu_accumulate_device_noalloc", "pt_dpp_accumulate",
     "pt_dpp_accumulate_device", "pt_energy_snapshots", "pt_energy_histogram_device", "pt_reconstruct_mu",
 )
@@ -57,6 +59,17 @@ class PushParams(C.Structure):
         ("periodic", C.c_int32), ("cache_mode", C.c_int32), ("cache_f64", C.c_int32), ("precision", C.c_int32),
         ("steps_per_launch", C.c_int32), ("sort_every", C.c_int32), ("kernel_variant", C.c_int32),
         ("reserved", C.c_int32),
+    ]
+
+
+class CampaignDesc(C.Structure):
+    _fields_ = [
+        ("field", C.c_void_p), ("dt", C.c_double), ("nsteps", C.c_int64), ("stride", C.c_int64),
+        ("periodic", C.c_int32), ("cache_f64", C.c_int32), ("n", C.c_int64),
+        ("d_x1", C.c_void_p), ("d_x2", C.c_void_p), ("d_x3", C.c_void_p), ("d_p1", C.c_void_p),
+        ("d_p2", C.c_void_p), ("d_p3", C.c_void_p), ("d_alive", C.c_void_p),
+        ("d_cache", C.c_void_p), ("cache_rows", C.c_int64), ("cache_ring", C.c_int32), ("reserved", C.c_int32),
+        ("d_deaths", C.c_void_p),
     ]
 
 
@@ -98,6 +111,13 @@ def load():
             "pt_fast_state_destroy": (i32, [P]),
             "pt_fast_state_sort": (i32, [P, P]),
             "pt_push_advance_fast": (i32, [P, P, P, C.POINTER(PushParams), i64, i64, P, i64, i64, P]),
+            "pt_batch_create": (i32, [P, i64, i32, i32, i32, i32, i32, PP]),
+            "pt_batch_add": (i32, [P, P, C.POINTER(CampaignDesc), C.POINTER(C.c_int)]),
+            "pt_batch_remove": (i32, [P, P, i32]),
+            "pt_batch_run": (i32, [P, P, i64, i32]),
+            "pt_batch_step": (i32, [P, P, i32, C.POINTER(C.c_int64)]),
+            "pt_batch_export": (i32, [P, P, i32, P, P, P, P, P, P, P]),
+            "pt_batch_destroy": (i32, [P]),
             "pt_dmumu_accumulate": (i32, [P, P, i64, i64, i64, i64, P, i32, P, i32, i32, i32, P, P, P, P, P, P, P,
                                           P]),
             "pt_dmumu_accumulate_device": (i32, [P, P, i64, i64, i64, i64, P, i32, P, i32, i32, i32, P, P, P, P, P,

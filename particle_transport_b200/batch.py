@@ -1,0 +1,174 @@
+"""Batched campaigns on one device (pt_batch_*) and the launch-shape autotuner.
+
+A Batch holds many campaigns -- the mode x energy campaigns of a run
+(run_mode_campaigns, src/multimode_multienergy_cache_pipeline.jl:2924, which
+the reference runs one after another), or the jobs of the campaign server --
+in one arena of particle slots.  Every epoch one persistent kernel advances
+all of them by steps_per_epoch steps from their own device-resident step
+counters; epochs replay as CUDA graphs.  Campaigns are added and removed
+between epochs.
+
+The autotuner times candidate (steps per epoch = sort cadence, resident
+blocks per SM) pairs on a throw-away copy of the campaigns and caches the
+winner per (device, storage, particle count, field size) in a JSON file.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import json
+import math
+import os
+import time
+
+import numpy as np
+
+from . import _lib
+from .fields import STORAGE, FieldLibrary
+
+KEYS = ("x1", "x2", "x3", "p1", "p2", "p3")
+
+
+class Batch:
+    def __init__(self, capacity: int, max_campaigns: int = 64, storage: str = "brick_bf16", steps_per_epoch: int = 64,
+                 sort: bool = True, blocks_per_sm: int = 0, device: int = 0):
+        import torch
+
+        self.storage = storage
+        self.K = int(steps_per_epoch)
+        self.device = torch.device("cuda", device)
+        ctx = _lib.torch_context(device)
+        out = C.c_void_p()
+        _lib.call("pt_batch_create", ctx.handle, int(capacity), int(max_campaigns), STORAGE[storage], self.K,
+                  int(bool(sort)), int(blocks_per_sm), C.byref(out))
+        self.handle = out
+        self.campaigns = {}
+
+    def add(self, field: FieldLibrary, state: dict, dt: float, nsteps: int, stride: int, periodic: bool = True,
+            cache=None, ring: bool = False, deaths=None, alive=None) -> int:
+        """Add a campaign; state: SI arrays x1..p3 (numpy or CUDA tensors);
+        cache: CUDA float32 tensor [rows][n] for the mu rows (or None)."""
+        import torch
+
+        n = int(len(state["x1"]))
+        st = {k: torch.as_tensor(np.asarray(state[k]) if not hasattr(state[k], "is_cuda") else state[k],
+                                 dtype=torch.float64, device=self.device).contiguous() for k in KEYS}
+        al = (torch.ones(n, dtype=torch.uint8, device=self.device) if alive is None
+              else torch.as_tensor(alive, dtype=torch.uint8, device=self.device).contiguous())
+        if cache is not None:
+            if cache.dtype not in (torch.float32, torch.float64) or cache.shape[-1] != n or not cache.is_contiguous():
+                raise ValueError("cache must be a contiguous float tensor [rows][n]")
+        d = _lib.CampaignDesc(field.handle, float(dt), int(nsteps), int(stride), int(bool(periodic)),
+                              int(cache is not None and cache.dtype == torch.float64), n,
+                              *[st[k].data_ptr() for k in KEYS], al.data_ptr(),
+                              cache.data_ptr() if cache is not None else None,
+                              int(cache.shape[0]) if cache is not None else 0, int(bool(ring)), 0,
+                              deaths.data_ptr() if deaths is not None else None)
+        cid = C.c_int()
+        ctx = _lib.torch_context(self.device.index)
+        _lib.call("pt_batch_add", ctx.handle, self.handle, C.byref(d), C.byref(cid))
+        self.campaigns[cid.value] = {"field": field, "n": n, "nsteps": int(nsteps), "cache": cache, "deaths": deaths}
+        return cid.value
+
+    def remove(self, cid: int) -> None:
+        ctx = _lib.torch_context(self.device.index)
+        _lib.call("pt_batch_remove", ctx.handle, self.handle, int(cid))
+        self.campaigns.pop(cid, None)
+
+    def run(self, epochs: int, use_graph: bool = True) -> None:
+        ctx = _lib.torch_context(self.device.index)
+        _lib.call("pt_batch_run", ctx.handle, self.handle, int(epochs), int(bool(use_graph)))
+
+    def step(self, cid: int) -> int:
+        v = C.c_int64()
+        ctx = _lib.torch_context(self.device.index)
+        _lib.call("pt_batch_step", ctx.handle, self.handle, int(cid), C.byref(v))
+        return int(v.value)
+
+    def done(self, cid: int) -> bool:
+        return self.step(cid) >= self.campaigns[cid]["nsteps"]
+
+    def export(self, cid: int):
+        import torch
+
+        n = self.campaigns[cid]["n"]
+        st = {k: torch.empty(n, dtype=torch.float64, device=self.device) for k in KEYS}
+        al = torch.empty(n, dtype=torch.uint8, device=self.device)
+        ctx = _lib.torch_context(self.device.index)
+        _lib.call("pt_batch_export", ctx.handle, self.handle, int(cid), *[st[k].data_ptr() for k in KEYS],
+                  al.data_ptr())
+        return st, al
+
+    def close(self):
+        if getattr(self, "handle", None):
+            _lib.load().pt_batch_destroy(self.handle)
+            self.handle = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+# --------------------------------------------------------------------------
+# autotuner
+# --------------------------------------------------------------------------
+CANDIDATES = ((64, 2), (128, 2), (32, 2), (64, 1), (64, 3))
+
+
+def _cache_path():
+    base = os.environ.get("PTB200_TUNE_CACHE") or os.path.join(os.path.expanduser("~"), ".cache", "ptb200")
+    os.makedirs(base, exist_ok=True)
+    return os.path.join(base, "autotune.json")
+
+
+def tune_key(storage: str, n_total: int, grid_n: int) -> str:
+    import torch
+
+    name = torch.cuda.get_device_name() if torch.cuda.is_available() else "cpu"
+    return f"{name}|{storage}|n2^{int(round(math.log2(max(n_total, 1))))}|grid{grid_n}"
+
+
+def autotune(campaigns, storage: str, capacity: int, epochs: int = 2, candidates=CANDIDATES, use_cache: bool = True):
+    """Pick (steps_per_epoch, blocks_per_sm) for a set of campaigns.
+
+    campaigns: list of dicts with the keyword arguments of Batch.add (field,
+    state, dt, nsteps, stride).  Each candidate runs `epochs` epochs on a fresh
+    batch of the same campaigns without caches; the fastest particle-step rate
+    wins.  Returns (best, timings)."""
+    import torch
+
+    n_total = sum(len(c["state"]["x1"]) for c in campaigns)
+    grid_n = max(c["field"].grid.nx for c in campaigns)
+    key = tune_key(storage, n_total, grid_n)
+    path = _cache_path()
+    table = {}
+    if use_cache and os.path.exists(path):
+        try:
+            table = json.load(open(path))
+        except Exception:
+            table = {}
+        if key in table:
+            return tuple(table[key]["best"]), table[key]["timings"]
+    timings = {}
+    for K, bps in candidates:
+        b = Batch(capacity, max_campaigns=max(len(campaigns), 1), storage=storage, steps_per_epoch=K, sort=True,
+                  blocks_per_sm=bps)
+        for c in campaigns:
+            b.add(c["field"], c["state"], c["dt"], c["nsteps"], c["stride"], c.get("periodic", True))
+        b.run(1)  # warm-up (graph capture)
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        b.run(epochs)
+        torch.cuda.synchronize()
+        el = time.perf_counter() - t0
+        b.close()
+        timings[f"{K}x{bps}"] = n_total * K * epochs / el
+    best_s = max(timings, key=timings.get)
+    best = tuple(int(v) for v in best_s.split("x"))
+    table[key] = {"best": list(best), "timings": timings}
+    try:
+        json.dump(table, open(path, "w"), indent=1)
+    except Exception:
+        pass
+    return best, timings

@@ -26,6 +26,7 @@ UNITS = {
     "push_fast.cu": [],
     "lagstats.cu": [],
     "pt_api.cu": [],
+    "pt_batch.cu": [],
 }
 
 

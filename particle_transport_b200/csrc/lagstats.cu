@@ -77,6 +77,7 @@ struct DmumuLaunch {
     const double* edges;
     int n_bins, bin_abs;
     int ppc, groups;           // particle slots per CTA, 32-lag groups per slot
+    int parts;                 // warps splitting the bins of one (slot, lag group)
     size_t slot_bytes;
     char* gslots;              // global staging when the slots do not fit on chip
     // per-CTA outputs
@@ -109,20 +110,56 @@ __global__ void __launch_bounds__(1024) dmumu_kernel(DmumuLaunch a)
         acc_sd2[i] = 0.0;
     }
 
+    // Lags are dealt to the 32-lane groups so that lags equal modulo 32 --
+    // which read the same shared-memory bank at every start -- fall into
+    // different groups where possible.  s_lane_lag[g*32 + lane] = lag index
+    // (-1: idle lane), s_lag_pos[lag] = g*32 + lane.
+    __shared__ int s_lane_lag[8 * kWarp];
+    __shared__ int s_lag_pos[8 * kWarp];
+    __shared__ unsigned char cnt[8][kWarp];
+    __shared__ int fill[8];
+    for (int i = threadIdx.x; i < 8 * kWarp; i += blockDim.x) {
+        s_lane_lag[i] = -1;
+        cnt[i / kWarp][i % kWarp] = 0;
+    }
+    if (threadIdx.x < 8) fill[threadIdx.x] = 0;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        for (int i = 0; i < nl; ++i) {
+            const int r = (int)(((a.lags[i] % kWarp) + kWarp) % kWarp);
+            int best = -1;
+            for (int g = 0; g < a.groups; ++g) {
+                if (fill[g] >= kWarp) continue;
+                if (best < 0 || cnt[g][r] < cnt[best][r] || (cnt[g][r] == cnt[best][r] && fill[g] < fill[best]))
+                    best = g;
+            }
+            const int pos = best * kWarp + fill[best]++;
+            cnt[best][r]++;
+            s_lane_lag[pos] = i;
+            s_lag_pos[i] = pos;
+        }
+    }
+    __syncthreads();
+
     const int warp = threadIdx.x / kWarp, lane = threadIdx.x % kWarp;
-    const int slot = warp / a.groups, group = warp % a.groups;
-    const int li = group * kWarp + lane;
-    const bool lane_on = li < nl;
+    const int wps = a.groups * a.parts;  // warps per particle slot
+    const int slot = warp / wps, group = (warp % wps) / a.parts, part = warp % a.parts;
+    const int li = s_lane_lag[group * kWarp + lane];
+    const bool lane_on = li >= 0;
     int64_t L = lane_on ? a.lags[li] : 0;
     if (L < 1 || L >= a.nsave) L = a.nsave;  // reference: lag >= nsteps -> skipped
     const int64_t lim = a.nsave - L;         // valid starts: s < lim
 
     // slot layout: series[nsave] float | list[nsave] IdxT | hist[nb+1] int | cur[nb+2] int
+    //              | tot_c[nl] u64 | tot_sd2[nl] f64 (per-particle totals over the bins)
     unsigned char* sb = slot_base + (size_t)slot * a.slot_bytes;
     float* series = (float*)sb;
     IdxT* list = (IdxT*)(sb + ((a.nsave * sizeof(float) + 15) & ~(size_t)15));
     int* hist = (int*)((unsigned char*)list + ((a.nsave * sizeof(IdxT) + 15) & ~(size_t)15));
     int* cur = hist + (nb + 1);
+    unsigned long long* tot_c =
+        (unsigned long long*)((unsigned char*)hist + ((sizeof(int) * (size_t)(2 * nb + 3) + 15) & ~(size_t)15));
+    double* tot_sd2 = (double*)(tot_c + nl);
 
     long long wc = 0, pn = 0;
     double wm = 0.0, wm2 = 0.0, pss = 0.0;
@@ -134,9 +171,13 @@ __global__ void __launch_bounds__(1024) dmumu_kernel(DmumuLaunch a)
     for (int64_t tile = blockIdx.x; tile < tiles; tile += gridDim.x) {
         const int64_t p = tile * a.ppc + slot;
         const bool have = p < a.n;
-        // ---- stage (group-0 warp of each slot)
-        if (group == 0 && have) {
+        // ---- stage (first warp of each slot)
+        if (group == 0 && part == 0 && have) {
             for (int b = lane; b <= nb; b += kWarp) hist[b] = 0;
+            for (int l = lane; l < nl; l += kWarp) {
+                tot_c[l] = 0ull;
+                tot_sd2[l] = 0.0;
+            }
             __syncwarp();
             const float* src = a.mu + p * a.sp;
             for (int64_t s0 = 0; s0 < a.nsave; s0 += kWarp) {
@@ -183,14 +224,15 @@ __global__ void __launch_bounds__(1024) dmumu_kernel(DmumuLaunch a)
             }
         }
         __syncthreads();
-        // ---- pairs: bin by bin
+        // ---- pairs: bin by bin; the `parts` warps of a (slot, lag group) take
+        // bins part, part + parts, ...; every lane keeps two accumulator chains
         if (have) {
-            long long tot_c = 0;
-            double tot_sd2 = 0.0;
-            for (int b = 0; b <= nb; ++b) {
+            long long my_c = 0;
+            double my_sd2 = 0.0;
+            for (int b = part; b <= nb; b += a.parts) {
                 const int e0 = cur[b], e1 = cur[b + 1];
                 long long c = 0;
-                double sd = 0.0, sd2 = 0.0;
+                double sd0 = 0.0, sd1 = 0.0, sq0 = 0.0, sq1 = 0.0;
                 int e = e0;
                 for (; e + 4 <= e1; e += 4) {
                     int64_t s_[4];
@@ -202,12 +244,18 @@ __global__ void __launch_bounds__(1024) dmumu_kernel(DmumuLaunch a)
                         v_[k] = s_[k] < lim ? series[s_[k] + L] : NAN;
                     }
 #pragma unroll
-                    for (int k = 0; k < 4; ++k) {
-                        const double d = (double)v_[k] - (double)a_[k];
-                        if (isfinite(d)) {
+                    for (int k = 0; k < 4; k += 2) {
+                        const double d0 = (double)v_[k] - (double)a_[k];
+                        const double d1 = (double)v_[k + 1] - (double)a_[k + 1];
+                        if (isfinite(d0)) {
                             c += 1;
-                            sd += d;
-                            sd2 = fma(d, d, sd2);
+                            sd0 += d0;
+                            sq0 = fma(d0, d0, sq0);
+                        }
+                        if (isfinite(d1)) {
+                            c += 1;
+                            sd1 += d1;
+                            sq1 = fma(d1, d1, sq1);
                         }
                     }
                 }
@@ -218,29 +266,39 @@ __global__ void __launch_bounds__(1024) dmumu_kernel(DmumuLaunch a)
                     const double d = (double)vv - (double)av;
                     if (isfinite(d)) {
                         c += 1;
-                        sd += d;
-                        sd2 = fma(d, d, sd2);
+                        sd0 += d;
+                        sq0 = fma(d, d, sq0);
                     }
                 }
+                const double sd = sd0 + sd1, sd2 = sq0 + sq1;
                 if (b < nb && c > 0 && lane_on) {
                     const int ai = li * nb + b;
                     atomicAdd(&acc_cnt[ai], (unsigned long long)c);
                     atomicAdd(&acc_sd[ai], sd);
                     atomicAdd(&acc_sd2[ai], sd2);
                 }
-                tot_c += c;
-                tot_sd2 += sd2;
+                my_c += c;
+                my_sd2 += sd2;
             }
-            if (tot_c > 0) {
+            if (lane_on && my_c > 0) {
+                atomicAdd(&tot_c[li], (unsigned long long)my_c);
+                atomicAdd(&tot_sd2[li], my_sd2);
+            }
+        }
+        __syncthreads();
+        if (have && part == 0 && lane_on) {
+            const long long tc = (long long)tot_c[li];
+            const double ts = tot_sd2[li];
+            if (tc > 0) {
                 // per-particle value: mean dmu^2 over its valid pairs (dmumu:528-537);
-                // for the injection estimator tot_c == 1 and the value is dmu^2 (:625-631)
-                const double value = tot_sd2 / (double)tot_c;
+                // for the injection estimator tc == 1 and the value is dmu^2 (:625-631)
+                const double value = ts / (double)tc;
                 wc += 1;
                 const double delta = value - wm;
                 wm += delta / (double)wc;
                 wm2 += delta * (value - wm);
-                pss += tot_sd2;
-                pn += tot_c;
+                pss += ts;
+                pn += tc;
             }
         }
         __syncthreads();
@@ -260,11 +318,11 @@ __global__ void __launch_bounds__(1024) dmumu_kernel(DmumuLaunch a)
     wp[warp * kWarp + lane] = WelfordPart{wc, wm, wm2, pss, pn};
     __syncthreads();
     for (int l = threadIdx.x; l < nl; l += blockDim.x) {
-        const int g = l / kWarp, ln = l % kWarp;
+        const int g = s_lag_pos[l] / kWarp, ln = s_lag_pos[l] % kWarp;
         long long c = 0, n2 = 0;
         double m = 0.0, m2 = 0.0, ss = 0.0;
         for (int sl = 0; sl < a.ppc; ++sl) {
-            const int w = sl * a.groups + g;
+            const int w = sl * wps + g * a.parts;  // the part-0 warp holds the slot's Welford triple
             if (w >= nwarps) break;
             const WelfordPart q = wp[w * kWarp + ln];
             welford_merge(c, m, m2, q.count, q.mean, q.m2);
@@ -489,12 +547,12 @@ int run_dmumu(pt_ctx* ctx, const DmumuArgs& a, cudaStream_t s)
     const size_t budget = (size_t)std::min(max_smem, 200 * 1024);
     const bool small_idx = a.nsave <= 65535;
     const size_t idx_bytes = small_idx ? 2 : 4;
-    const size_t slot_bytes = align16(a.nsave * sizeof(float)) + align16(a.nsave * idx_bytes) +
-                              align16(sizeof(int) * (size_t)(2 * a.n_bins + 3));
     const size_t edge_bytes = align16(sizeof(double) * (size_t)(a.n_bins + 1));
     // lags per launch: multiple of 32 with the accumulators taking <= ~half the budget
     int nl_cap = (int)std::max<size_t>(32, ((budget / 2) / ((size_t)a.n_bins * 24)) / 32 * 32);
     nl_cap = std::min(nl_cap, 32 * 8);
+    const size_t slot_bytes = align16(a.nsave * sizeof(float)) + align16(a.nsave * idx_bytes) +
+                              align16(sizeof(int) * (size_t)(2 * a.n_bins + 3)) + align16(16 * (size_t)nl_cap);
     const int lag_batches = (a.n_lags + nl_cap - 1) / nl_cap;
     for (int lb = 0; lb < lag_batches; ++lb) {
         const int lag0 = lb * nl_cap;
@@ -507,7 +565,9 @@ int run_dmumu(pt_ctx* ctx, const DmumuArgs& a, cudaStream_t s)
         if (smem_slots) ppc = (int)std::min<size_t>((budget - fixed) / slot_bytes, (size_t)(32 / groups));
         else ppc = std::max(1, std::min(8, 32 / groups));
         ppc = std::max(1, ppc);
-        const int threads = ppc * groups * kWarp;
+        // more warps share each staged series: split its bins over `parts` warps
+        const int parts = std::max(1, std::min(4, 32 / (ppc * groups)));
+        const int threads = ppc * groups * parts * kWarp;
         size_t smem = fixed + (smem_slots ? (size_t)ppc * slot_bytes : 0);
         const int64_t tiles = (a.n + ppc - 1) / ppc;
         int per_sm = 1;
@@ -529,7 +589,7 @@ int run_dmumu(pt_ctx* ctx, const DmumuArgs& a, cudaStream_t s)
         L.mu = a.mu; L.n = a.n; L.nsave = a.nsave; L.sp = a.sp; L.ss = a.ss;
         L.start_cap = a.injection ? 1 : a.nsave;
         L.lags = a.lags + lag0; L.nl = nl; L.edges = a.edges; L.n_bins = a.n_bins; L.bin_abs = a.bin_abs;
-        L.ppc = ppc; L.groups = groups; L.slot_bytes = slot_bytes;
+        L.ppc = ppc; L.groups = groups; L.parts = parts; L.slot_bytes = slot_bytes;
         L.part_cnt = (unsigned long long*)base;
         L.part_sd = (double*)(base + align16(part_acc * 8));
         L.part_sd2 = (double*)(base + 2 * align16(part_acc * 8));
@@ -692,11 +752,11 @@ int run_dmumu_noalloc(pt_ctx* ctx, const DmumuArgs& a, cudaStream_t s)
     const size_t budget = (size_t)std::min(max_smem, 200 * 1024);
     const bool small_idx = a.nsave <= 65535;
     const size_t idx_bytes = small_idx ? 2 : 4;
-    const size_t slot_bytes = align16(a.nsave * sizeof(float)) + align16(a.nsave * idx_bytes) +
-                              align16(sizeof(int) * (size_t)(2 * a.n_bins + 3));
     const size_t edge_bytes = align16(sizeof(double) * (size_t)(a.n_bins + 1));
     int nl_cap = (int)std::max<size_t>(32, ((budget / 2) / ((size_t)a.n_bins * 24)) / 32 * 32);
     nl_cap = std::min(nl_cap, 32 * 8);
+    const size_t slot_bytes = align16(a.nsave * sizeof(float)) + align16(a.nsave * idx_bytes) +
+                              align16(sizeof(int) * (size_t)(2 * a.n_bins + 3)) + align16(16 * (size_t)nl_cap);
     for (int lag0 = 0; lag0 < a.n_lags; lag0 += nl_cap) {
         const int nl = std::min(nl_cap, a.n_lags - lag0);
         const int groups = (nl + kWarp - 1) / kWarp;
@@ -708,7 +768,8 @@ int run_dmumu_noalloc(pt_ctx* ctx, const DmumuArgs& a, cudaStream_t s)
                                         " bins; use pt_dmumu_accumulate_device");
         int ppc = (int)std::min<size_t>((budget - fixed) / slot_bytes, (size_t)(32 / groups));
         ppc = std::max(1, ppc);
-        const int threads = ppc * groups * kWarp;
+        const int parts = std::max(1, std::min(4, 32 / (ppc * groups)));
+        const int threads = ppc * groups * parts * kWarp;
         const size_t smem = fixed + (size_t)ppc * slot_bytes;
         // per-CTA partials: counts, sum, sum^2 per (lag, bin) and a Welford triple per lag
         const size_t per_cta = (size_t)nl * a.n_bins * 24 + sizeof(WelfordPart) * (size_t)nl + 64;
@@ -730,7 +791,7 @@ int run_dmumu_noalloc(pt_ctx* ctx, const DmumuArgs& a, cudaStream_t s)
         L.mu = a.mu; L.n = a.n; L.nsave = a.nsave; L.sp = a.sp; L.ss = a.ss;
         L.start_cap = a.injection ? 1 : a.nsave;
         L.lags = a.lags + lag0; L.nl = nl; L.edges = a.edges; L.n_bins = a.n_bins; L.bin_abs = a.bin_abs;
-        L.ppc = ppc; L.groups = groups; L.slot_bytes = slot_bytes;
+        L.ppc = ppc; L.groups = groups; L.parts = parts; L.slot_bytes = slot_bytes;
         L.part_cnt = (unsigned long long*)base;
         L.part_sd = (double*)(base + align16(part_acc * 8));
         L.part_sd2 = (double*)(base + 2 * align16(part_acc * 8));

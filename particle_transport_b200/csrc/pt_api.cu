@@ -238,6 +238,8 @@ PushArgsFast fast_args(const pt_field* f, pt_fast_state* st, const pt_push_param
     a.nsteps = p->nsteps; a.stride = p->stride;
     a.periodic = p->periodic; a.cache_mode = p->cache_mode; a.cache_f64 = p->cache_f64;
     a.variant = p->kernel_variant;
+    a.ring = 0;
+    a.n_cache = st->n;
     return a;
 }
 

@@ -1,0 +1,404 @@
+// Batched campaigns (pt_batch_*): an arena of particle slots shared by many
+// campaigns, advanced together by push_batch_kernel.  See include/ptb200.h.
+#include "pt_internal.cuh"
+
+#include <algorithm>
+#include <cmath>
+#include <new>
+#include <string>
+#include <vector>
+
+using namespace pt;
+
+struct pt_batch {
+    pt_ctx* ctx = nullptr;
+    int64_t cap = 0;
+    int max_camps = 0;
+    int storage = PT_FIELD_BRICK_BF16;
+    int K = 64;
+    int sort = 1;
+    int grid = 148;
+    BatchStateDev buf[2]{};   // ping-pong state
+    int cur = 0;              // buffer holding the current state
+    int32_t* camp_of = nullptr;
+    BatchCampaignDev* d_camps = nullptr;
+    std::vector<BatchCampaignDev> h_camps;
+    std::vector<const pt_field*> fields;
+    BatchTile* d_tiles = nullptr;
+    int* d_ntiles = nullptr;
+    int* d_counter = nullptr;
+    uint32_t* keys = nullptr;
+    uint32_t* hist = nullptr;
+    uint32_t* cursor = nullptr;
+    int64_t hist_cap = 0;
+    int64_t* d_m = nullptr;
+    int smem_words = 1;
+    std::vector<std::pair<int64_t, int64_t>> free_ranges;  // (start, length), sorted
+    cudaStream_t cap_stream = nullptr;
+    cudaGraphExec_t graph[2] = {nullptr, nullptr};
+    bool graph_dirty = true;
+};
+
+namespace {
+
+void free_state(BatchStateDev& s)
+{
+    if (s.x) cudaFree(s.x);
+    if (s.p) cudaFree(s.p);
+    if (s.p2) cudaFree(s.p2);
+    if (s.pid) cudaFree(s.pid);
+    if (s.alive) cudaFree(s.alive);
+    s = BatchStateDev{};
+}
+
+int alloc_state(BatchStateDev& s, int64_t cap)
+{
+    s.cap = cap;
+    const size_t m = (size_t)std::max<int64_t>(cap, 1);
+    cudaError_t e = cudaMalloc((void**)&s.x, sizeof(double) * 3 * m);
+    if (e == cudaSuccess) e = cudaMalloc((void**)&s.p, sizeof(float) * 3 * m);
+    if (e == cudaSuccess) e = cudaMalloc((void**)&s.p2, sizeof(double) * m);
+    if (e == cudaSuccess) e = cudaMalloc((void**)&s.pid, sizeof(int32_t) * m);
+    if (e == cudaSuccess) e = cudaMalloc((void**)&s.alive, m);
+    if (e != cudaSuccess) {
+        cudaGetLastError();
+        return fail(PT_ERR_OOM, "batch state allocation failed");
+    }
+    return PT_OK;
+}
+
+void drop_graphs(pt_batch* b)
+{
+    for (auto& g : b->graph)
+        if (g) {
+            cudaGraphExecDestroy(g);
+            g = nullptr;
+        }
+    b->graph_dirty = true;
+}
+
+// Recompute sort buckets and tile table after the campaign set changed.  The
+// step counters live on the device (advanced by every epoch): they are read
+// back first so that uploading the table does not rewind running campaigns;
+// `fresh` is a campaign just added (its step stays 0).
+int rebuild_tables(pt_batch* b, int fresh)
+{
+    {
+        std::vector<BatchCampaignDev> dev((size_t)b->max_camps);
+        PT_CUDA(cudaStreamSynchronize(b->ctx->stream));
+        PT_CUDA(cudaMemcpy(dev.data(), b->d_camps, sizeof(BatchCampaignDev) * b->max_camps, cudaMemcpyDeviceToHost));
+        for (int i = 0; i < b->max_camps; ++i)
+            if (i != fresh && b->h_camps[i].active) b->h_camps[i].step = dev[i].step;
+    }
+    int64_t key = 0, dense = 0;
+    std::vector<BatchTile> tiles;
+    for (int c = 0; c < b->max_camps; ++c) {
+        BatchCampaignDev& C = b->h_camps[c];
+        if (!C.active) continue;
+        C.key_base = key;
+        key += C.n_bricks + 1;
+        C.shift = C.slot0 - dense;
+        dense += C.n;
+        for (int64_t s = 0; s < C.n; s += 256)
+            tiles.push_back(BatchTile{c, (int32_t)std::min<int64_t>(256, C.n - s), C.slot0 + s});
+    }
+    if (key > UINT32_MAX) return fail(PT_ERR_ARG, "too many sort buckets in the batch");
+    if (key > b->hist_cap) {
+        if (b->hist) cudaFree(b->hist);
+        if (b->cursor) cudaFree(b->cursor);
+        b->hist = b->cursor = nullptr;
+        b->hist_cap = 0;
+        const int64_t want = std::max<int64_t>(key, 2 * b->hist_cap);
+        cudaError_t e = cudaMalloc((void**)&b->hist, sizeof(uint32_t) * want);
+        if (e == cudaSuccess) e = cudaMalloc((void**)&b->cursor, sizeof(uint32_t) * want);
+        if (e != cudaSuccess) {
+            cudaGetLastError();
+            return fail(PT_ERR_OOM, "batch sort buckets allocation failed");
+        }
+        b->hist_cap = want;
+        drop_graphs(b);
+    }
+    const int nt = (int)tiles.size();
+    const int64_t max_tiles = b->cap / 256 + b->max_camps + 1;
+    if (nt > max_tiles) return fail(PT_ERR_ARG, "internal: tile table overflow");
+    cudaStream_t s = b->ctx->stream;
+    PT_CUDA(cudaMemcpyAsync(b->d_camps, b->h_camps.data(), sizeof(BatchCampaignDev) * b->max_camps,
+                            cudaMemcpyHostToDevice, s));
+    if (nt) PT_CUDA(cudaMemcpyAsync(b->d_tiles, tiles.data(), sizeof(BatchTile) * nt, cudaMemcpyHostToDevice, s));
+    PT_CUDA(cudaMemcpyAsync(b->d_ntiles, &nt, sizeof(int), cudaMemcpyHostToDevice, s));
+    PT_CUDA(cudaMemcpyAsync(b->d_m, &key, sizeof(int64_t), cudaMemcpyHostToDevice, s));
+    PT_CUDA(cudaStreamSynchronize(s));  // host vectors are reused right away
+    return PT_OK;
+}
+
+int enqueue_epoch(pt_batch* b, cudaStream_t s)
+{
+    int cur = b->cur;
+    if (b->sort) {
+        int rc = launch_batch_sort(b->d_camps, b->camp_of, b->buf[cur], b->buf[1 - cur], b->keys, b->hist, b->cursor,
+                                   b->d_m, b->hist_cap, b->ctx->num_sms, s);
+        if (rc) return rc;
+        cur = 1 - cur;
+    }
+    BatchLaunch L{b->d_camps, b->d_tiles, b->d_ntiles, b->d_counter, b->buf[cur],
+                  b->storage == PT_FIELD_BRICK_BF16, b->smem_words, b->grid};
+    int rc = launch_push_batch(L, s);
+    if (rc) return rc;
+    return launch_batch_epoch_end(b->d_camps, b->max_camps, b->d_counter, s);
+}
+
+int capture(pt_batch* b, int parity)
+{
+    const int saved = b->cur;
+    b->cur = parity;
+    cudaGraph_t g = nullptr;
+    PT_CUDA(cudaStreamBeginCapture(b->cap_stream, cudaStreamCaptureModeThreadLocal));
+    int rc = enqueue_epoch(b, b->cap_stream);
+    cudaError_t e = cudaStreamEndCapture(b->cap_stream, &g);
+    b->cur = saved;
+    if (rc) {
+        if (g) cudaGraphDestroy(g);
+        return rc;
+    }
+    if (e != cudaSuccess) return cuda_fail(e, "cudaStreamEndCapture");
+    e = cudaGraphInstantiate(&b->graph[parity], g, 0);
+    cudaGraphDestroy(g);
+    if (e != cudaSuccess) return cuda_fail(e, "cudaGraphInstantiate");
+    return PT_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+int pt_batch_create(pt_ctx* ctx, int64_t capacity, int max_campaigns, int storage, int steps_per_epoch, int sort,
+                    int blocks_per_sm, pt_batch** out)
+{
+    if (!ctx || !out) return fail(PT_ERR_ARG, "null argument");
+    if (capacity < 1 || capacity > INT32_MAX) return fail(PT_ERR_ARG, "capacity must be in [1, 2^31)");
+    if (max_campaigns < 1 || max_campaigns > 4096) return fail(PT_ERR_ARG, "max_campaigns must be in [1, 4096]");
+    if (storage != PT_FIELD_BRICK_BF16 && storage != PT_FIELD_BRICK_F32)
+        return fail(PT_ERR_ARG, "batches run the FP32 push: storage must be a brick form");
+    if (steps_per_epoch < 1) return fail(PT_ERR_ARG, "steps_per_epoch must be >= 1");
+    PT_CUDA(cudaSetDevice(ctx->device));
+    pt_batch* b = new (std::nothrow) pt_batch();
+    if (!b) return fail(PT_ERR_OOM, "host allocation failed");
+    b->ctx = ctx;
+    b->cap = capacity;
+    b->max_camps = max_campaigns;
+    b->storage = storage;
+    b->K = steps_per_epoch;
+    b->sort = sort ? 1 : 0;
+    b->h_camps.assign(max_campaigns, BatchCampaignDev{});
+    b->fields.assign(max_campaigns, nullptr);
+    b->free_ranges.push_back({0, capacity});
+    int rc = alloc_state(b->buf[0], capacity);
+    if (!rc && b->sort) rc = alloc_state(b->buf[1], capacity);
+    const int64_t max_tiles = capacity / 256 + max_campaigns + 1;
+    cudaError_t e = cudaSuccess;
+    if (!rc) {
+        e = cudaMalloc((void**)&b->camp_of, sizeof(int32_t) * capacity);
+        if (e == cudaSuccess) e = cudaMalloc((void**)&b->d_camps, sizeof(BatchCampaignDev) * max_campaigns);
+        if (e == cudaSuccess) e = cudaMalloc((void**)&b->d_tiles, sizeof(BatchTile) * max_tiles);
+        if (e == cudaSuccess) e = cudaMalloc((void**)&b->d_ntiles, sizeof(int));
+        if (e == cudaSuccess) e = cudaMalloc((void**)&b->d_counter, sizeof(int));
+        if (e == cudaSuccess) e = cudaMalloc((void**)&b->d_m, sizeof(int64_t));
+        if (e == cudaSuccess && b->sort) e = cudaMalloc((void**)&b->keys, sizeof(uint32_t) * capacity);
+        if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&b->cap_stream, cudaStreamNonBlocking);
+        if (e != cudaSuccess) {
+            cudaGetLastError();
+            rc = fail(PT_ERR_OOM, "batch allocation failed");
+        }
+    }
+    if (!rc) {
+        cudaStream_t s = ctx->stream;
+        const int zero = 0;
+        const int64_t zero64 = 0;
+        e = cudaMemsetAsync(b->camp_of, 0xff, sizeof(int32_t) * capacity, s);  // -1: free slot
+        if (e == cudaSuccess) e = cudaMemsetAsync(b->d_camps, 0, sizeof(BatchCampaignDev) * max_campaigns, s);
+        if (e == cudaSuccess) e = cudaMemcpyAsync(b->d_ntiles, &zero, sizeof(int), cudaMemcpyHostToDevice, s);
+        if (e == cudaSuccess) e = cudaMemcpyAsync(b->d_counter, &zero, sizeof(int), cudaMemcpyHostToDevice, s);
+        if (e == cudaSuccess) e = cudaMemcpyAsync(b->d_m, &zero64, sizeof(int64_t), cudaMemcpyHostToDevice, s);
+        if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+        if (e != cudaSuccess) rc = cuda_fail(e, "batch init");
+    }
+    if (rc) {
+        pt_batch_destroy(b);
+        return rc;
+    }
+    // persistent grid: resident blocks of push_batch_kernel per SM
+    const int per_sm = blocks_per_sm > 0 ? std::min(blocks_per_sm, 8) : 2;
+    b->grid = ctx->num_sms * per_sm;
+    *out = b;
+    return PT_OK;
+}
+
+int pt_batch_add(pt_ctx* ctx, pt_batch* b, const pt_campaign_desc* d, int* id)
+{
+    if (!ctx || !b || !d || !id) return fail(PT_ERR_ARG, "null argument");
+    const pt_field* f = d->field;
+    if (!f || f->storage != b->storage) return fail(PT_ERR_ARG, "campaign field must use the batch's brick storage");
+    if (!(d->dt > 0 && std::isfinite(d->dt))) return fail(PT_ERR_ARG, "dt must be finite and positive");
+    if (d->nsteps < 1 || d->stride < 1) return fail(PT_ERR_ARG, "nsteps and stride must be >= 1");
+    if (d->n < 1) return fail(PT_ERR_ARG, "a campaign needs at least one particle");
+    if (!(d->d_x1 && d->d_x2 && d->d_x3 && d->d_p1 && d->d_p2 && d->d_p3 && d->d_alive))
+        return fail(PT_ERR_ARG, "null state");
+    if (d->d_cache && d->cache_rows < 1) return fail(PT_ERR_ARG, "cache_rows must be >= 1");
+    if (d->d_cache && !d->cache_ring && d->cache_rows < (d->nsteps - 1) / d->stride + 1)
+        return fail(PT_ERR_ARG, "a non-ring cache needs one row per save");
+    int c = -1;
+    for (int i = 0; i < b->max_camps; ++i)
+        if (!b->h_camps[i].active) {
+            c = i;
+            break;
+        }
+    if (c < 0) return fail(PT_ERR_STATE, "batch is full (max_campaigns)");
+    int64_t slot0 = -1;
+    for (auto& r : b->free_ranges)
+        if (r.second >= d->n) {
+            slot0 = r.first;
+            r.first += d->n;
+            r.second -= d->n;
+            break;
+        }
+    if (slot0 < 0) return fail(PT_ERR_OOM, "no free slot range of " + std::to_string(d->n) + " particles in the batch");
+    b->free_ranges.erase(std::remove_if(b->free_ranges.begin(), b->free_ranges.end(),
+                                        [](const std::pair<int64_t, int64_t>& r) { return r.second == 0; }),
+                         b->free_ranges.end());
+    cudaStream_t s = ctx->stream;
+    int rc = launch_batch_import(b->buf[b->cur], slot0, d->n, f, d->d_x1, d->d_x2, d->d_x3, d->d_p1, d->d_p2,
+                                 d->d_p3, d->d_alive, ctx->num_sms, s);
+    if (rc) return rc;
+    // camp_of[slot0 .. slot0 + n) = c
+    std::vector<int32_t> tag((size_t)d->n, c);
+    PT_CUDA(cudaMemcpyAsync(b->camp_of + slot0, tag.data(), sizeof(int32_t) * d->n, cudaMemcpyHostToDevice, s));
+    BatchCampaignDev C{};
+    const pt_grid& g = f->grid;
+    PushArgsFast& a = C.a;
+    a.fld.nodes = f->nodes;
+    a.fld.offs = f->offs;
+    a.fld.nx = g.nx; a.fld.ny = g.ny; a.fld.nz = g.nz;
+    a.fld.bf16 = f->storage == PT_FIELD_BRICK_BF16;
+    a.wx = (g.xmax - g.xmin) / g.dx;
+    a.wy = (g.ymax - g.ymin) / g.dy;
+    a.wz = (g.zmax - g.zmin) / g.dz;
+    a.n = d->n;
+    a.hB = (float)(Q_E * f->B_ref * d->dt / (2.0 * M_P));
+    a.vfac[0] = (float)(C_LIGHT * d->dt / g.dx);
+    a.vfac[1] = (float)(C_LIGHT * d->dt / g.dy);
+    a.vfac[2] = (float)(C_LIGHT * d->dt / g.dz);
+    a.xmin[0] = g.xmin; a.xmin[1] = g.ymin; a.xmin[2] = g.zmin;
+    a.dxs[0] = g.dx; a.dxs[1] = g.dy; a.dxs[2] = g.dz;
+    a.nsteps = d->nsteps;
+    a.stride = d->stride;
+    a.periodic = d->periodic;
+    a.cache_mode = d->d_cache ? PT_CACHE_MU : PT_CACHE_NONE;
+    a.cache_f64 = d->cache_f64;
+    a.cache = d->d_cache;
+    a.row_base = 0;
+    a.rows = d->cache_rows;
+    a.ring = d->cache_ring;
+    a.n_cache = d->n;
+    a.deaths = d->d_deaths;
+    C.slot0 = slot0;
+    C.n = d->n;
+    C.step = 0;
+    C.K = b->K;
+    C.n_bricks = (f->n_nodes + 511) / 512;
+    C.active = 1;
+    b->h_camps[c] = C;
+    b->fields[c] = f;
+    const int words = (int)(g.nx + g.ny + g.nz);
+    if (words > b->smem_words) {
+        b->smem_words = words;
+        drop_graphs(b);
+    }
+    rc = rebuild_tables(b, c);
+    if (rc) return rc;
+    *id = c;
+    return PT_OK;
+}
+
+int pt_batch_remove(pt_ctx* ctx, pt_batch* b, int id)
+{
+    if (!ctx || !b) return fail(PT_ERR_ARG, "null argument");
+    if (id < 0 || id >= b->max_camps || !b->h_camps[id].active) return fail(PT_ERR_ARG, "no such campaign");
+    BatchCampaignDev& C = b->h_camps[id];
+    PT_CUDA(cudaStreamSynchronize(ctx->stream));  // the step counter on the host mirror is stale: keep device's
+    PT_CUDA(cudaMemsetAsync(b->camp_of + C.slot0, 0xff, sizeof(int32_t) * C.n, ctx->stream));
+    b->free_ranges.push_back({C.slot0, C.n});
+    std::sort(b->free_ranges.begin(), b->free_ranges.end());
+    std::vector<std::pair<int64_t, int64_t>> merged;
+    for (auto& r : b->free_ranges) {
+        if (!merged.empty() && merged.back().first + merged.back().second == r.first) merged.back().second += r.second;
+        else merged.push_back(r);
+    }
+    b->free_ranges.swap(merged);
+    C = BatchCampaignDev{};
+    b->fields[id] = nullptr;
+    return rebuild_tables(b, -1);
+}
+
+int pt_batch_run(pt_ctx* ctx, pt_batch* b, int64_t epochs, int use_graph)
+{
+    if (!ctx || !b) return fail(PT_ERR_ARG, "null argument");
+    if (epochs < 0) return fail(PT_ERR_ARG, "epochs must be >= 0");
+    cudaStream_t s = ctx->stream;
+    if (use_graph) {
+        if (b->graph_dirty) {
+            drop_graphs(b);
+            int rc = capture(b, 0);
+            if (!rc && b->sort) rc = capture(b, 1);
+            if (rc) return rc;
+            b->graph_dirty = false;
+        }
+        for (int64_t e = 0; e < epochs; ++e) {
+            PT_CUDA(cudaGraphLaunch(b->graph[b->sort ? b->cur : 0], s));
+            if (b->sort) b->cur = 1 - b->cur;
+        }
+        return PT_OK;
+    }
+    for (int64_t e = 0; e < epochs; ++e) {
+        int rc = enqueue_epoch(b, s);
+        if (rc) return rc;
+        if (b->sort) b->cur = 1 - b->cur;
+    }
+    return PT_OK;
+}
+
+int pt_batch_step(pt_ctx* ctx, pt_batch* b, int id, int64_t* step)
+{
+    if (!ctx || !b || !step) return fail(PT_ERR_ARG, "null argument");
+    if (id < 0 || id >= b->max_camps || !b->h_camps[id].active) return fail(PT_ERR_ARG, "no such campaign");
+    PT_CUDA(cudaStreamSynchronize(ctx->stream));
+    PT_CUDA(cudaMemcpy(step, &b->d_camps[id].step, sizeof(int64_t), cudaMemcpyDeviceToHost));
+    return PT_OK;
+}
+
+int pt_batch_export(pt_ctx* ctx, pt_batch* b, int id, double* x1, double* x2, double* x3, double* p1, double* p2,
+                    double* p3, uint8_t* alive)
+{
+    if (!ctx || !b) return fail(PT_ERR_ARG, "null argument");
+    if (id < 0 || id >= b->max_camps || !b->h_camps[id].active) return fail(PT_ERR_ARG, "no such campaign");
+    if (!(x1 && x2 && x3 && p1 && p2 && p3 && alive)) return fail(PT_ERR_ARG, "null state");
+    const BatchCampaignDev& C = b->h_camps[id];
+    return launch_batch_export(b->buf[b->cur], C.slot0, C.n, b->fields[id], x1, x2, x3, p1, p2, p3, alive,
+                               ctx->num_sms, ctx->stream);
+}
+
+int pt_batch_destroy(pt_batch* b)
+{
+    if (!b) return PT_OK;
+    if (b->ctx) cudaStreamSynchronize(b->ctx->stream);
+    drop_graphs(b);
+    free_state(b->buf[0]);
+    free_state(b->buf[1]);
+    for (void* p : {(void*)b->camp_of, (void*)b->d_camps, (void*)b->d_tiles, (void*)b->d_ntiles, (void*)b->d_counter,
+                    (void*)b->keys, (void*)b->hist, (void*)b->cursor, (void*)b->d_m})
+        if (p) cudaFree(p);
+    if (b->cap_stream) cudaStreamDestroy(b->cap_stream);
+    delete b;
+    return PT_OK;
+}
+
+}  // extern "C"

@@ -136,8 +136,57 @@ struct PushArgsFast {
     int64_t row_base, rows;
     int64_t* deaths;
     int variant;           // launch shape, see pt_push_params.kernel_variant
+    int ring;              // 1: save row r goes to cache row r % rows
+    int64_t n_cache;       // particles per cache row
 };
 int launch_push_fast(const PushArgsFast& a, cudaStream_t s);
+
+// ---------------------------------------------------------------- batches
+// A batch is an arena of particle slots shared by many campaigns (each a
+// contiguous slot range with its own field, dt, step counter and cache).
+struct BatchCampaignDev {
+    PushArgsFast a;    // per-campaign constants (state pointers unused)
+    int64_t slot0, n;  // slot range in the arena
+    int64_t step, K;   // next step; steps per epoch
+    int64_t key_base;  // first sort bucket
+    int64_t n_bricks;  // bricks of the campaign's field (bucket n_bricks = dead)
+    int64_t shift;     // arena slot = dense sort position + shift
+    int32_t active;    // holds particles (keyed by the sort)
+    int32_t pad;
+};
+struct BatchTile {
+    int32_t campaign;
+    int32_t count;
+    int64_t begin;     // first slot of the tile (arena index)
+};
+struct BatchStateDev {
+    double* x;         // [3][cap]
+    float* p;          // [3][cap]
+    double* p2;
+    int32_t* pid;      // campaign-local particle index
+    uint8_t* alive;
+    int64_t cap;
+};
+struct BatchLaunch {
+    const BatchCampaignDev* camps;
+    const BatchTile* tiles;
+    const int* n_tiles;
+    int* tile_counter;
+    BatchStateDev st;
+    int bf16;
+    int smem_words;    // max (nx + ny + nz) over the batch's fields
+    int grid;
+};
+int launch_push_batch(const BatchLaunch& L, cudaStream_t s);
+int launch_batch_epoch_end(BatchCampaignDev* camps, int n_camps, int* tile_counter, cudaStream_t s);
+int launch_batch_sort(const BatchCampaignDev* camps, const int32_t* camp_of, BatchStateDev from, BatchStateDev to,
+                      uint32_t* keys, uint32_t* hist, uint32_t* cursor, const int64_t* d_m_buckets,
+                      int64_t max_buckets, int num_sms, cudaStream_t s);
+int launch_batch_import(BatchStateDev st, int64_t slot0, int64_t n, const pt_field* f, const double* x1,
+                        const double* x2, const double* x3, const double* p1, const double* p2, const double* p3,
+                        const uint8_t* alive, int num_sms, cudaStream_t s);
+int launch_batch_export(BatchStateDev st, int64_t slot0, int64_t n, const pt_field* f, double* x1, double* x2,
+                        double* x3, double* p1, double* p2, double* p3, uint8_t* alive, int num_sms, cudaStream_t s);
 int launch_fast_import(pt_fast_state* st, const pt_field* f, const double* x1, const double* x2, const double* x3,
                        const double* p1, const double* p2, const double* p3, const uint8_t* alive, cudaStream_t s);
 int launch_fast_export(const pt_fast_state* st, const pt_field* f, double* x1, double* x2, double* x3, double* p1,

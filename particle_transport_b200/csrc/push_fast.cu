@@ -107,36 +107,30 @@ __device__ __forceinline__ double wrap_cells(double x, double w)
     return x;
 }
 
-template <bool BF16, int BLOCK, int MINB>
-__global__ void __launch_bounds__(BLOCK, MINB) push_fast_kernel(PushArgsFast a)
+// K steps of one particle held in registers.  State is (x, y, z) in cells
+// (FP64), p/(mc) (FP32) and |p/(mc)|^2 (FP64); pid indexes the cache row.
+// Cache rows of a.n_cache particles: row r at (r - a.row_base) or, with
+// a.ring, at (r % a.rows).
+template <bool BF16>
+__device__ __forceinline__ void advance_particle(double& x, double& y, double& z, float& px, float& py, float& pz,
+                                                 double& P2, bool& al, const int64_t pid, const PushArgsFast& a,
+                                                 const uint32_t* ox, const uint32_t* oy, const uint32_t* oz,
+                                                 const int64_t s_begin, const int64_t s_end)
 {
-    extern __shared__ uint32_t s_offs[];
     const int nx = (int)a.fld.nx, ny = (int)a.fld.ny, nz = (int)a.fld.nz;
-    for (int i = threadIdx.x; i < nx + ny + nz; i += blockDim.x) s_offs[i] = a.fld.offs[i];
-    __syncthreads();
-    const uint32_t* ox = s_offs;
-    const uint32_t* oy = s_offs + nx;
-    const uint32_t* oz = s_offs + nx + ny;
     const float hB = a.hB;
-    const int64_t s_end = a.step_begin + a.step_count;
-    const int64_t n = a.n;
-
-    for (int64_t slot = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; slot < n;
-         slot += (int64_t)gridDim.x * blockDim.x) {
-        double x = a.x[slot], y = a.x[n + slot], z = a.x[2 * n + slot];
-        float px = a.p[slot], py = a.p[n + slot], pz = a.p[2 * n + slot];
-        double P2 = a.p2[slot];
-        bool al = a.alive[slot] != 0;
-        const int64_t pid = a.pid[slot];
-        int64_t next_save = ((a.step_begin + a.stride - 1) / a.stride) * a.stride;
-        for (int64_t s = a.step_begin; s < s_end; ++s) {
+    const int64_t n = a.n_cache;
+    {
+        int64_t next_save = ((s_begin + a.stride - 1) / a.stride) * a.stride;
+        for (int64_t s = s_begin; s < s_end; ++s) {
             const bool do_push = s < a.nsteps - 1;
             bool is_save = false;
             int64_t row = 0;
             if (s == next_save) {
                 row = s / a.stride;
                 next_save += a.stride;
-                is_save = a.cache_mode != PT_CACHE_NONE && row >= a.row_base && row < a.row_base + a.rows;
+                is_save = a.cache_mode != PT_CACHE_NONE &&
+                          (a.ring || (row >= a.row_base && row < a.row_base + a.rows));
             }
             float f[6] = {0, 0, 0, 0, 0, 0};
             if (al && (do_push || (is_save && a.cache_mode == PT_CACHE_MU))) {
@@ -144,7 +138,7 @@ __global__ void __launch_bounds__(BLOCK, MINB) push_fast_kernel(PushArgsFast a)
                 gather6<BF16>(a.fld.nodes, c, f);
             }
             if (is_save) {
-                const int64_t r = row - a.row_base;
+                const int64_t r = a.ring ? row % a.rows : row - a.row_base;
                 if (a.cache_mode == PT_CACHE_MU) {
                     float mu = NAN;
                     if (al && x >= 0.0 && x <= a.wx && y >= 0.0 && y <= a.wy && z >= 0.0 && z <= a.wz)
@@ -209,6 +203,28 @@ __global__ void __launch_bounds__(BLOCK, MINB) push_fast_kernel(PushArgsFast a)
                 }
             }
         }
+    }
+}
+
+template <bool BF16, int BLOCK, int MINB>
+__global__ void __launch_bounds__(BLOCK, MINB) push_fast_kernel(PushArgsFast a)
+{
+    extern __shared__ uint32_t s_offs[];
+    const int nx = (int)a.fld.nx, ny = (int)a.fld.ny, nz = (int)a.fld.nz;
+    for (int i = threadIdx.x; i < nx + ny + nz; i += blockDim.x) s_offs[i] = a.fld.offs[i];
+    __syncthreads();
+    const uint32_t* ox = s_offs;
+    const uint32_t* oy = s_offs + nx;
+    const uint32_t* oz = s_offs + nx + ny;
+    const int64_t s_end = a.step_begin + a.step_count;
+    const int64_t n = a.n;
+    for (int64_t slot = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; slot < n;
+         slot += (int64_t)gridDim.x * blockDim.x) {
+        double x = a.x[slot], y = a.x[n + slot], z = a.x[2 * n + slot];
+        float px = a.p[slot], py = a.p[n + slot], pz = a.p[2 * n + slot];
+        double P2 = a.p2[slot];
+        bool al = a.alive[slot] != 0;
+        advance_particle<BF16>(x, y, z, px, py, pz, P2, al, a.pid[slot], a, ox, oy, oz, a.step_begin, s_end);
         a.x[slot] = x; a.x[n + slot] = y; a.x[2 * n + slot] = z;
         a.p[slot] = px; a.p[n + slot] = py; a.p[2 * n + slot] = pz;
         a.p2[slot] = P2;
@@ -516,6 +532,281 @@ int fast_sort(pt_ctx* ctx, pt_fast_state* st, const pt_field* f, cudaStream_t s)
     std::swap(st->p2, st->p2_alt);
     std::swap(st->pid, st->pid_alt);
     std::swap(st->alive, st->alive_alt);
+    return PT_OK;
+}
+
+// ------------------------------------------------------------ batches
+namespace {
+
+// One persistent kernel for every campaign of a batch: each CTA pulls
+// 256-particle tiles from the tile table (atomic counter), loads the tile's
+// campaign constants and field offset tables into shared memory when the
+// campaign changes, and runs K steps of its particles from the campaign's
+// device-resident step counter.  The per-particle arithmetic is
+// advance_particle, so a particle's trajectory is the same alone or batched.
+template <bool BF16>
+__global__ void __launch_bounds__(256, 1) push_batch_kernel(BatchLaunch L)
+{
+    extern __shared__ uint32_t s_offs[];
+    __shared__ PushArgsFast s_a;
+    __shared__ int s_tile, s_camp;
+    __shared__ const uint32_t* s_loaded;
+    __shared__ long long s_begin, s_end;
+    if (threadIdx.x == 0) {
+        s_camp = -1;
+        s_loaded = nullptr;
+    }
+    const int n_tiles = *L.n_tiles;
+    const int64_t cap = L.st.cap;
+    for (;;) {
+        __syncthreads();
+        if (threadIdx.x == 0) s_tile = atomicAdd(L.tile_counter, 1);
+        __syncthreads();
+        const int t = s_tile;
+        if (t >= n_tiles) break;
+        const BatchTile T = L.tiles[t];
+        if (T.campaign != s_camp) {
+            const BatchCampaignDev* C = L.camps + T.campaign;
+            constexpr int words = (int)(sizeof(PushArgsFast) / sizeof(uint32_t));
+            for (int i = threadIdx.x; i < words; i += blockDim.x)
+                reinterpret_cast<uint32_t*>(&s_a)[i] = reinterpret_cast<const uint32_t*>(&C->a)[i];
+            if (threadIdx.x == 0) {
+                s_begin = C->step;
+                s_end = min(C->step + C->K, C->a.nsteps);
+            }
+            __syncthreads();
+            if (threadIdx.x == 0) s_camp = T.campaign;
+            if (s_a.fld.offs != s_loaded) {
+                const int tot = (int)(s_a.fld.nx + s_a.fld.ny + s_a.fld.nz);
+                for (int i = threadIdx.x; i < tot; i += blockDim.x) s_offs[i] = s_a.fld.offs[i];
+            }
+            __syncthreads();
+            if (threadIdx.x == 0) s_loaded = s_a.fld.offs;
+        }
+        const int64_t sb = s_begin, se = s_end;
+        if (sb >= se) continue;
+        if ((int)threadIdx.x < T.count) {
+            const uint32_t* ox = s_offs;
+            const uint32_t* oy = s_offs + s_a.fld.nx;
+            const uint32_t* oz = s_offs + s_a.fld.nx + s_a.fld.ny;
+            const int64_t slot = T.begin + threadIdx.x;
+            double x = L.st.x[slot], y = L.st.x[cap + slot], z = L.st.x[2 * cap + slot];
+            float px = L.st.p[slot], py = L.st.p[cap + slot], pz = L.st.p[2 * cap + slot];
+            double P2 = L.st.p2[slot];
+            bool al = L.st.alive[slot] != 0;
+            advance_particle<BF16>(x, y, z, px, py, pz, P2, al, L.st.pid[slot], s_a, ox, oy, oz, sb, se);
+            L.st.x[slot] = x; L.st.x[cap + slot] = y; L.st.x[2 * cap + slot] = z;
+            L.st.p[slot] = px; L.st.p[cap + slot] = py; L.st.p[2 * cap + slot] = pz;
+            L.st.p2[slot] = P2;
+            L.st.alive[slot] = al ? 1 : 0;
+        }
+    }
+}
+
+__global__ void batch_epoch_end_kernel(BatchCampaignDev* camps, int n, int* tile_counter)
+{
+    const int c = blockIdx.x * blockDim.x + threadIdx.x;
+    if (c < n && camps[c].active) camps[c].step = min(camps[c].step + camps[c].K, camps[c].a.nsteps);
+    if (c == 0) *tile_counter = 0;
+}
+
+__global__ void zero_counted_kernel(uint32_t* a, const int64_t* m)
+{
+    const int64_t mm = *m;
+    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < mm; i += (int64_t)gridDim.x * blockDim.x)
+        a[i] = 0u;
+}
+
+// exclusive scan of hist[0..*m) by one block (bucket count read on the device)
+__global__ void __launch_bounds__(1024) scan_counted_kernel(const uint32_t* __restrict__ hist, uint32_t* cursor,
+                                                            const int64_t* m_dev)
+{
+    __shared__ uint32_t part[1024];
+    const int64_t m = *m_dev;
+    const int t = threadIdx.x;
+    const int64_t per = (m + 1023) / 1024;
+    const int64_t b = t * per, e = min(m, b + per);
+    uint32_t sum = 0;
+    for (int64_t i = b; i < e; ++i) sum += hist[i];
+    part[t] = sum;
+    __syncthreads();
+    for (int off = 1; off < 1024; off <<= 1) {
+        uint32_t v = t >= off ? part[t - off] : 0u;
+        __syncthreads();
+        part[t] += v;
+        __syncthreads();
+    }
+    uint32_t run = part[t] - sum;
+    for (int64_t i = b; i < e; ++i) {
+        uint32_t h = hist[i];
+        cursor[i] = run;
+        run += h;
+    }
+}
+
+// Sort key of every occupied slot: the campaign's first bucket + the brick of
+// the particle's cell (the campaign's dead bucket for dead particles).  Free
+// slots (camp_of < 0) take no part.
+__global__ void batch_key_kernel(const BatchCampaignDev* __restrict__ camps, const int32_t* __restrict__ camp_of,
+                                 BatchStateDev st, uint32_t* __restrict__ keys, uint32_t* __restrict__ hist)
+{
+    const int lane = threadIdx.x & 31;
+    const unsigned lt = (1u << lane) - 1u;
+    const int64_t cap = st.cap;
+    const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+    for (int64_t base = (int64_t)blockIdx.x * blockDim.x + (threadIdx.x & ~31); base < cap; base += stride) {
+        const int64_t i = base + lane;
+        const int c = i < cap ? camp_of[i] : -1;
+        const bool valid = c >= 0;
+        uint32_t key = 0;
+        if (valid) {
+            const BatchCampaignDev& C = camps[c];
+            key = (uint32_t)(C.key_base + C.n_bricks);
+            if (st.alive[i]) {
+                const int nx = (int)C.a.fld.nx, ny = (int)C.a.fld.ny, nz = (int)C.a.fld.nz;
+                const uint32_t* offs = C.a.fld.offs;
+                int ix = min(max((int)floor(st.x[i]), 0), nx - 2);
+                int iy = min(max((int)floor(st.x[cap + i]), 0), ny - 2);
+                int iz = min(max((int)floor(st.x[2 * cap + i]), 0), nz - 2);
+                key = (uint32_t)C.key_base + ((offs[ix] + offs[nx + iy] + offs[nx + ny + iz]) >> 9);
+            }
+            keys[i] = key;
+        }
+        const unsigned act = __ballot_sync(0xffffffffu, valid);
+        if (valid) {
+            const unsigned same = __match_any_sync(act, key);
+            if ((same & lt) == 0) atomicAdd(&hist[key], (uint32_t)__popc(same));
+        }
+    }
+}
+
+__global__ void batch_scatter_kernel(const uint32_t* __restrict__ keys, uint32_t* cursor,
+                                     const BatchCampaignDev* __restrict__ camps, const int32_t* __restrict__ camp_of,
+                                     BatchStateDev from, BatchStateDev to)
+{
+    const int lane = threadIdx.x & 31;
+    const unsigned lt = (1u << lane) - 1u;
+    const int64_t cap = from.cap;
+    const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+    for (int64_t base = (int64_t)blockIdx.x * blockDim.x + (threadIdx.x & ~31); base < cap; base += stride) {
+        const int64_t i = base + lane;
+        const int c = i < cap ? camp_of[i] : -1;
+        const bool valid = c >= 0;
+        const unsigned act = __ballot_sync(0xffffffffu, valid);
+        if (!valid) continue;
+        const uint32_t key = keys[i];
+        const unsigned same = __match_any_sync(act, key);
+        const int leader = __ffs(same) - 1;
+        uint32_t first = 0;
+        if (lane == leader) first = atomicAdd(&cursor[key], (uint32_t)__popc(same));
+        first = __shfl_sync(same, first, leader);
+        const int64_t d = (int64_t)first + __popc(same & lt) + camps[c].shift;
+        to.x[d] = from.x[i]; to.x[cap + d] = from.x[cap + i]; to.x[2 * cap + d] = from.x[2 * cap + i];
+        to.p[d] = from.p[i]; to.p[cap + d] = from.p[cap + i]; to.p[2 * cap + d] = from.p[2 * cap + i];
+        to.p2[d] = from.p2[i];
+        to.pid[d] = from.pid[i];
+        to.alive[d] = from.alive[i];
+    }
+}
+
+// SI state of one campaign <-> arena slots [slot0, slot0 + n); same formulas
+// as fast_import_kernel / fast_export_kernel.
+__global__ void batch_import_kernel(BatchStateDev st, int64_t slot0, int64_t n, const double* __restrict__ x1,
+                                    const double* __restrict__ x2, const double* __restrict__ x3,
+                                    const double* __restrict__ p1, const double* __restrict__ p2,
+                                    const double* __restrict__ p3, const uint8_t* __restrict__ alive, double xmin,
+                                    double ymin, double zmin, double dx, double dy, double dz)
+{
+    const double inv_mc = 1.0 / (M_P * C_LIGHT);
+    const int64_t cap = st.cap;
+    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+        const int64_t s = slot0 + i;
+        st.x[s] = (x1[i] - xmin) / dx;
+        st.x[cap + s] = (x2[i] - ymin) / dy;
+        st.x[2 * cap + s] = (x3[i] - zmin) / dz;
+        const double qx = p1[i] * inv_mc, qy = p2[i] * inv_mc, qz = p3[i] * inv_mc;
+        st.p[s] = (float)qx; st.p[cap + s] = (float)qy; st.p[2 * cap + s] = (float)qz;
+        st.p2[s] = qx * qx + qy * qy + qz * qz;
+        st.pid[s] = (int32_t)i;
+        st.alive[s] = alive[i];
+    }
+}
+
+__global__ void batch_export_kernel(BatchStateDev st, int64_t slot0, int64_t n, double xmin, double ymin, double zmin,
+                                    double dx, double dy, double dz, double* x1, double* x2, double* x3, double* p1,
+                                    double* p2, double* p3, uint8_t* alive)
+{
+    const int64_t cap = st.cap;
+    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+        const int64_t s = slot0 + i;
+        const int64_t q = st.pid[s];
+        x1[q] = xmin + st.x[s] * dx;
+        x2[q] = ymin + st.x[cap + s] * dy;
+        x3[q] = zmin + st.x[2 * cap + s] * dz;
+        const double px = st.p[s], py = st.p[cap + s], pz = st.p[2 * cap + s];
+        const double sc = sqrt(st.p2[s] / (px * px + py * py + pz * pz)) * (M_P * C_LIGHT);
+        p1[q] = px * sc; p2[q] = py * sc; p3[q] = pz * sc;
+        alive[q] = st.alive[s];
+    }
+}
+
+}  // namespace
+
+int launch_push_batch(const BatchLaunch& L, cudaStream_t s)
+{
+    const size_t smem = sizeof(uint32_t) * (size_t)std::max(L.smem_words, 1);
+    void* kfn = L.bf16 ? (void*)push_batch_kernel<true> : (void*)push_batch_kernel<false>;
+    if (smem > 48 * 1024) PT_CUDA(cudaFuncSetAttribute(kfn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    if (L.bf16) push_batch_kernel<true><<<L.grid, 256, smem, s>>>(L);
+    else push_batch_kernel<false><<<L.grid, 256, smem, s>>>(L);
+    PT_CHECK_LAUNCH("push_batch_kernel");
+    return PT_OK;
+}
+
+int launch_batch_epoch_end(BatchCampaignDev* camps, int n_camps, int* tile_counter, cudaStream_t s)
+{
+    batch_epoch_end_kernel<<<(std::max(n_camps, 1) + 127) / 128, 128, 0, s>>>(camps, n_camps, tile_counter);
+    PT_CHECK_LAUNCH("batch_epoch_end_kernel");
+    return PT_OK;
+}
+
+int launch_batch_sort(const BatchCampaignDev* camps, const int32_t* camp_of, BatchStateDev from, BatchStateDev to,
+                      uint32_t* keys, uint32_t* hist, uint32_t* cursor, const int64_t* d_m, int64_t max_buckets,
+                      int num_sms, cudaStream_t s)
+{
+    const int zb = (int)std::min<int64_t>((max_buckets + 255) / 256, (int64_t)num_sms * 8);
+    zero_counted_kernel<<<std::max(zb, 1), 256, 0, s>>>(hist, d_m);
+    PT_CHECK_LAUNCH("zero_counted_kernel");
+    const int gb = grid_for(from.cap, 256, num_sms);
+    batch_key_kernel<<<gb, 256, 0, s>>>(camps, camp_of, from, keys, hist);
+    PT_CHECK_LAUNCH("batch_key_kernel");
+    scan_counted_kernel<<<1, 1024, 0, s>>>(hist, cursor, d_m);
+    PT_CHECK_LAUNCH("scan_counted_kernel");
+    batch_scatter_kernel<<<gb, 256, 0, s>>>(keys, cursor, camps, camp_of, from, to);
+    PT_CHECK_LAUNCH("batch_scatter_kernel");
+    return PT_OK;
+}
+
+int launch_batch_import(BatchStateDev st, int64_t slot0, int64_t n, const pt_field* f, const double* x1,
+                        const double* x2, const double* x3, const double* p1, const double* p2, const double* p3,
+                        const uint8_t* alive, int num_sms, cudaStream_t s)
+{
+    if (n <= 0) return PT_OK;
+    const pt_grid& g = f->grid;
+    batch_import_kernel<<<grid_for(n, 256, num_sms), 256, 0, s>>>(st, slot0, n, x1, x2, x3, p1, p2, p3, alive,
+                                                                 g.xmin, g.ymin, g.zmin, g.dx, g.dy, g.dz);
+    PT_CHECK_LAUNCH("batch_import_kernel");
+    return PT_OK;
+}
+
+int launch_batch_export(BatchStateDev st, int64_t slot0, int64_t n, const pt_field* f, double* x1, double* x2,
+                        double* x3, double* p1, double* p2, double* p3, uint8_t* alive, int num_sms, cudaStream_t s)
+{
+    if (n <= 0) return PT_OK;
+    const pt_grid& g = f->grid;
+    batch_export_kernel<<<grid_for(n, 256, num_sms), 256, 0, s>>>(st, slot0, n, g.xmin, g.ymin, g.zmin, g.dx, g.dy,
+                                                                 g.dz, x1, x2, x3, p1, p2, p3, alive);
+    PT_CHECK_LAUNCH("batch_export_kernel");
     return PT_OK;
 }
 

@@ -1,0 +1,242 @@
+"""Campaign server: continuous batching of transport jobs on one B200.
+
+A job is one campaign (field library, mode, energy, particle count,
+duration, injection) plus its D_mumu / <dmu^2> products.  Jobs arrive at
+any time (submit); each scheduler tick
+
+  1. admits waiting jobs, in arrival order, while the HBM budget and the
+     batch's slot arena have room (the job's particle state, mu cache and
+     accumulators are charged against the budget);
+  2. runs one epoch (steps_per_epoch pushes of every admitted job, one
+     persistent launch replayed from a CUDA graph);
+  3. for each job that reached its last step, launches its lag-pair binning
+     on a side stream -- overlapping the next epoch -- and, once that
+     finished, computes the products, records the latency and frees the job.
+
+Particle state stays on the device from admission to the job's results; a
+job's trajectory (and so its mu cache) is bit-identical whether it runs
+alone or among others, and its D_mumu sums differ only by summation order.
+The reference has no serving mode; it runs campaigns back to back
+(run_mode_campaigns, src/multimode_multienergy_cache_pipeline.jl:2924).
+"""
+from __future__ import annotations
+
+import math
+import time
+from dataclasses import dataclass, field as dfield
+
+import numpy as np
+
+from . import _lib
+from . import stats as S
+from .batch import Batch
+from .fields import FieldLibrary, M_P, Q_E
+from .particles import energy_to_gamma, init_particles
+from .time_units import build_mu_edges_full, log_spaced_lag_steps, reference_Omega0
+
+
+@dataclass
+class JobSpec:
+    library: str                 # key of the field library (e.g. "256", "512")
+    mode: str                    # total / alfven / fast / slow
+    energy_GeV: float
+    n_particles: int
+    duration_gyroperiods: float
+    injection: str = "isotropic"  # or "fixed_mu"
+    mu0: float = 0.0
+    seed: int = 0
+    steps_per_gyroperiod: int = 64
+    saves_per_gyroperiod: int = 8
+    n_lags: int = 32
+    n_bins: int = 20
+    start_mode: str = "sliding"
+
+
+@dataclass
+class JobResult:
+    job_id: int
+    spec: JobSpec
+    arrival: float
+    admitted: float
+    finished: float
+    particle_steps: int
+    acc: dict = dfield(default_factory=dict)
+    lags: np.ndarray = None
+    edges: np.ndarray = None
+    mu: np.ndarray = None        # the mu cache, when the server keeps it (keep_cache=True)
+
+    @property
+    def latency(self) -> float:
+        return self.finished - self.arrival
+
+
+class CampaignServer:
+    def __init__(self, libraries: dict, B0_ref_T: dict, hbm_budget_bytes: float = 150e9, storage: str = "brick_bf16",
+                 steps_per_epoch: int = 64, capacity: int = 1 << 26, max_jobs: int = 256, blocks_per_sm: int = 0,
+                 host_fields: dict = None, keep_cache: bool = False, device: int = 0):
+        """libraries: {library: {mode: FieldLibrary}} (brick storage);
+        B0_ref_T: {library: total-field mean |B|} (time reference of every mode);
+        host_fields: {library: {mode: (Bx, By, Bz) host arrays}} for fixed-mu injection."""
+        import torch
+
+        self.torch = torch
+        self.libraries = libraries
+        self.B0 = B0_ref_T
+        self.budget = float(hbm_budget_bytes)
+        self.K = int(steps_per_epoch)
+        self.batch = Batch(capacity, max_campaigns=max_jobs, storage=storage, steps_per_epoch=self.K,
+                           blocks_per_sm=blocks_per_sm, device=device)
+        self.device = torch.device("cuda", device)
+        self.side = torch.cuda.Stream(device=self.device)
+        self.side_ctx = _lib.Context(device)
+        self.host_fields = host_fields or {}
+        self.keep_cache = keep_cache
+        self.queue = []      # (job_id, spec, arrival)
+        self.active = {}     # job_id -> record
+        self.binning = {}    # job_id -> record (lag pairs running on the side stream)
+        self.results = []
+        self.used = 0.0
+        self.next_id = 0
+        self.epochs = 0
+
+    # ------------------------------------------------------------ admission
+    @staticmethod
+    def job_bytes(spec: JobSpec) -> float:
+        nsteps = int(round(spec.duration_gyroperiods * spec.steps_per_gyroperiod)) + 1
+        stride = spec.steps_per_gyroperiod // spec.saves_per_gyroperiod
+        nsave = (nsteps - 1) // stride + 1
+        n = spec.n_particles
+        return n * (2 * 49 + 49) + 4.0 * n * nsave + 64 * spec.n_lags * (spec.n_bins + 1)
+
+    def submit(self, spec: JobSpec, arrival: float = None) -> int:
+        jid = self.next_id
+        self.next_id += 1
+        self.queue.append((jid, spec, time.perf_counter() if arrival is None else arrival))
+        return jid
+
+    def _admit(self, jid, spec, arrival):
+        torch = self.torch
+        fl = self.libraries[spec.library][spec.mode]
+        g0 = energy_to_gamma(spec.energy_GeV)
+        Om = reference_Omega0(self.B0[spec.library], g0, Q_E, M_P)
+        dt = (2 * math.pi / spec.steps_per_gyroperiod) / Om
+        nsteps = int(round(spec.duration_gyroperiods * spec.steps_per_gyroperiod)) + 1
+        stride = spec.steps_per_gyroperiod // spec.saves_per_gyroperiod
+        nsave = (nsteps - 1) // stride + 1
+        B = None
+        if spec.injection.replace("-", "_") == "fixed_mu":
+            B = self.host_fields[spec.library][spec.mode]
+        st = init_particles(spec.n_particles, fl.grid, spec.energy_GeV, seed=spec.seed,
+                            injection_mode=spec.injection, mu0=spec.mu0, B=B)
+        cache = torch.empty((nsave, spec.n_particles), dtype=torch.float32, device=self.device)
+        cid = self.batch.add(fl, st, dt, nsteps, stride, cache=cache)
+        self.active[jid] = dict(spec=spec, cid=cid, cache=cache, nsteps=nsteps, nsave=nsave, arrival=arrival,
+                                admitted=time.perf_counter(), bytes=self.job_bytes(spec))
+        self.used += self.job_bytes(spec)
+
+    def admit(self) -> int:
+        n = 0
+        keep = []
+        for jid, spec, arrival in self.queue:
+            need = self.job_bytes(spec)
+            if not keep and self.used + need <= self.budget:
+                try:
+                    self._admit(jid, spec, arrival)
+                    n += 1
+                    continue
+                except _lib.PtError as e:  # no slot range free yet
+                    if e.code not in (-3, -6):
+                        raise
+            keep.append((jid, spec, arrival))
+        self.queue = keep
+        return n
+
+    # ------------------------------------------------------------ ticks
+    def _start_binning(self, jid, rec):
+        torch = self.torch
+        spec = rec["spec"]
+        done = torch.cuda.Event()
+        done.record()  # after the job's last epoch on the main stream
+        lags = log_spaced_lag_steps(rec["nsave"] - 1, spec.n_lags)
+        edges, _ = build_mu_edges_full(0.0, 1.0, spec.n_bins)
+        with torch.cuda.stream(self.side):
+            self.side.wait_event(done)
+            acc = S.new_dmumu_accumulators(len(lags), spec.n_bins, device=self.device)
+            d_lags = torch.as_tensor(lags, device=self.device)
+            d_edges = torch.as_tensor(edges, device=self.device)
+            self.side_ctx.use_stream(self.side)
+            cache = rec["cache"]
+            _lib.call("pt_dmumu_accumulate_device", self.side_ctx.handle, _lib.ptr(cache), spec.n_particles,
+                      rec["nsave"], 1, spec.n_particles, _lib.ptr(d_lags), len(lags), _lib.ptr(d_edges),
+                      spec.n_bins, S.START[spec.start_mode], 1,
+                      *[_lib.ptr(acc[k]) for k in ("dmumu_counts", "dmumu_sum_delta", "dmumu_sum_delta2",
+                                                   "particle_counts", "particle_means", "particle_m2s",
+                                                   "pair_sum_squares", "pair_counts")])
+            ev = torch.cuda.Event()
+            ev.record(self.side)
+        rec.update(acc=acc, lags=lags, edges=edges, ev=ev, keep=(d_lags, d_edges))
+        self.binning[jid] = rec
+
+    def tick(self):
+        """One scheduling step; returns the jobs finished in it."""
+        self.admit()
+        if self.active:
+            self.batch.run(1)
+            self.epochs += 1
+            for jid in list(self.active):
+                rec = self.active[jid]
+                # every job advances K steps per epoch from its admission
+                rec.setdefault("epochs", 0)
+                rec["epochs"] += 1
+                if rec["epochs"] * self.K >= rec["nsteps"]:
+                    del self.active[jid]
+                    self._start_binning(jid, rec)
+        out = []
+        for jid in list(self.binning):
+            rec = self.binning[jid]
+            if rec["ev"].query():
+                spec = rec["spec"]
+                res = JobResult(jid, spec, rec["arrival"], rec["admitted"], time.perf_counter(),
+                                spec.n_particles * (rec["nsteps"] - 1),
+                                {k: v.cpu().numpy() for k, v in rec["acc"].items()}, rec["lags"], rec["edges"],
+                                rec["cache"].cpu().numpy() if self.keep_cache else None)
+                self.batch.remove(rec["cid"])
+                self.used -= rec["bytes"]
+                del self.binning[jid]
+                self.results.append(res)
+                out.append(res)
+        return out
+
+    def idle(self) -> bool:
+        return not (self.queue or self.active or self.binning)
+
+    def run_until_idle(self, max_ticks: int = 10 ** 7):
+        for _ in range(max_ticks):
+            if self.idle():
+                break
+            if not self.active and not self.queue:
+                time.sleep(1e-4)
+            self.tick()
+        return self.results
+
+    def close(self):
+        self.batch.close()
+        self.side_ctx.close()
+
+
+def sample_jobs(n_jobs: int, rate_per_s: float, libraries, seed: int = 2026, n_range=(16_384, 8_388_608),
+                energy_range=(1.0, 300.0), duration_range=(10.0, 300.0)):
+    """A Poisson stream of jobs: arrival offsets (s) and specs, seeded by job index."""
+    rng = np.random.default_rng(seed)
+    t = np.cumsum(rng.exponential(1.0 / rate_per_s, size=n_jobs))
+    specs = []
+    for i in range(n_jobs):
+        lib = libraries[int(rng.integers(len(libraries)))]
+        mode = ("total", "alfven", "fast", "slow")[int(rng.integers(4))]
+        E = float(np.exp(rng.uniform(np.log(energy_range[0]), np.log(energy_range[1]))))
+        n = int(np.exp(rng.uniform(np.log(n_range[0]), np.log(n_range[1]))))
+        dur = float(rng.uniform(*duration_range))
+        inj = "isotropic" if rng.random() < 0.5 else "fixed_mu"
+        mu0 = float(rng.uniform(-1, 1))
+        specs.append(JobSpec(lib, mode, E, n, dur, inj, mu0, seed=1000 + i))
+    return t, specs

@@ -1,0 +1,152 @@
+"""Batched campaigns (pt_batch_*) on a B200.
+
+Every campaign's mu cache and final state must be bit-identical to the
+same campaign run alone through pt_push_advance_fast: the batch changes only
+which slot and which CTA a particle lands on, never its arithmetic.  That
+holds with the per-campaign brick sort, with CUDA-graph epochs, and when
+campaigns join and leave between epochs (continuous batching)."""
+import math
+
+import numpy as np
+import pytest
+
+from helpers import small_problem
+from particle_transport_b200 import runner as R
+from particle_transport_b200.batch import Batch, autotune
+from particle_transport_b200.fields import FieldLibrary
+from particle_transport_b200.particles import energy_to_gamma, init_particles
+from particle_transport_b200.time_units import reference_Omega0
+from particle_transport_b200 import fields as F
+
+pytestmark = pytest.mark.gpu
+
+
+def campaigns(torch, storage="brick_bf16"):
+    pa = small_problem(n=16, n_particles=1000, u_over_c=1e-4, seed=3)
+    pb = small_problem(n=16, n_particles=10, u_over_c=2e-4, seed=8)
+    fa = FieldLibrary(pa.fields, pa.grid, storage)
+    fb = FieldLibrary(pb.fields, pb.grid, storage)
+    out = []
+    for i, (fl, pbm, E, n, nsteps, stride) in enumerate([(fa, pa, 1.0, 1000, 301, 4), (fb, pb, 10.0, 700, 129, 8),
+                                                          (fa, pa, 3.0, 257, 200, 5), (fb, pb, 1.0, 3, 77, 1)]):
+        g0 = energy_to_gamma(E)
+        Om = reference_Omega0(pa.B0, g0, F.Q_E, F.M_P)
+        dt = (2 * math.pi / 64) / Om
+        st = init_particles(n, pbm.grid, E, seed=100 + i)
+        out.append(dict(field=fl, state=st, dt=dt, nsteps=nsteps, stride=stride))
+    return out
+
+
+def run_alone(torch, c):
+    ens = R.FastEnsemble(c["field"], c["state"], np.ones(len(c["state"]["x1"]), np.uint8))
+    nsave = R.n_saves(c["nsteps"], c["stride"])
+    cache = torch.full((nsave, ens.n), float("nan"), dtype=torch.float32, device="cuda")
+    ens.advance(R.push_params(c["dt"], c["nsteps"], c["stride"], cache="mu", precision="f32"), 0, c["nsteps"],
+                cache, 0, nsave)
+    st, al = ens.export()
+    torch.cuda.synchronize()
+    return cache.cpu().numpy(), {k: v.cpu().numpy() for k, v in st.items()}
+
+
+def new_cache(torch, c):
+    return torch.full((R.n_saves(c["nsteps"], c["stride"]), len(c["state"]["x1"])), float("nan"),
+                      dtype=torch.float32, device="cuda")
+
+
+@pytest.mark.parametrize("sort,graph,K", [(True, True, 64), (True, False, 32), (False, True, 50)])
+def test_batch_bit_identical_to_single_runs(cuda, sort, graph, K):
+    torch = cuda
+    cs = campaigns(torch)
+    ref = [run_alone(torch, c) for c in cs]
+    b = Batch(5000, max_campaigns=8, steps_per_epoch=K, sort=sort)
+    caches = [new_cache(torch, c) for c in cs]
+    ids = [b.add(c["field"], c["state"], c["dt"], c["nsteps"], c["stride"], cache=ch) for c, ch in zip(cs, caches)]
+    epochs = max(math.ceil(c["nsteps"] / K) for c in cs)
+    b.run(epochs, use_graph=graph)
+    for c, cid, ch, (mu_ref, st_ref) in zip(cs, ids, caches, ref):
+        assert b.step(cid) == c["nsteps"]
+        assert np.array_equal(ch.cpu().numpy(), mu_ref, equal_nan=True)
+        st, _ = b.export(cid)
+        for k in st:
+            assert np.array_equal(st[k].cpu().numpy(), st_ref[k]), k
+    b.close()
+
+
+def test_batch_join_and_leave(cuda):
+    torch = cuda
+    cs = campaigns(torch)
+    ref = [run_alone(torch, c) for c in cs]
+    b = Batch(1300, max_campaigns=3, steps_per_epoch=64)
+    caches = [new_cache(torch, c) for c in cs]
+    live = {}
+    live[0] = b.add(cs[0]["field"], cs[0]["state"], cs[0]["dt"], cs[0]["nsteps"], cs[0]["stride"], cache=caches[0])
+    b.run(2)
+    live[2] = b.add(cs[2]["field"], cs[2]["state"], cs[2]["dt"], cs[2]["nsteps"], cs[2]["stride"], cache=caches[2])
+    b.run(1)
+    live[3] = b.add(cs[3]["field"], cs[3]["state"], cs[3]["dt"], cs[3]["nsteps"], cs[3]["stride"], cache=caches[3])
+    finished = {}
+    pending = [1]
+    for _ in range(40):
+        b.run(1)
+        for j, cid in list(live.items()):
+            if b.done(cid):
+                st, _ = b.export(cid)
+                finished[j] = {k: v.cpu().numpy() for k, v in st.items()}
+                b.remove(cid)
+                del live[j]
+        # campaign 1 joins when slots free up (capacity 1300 < sum of all)
+        if pending:
+            try:
+                j = pending[0]
+                live[j] = b.add(cs[j]["field"], cs[j]["state"], cs[j]["dt"], cs[j]["nsteps"], cs[j]["stride"],
+                                cache=caches[j])
+                pending.pop()
+            except Exception:
+                pass
+        if not live and not pending:
+            break
+    assert sorted(finished) == [0, 1, 2, 3]
+    for j, (mu_ref, st_ref) in enumerate(ref):
+        assert np.array_equal(caches[j].cpu().numpy(), mu_ref, equal_nan=True), j
+        for k in st_ref:
+            assert np.array_equal(finished[j][k], st_ref[k]), (j, k)
+    b.close()
+
+
+def test_batch_ring_cache(cuda):
+    torch = cuda
+    c = campaigns(torch)[1]
+    mu_ref, _ = run_alone(torch, c)
+    b = Batch(1000, max_campaigns=2, steps_per_epoch=64)
+    ring = torch.full((5, len(c["state"]["x1"])), float("nan"), dtype=torch.float32, device="cuda")
+    cid = b.add(c["field"], c["state"], c["dt"], c["nsteps"], c["stride"], cache=ring, ring=True)
+    b.run(math.ceil(c["nsteps"] / 64))
+    nsave = mu_ref.shape[0]
+    got = ring.cpu().numpy()
+    for r in range(nsave - 5, nsave):
+        assert np.array_equal(got[r % 5], mu_ref[r], equal_nan=True)
+    b.close()
+
+
+def test_batch_rejects_bad_input(cuda):
+    torch = cuda
+    from particle_transport_b200._lib import PtError
+    c = campaigns(torch)[0]
+    b = Batch(100, max_campaigns=1)
+    with pytest.raises(PtError, match="no free slot"):
+        b.add(c["field"], c["state"], c["dt"], c["nsteps"], c["stride"])
+    fr = FieldLibrary(*[small_problem(n=8, n_particles=2).__dict__[k] for k in ("fields", "grid")], "ref_f64")
+    st = {k: v[:10] for k, v in c["state"].items()}
+    with pytest.raises(PtError, match="storage"):
+        b.add(fr, st, c["dt"], c["nsteps"], c["stride"])
+    b.close()
+
+
+def test_autotune_picks_a_candidate(cuda, tmp_path, monkeypatch):
+    torch = cuda
+    monkeypatch.setenv("PTB200_TUNE_CACHE", str(tmp_path))
+    cs = campaigns(torch)
+    best, timings = autotune(cs, "brick_bf16", 5000, epochs=1, candidates=((64, 2), (32, 1)))
+    assert best in ((64, 2), (32, 1)) and len(timings) == 2
+    best2, _ = autotune(cs, "brick_bf16", 5000, epochs=1, candidates=((64, 2), (32, 1)))
+    assert best2 == best  # served from the cache file
