@@ -59,13 +59,18 @@ def parse():
     ap.add_argument("--grid", type=int, default=512)
     ap.add_argument("--particles", type=int, default=16_777_216)
     ap.add_argument("--energy", type=float, default=10.0)
-    ap.add_argument("--storage", default="brick_bf16", choices=["brick_bf16", "brick_f32"])
+    ap.add_argument("--storage", default="brick_bf16", choices=["brick_bf16", "brick_bf16x", "brick_f32"])
     ap.add_argument("--sort-every", type=int, default=64, help="re-sort particles by brick every N pushes (0: never)")
     ap.add_argument("--variant", type=int, default=1, help="push launch shape (pt_push_params.kernel_variant)")
     ap.add_argument("--lag-particles", type=int, default=1_048_576)
     ap.add_argument("--e2e-gyroperiods", type=int, default=8)
     ap.add_argument("--skip", default="", help="comma list of legs to skip: fp64,lag,e2e,cpu,batch,serve")
     ap.add_argument("--cpu-seconds", type=float, default=10.0)
+    ap.add_argument("--precision", action="store_true",
+                    help="run only the plain-vs-precision study (256^3, 3 energies) and print its JSON line")
+    ap.add_argument("--precision-grid", type=int, default=256)
+    ap.add_argument("--precision-particles", type=int, default=1_048_576)
+    ap.add_argument("--precision-gyroperiods", type=int, default=200)
     return ap.parse_args()
 
 
@@ -573,6 +578,165 @@ def run_batched(args, dev, rank):
                               "T_g0": (c["nsteps"] - 1) / 64} for c in camps]}
 
 
+def run_precision(args, dev):
+    """Plain vs precision forms at 256^3 (total field, dB/B0 = 0.5, k = 2..128,
+    u_rms = 1e-4 c): 1,048,576 protons per energy at 1, 10 and 100 GeV,
+    fixed mu0 = 0.5 with random gyrophase, 128 steps per T_g0 for 200 T_g0
+    (25,600 pushes), mu cache every 8 steps (3201 saves).  Each energy is
+    pushed in FP64 over the reference layout and as the FP32 push over FP32
+    and BF16 bricks; each product's error against the FP64 form is reported:
+    trajectory deviation (first 65,536 particles, phase-space cache, in
+    gyroradii, at 1 and 10 T_g0), |dgamma|/gamma at the end, mu at 10 T_g0,
+    D_mumu(mu, tau) and <dmu^2>(tau) (32 log lags x 20 |mu| bins, cells with
+    >= 100 pairs) and D_pp(tau) (same lags, all particles).  An FP64 run from
+    positions moved by one ulp gives the floor set by chaotic divergence: the
+    statistics of two FP64 runs differ by that much already."""
+    import torch
+
+    from particle_transport_b200 import fields as F
+    from particle_transport_b200 import runner as R
+    from particle_transport_b200 import stats as S
+    from particle_transport_b200.fields import FieldLibrary
+    from particle_transport_b200.particles import energy_to_gamma, init_particles
+    from particle_transport_b200.time_units import build_mu_edges_full, log_spaced_lag_steps, reference_Omega0
+
+    n = args.precision_grid
+    npart = args.precision_particles
+    nsub = min(65536, npart)
+    ps_chunk = 262144
+    spg, dur, stride = 128, args.precision_gyroperiods, 8
+    nsteps = spg * dur + 1
+    nsave = (nsteps - 1) // stride + 1
+    rg1 = F.gyroradius_m(1.0, 1e-10)
+    grid = F.build_uniform_grid((n - 1) * rg1, n, n, n)
+    L = grid.xmax - grid.xmin
+    fields = F.to_si(F.synthetic_mhd_fields(n, 2, n // 2, 0.5, 1.0, 1e-4, seed=5, spectrum="isotropic", device=dev))
+    B0 = F.reference_B0_T(*fields[:3])
+    hostB = [f.cpu().numpy() for f in fields[:3]]
+    libs = {"f64": FieldLibrary(fields, grid, "ref_f64"), "f32": FieldLibrary(fields, grid, "brick_f32", B_ref_T=B0),
+            "bf16": FieldLibrary(fields, grid, "brick_bf16x", B_ref_T=B0)}
+    del fields
+    lags = log_spaced_lag_steps(nsave - 1, 32)
+    edges, _ = build_mu_edges_full(0.0, 1.0, 20)
+    tau = np.array([l * stride * 2 * math.pi / spg for l in lags])
+    out = {"grid": n, "field": "total, dB/B0=0.5, k=2..128, u_rms=1e-4 c", "particles_per_energy": npart,
+           "trajectory_subset": nsub, "steps_per_gyroperiod": spg, "gyroperiods": dur, "save_stride": stride,
+           "saves": nsave, "lags": int(len(lags)), "mu_bins": 20, "min_count_per_cell": 100,
+           "bf16_storage": "brick_bf16x", "energies": {}}
+
+    def run(form, st, dt, cache_mode, c0, c1):
+        count = c1 - c0
+        sub = {k: np.ascontiguousarray(v[c0:c1]) for k, v in st.items()}
+        shape = (nsave, count) if cache_mode == "mu" else (nsave, 6, count)
+        cache = torch.empty(shape, dtype=torch.float32, device=dev)
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        if form.startswith("f64"):
+            ens = R.DeviceEnsemble(libs["f64"], sub, np.ones(count, np.uint8))
+            ens.advance(R.push_params(dt, nsteps, stride, cache=cache_mode, precision="f64", steps_per_launch=64),
+                        0, nsteps, cache, 0, nsave)
+            torch.cuda.synchronize()
+            final = {k: v.cpu().numpy() for k, v in ens.state.items()}
+        else:
+            ens = R.FastEnsemble(libs[form], sub, np.ones(count, np.uint8))
+            ens.advance(R.push_params(dt, nsteps, stride, cache=cache_mode, precision="f32", sort_every=64,
+                                      kernel_variant=1), 0, nsteps, cache, 0, nsave)
+            st_out, _ = ens.export()
+            torch.cuda.synchronize()
+            final = {k: v.cpu().numpy() for k, v in st_out.items()}
+            ens.close()
+        return cache, final, time.perf_counter() - t0
+
+    def dmumu(mu):
+        acc = S.new_dmumu_accumulators(len(lags), 20, device=dev)
+        S.process_mu_chunk_dmumu(mu, lags, edges, acc["particle_counts"], acc["particle_means"],
+                                 acc["particle_m2s"], acc["pair_sum_squares"], acc["pair_counts"],
+                                 acc["dmumu_counts"], acc["dmumu_sum_delta"], acc["dmumu_sum_delta2"],
+                                 layout="particle_fastest")
+        a = {k: v.cpu().numpy() for k, v in acc.items()}
+        d = S.compute_dmumu_arrays_full(a["dmumu_counts"], a["dmumu_sum_delta"], a["dmumu_sum_delta2"], tau, tau, 100)
+        return d["dmumu_raw_norm"], a["particle_means"], a["dmumu_counts"]
+
+    def phase_space(form, st, dt, p0):
+        """D_pp over all particles from phase-space caches of ps_chunk
+        particles (add-into accumulators, p0 fixed across chunks), plus the
+        positions of the first nsub particles at 1 and 10 T_g0."""
+        acc = S.new_dpp_accumulators(len(lags), device=dev)
+        rows = {}
+        for c0 in range(0, npart, ps_chunk):
+            ps, _, _ = run(form, st, dt, "phase_space", c0, min(npart, c0 + ps_chunk))
+            if p0 is None:
+                p0 = float(torch.linalg.vector_norm(ps[0, 3:6, 0].double()).item())
+            if c0 == 0:
+                for t in (1, 10):
+                    rows[t] = ps[t * spg // stride, 0:3, :nsub].double().cpu().numpy()
+            mom = ps[:, 3:6, :].contiguous()
+            del ps
+            S.process_momenta_chunk_dpp(mom, lags, p0, acc["counts"], acc["sum_delta_p"], acc["sum_delta_p2"],
+                                        acc["sum_delta_p_norm"], acc["sum_delta_p_norm2"])
+            del mom
+        a = {k: v.cpu().numpy() for k, v in acc.items()}
+        d = S.compute_dpp_arrays(a["counts"], a["sum_delta_p"], a["sum_delta_p2"], a["sum_delta_p_norm"],
+                                 a["sum_delta_p_norm2"], tau, tau)
+        return d["dpp_raw_norm"], rows, p0
+
+    def rel(a, b, w=None):
+        m = np.isfinite(a) & np.isfinite(b) & (np.abs(b) > 0)
+        r = np.abs(a[m] - b[m]) / np.abs(b[m])
+        res = {"median": float(np.median(r)), "max": float(r.max()), "cells": int(m.sum())}
+        if w is not None:
+            res["count_weighted_mean"] = float(np.sum(r * w[m]) / np.sum(w[m]))
+        return res
+
+    def traj_dev(xa, xb, rg):
+        d = xa - xb
+        d -= L * np.round(d / L)  # minimum image across the periodic box
+        r = np.sqrt((d * d).sum(axis=0)) / rg
+        return {"median_rg": float(np.median(r)), "p99_rg": float(np.percentile(r, 99)), "max_rg": float(r.max())}
+
+    for E in (1.0, 10.0, 100.0):
+        g0 = energy_to_gamma(E)
+        rgE = F.gyroradius_m(E, B0)
+        dt = (2 * math.pi / spg) / reference_Omega0(B0, g0, F.Q_E, F.M_P)
+        st = init_particles(npart, grid, E, seed=int(E) + 7, injection_mode="fixed_mu", mu0=0.5, B=hostB)
+        # noise floor: the FP64 push from positions moved by one ulp
+        st_pert = dict(st, x1=np.nextafter(st["x1"], np.inf))
+        res = {}
+        p0 = None
+        for form in ("f64", "f64_1ulp", "f32", "bf16"):
+            mu, final, secs = run(form, st_pert if form == "f64_1ulp" else st, dt, "mu", 0, npart)
+            D, pmean, counts = dmumu(mu)
+            mu10 = mu[10 * spg // stride].cpu().numpy()
+            del mu
+            torch.cuda.empty_cache()
+            Dpp, rows, p0 = phase_space(form, st_pert if form == "f64_1ulp" else st, dt, p0)
+            p = np.stack([final[k] for k in ("p1", "p2", "p3")])
+            gam = np.sqrt(1 + (np.linalg.norm(p, axis=0) / (F.M_P * F.C_LIGHT)) ** 2)
+            res[form] = dict(D=D, pm=pmean, counts=counts, Dpp=Dpp, rows=rows, gam=gam, mu10=mu10,
+                             rate=npart * (nsteps - 1) / secs, secs=secs)
+            torch.cuda.empty_cache()
+        ref = res["f64"]
+        e = {"f64_particle_steps_per_s": ref["rate"], "f64_s": ref["secs"],
+             "gamma_drift_f64_end": float(np.median(np.abs(ref["gam"] / g0 - 1)))}
+        for form in ("f64_1ulp", "f32", "bf16"):
+            r = res[form]
+            dmu = np.abs(r["mu10"] - ref["mu10"])
+            dmu = dmu[np.isfinite(dmu)]
+            e[form] = {"particle_steps_per_s": r["rate"], "s": r["secs"], "speedup_vs_f64": r["rate"] / ref["rate"],
+                       "trajectory_1_Tg0": traj_dev(r["rows"][1], ref["rows"][1], rgE),
+                       "trajectory_10_Tg0": traj_dev(r["rows"][10], ref["rows"][10], rgE),
+                       "mu_abs_err_10_Tg0": {"median": float(np.median(dmu)), "p99": float(np.percentile(dmu, 99))},
+                       "gamma_rel_err_end": {"median": float(np.median(np.abs(r["gam"] / ref["gam"] - 1))),
+                                             "max": float(np.max(np.abs(r["gam"] / ref["gam"] - 1)))},
+                       "D_mumu_raw_norm_rel_err": rel(r["D"], ref["D"], ref["counts"].astype(np.float64)),
+                       "delta_mu2_particle_mean_rel_err": rel(r["pm"], ref["pm"]),
+                       "D_pp_raw_norm_rel_err": rel(r["Dpp"], ref["Dpp"])}
+        out["energies"][f"{E:g}"] = e
+        print(json.dumps({"precision_energy_GeV": E, **e}), flush=True)
+        torch.cuda.empty_cache()
+    return out
+
+
 def run_serving(args, dev, n_jobs=16, rate=4.0):
     """Serving: a Poisson stream (mean 4 jobs/s) of transport jobs against
     resident 256^3 and 512^3 BF16 libraries (4 modes each), admitted against a
@@ -642,6 +806,11 @@ def main():
         ws = int(os.environ.get("WORLD_SIZE", "1"))
         if int(os.environ.get("RANK", "0")) == 0:
             run_reference(args, ws, 0)
+        return
+    if args.precision:
+        import torch
+        out = run_precision(args, torch.device("cuda", 0))
+        print(json.dumps({"precision_study": out}), flush=True)
         return
     ws, rank, local = dist_setup(args)
     try:

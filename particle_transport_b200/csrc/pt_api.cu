@@ -130,7 +130,8 @@ int field_create(pt_ctx* ctx, const double* const comps[6], bool on_device, cons
     if (rc) return rc;
     for (int c = 0; c < 6; ++c)
         if (!comps[c]) return fail(PT_ERR_ARG, "field component is null");
-    if (storage < PT_FIELD_REF_F64 || storage > PT_FIELD_BRICK_BF16) return fail(PT_ERR_ARG, "unknown field storage");
+    if (storage < PT_FIELD_REF_F64 || storage > PT_FIELD_BRICK_BF16_XPAIR)
+        return fail(PT_ERR_ARG, "unknown field storage");
     if (storage != PT_FIELD_REF_F64 && !(B_ref > 0 && std::isfinite(B_ref)))
         return fail(PT_ERR_ARG, "B_ref_T must be finite and positive for brick storage");
     if (grid->nx > 4096 || grid->ny > 4096 || grid->nz > 4096) return fail(PT_ERR_ARG, "grid axis above 4096 nodes");
@@ -176,7 +177,7 @@ int field_create(pt_ctx* ctx, const double* const comps[6], bool on_device, cons
     }
     std::vector<uint32_t> offs;
     brick_offsets(*grid, offs, f->n_nodes);
-    const size_t node_bytes = storage == PT_FIELD_BRICK_BF16 ? 16 : 32;
+    const size_t node_bytes = record_bytes(storage);
     cudaError_t e = cudaMalloc(&f->nodes, node_bytes * (size_t)f->n_nodes);
     if (e == cudaSuccess) e = cudaMalloc((void**)&f->offs, sizeof(uint32_t) * offs.size());
     if (e != cudaSuccess) {
@@ -193,7 +194,7 @@ int field_create(pt_ctx* ctx, const double* const comps[6], bool on_device, cons
     }
     const double* src[6];
     for (int c = 0; c < 6; ++c) src[c] = on_device ? comps[c] : tmp[c];
-    rc = launch_brick_convert(src, *grid, B_ref, storage == PT_FIELD_BRICK_BF16, f->nodes, f->offs, s);
+    rc = launch_brick_convert(src, *grid, B_ref, field_layout(storage), f->nodes, f->offs, s);
     e = cudaStreamSynchronize(s);
     for (int c = 0; c < 6; ++c) if (tmp[c]) cudaFree(tmp[c]);
     if (rc) return cleanup(rc);
@@ -224,7 +225,8 @@ PushArgsFast fast_args(const pt_field* f, pt_fast_state* st, const pt_push_param
     a.fld.nodes = f->nodes;
     a.fld.offs = f->offs;
     a.fld.nx = g.nx; a.fld.ny = g.ny; a.fld.nz = g.nz;
-    a.fld.bf16 = f->storage == PT_FIELD_BRICK_BF16;
+    a.fld.bf16 = f->storage != PT_FIELD_BRICK_F32;
+    a.fld.layout = field_layout(f->storage);
     a.wx = (g.xmax - g.xmin) / g.dx;
     a.wy = (g.ymax - g.ymin) / g.dy;
     a.wz = (g.zmax - g.zmin) / g.dz;

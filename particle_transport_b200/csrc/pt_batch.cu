@@ -141,7 +141,7 @@ int enqueue_epoch(pt_batch* b, cudaStream_t s)
         cur = 1 - cur;
     }
     BatchLaunch L{b->d_camps, b->d_tiles, b->d_ntiles, b->d_counter, b->buf[cur],
-                  b->storage == PT_FIELD_BRICK_BF16, b->smem_words, b->grid};
+                  field_layout(b->storage), b->smem_words, b->grid};
     int rc = launch_push_batch(L, s);
     if (rc) return rc;
     return launch_batch_epoch_end(b->d_camps, b->max_camps, b->d_counter, s);
@@ -177,7 +177,7 @@ int pt_batch_create(pt_ctx* ctx, int64_t capacity, int max_campaigns, int storag
     if (!ctx || !out) return fail(PT_ERR_ARG, "null argument");
     if (capacity < 1 || capacity > INT32_MAX) return fail(PT_ERR_ARG, "capacity must be in [1, 2^31)");
     if (max_campaigns < 1 || max_campaigns > 4096) return fail(PT_ERR_ARG, "max_campaigns must be in [1, 4096]");
-    if (storage != PT_FIELD_BRICK_BF16 && storage != PT_FIELD_BRICK_F32)
+    if (storage != PT_FIELD_BRICK_BF16 && storage != PT_FIELD_BRICK_F32 && storage != PT_FIELD_BRICK_BF16_XPAIR)
         return fail(PT_ERR_ARG, "batches run the FP32 push: storage must be a brick form");
     if (steps_per_epoch < 1) return fail(PT_ERR_ARG, "steps_per_epoch must be >= 1");
     PT_CUDA(cudaSetDevice(ctx->device));
@@ -278,7 +278,8 @@ int pt_batch_add(pt_ctx* ctx, pt_batch* b, const pt_campaign_desc* d, int* id)
     a.fld.nodes = f->nodes;
     a.fld.offs = f->offs;
     a.fld.nx = g.nx; a.fld.ny = g.ny; a.fld.nz = g.nz;
-    a.fld.bf16 = f->storage == PT_FIELD_BRICK_BF16;
+    a.fld.bf16 = f->storage != PT_FIELD_BRICK_F32;
+    a.fld.layout = field_layout(f->storage);
     a.wx = (g.xmax - g.xmin) / g.dx;
     a.wy = (g.ymax - g.ymin) / g.dy;
     a.wz = (g.zmax - g.zmin) / g.dz;

@@ -111,11 +111,24 @@ struct PushArgsRef {
 };
 int launch_push_ref(const PushArgsRef& a, cudaStream_t s);
 
+// node record layouts of the brick forms
+enum { LAYOUT_BF16 = 0, LAYOUT_F32 = 1, LAYOUT_BF16_XPAIR = 2 };
+inline int field_layout(int storage)
+{
+    return storage == PT_FIELD_BRICK_F32 ? LAYOUT_F32 : (storage == PT_FIELD_BRICK_BF16_XPAIR ? LAYOUT_BF16_XPAIR
+                                                                                               : LAYOUT_BF16);
+}
+inline size_t record_bytes(int storage)
+{
+    return storage == PT_FIELD_BRICK_BF16 ? 16 : 32;
+}
+
 struct FieldArgsBrick {
     const void* nodes;
     const uint32_t* offs;
     int64_t nx, ny, nz;
-    int bf16;
+    int bf16;    // 1 for the BF16 forms
+    int layout;  // LAYOUT_*
 };
 struct PushArgsFast {
     FieldArgsBrick fld;
@@ -173,7 +186,7 @@ struct BatchLaunch {
     const int* n_tiles;
     int* tile_counter;
     BatchStateDev st;
-    int bf16;
+    int layout;        // LAYOUT_* shared by the batch's fields
     int smem_words;    // max (nx + ny + nz) over the batch's fields
     int grid;
 };
@@ -193,7 +206,7 @@ int launch_fast_export(const pt_fast_state* st, const pt_field* f, double* x1, d
                        double* p2, double* p3, uint8_t* alive, cudaStream_t s);
 int fast_sort(pt_ctx* ctx, pt_fast_state* st, const pt_field* f, cudaStream_t s);
 
-int launch_brick_convert(const double* const comps[6], const pt_grid& g, double B_ref, int bf16, void* nodes,
+int launch_brick_convert(const double* const comps[6], const pt_grid& g, double B_ref, int layout, void* nodes,
                          const uint32_t* offs, cudaStream_t s);
 
 struct DmumuArgs {

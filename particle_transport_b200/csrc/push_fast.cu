@@ -49,12 +49,59 @@ __device__ __forceinline__ Corners locate_brick(double x, double y, double z, co
     return c;
 }
 
-template <bool BF16>
+// 32-byte read-only load (sm_100 256-bit vector load; the address is 32-byte aligned)
+__device__ __forceinline__ void ldg256(const void* p, uint32_t w[8])
+{
+    asm volatile("ld.global.nc.v8.u32 {%0, %1, %2, %3, %4, %5, %6, %7}, [%8];"
+                 : "=r"(w[0]), "=r"(w[1]), "=r"(w[2]), "=r"(w[3]), "=r"(w[4]), "=r"(w[5]), "=r"(w[6]), "=r"(w[7])
+                 : "l"(p));
+}
+
+__device__ __forceinline__ void acc_bf16x3(float f[6], float w, uint32_t a, uint32_t b, uint32_t c)
+{
+    f[0] = fmaf(w, bf_lo(a), f[0]);
+    f[1] = fmaf(w, bf_hi(a), f[1]);
+    f[2] = fmaf(w, bf_lo(b), f[2]);
+    f[3] = fmaf(w, bf_hi(b), f[3]);
+    f[4] = fmaf(w, bf_lo(c), f[4]);
+    f[5] = fmaf(w, bf_hi(c), f[5]);
+}
+
+// Interpolate the six components at a cell: 8 weighted corners.
+//  LAYOUT_BF16        16-byte node (Bx,By | Bz,ux | uy,uz | pad), 8 x 16-byte loads
+//  LAYOUT_F32         32-byte node (Bx,By,Bz,ux,uy,uz,pad,pad), 8 x 32-byte loads
+//  LAYOUT_BF16_XPAIR  32-byte record = node (i) + node (i+1), 4 x 32-byte loads
+template <int LAYOUT>
 __device__ __forceinline__ void gather6(const void* __restrict__ nodes, const Corners& c, float f[6])
 {
 #pragma unroll
     for (int k = 0; k < 6; ++k) f[k] = 0.0f;
-    if (BF16) {
+    if (LAYOUT == LAYOUT_F32) {
+        const char* N = (const char*)nodes;
+        uint32_t v[8][8];
+#pragma unroll
+        for (int q = 0; q < 8; ++q) ldg256(N + 32 * (size_t)c.idx[q], v[q]);
+#pragma unroll
+        for (int q = 0; q < 8; ++q) {
+            const float w = c.w[q];
+#pragma unroll
+            for (int k = 0; k < 6; ++k) f[k] = fmaf(w, __uint_as_float(v[q][k]), f[k]);
+        }
+        return;
+    }
+    if (LAYOUT == LAYOUT_BF16_XPAIR) {
+        const char* N = (const char*)nodes;
+        uint32_t v[4][8];
+#pragma unroll
+        for (int q = 0; q < 4; ++q) ldg256(N + 32 * (size_t)c.idx[2 * q], v[q]);
+#pragma unroll
+        for (int q = 0; q < 4; ++q) {
+            acc_bf16x3(f, c.w[2 * q], v[q][0], v[q][1], v[q][2]);
+            acc_bf16x3(f, c.w[2 * q + 1], v[q][3], v[q][4], v[q][5]);
+        }
+        return;
+    }
+    {
         const uint4* N = (const uint4*)nodes;
         uint4 v[8];
 #pragma unroll
@@ -68,24 +115,6 @@ __device__ __forceinline__ void gather6(const void* __restrict__ nodes, const Co
             f[3] = fmaf(w, bf_hi(v[q].y), f[3]);
             f[4] = fmaf(w, bf_lo(v[q].z), f[4]);
             f[5] = fmaf(w, bf_hi(v[q].z), f[5]);
-        }
-    } else {
-        const float4* N = (const float4*)nodes;
-        float4 va[8], vb[8];
-#pragma unroll
-        for (int q = 0; q < 8; ++q) {
-            va[q] = __ldg(N + 2 * (size_t)c.idx[q]);
-            vb[q] = __ldg(N + 2 * (size_t)c.idx[q] + 1);
-        }
-#pragma unroll
-        for (int q = 0; q < 8; ++q) {
-            const float w = c.w[q];
-            f[0] = fmaf(w, va[q].x, f[0]);
-            f[1] = fmaf(w, va[q].y, f[1]);
-            f[2] = fmaf(w, va[q].z, f[2]);
-            f[3] = fmaf(w, va[q].w, f[3]);
-            f[4] = fmaf(w, vb[q].x, f[4]);
-            f[5] = fmaf(w, vb[q].y, f[5]);
         }
     }
 }
@@ -111,7 +140,7 @@ __device__ __forceinline__ double wrap_cells(double x, double w)
 // (FP64), p/(mc) (FP32) and |p/(mc)|^2 (FP64); pid indexes the cache row.
 // Cache rows of a.n_cache particles: row r at (r - a.row_base) or, with
 // a.ring, at (r % a.rows).
-template <bool BF16>
+template <int LAYOUT>
 __device__ __forceinline__ void advance_particle(double& x, double& y, double& z, float& px, float& py, float& pz,
                                                  double& P2, bool& al, const int64_t pid, const PushArgsFast& a,
                                                  const uint32_t* ox, const uint32_t* oy, const uint32_t* oz,
@@ -135,7 +164,7 @@ __device__ __forceinline__ void advance_particle(double& x, double& y, double& z
             float f[6] = {0, 0, 0, 0, 0, 0};
             if (al && (do_push || (is_save && a.cache_mode == PT_CACHE_MU))) {
                 Corners c = locate_brick(x, y, z, ox, oy, oz, nx, ny, nz);
-                gather6<BF16>(a.fld.nodes, c, f);
+                gather6<LAYOUT>(a.fld.nodes, c, f);
             }
             if (is_save) {
                 const int64_t r = a.ring ? row % a.rows : row - a.row_base;
@@ -206,7 +235,7 @@ __device__ __forceinline__ void advance_particle(double& x, double& y, double& z
     }
 }
 
-template <bool BF16, int BLOCK, int MINB>
+template <int LAYOUT, int BLOCK, int MINB>
 __global__ void __launch_bounds__(BLOCK, MINB) push_fast_kernel(PushArgsFast a)
 {
     extern __shared__ uint32_t s_offs[];
@@ -224,7 +253,7 @@ __global__ void __launch_bounds__(BLOCK, MINB) push_fast_kernel(PushArgsFast a)
         float px = a.p[slot], py = a.p[n + slot], pz = a.p[2 * n + slot];
         double P2 = a.p2[slot];
         bool al = a.alive[slot] != 0;
-        advance_particle<BF16>(x, y, z, px, py, pz, P2, al, a.pid[slot], a, ox, oy, oz, a.step_begin, s_end);
+        advance_particle<LAYOUT>(x, y, z, px, py, pz, P2, al, a.pid[slot], a, ox, oy, oz, a.step_begin, s_end);
         a.x[slot] = x; a.x[n + slot] = y; a.x[2 * n + slot] = z;
         a.p[slot] = px; a.p[n + slot] = py; a.p[2 * n + slot] = pz;
         a.p2[slot] = P2;
@@ -236,24 +265,42 @@ __global__ void __launch_bounds__(BLOCK, MINB) push_fast_kernel(PushArgsFast a)
 __global__ void brick_convert_kernel(const double* __restrict__ bx, const double* __restrict__ by,
                                      const double* __restrict__ bz, const double* __restrict__ ux,
                                      const double* __restrict__ uy, const double* __restrict__ uz, int64_t nx,
-                                     int64_t ny, int64_t nz, double inv_b, double inv_c, int bf16, void* nodes,
+                                     int64_t ny, int64_t nz, double inv_b, double inv_c, int layout, void* nodes,
                                      const uint32_t* __restrict__ offs)
 {
     const int64_t total = nx * ny * nz;
+    auto comps = [&](int64_t t, float v[6]) {
+        v[0] = (float)(bx[t] * inv_b); v[1] = (float)(by[t] * inv_b); v[2] = (float)(bz[t] * inv_b);
+        v[3] = (float)(ux[t] * inv_c); v[4] = (float)(uy[t] * inv_c); v[5] = (float)(uz[t] * inv_c);
+    };
+    auto pack3 = [](const float v[6], uint32_t w[3]) {
+        for (int q = 0; q < 3; ++q) {
+            const uint32_t lo = __bfloat16_as_ushort(__float2bfloat16_rn(v[2 * q]));
+            const uint32_t hi = __bfloat16_as_ushort(__float2bfloat16_rn(v[2 * q + 1]));
+            w[q] = lo | (hi << 16);
+        }
+    };
     for (int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; t < total;
          t += (int64_t)gridDim.x * blockDim.x) {
         const int64_t i = t % nx, j = (t / nx) % ny, k = t / (nx * ny);
         const uint32_t node = offs[i] + offs[nx + j] + offs[nx + ny + k];
-        float v[6] = {(float)(bx[t] * inv_b), (float)(by[t] * inv_b), (float)(bz[t] * inv_b),
-                      (float)(ux[t] * inv_c), (float)(uy[t] * inv_c), (float)(uz[t] * inv_c)};
-        if (bf16) {
+        float v[6];
+        comps(t, v);
+        if (layout == LAYOUT_BF16) {
             uint32_t w[3];
-            for (int q = 0; q < 3; ++q) {
-                const uint32_t lo = __bfloat16_as_ushort(__float2bfloat16_rn(v[2 * q]));
-                const uint32_t hi = __bfloat16_as_ushort(__float2bfloat16_rn(v[2 * q + 1]));
-                w[q] = lo | (hi << 16);
-            }
+            pack3(v, w);
             ((uint4*)nodes)[node] = make_uint4(w[0], w[1], w[2], 0u);
+        } else if (layout == LAYOUT_BF16_XPAIR) {
+            uint32_t w[3], w2[3] = {0u, 0u, 0u};
+            pack3(v, w);
+            if (i + 1 < nx) {
+                float v2[6];
+                comps(t + 1, v2);
+                pack3(v2, w2);
+            }
+            uint4* N = (uint4*)nodes;
+            N[2 * (size_t)node] = make_uint4(w[0], w[1], w[2], w2[0]);
+            N[2 * (size_t)node + 1] = make_uint4(w2[1], w2[2], 0u, 0u);
         } else {
             float4* N = (float4*)nodes;
             N[2 * (size_t)node] = make_float4(v[0], v[1], v[2], v[3]);
@@ -400,14 +447,14 @@ int grid_for(int64_t n, int threads, int num_sms)
 
 // Persistent launch: (SM count) x (resident blocks per SM, optionally capped).
 // The gather is cache-bound, so fewer resident warps can win (less L1 churn).
-template <bool BF16, int BLOCK, int MINB>
+template <int LAYOUT, int BLOCK, int MINB>
 int launch_push_fast_shape(const PushArgsFast& a, cudaStream_t s, int cap_per_sm = 0)
 {
     const size_t smem = sizeof(uint32_t) * (size_t)(a.fld.nx + a.fld.ny + a.fld.nz);
     int dev = 0, sms = 148, per_sm = 1;
     cudaGetDevice(&dev);
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-    auto kfn = push_fast_kernel<BF16, BLOCK, MINB>;
+    auto kfn = push_fast_kernel<LAYOUT, BLOCK, MINB>;
     if (smem > 48 * 1024) PT_CUDA(cudaFuncSetAttribute(kfn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
     cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kfn, BLOCK, smem);
     per_sm = std::max(per_sm, 1);
@@ -418,37 +465,41 @@ int launch_push_fast_shape(const PushArgsFast& a, cudaStream_t s, int cap_per_sm
     return PT_OK;
 }
 
-template <bool BF16>
+template <int LAYOUT>
 int launch_push_fast_t(const PushArgsFast& a, cudaStream_t s)
 {
     switch (a.variant) {
-    case 2: return launch_push_fast_shape<BF16, 256, 4>(a, s);
-    case 3: return launch_push_fast_shape<BF16, 128, 8>(a, s);
-    case 4: return launch_push_fast_shape<BF16, 512, 2>(a, s);
-    case 5: return launch_push_fast_shape<BF16, 256, 1>(a, s, 1);
-    case 6: return launch_push_fast_shape<BF16, 512, 1>(a, s, 1);
-    case 7: return launch_push_fast_shape<BF16, 128, 1>(a, s, 3);
-    case 8: return launch_push_fast_shape<BF16, 128, 1>(a, s, 2);
+    case 2: return launch_push_fast_shape<LAYOUT,256, 4>(a, s);
+    case 3: return launch_push_fast_shape<LAYOUT,128, 8>(a, s);
+    case 4: return launch_push_fast_shape<LAYOUT,512, 2>(a, s);
+    case 5: return launch_push_fast_shape<LAYOUT,256, 1>(a, s, 1);
+    case 6: return launch_push_fast_shape<LAYOUT,512, 1>(a, s, 1);
+    case 7: return launch_push_fast_shape<LAYOUT,128, 1>(a, s, 3);
+    case 8: return launch_push_fast_shape<LAYOUT,128, 1>(a, s, 2);
     case 0:
     case 1:
-    default: return launch_push_fast_shape<BF16, 256, 1>(a, s);
+    default: return launch_push_fast_shape<LAYOUT,256, 1>(a, s);
     }
 }
 
 int launch_push_fast(const PushArgsFast& a, cudaStream_t s)
 {
     if (a.n <= 0 || a.step_count <= 0) return PT_OK;
-    return a.fld.bf16 ? launch_push_fast_t<true>(a, s) : launch_push_fast_t<false>(a, s);
+    switch (a.fld.layout) {
+    case LAYOUT_F32: return launch_push_fast_t<LAYOUT_F32>(a, s);
+    case LAYOUT_BF16_XPAIR: return launch_push_fast_t<LAYOUT_BF16_XPAIR>(a, s);
+    default: return launch_push_fast_t<LAYOUT_BF16>(a, s);
+    }
 }
 
-int launch_brick_convert(const double* const comps[6], const pt_grid& g, double B_ref, int bf16, void* nodes,
+int launch_brick_convert(const double* const comps[6], const pt_grid& g, double B_ref, int layout, void* nodes,
                          const uint32_t* offs, cudaStream_t s)
 {
     const int64_t total = g.nx * g.ny * g.nz;
     const int threads = 256;
     int blocks = (int)std::min<int64_t>((total + threads - 1) / threads, 148 * 32);
     brick_convert_kernel<<<blocks, threads, 0, s>>>(comps[0], comps[1], comps[2], comps[3], comps[4], comps[5],
-                                                    g.nx, g.ny, g.nz, 1.0 / B_ref, 1.0 / C_LIGHT, bf16, nodes, offs);
+                                                    g.nx, g.ny, g.nz, 1.0 / B_ref, 1.0 / C_LIGHT, layout, nodes, offs);
     PT_CHECK_LAUNCH("brick_convert_kernel");
     return PT_OK;
 }
@@ -544,7 +595,7 @@ namespace {
 // campaign changes, and runs K steps of its particles from the campaign's
 // device-resident step counter.  The per-particle arithmetic is
 // advance_particle, so a particle's trajectory is the same alone or batched.
-template <bool BF16>
+template <int LAYOUT>
 __global__ void __launch_bounds__(256, 1) push_batch_kernel(BatchLaunch L)
 {
     extern __shared__ uint32_t s_offs[];
@@ -594,7 +645,7 @@ __global__ void __launch_bounds__(256, 1) push_batch_kernel(BatchLaunch L)
             float px = L.st.p[slot], py = L.st.p[cap + slot], pz = L.st.p[2 * cap + slot];
             double P2 = L.st.p2[slot];
             bool al = L.st.alive[slot] != 0;
-            advance_particle<BF16>(x, y, z, px, py, pz, P2, al, L.st.pid[slot], s_a, ox, oy, oz, sb, se);
+            advance_particle<LAYOUT>(x, y, z, px, py, pz, P2, al, L.st.pid[slot], s_a, ox, oy, oz, sb, se);
             L.st.x[slot] = x; L.st.x[cap + slot] = y; L.st.x[2 * cap + slot] = z;
             L.st.p[slot] = px; L.st.p[cap + slot] = py; L.st.p[2 * cap + slot] = pz;
             L.st.p2[slot] = P2;
@@ -755,10 +806,13 @@ __global__ void batch_export_kernel(BatchStateDev st, int64_t slot0, int64_t n, 
 int launch_push_batch(const BatchLaunch& L, cudaStream_t s)
 {
     const size_t smem = sizeof(uint32_t) * (size_t)std::max(L.smem_words, 1);
-    void* kfn = L.bf16 ? (void*)push_batch_kernel<true> : (void*)push_batch_kernel<false>;
+    void* kfn = L.layout == LAYOUT_F32 ? (void*)push_batch_kernel<LAYOUT_F32>
+                : (L.layout == LAYOUT_BF16_XPAIR ? (void*)push_batch_kernel<LAYOUT_BF16_XPAIR>
+                                                 : (void*)push_batch_kernel<LAYOUT_BF16>);
     if (smem > 48 * 1024) PT_CUDA(cudaFuncSetAttribute(kfn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-    if (L.bf16) push_batch_kernel<true><<<L.grid, 256, smem, s>>>(L);
-    else push_batch_kernel<false><<<L.grid, 256, smem, s>>>(L);
+    if (L.layout == LAYOUT_F32) push_batch_kernel<LAYOUT_F32><<<L.grid, 256, smem, s>>>(L);
+    else if (L.layout == LAYOUT_BF16_XPAIR) push_batch_kernel<LAYOUT_BF16_XPAIR><<<L.grid, 256, smem, s>>>(L);
+    else push_batch_kernel<LAYOUT_BF16><<<L.grid, 256, smem, s>>>(L);
     PT_CHECK_LAUNCH("push_batch_kernel");
     return PT_OK;
 }

@@ -30,7 +30,7 @@ PC_TO_M = 3.085677581e16
 GEV_TO_J = 1e9 * 1.602176634e-19
 
 STORAGE = {"ref_f64": _lib.PT_FIELD_REF_F64, "brick_f32": _lib.PT_FIELD_BRICK_F32,
-           "brick_bf16": _lib.PT_FIELD_BRICK_BF16}
+           "brick_bf16": _lib.PT_FIELD_BRICK_BF16, "brick_bf16x": _lib.PT_FIELD_BRICK_BF16_XPAIR}
 
 
 @dataclass
