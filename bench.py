@@ -748,22 +748,21 @@ def run_serving(args, dev, n_jobs=16, rate=4.0):
     from particle_transport_b200.fields import FieldLibrary
     from particle_transport_b200.server import CampaignServer, sample_jobs
 
-    libs, B0, host = {}, {}, {}
+    libs, B0 = {}, {}
     for n in (256, 512):
         rg = F.gyroradius_m(1.0, 1e-10)
         grid = F.build_uniform_grid((n - 1) * rg, n, n, n)
-        libs[str(n)], host[str(n)] = {}, {}
+        libs[str(n)] = {}
         for m in ("total", "alfven", "fast", "slow"):
             f = F.to_si(F.synthetic_mhd_fields(n, 2, n // 2, 0.5 if n == 256 else 1.0, 1.0, 1e-4, seed=91 + n,
                                                spectrum="isotropic" if n == 256 else "gs", modes=m, device=dev))
             if m == "total":
                 B0[str(n)] = F.reference_B0_T(*f[:3])
             libs[str(n)][m] = FieldLibrary(f, grid, "brick_bf16", B_ref_T=B0[str(n)])
-            host[str(n)][m] = [x.cpu().numpy() for x in f[:3]]
             del f
         torch.cuda.empty_cache()
     arrivals, specs = sample_jobs(n_jobs, rate, ["256", "512"], seed=2026)
-    srv = CampaignServer(libs, B0, hbm_budget_bytes=150e9, capacity=1 << 27, max_jobs=n_jobs, host_fields=host)
+    srv = CampaignServer(libs, B0, hbm_budget_bytes=150e9, capacity=1 << 27, max_jobs=n_jobs)
     torch.cuda.synchronize()
     t_start = time.perf_counter()
     nxt = 0
@@ -776,11 +775,13 @@ def run_serving(args, dev, n_jobs=16, rate=4.0):
     wall = time.perf_counter() - t_start
     lat = np.array([r.latency for r in srv.results])
     steps = sum(r.particle_steps for r in srv.results)
+    busy = srv.device_busy_s()
     srv.close()
     return {"jobs": n_jobs, "rate_per_s": rate, "p50_s": float(np.percentile(lat, 50)),
             "p99_s": float(np.percentile(lat, 99)), "mean_s": float(lat.mean()), "wall_s": wall,
-            "particle_steps": int(steps), "aggregate_rate": steps / wall, "unit": UNIT, "push": "FP32 / BF16 bricks",
-            "hbm_budget_GB": 150, "epochs": srv.epochs}
+            "particle_steps": int(steps), "aggregate_rate": steps / wall, "device_busy_s": busy,
+            "busy_rate": steps / busy, "admit_host_s": srv.admit_s, "unit": UNIT, "push": "FP32 / BF16 bricks",
+            "init": "on the device (pt_particles_init_device)", "hbm_budget_GB": 150, "epochs": srv.epochs}
 
 
 def dist_barrier(ws):

@@ -313,6 +313,40 @@ int pt_energy_histogram_device(pt_ctx* ctx, const float* d_mom, int64_t chunk, i
 int pt_reconstruct_mu(pt_ctx* ctx, const void* pos, const void* mom, int64_t chunk, int64_t nsave,
                       const void* const bfield[3], const pt_grid* grid, int f64, void* mu_out);
 
+/*
+ * Initial particle state written on the device: the formulas of
+ * init_particles, rand_unit_vector and fixed_mu_unit_vector
+ * (src/phase_space_gpu_runner.jl:61-66, 170-245) -- uniform positions
+ * u (xmax - xmin) + xmin, isotropic directions (z = 2u - 1, phi = 2 pi u) or
+ * pitch cosine mu0 about the local B with a random gyrophase, |p| = gamma0 m v0
+ * (gamma0, v0 from the kinetic energy, src/phase_space_gpu_runner.jl:51-59).
+ * The reference draws from a Julia MersenneTwister, which is not restated:
+ * draw d of particle i here is the SplitMix64 output of counter 8 i + d + 1
+ * under the key mix64(seed), as a double (h >> 11) 2^-53.  Draws 0-2: the
+ * position (random mode); draw 3: z (isotropic) or phi (fixed mu); draw 4:
+ * phi (isotropic).  For fixed mu, B at the position is the trilinear sample
+ * of the field's own values (FP64 for PT_FIELD_REF_F64; the stored FP32/BF16
+ * values for bricks).  Positions are exact; momenta agree with a host
+ * restatement to the last bits of cos/sin.  Synchronous: returns PT_ERR_ARG
+ * ("cannot use fixed-mu injection where local B is zero or non-finite", as
+ * the reference) after the kernel if any particle met such a field.
+ * No reference counterpart as a C entry (the reference initialises on the
+ * host); it lets a serving loop admit jobs without host work.
+ */
+enum { PT_INJECT_ISOTROPIC = 0, PT_INJECT_FIXED_MU = 1 };
+enum { PT_POSITION_RANDOM = 0, PT_POSITION_FIXED = 1 };
+typedef struct pt_init_params {
+    int64_t n;
+    uint64_t seed;
+    double energy_GeV;   /* kinetic energy of every particle */
+    int32_t injection;   /* PT_INJECT_* */
+    int32_t position_mode; /* PT_POSITION_* */
+    double mu0;          /* fixed mu, in [-1, 1] */
+    double position[3];  /* PT_POSITION_FIXED: box fractions, in [0, 1] */
+} pt_init_params;
+int pt_particles_init_device(pt_ctx* ctx, const pt_field* field, const pt_init_params* params, double* d_x1,
+                             double* d_x2, double* d_x3, double* d_p1, double* d_p2, double* d_p3);
+
 #ifdef __cplusplus
 }
 #endif

@@ -62,6 +62,8 @@ def lib():
         L.or_kinetic_energy_gev.restype = d
         L.or_kinetic_energy_gev.argtypes = [d]
         L.or_num_threads.restype = i32
+        L.or_init_particles.restype = i64
+        L.or_init_particles.argtypes = [i64, C.c_uint64, d, i32, i32, d, P, P, C.POINTER(Grid), P, P, P, P, P, P]
         _lib = L
     return _lib
 
@@ -185,3 +187,20 @@ def energy_snapshots(mom, snap_steps, out, particle_offset=0):
     snaps = np.ascontiguousarray(snap_steps, dtype=np.int64)
     lib().or_energy_snapshots(_p(mom), chunk, nsave, _p(snaps), len(snaps), particle_offset, _p(out))
     return out
+
+
+def init_particles(n, seed, energy_GeV, grid, injection="isotropic", mu0=0.0, position_mode="random",
+                   position=(0.5, 0.5, 0.5), bfield=None):
+    """Counter-stream restatement of the device initialiser; bfield = (Bx, By,
+    Bz) C-ordered (nz, ny, nx) FP64 arrays for fixed-mu injection.  Returns
+    (state dict, number of particles with zero or non-finite |B|)."""
+    out = {k: np.empty(int(n), dtype=np.float64) for k in ("x1", "x2", "x3", "p1", "p2", "p3")}
+    pos = np.ascontiguousarray(position, dtype=np.float64)
+    fixed_mu = injection.replace("-", "_") == "fixed_mu"
+    bs = [np.ascontiguousarray(b, dtype=np.float64) for b in bfield] if fixed_mu else []
+    g = grid_struct(grid)
+    bad = lib().or_init_particles(int(n), int(seed) & 0xFFFFFFFFFFFFFFFF, float(energy_GeV), int(fixed_mu),
+                                  int(position_mode == "random"), float(mu0), _p(pos),
+                                  _ptr_array(bs) if bs else None, C.byref(g),
+                                  *[_p(out[k]) for k in ("x1", "x2", "x3", "p1", "p2", "p3")])
+    return out, int(bad)

@@ -537,6 +537,91 @@ void or_energy_snapshots(const float* mom, int64_t chunk, int64_t nsave, const i
     }
 }
 
+/* ------------------------------------------------------------------------
+ * Particle initialisation: init_particles / rand_unit_vector /
+ * fixed_mu_unit_vector (src/phase_space_gpu_runner.jl:51-66, 170-245) over
+ * the counter-based stream of the device initialiser: draw d of particle i
+ * is the SplitMix64 output of counter 8 i + d + 1 under key mix64(seed)
+ * (Steele, Lea, Flood 2014), as (h >> 11) * 2^-53.  Draws 0-2 position,
+ * draw 3 z (isotropic) or phi (fixed mu), draw 4 phi (isotropic).
+ * Returns the number of particles where fixed-mu injection met a zero or
+ * non-finite |B| (their momenta are NaN).
+ * --------------------------------------------------------------------- */
+static inline uint64_t or_mix64(uint64_t z)
+{
+    z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ull;
+    z = (z ^ (z >> 27)) * 0x94D049BB133111EBull;
+    return z ^ (z >> 31);
+}
+
+static inline double or_draw(uint64_t key, int64_t i, int d)
+{
+    uint64_t c = (uint64_t)i * 8u + (uint64_t)d + 1u;
+    return (double)(or_mix64(key + c * 0x9E3779B97F4A7C15ull) >> 11) * 0x1.0p-53;
+}
+
+int64_t or_init_particles(int64_t n, uint64_t seed, double energy_GeV, int fixed_mu, int random_pos, double mu0,
+                          const double* position, const double* const* bfield, const or_grid* g, double* x1,
+                          double* x2, double* x3, double* p1, double* p2, double* p3)
+{
+    const double two_pi = 6.283185307179586; /* Float64(2 * pi) */
+    const double gev_to_j = 1e9 * 1.602176634e-19;
+    double kinetic = energy_GeV * gev_to_j;
+    double gamma0 = kinetic / (OR_M_P * (OR_C_LIGHT * OR_C_LIGHT)) + 1.0;
+    double v0 = OR_C_LIGHT * sqrt(1.0 - 1.0 / (gamma0 * gamma0));
+    double pscale = gamma0 * OR_M_P * v0;
+    double perp = sqrt(fmax(0.0, 1.0 - mu0 * mu0));
+    double lo[3] = {g->xmin, g->ymin, g->zmin}, len[3], fixed[3];
+    double hi[3] = {g->xmax, g->ymax, g->zmax};
+    uint64_t key = or_mix64(seed);
+    int64_t bad = 0;
+    for (int d = 0; d < 3; ++d) {
+        len[d] = hi[d] - lo[d];
+        fixed[d] = lo[d] + position[d] * (hi[d] - lo[d]);
+    }
+    for (int64_t i = 0; i < n; ++i) {
+        double x[3], ux, uy, uz;
+        for (int d = 0; d < 3; ++d) x[d] = random_pos ? or_draw(key, i, d) * len[d] + lo[d] : fixed[d];
+        if (fixed_mu) {
+            double bx = or_trilinear(bfield[0], x[0], x[1], x[2], g);
+            double by = or_trilinear(bfield[1], x[0], x[1], x[2], g);
+            double bz = or_trilinear(bfield[2], x[0], x[1], x[2], g);
+            double bn = sqrt(bx * bx + by * by + bz * bz);
+            if (!isfinite(bn) || bn == 0.0) {
+                ++bad;
+                ux = uy = uz = NAN;
+            } else {
+                double bhx = bx / bn, bhy = by / bn, bhz = bz / bn, e1x, e1y, e1z;
+                if (fabs(bhx) < 0.9) {
+                    e1x = 0.0; e1y = bhz; e1z = -bhy;
+                } else {
+                    e1x = -bhz; e1y = 0.0; e1z = bhx;
+                }
+                double e1n = sqrt(e1x * e1x + e1y * e1y + e1z * e1z);
+                e1x = e1x / e1n; e1y = e1y / e1n; e1z = e1z / e1n;
+                double e2x = bhy * e1z - bhz * e1y;
+                double e2y = bhz * e1x - bhx * e1z;
+                double e2z = bhx * e1y - bhy * e1x;
+                double phi = two_pi * or_draw(key, i, 3);
+                double cphi = cos(phi), sphi = sin(phi);
+                ux = mu0 * bhx + perp * (cphi * e1x + sphi * e2x);
+                uy = mu0 * bhy + perp * (cphi * e1y + sphi * e2y);
+                uz = mu0 * bhz + perp * (cphi * e1z + sphi * e2z);
+            }
+        } else {
+            double z = 2.0 * or_draw(key, i, 3) - 1.0;
+            double phi = two_pi * or_draw(key, i, 4);
+            double r = sqrt(fmax(0.0, 1.0 - z * z));
+            ux = r * cos(phi);
+            uy = r * sin(phi);
+            uz = z;
+        }
+        x1[i] = x[0]; x2[i] = x[1]; x3[i] = x[2];
+        p1[i] = pscale * ux; p2[i] = pscale * uy; p3[i] = pscale * uz;
+    }
+    return bad;
+}
+
 int or_num_threads(void)
 {
 #ifdef _OPENMP

@@ -21,6 +21,8 @@ PT_FIELD_REF_F64, PT_FIELD_BRICK_F32, PT_FIELD_BRICK_BF16, PT_FIELD_BRICK_BF16_X
 PT_CACHE_NONE, PT_CACHE_MU, PT_CACHE_PHASE_SPACE = 0, 1, 2
 PT_PUSH_F64, PT_PUSH_F32 = 0, 1
 PT_START_SLIDING, PT_START_INJECTION = 0, 1
+PT_INJECT_ISOTROPIC, PT_INJECT_FIXED_MU = 0, 1
+PT_POSITION_RANDOM, PT_POSITION_FIXED = 0, 1
 CUDA_STREAM_LEGACY = 0x1  # cudaStreamLegacy
 
 # every exported entry point of include/ptb200.h
@@ -33,6 +35,7 @@ EXPORTS = (
     "pt_dmumu_accumulate_device",
     "pt_dmumu_accumulate_device_noalloc", "pt_dpp_accumulate",
     "pt_dpp_accumulate_device", "pt_energy_snapshots", "pt_energy_histogram_device", "pt_reconstruct_mu",
+    "pt_particles_init_device",
 )
 
 
@@ -70,6 +73,13 @@ class CampaignDesc(C.Structure):
         ("d_p2", C.c_void_p), ("d_p3", C.c_void_p), ("d_alive", C.c_void_p),
         ("d_cache", C.c_void_p), ("cache_rows", C.c_int64), ("cache_ring", C.c_int32), ("reserved", C.c_int32),
         ("d_deaths", C.c_void_p),
+    ]
+
+
+class InitParams(C.Structure):
+    _fields_ = [
+        ("n", C.c_int64), ("seed", C.c_uint64), ("energy_GeV", C.c_double), ("injection", C.c_int32),
+        ("position_mode", C.c_int32), ("mu0", C.c_double), ("position", C.c_double * 3),
     ]
 
 
@@ -129,6 +139,7 @@ def load():
             "pt_energy_snapshots": (i32, [P, P, i64, i64, P, i32, i64, P]),
             "pt_energy_histogram_device": (i32, [P, P, i64, i64, P, i32, d, d, i32, P]),
             "pt_reconstruct_mu": (i32, [P, P, P, i64, i64, P, C.POINTER(Grid), i32, P]),
+            "pt_particles_init_device": (i32, [P, P, C.POINTER(InitParams), P, P, P, P, P, P]),
         }
         for name, (res, args) in sig.items():
             fn = getattr(L, name)

@@ -1,10 +1,10 @@
 """Build recipe for libptb200.so (sm_100a).
 
 Each translation unit is compiled by nvcc for ``sm_100a`` only and linked
-in-tree into ``particle_transport_b200/libptb200.so``.  ``push_exact.cu`` is
-compiled with ``--fmad=false`` so that the FP64 parity push and the mu
-reconstruction keep the reference's rounding (no fused multiply-add); the
-other units keep FMA contraction on.
+in-tree into ``particle_transport_b200/libptb200.so``.  ``push_exact.cu`` and
+``init.cu`` are compiled with ``--fmad=false`` so that the FP64 parity push,
+the mu reconstruction and the particle initialisation keep the reference's
+rounding (no fused multiply-add); the other units keep FMA contraction on.
 """
 from __future__ import annotations
 
@@ -23,6 +23,7 @@ ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 COMMON = ["-O3", "-std=c++17", "-lineinfo", "-Xcompiler", "-fPIC", "-I", INCLUDE, *ARCH]
 UNITS = {
     "push_exact.cu": ["--fmad=false"],
+    "init.cu": ["--fmad=false"],
     "push_fast.cu": [],
     "lagstats.cu": [],
     "pt_api.cu": [],

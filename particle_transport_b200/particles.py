@@ -112,3 +112,31 @@ def init_particles(n: int, grid: UniformGrid, energy_GeV: float, seed: int = 42,
     return {"x1": np.ascontiguousarray(x1), "x2": np.ascontiguousarray(x2), "x3": np.ascontiguousarray(x3),
             "p1": np.ascontiguousarray(pscale * ux), "p2": np.ascontiguousarray(pscale * uy),
             "p3": np.ascontiguousarray(pscale * uz)}
+
+
+def init_particles_device(field, n: int, energy_GeV: float, seed: int = 42, injection_mode: str = "isotropic",
+                          mu0: float = 0.0, position_mode: str = "random", position=(0.5, 0.5, 0.5)):
+    """Initial SI state written on the device (pt_particles_init_device): the
+    reference's formulas over a counter-based SplitMix64 stream, so a job's
+    state depends only on (seed, n, energy, injection, field) and needs no
+    host work.  Fixed-mu injection samples B from the field library's own
+    stored values.  Returns a dict of CUDA float64 tensors x1..p3."""
+    import torch
+
+    from . import _lib
+
+    injection_mode = injection_mode.replace("-", "_")
+    modes = {"isotropic": _lib.PT_INJECT_ISOTROPIC, "fixed_mu": _lib.PT_INJECT_FIXED_MU}
+    pmodes = {"random": _lib.PT_POSITION_RANDOM, "fixed": _lib.PT_POSITION_FIXED}
+    if injection_mode not in modes:
+        raise ValueError("injection_mode must be isotropic or fixed-mu")
+    if position_mode not in pmodes:
+        raise ValueError("position_mode must be random or fixed")
+    dev = torch.device("cuda", field.ctx.device)
+    out = {k: torch.empty(int(n), dtype=torch.float64, device=dev) for k in ("x1", "x2", "x3", "p1", "p2", "p3")}
+    prm = _lib.InitParams(int(n), int(seed) & 0xFFFFFFFFFFFFFFFF, float(energy_GeV), modes[injection_mode],
+                          pmodes[position_mode], float(mu0), (_lib.C.c_double * 3)(*[float(v) for v in position]))
+    ctx = _lib.torch_context(out["x1"])
+    _lib.call("pt_particles_init_device", ctx.handle, field.handle, _lib.C.byref(prm),
+              *[_lib.ptr(out[k]) for k in ("x1", "x2", "x3", "p1", "p2", "p3")])
+    return out

@@ -31,7 +31,7 @@ from . import _lib
 from . import stats as S
 from .batch import Batch
 from .fields import FieldLibrary, M_P, Q_E
-from .particles import energy_to_gamma, init_particles
+from .particles import energy_to_gamma, init_particles_device
 from .time_units import build_mu_edges_full, log_spaced_lag_steps, reference_Omega0
 
 
@@ -73,10 +73,12 @@ class JobResult:
 class CampaignServer:
     def __init__(self, libraries: dict, B0_ref_T: dict, hbm_budget_bytes: float = 150e9, storage: str = "brick_bf16",
                  steps_per_epoch: int = 64, capacity: int = 1 << 26, max_jobs: int = 256, blocks_per_sm: int = 0,
-                 host_fields: dict = None, keep_cache: bool = False, device: int = 0):
+                 keep_cache: bool = False, device: int = 0):
         """libraries: {library: {mode: FieldLibrary}} (brick storage);
-        B0_ref_T: {library: total-field mean |B|} (time reference of every mode);
-        host_fields: {library: {mode: (Bx, By, Bz) host arrays}} for fixed-mu injection."""
+        B0_ref_T: {library: total-field mean |B|} (time reference of every mode).
+        A job's initial state is written on the device from its seed
+        (pt_particles_init_device); fixed-mu injection takes the local field
+        direction from the job's own field library."""
         import torch
 
         self.torch = torch
@@ -89,7 +91,6 @@ class CampaignServer:
         self.device = torch.device("cuda", device)
         self.side = torch.cuda.Stream(device=self.device)
         self.side_ctx = _lib.Context(device)
-        self.host_fields = host_fields or {}
         self.keep_cache = keep_cache
         self.queue = []      # (job_id, spec, arrival)
         self.active = {}     # job_id -> record
@@ -98,6 +99,8 @@ class CampaignServer:
         self.used = 0.0
         self.next_id = 0
         self.epochs = 0
+        self.admit_s = 0.0   # host seconds spent admitting jobs
+        self._epoch_events = []
 
     # ------------------------------------------------------------ admission
     @staticmethod
@@ -123,11 +126,8 @@ class CampaignServer:
         nsteps = int(round(spec.duration_gyroperiods * spec.steps_per_gyroperiod)) + 1
         stride = spec.steps_per_gyroperiod // spec.saves_per_gyroperiod
         nsave = (nsteps - 1) // stride + 1
-        B = None
-        if spec.injection.replace("-", "_") == "fixed_mu":
-            B = self.host_fields[spec.library][spec.mode]
-        st = init_particles(spec.n_particles, fl.grid, spec.energy_GeV, seed=spec.seed,
-                            injection_mode=spec.injection, mu0=spec.mu0, B=B)
+        st = init_particles_device(fl, spec.n_particles, spec.energy_GeV, seed=spec.seed,
+                                   injection_mode=spec.injection, mu0=spec.mu0)
         cache = torch.empty((nsave, spec.n_particles), dtype=torch.float32, device=self.device)
         cid = self.batch.add(fl, st, dt, nsteps, stride, cache=cache)
         self.active[jid] = dict(spec=spec, cid=cid, cache=cache, nsteps=nsteps, nsave=nsave, arrival=arrival,
@@ -135,6 +135,13 @@ class CampaignServer:
         self.used += self.job_bytes(spec)
 
     def admit(self) -> int:
+        t0 = time.perf_counter()
+        try:
+            return self._admit_waiting()
+        finally:
+            self.admit_s += time.perf_counter() - t0
+
+    def _admit_waiting(self) -> int:
         n = 0
         keep = []
         for jid, spec, arrival in self.queue:
@@ -181,7 +188,11 @@ class CampaignServer:
         """One scheduling step; returns the jobs finished in it."""
         self.admit()
         if self.active:
+            ev0, ev1 = self.torch.cuda.Event(enable_timing=True), self.torch.cuda.Event(enable_timing=True)
+            ev0.record()
             self.batch.run(1)
+            ev1.record()
+            self._epoch_events.append((ev0, ev1))
             self.epochs += 1
             for jid in list(self.active):
                 rec = self.active[jid]
@@ -206,6 +217,11 @@ class CampaignServer:
                 self.results.append(res)
                 out.append(res)
         return out
+
+    def device_busy_s(self) -> float:
+        """Device seconds spent in epochs so far (CUDA events around each)."""
+        self.torch.cuda.synchronize(self.device)
+        return sum(a.elapsed_time(b) for a, b in self._epoch_events) / 1e3
 
     def idle(self) -> bool:
         return not (self.queue or self.active or self.binning)

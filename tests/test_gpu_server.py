@@ -22,8 +22,7 @@ def library(cuda):
     libs = {"16": {"total": FieldLibrary(pa.fields, pa.grid, "brick_bf16"),
                    "alfven": FieldLibrary(pb.fields, pb.grid, "brick_bf16")}}
     B0 = {"16": reference_B0_T(*pa.fields[:3])}
-    host = {"16": {"total": pa.fields[:3], "alfven": pb.fields[:3]}}
-    return libs, B0, host
+    return libs, B0
 
 
 JOBS = [JobSpec("16", "total", 1.0, 3000, 6.0, seed=1),
@@ -33,9 +32,8 @@ JOBS = [JobSpec("16", "total", 1.0, 3000, 6.0, seed=1),
 
 
 def run_jobs(library, jobs, budget=150e9, stagger_ticks=0):
-    libs, B0, host = library
-    srv = CampaignServer(libs, B0, hbm_budget_bytes=budget, capacity=20000, max_jobs=8, host_fields=host,
-                         keep_cache=True)
+    libs, B0 = library
+    srv = CampaignServer(libs, B0, hbm_budget_bytes=budget, capacity=20000, max_jobs=8, keep_cache=True)
     pending = list(jobs)
     ids = []
     while pending or not srv.idle():
