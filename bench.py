@@ -63,8 +63,9 @@ def parse():
     ap.add_argument("--sort-every", type=int, default=64, help="re-sort particles by brick every N pushes (0: never)")
     ap.add_argument("--variant", type=int, default=1, help="push launch shape (pt_push_params.kernel_variant)")
     ap.add_argument("--lag-particles", type=int, default=1_048_576)
+    ap.add_argument("--dpp-particles", type=int, default=262_144)
     ap.add_argument("--e2e-gyroperiods", type=int, default=8)
-    ap.add_argument("--skip", default="", help="comma list of legs to skip: fp64,lag,e2e,cpu,batch,serve")
+    ap.add_argument("--skip", default="", help="comma list of legs to skip: fp64,lag,dpp,e2e,cpu,batch,serve")
     ap.add_argument("--cpu-seconds", type=float, default=10.0)
     ap.add_argument("--precision", action="store_true",
                     help="run only the plain-vs-precision study (256^3, 3 energies) and print its JSON line")
@@ -240,6 +241,27 @@ def cpu_lag_rate(mu_chunk, lags, edges, seconds):
     pairs = int(acc["pair_n"].sum())
     return {"value": pairs / el, "unit": "lag-pairs/s", "cores": o.num_threads(), "kind": "port",
             "sample": f"{n} particles x {mu_chunk.shape[1]} saves x {len(lags)} lags ({pairs} pairs), {el:.1f} s"}
+
+
+def cpu_dpp_rate(mom, lags, p0, seconds):
+    """D_pp lag pairs/s of the oracle on host cores; mom (nsave, 3, n) float32."""
+    from oracle import oracle as o
+
+    nl = len(lags)
+    n = 64
+    while True:
+        acc = {"counts": np.zeros(nl, np.int64), **{k: np.zeros(nl) for k in ("sum_dp", "sum_dp2", "sum_dpn",
+                                                                               "sum_dpn2")}}
+        sub = np.ascontiguousarray(mom[:, :, :n])
+        t0 = time.perf_counter()
+        o.dpp_accumulate(sub, lags, p0, acc)
+        el = time.perf_counter() - t0
+        if el * 2 >= seconds or n >= mom.shape[2]:
+            break
+        n = min(mom.shape[2], int(n * max(2.0, min(16.0, seconds / 2 / max(el, 1e-3)))))
+    pairs = int(acc["counts"].sum())
+    return {"value": pairs / el, "unit": "lag-pairs/s", "cores": o.num_threads(), "kind": "port",
+            "sample": f"{n} particles x {mom.shape[0]} saves x {nl} lags ({pairs} pairs), {el:.1f} s"}
 
 
 # ---------------------------------------------------------------------------
@@ -424,6 +446,61 @@ def run_ours(args, ws, rank, local):
         del ens_l, cache
         torch.cuda.empty_cache()
 
+    # ---------------- D_pp (64 lags) and 16 energy-snapshot histograms on a phase-space campaign subset
+    dpp = None
+    if "dpp" not in skip:
+        from particle_transport_b200.time_units import selected_energy_snapshot_indices
+        from particle_transport_b200.particles import energy_to_gamma
+
+        npp = min(args.dpp_particles, n)
+        sub = {k: v[:npp] for k, v in state.items()}
+        ens_p = R.FastEnsemble(fb, sub, np.ones(npp, np.uint8))
+        nsave = (NSTEPS - 1) // STRIDE + 1
+        ps = torch.empty((nsave, 6, npp), dtype=torch.float32, device=dev)
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        ens_p.advance(R.push_params(dt, NSTEPS, STRIDE, cache="phase_space", precision="f32",
+                                    sort_every=args.sort_every, kernel_variant=args.variant), 0, NSTEPS, ps, 0, nsave)
+        torch.cuda.synchronize()
+        ps_push_s = time.perf_counter() - t0
+        mom = ps[:, 3:6, :].contiguous()
+        del ps, ens_p
+        torch.cuda.empty_cache()
+        lags_p = log_spaced_lag_steps(nsave - 1, 64)
+        p0 = float(torch.linalg.vector_norm(mom[0, :, 0].double()).item())
+
+        def dpp_pass(_k):
+            acc = S.new_dpp_accumulators(len(lags_p), device=dev)
+            S.process_momenta_chunk_dpp(mom, lags_p, p0, acc["counts"], acc["sum_delta_p"], acc["sum_delta_p2"],
+                                        acc["sum_delta_p_norm"], acc["sum_delta_p_norm2"])
+            dpp_pass.acc = acc
+
+        dms, _ = timed(dpp_pass, 2, 1, torch)
+        dpairs = int(dpp_pass.acc["counts"].sum().item())
+        snaps = selected_energy_snapshot_indices(nsave, 16) - 1
+        E0 = args.energy
+        e_lo, e_hi = E0 / 2, E0 * 2
+
+        def hist_pass(_k):
+            hist_pass.counts = S.energy_histogram(mom, snaps, e_lo, e_hi, 256)
+
+        hms, _ = timed(hist_pass, 3, 1, torch)
+        dpp_s = dms / 2 / 1e3
+        dpp = {"value": ws * dpairs / max_over_ranks(dpp_s * 1e3, ws, dev) * 1e3, "unit": "lag-pairs/s",
+               "pairs_per_pass": dpairs, "ms_per_pass": dms / 2, "particles": npp, "saves": nsave,
+               "lags": int(len(lags_p)), "estimator": "sliding, |p| recomputed per end in FP64",
+               "compulsory_bytes_per_pass": 12 * npp * nsave,
+               "hbm_frac_of_compulsory": (12 * npp * nsave / dpp_s / 1e9) / peaks["hbm_gbs"],
+               "phase_space_push_s": ps_push_s, "phase_space_push_rate": npp * (NSTEPS - 1) / ps_push_s,
+               "energy_histograms": {"snapshots": int(len(snaps)), "bins": 256, "range_GeV": [e_lo, e_hi],
+                                     "spacing": "log", "ms_per_pass": hms / 3,
+                                     "counted": int(hist_pass.counts.sum().item()),
+                                     "particles_x_snapshots": int(npp * len(snaps))}}
+        if "cpu" not in skip and rank == 0:
+            dpp["cpu_baseline"] = cpu_dpp_rate(mom[:, :, :4096].cpu().numpy(), lags_p, p0, args.cpu_seconds / 2)
+        del mom
+        torch.cuda.empty_cache()
+
     # ---------------- e2e through pt_push_run with host buffers
     e2e = None
     if "e2e" not in skip:
@@ -484,7 +561,8 @@ def run_ours(args, ws, rank, local):
                            "kernel_variant": args.variant,
                            "l2": "inputs larger than L2 (field and state exceed 126 MB); no flush",
                            "parallelism": f"particle-sharded replicas x{ws}"},
-                "roofline": roofline, "fp64_push": fp64, "lag_pairs": lag, "e2e": e2e, "cpu_baseline": cpu,
+                "roofline": roofline, "fp64_push": fp64, "lag_pairs": lag, "dpp": dpp, "e2e": e2e,
+                "cpu_baseline": cpu,
                 "clocks": clocks, "gpu_launches": launches["push"] + launches["sort"], "batched": batched,
                 "job_latency": ({"p50_s": serving["p50_s"], "p99_s": serving["p99_s"]} if serving else None),
                 "serving": serving}

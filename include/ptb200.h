@@ -108,6 +108,11 @@ int pt_ctx_destroy(pt_ctx* ctx);
  * for the legacy default stream. */
 int pt_ctx_set_stream(pt_ctx* ctx, void* cuda_stream);
 int pt_ctx_synchronize(pt_ctx* ctx);
+/* Free the buffers a context keeps between calls: device scratch, the pinned
+ * host staging and the particle state of pt_push_run (all grow-only, reused
+ * by the next call of the same size).  pt_ctx_destroy frees them too.  No
+ * reference counterpart (the reference allocates per run). */
+int pt_ctx_trim(pt_ctx* ctx);
 
 /* Upload a static field library (load_static_fields output,
  * src/phase_space_gpu_runner.jl:95-123; SI units: B in T, u in m/s).
@@ -130,6 +135,10 @@ int64_t pt_field_device_bytes(const pt_field* field);
  * bytes (1 live), updated in place.  Each save row is handed to `save` on the
  * calling thread while the next steps run on the GPU.  alive_count[nsteps]
  * receives sum(dalive) after each step (src/phase_space_gpu_runner.jl:576).
+ * The state crosses the link through the context's pinned staging chunks
+ * (host threads copy while the DMA engine moves the previous chunk); the
+ * device state, staging and the FP32-push state stay in the context for the
+ * next call (pt_ctx_trim releases them).
  */
 int pt_push_run(pt_ctx* ctx, const pt_field* field, double* x1, double* x2, double* x3, double* p1, double* p2,
                 double* p3, uint8_t* alive, int64_t n, const pt_push_params* params, pt_save_fn save, void* user,

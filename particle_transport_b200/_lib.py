@@ -28,6 +28,7 @@ CUDA_STREAM_LEGACY = 0x1  # cudaStreamLegacy
 # every exported entry point of include/ptb200.h
 EXPORTS = (
     "pt_last_error", "pt_version", "pt_ctx_create", "pt_ctx_destroy", "pt_ctx_set_stream", "pt_ctx_synchronize",
+    "pt_ctx_trim",
     "pt_field_upload", "pt_field_upload_device", "pt_field_destroy", "pt_field_device_bytes", "pt_push_run",
     "pt_push_advance_device", "pt_fast_state_create", "pt_fast_state_export", "pt_fast_state_destroy",
     "pt_fast_state_sort", "pt_push_advance_fast", "pt_batch_create", "pt_batch_add", "pt_batch_remove",
@@ -109,6 +110,7 @@ def load():
             "pt_ctx_destroy": (i32, [P]),
             "pt_ctx_set_stream": (i32, [P, P]),
             "pt_ctx_synchronize": (i32, [P]),
+            "pt_ctx_trim": (i32, [P]),
             "pt_field_upload": (i32, [P, P, C.POINTER(Grid), i32, d, PP]),
             "pt_field_upload_device": (i32, [P, P, C.POINTER(Grid), i32, d, PP]),
             "pt_field_destroy": (i32, [P]),
@@ -202,6 +204,10 @@ class Context:
 
     def synchronize(self) -> None:
         call("pt_ctx_synchronize", self.handle)
+
+    def trim(self) -> None:
+        """Release the buffers the context keeps between calls (pt_ctx_trim)."""
+        call("pt_ctx_trim", self.handle)
 
     def close(self) -> None:
         if self.handle:

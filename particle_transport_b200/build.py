@@ -28,6 +28,7 @@ UNITS = {
     "lagstats.cu": [],
     "pt_api.cu": [],
     "pt_batch.cu": [],
+    "hostio.cu": [],
 }
 
 

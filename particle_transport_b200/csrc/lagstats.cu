@@ -18,7 +18,10 @@
 // D_pp (process_momenta_chunk_dpp_cpu!, src/compute_dpp_full.jl:247-288)
 // ---------------------------------------------------------------------
 // Same layout without bins: |p| is computed once per (particle, save) in FP64
-// and every lane keeps its lag's five sums in registers for the whole launch.
+// and every lane keeps its lag's count, sum(dp) and sum(dp^2) in registers for
+// the whole launch; the normalised sums sum(dp/p0) = sum(dp)/p0 and
+// sum((dp/p0)^2) = sum(dp^2)/p0^2 are formed once per lag at the end, which
+// equals the reference's per-pair division up to rounding.
 #include "pt_internal.cuh"
 
 #include <algorithm>
@@ -391,7 +394,7 @@ __device__ __forceinline__ double pmag_exact(float px, float py, float pz)
 
 struct DppPart {
     long long count;
-    double sdp, sdp2, sdn, sdn2;
+    double sdp, sdp2;
 };
 
 struct DppLaunch {
@@ -420,7 +423,7 @@ __global__ void __launch_bounds__(1024) dpp_kernel(DppLaunch a)
     const int64_t lim = a.nsave - L;
     double* series = (double*)(slot_base + (size_t)slot * a.slot_bytes);
     long long c = 0;
-    double sdp = 0, sdp2 = 0, sdn = 0, sdn2 = 0;
+    double sdp = 0, sdp2 = 0;
     const int64_t tiles = (a.chunk + a.ppc - 1) / a.ppc;
     for (int64_t tile = blockIdx.x; tile < tiles; tile += gridDim.x) {
         // cooperative staging: thread t -> (save, particle slot)
@@ -434,17 +437,15 @@ __global__ void __launch_bounds__(1024) dpp_kernel(DppLaunch a)
         }
         __syncthreads();
         if (slot < np) {
+            // |p| >= 0 or NaN or +inf, so pe - ps is finite exactly when both
+            // ends are finite; the normalised sums are sum(d)/p0 and
+            // sum(d^2)/p0^2, formed once per lag in dpp_finalize_kernel.
             for (int64_t s = 0; s < lim; ++s) {
-                const double ps = series[s];
-                const double pe = series[s + L];
-                if (!(isfinite(ps) && isfinite(pe))) continue;
-                const double d = pe - ps;
-                const double dn = d / a.p0;
+                const double d = series[s + L] - series[s];
+                if (!isfinite(d)) continue;
                 c += 1;
                 sdp += d;
                 sdp2 = fma(d, d, sdp2);
-                sdn += dn;
-                sdn2 = fma(dn, dn, sdn2);
             }
         }
         __syncthreads();
@@ -452,38 +453,38 @@ __global__ void __launch_bounds__(1024) dpp_kernel(DppLaunch a)
     // CTA epilogue in fixed warp order
     DppPart* wp = (DppPart*)(SMEM_SLOTS ? smem : smem);
     __syncthreads();
-    wp[warp * kWarp + lane] = DppPart{c, sdp, sdp2, sdn, sdn2};
+    wp[warp * kWarp + lane] = DppPart{c, sdp, sdp2};
     __syncthreads();
     const int nwarps = blockDim.x / kWarp;
     for (int l = threadIdx.x; l < a.nl; l += blockDim.x) {
         const int g = l / kWarp, ln = l % kWarp;
-        DppPart r{0, 0, 0, 0, 0};
+        DppPart r{0, 0, 0};
         for (int sl = 0; sl < a.ppc; ++sl) {
             const int w = sl * a.groups + g;
             if (w >= nwarps) break;
             const DppPart q = wp[w * kWarp + ln];
-            r.count += q.count; r.sdp += q.sdp; r.sdp2 += q.sdp2; r.sdn += q.sdn; r.sdn2 += q.sdn2;
+            r.count += q.count; r.sdp += q.sdp; r.sdp2 += q.sdp2;
         }
         a.part[(int64_t)blockIdx.x * a.nl + l] = r;
     }
 }
 
-__global__ void dpp_finalize_kernel(const DppPart* __restrict__ part, int grid, int nl, int lag0, int64_t* counts,
-                                    double* sdp, double* sdp2, double* sdn, double* sdn2)
+__global__ void dpp_finalize_kernel(const DppPart* __restrict__ part, int grid, int nl, int lag0, double p0,
+                                    int64_t* counts, double* sdp, double* sdp2, double* sdn, double* sdn2)
 {
     const int t = blockIdx.x * blockDim.x + threadIdx.x;
     if (t >= nl) return;
-    DppPart r{0, 0, 0, 0, 0};
+    DppPart r{0, 0, 0};
     for (int g = 0; g < grid; ++g) {
         const DppPart q = part[(int64_t)g * nl + t];
-        r.count += q.count; r.sdp += q.sdp; r.sdp2 += q.sdp2; r.sdn += q.sdn; r.sdn2 += q.sdn2;
+        r.count += q.count; r.sdp += q.sdp; r.sdp2 += q.sdp2;
     }
     const int l = lag0 + t;
     counts[l] += r.count;
     sdp[l] += r.sdp;
     sdp2[l] += r.sdp2;
-    sdn[l] += r.sdn;
-    sdn2[l] += r.sdn2;
+    sdn[l] += r.sdp / p0;
+    sdn2[l] += r.sdp2 / p0 / p0;
 }
 
 // ------------------------------------------------------------------ energies
@@ -652,8 +653,8 @@ int run_dpp(pt_ctx* ctx, const DppArgs& a, cudaStream_t s)
         if (smem_slots) dpp_kernel<true><<<grid, threads, smem, s>>>(L);
         else dpp_kernel<false><<<grid, threads, smem, s>>>(L);
         PT_CHECK_LAUNCH("dpp_kernel");
-        dpp_finalize_kernel<<<(nl + 255) / 256, 256, 0, s>>>(L.part, grid, nl, lag0, a.counts, a.sdp, a.sdp2, a.sdn,
-                                                             a.sdn2);
+        dpp_finalize_kernel<<<(nl + 255) / 256, 256, 0, s>>>(L.part, grid, nl, lag0, a.p0, a.counts, a.sdp, a.sdp2,
+                                                             a.sdn, a.sdn2);
         PT_CHECK_LAUNCH("dpp_finalize_kernel");
     }
     return PT_OK;

@@ -70,21 +70,6 @@ struct DevBuf {
     template <typename T> T* as() const { return (T*)p; }
 };
 
-struct PinnedBuf {
-    void* p = nullptr;
-    ~PinnedBuf() { if (p) cudaFreeHost(p); }
-    int alloc(size_t bytes)
-    {
-        cudaError_t e = cudaMallocHost(&p, std::max<size_t>(bytes, 16));
-        if (e != cudaSuccess) {
-            cudaGetLastError();
-            p = nullptr;
-            return fail(PT_ERR_OOM, "pinned host allocation failed");
-        }
-        return PT_OK;
-    }
-};
-
 int check_grid(const pt_grid* g)
 {
     if (!g) return fail(PT_ERR_ARG, "grid is null");
@@ -318,11 +303,29 @@ int pt_ctx_destroy(pt_ctx* ctx)
     if (!ctx) return PT_OK;
     cudaSetDevice(ctx->device);
     cudaStreamSynchronize(ctx->stream);
-    for (auto& b : ctx->scratch)
-        if (b.ptr) cudaFree(b.ptr);
+    pt_ctx_trim(ctx);
     if (ctx->copy_stream) cudaStreamDestroy(ctx->copy_stream);
     if (ctx->own_stream) cudaStreamDestroy(ctx->own_stream);
     delete ctx;
+    return PT_OK;
+}
+
+int pt_ctx_trim(pt_ctx* ctx)
+{
+    if (!ctx) return fail(PT_ERR_ARG, "ctx is null");
+    PT_CUDA(cudaSetDevice(ctx->device));
+    PT_CUDA(cudaStreamSynchronize(ctx->stream));
+    if (ctx->copy_stream) PT_CUDA(cudaStreamSynchronize(ctx->copy_stream));
+    for (auto& b : ctx->scratch) {
+        if (b.ptr) cudaFree(b.ptr);
+        b.ptr = nullptr;
+        b.bytes = 0;
+    }
+    if (ctx->pinned.ptr) cudaFreeHost(ctx->pinned.ptr);
+    ctx->pinned.ptr = nullptr;
+    ctx->pinned.bytes = 0;
+    if (ctx->run_fs) pt_fast_state_destroy(ctx->run_fs);
+    ctx->run_fs = nullptr;
     return PT_OK;
 }
 
@@ -500,30 +503,53 @@ int pt_push_run(pt_ctx* ctx, const pt_field* f, double* x1, double* x2, double* 
     if (row_bytes > 0) R = std::max<int64_t>(1, std::min<int64_t>(R, (int64_t)((256u << 20) / row_bytes)));
     const int64_t chunk_steps = R * stride;
 
-    DevBuf dstate, ddeaths, dslots;
-    PinnedBuf hslots;
+    // device: state [6][m] doubles + alive [m] + deaths [nsteps] + two egress slots
+    // host: two pinned egress slots + the staging chunks of the state copies
+    // (both grow-only in the context, kept between calls)
     const size_t m = (size_t)std::max<int64_t>(n, 1);
-    if ((rc = dstate.alloc(sizeof(double) * 6 * m + m))) return rc;
-    if ((rc = ddeaths.alloc(sizeof(int64_t) * (size_t)nsteps))) return rc;
-    if (row_bytes) {
-        if ((rc = dslots.alloc(2 * (size_t)R * row_bytes))) return rc;
-        if ((rc = hslots.alloc(2 * (size_t)R * row_bytes))) return rc;
-    }
+    const size_t state_bytes = align_up(sizeof(double) * 6 * m + m, 256);
+    const size_t deaths_bytes = align_up(sizeof(int64_t) * (size_t)nsteps, 256);
+    const size_t slots_bytes = row_bytes ? 2 * (size_t)R * row_bytes : 0;
+    const size_t stage_chunk = 32u << 20;
+    const int stage_nbuf = 3;
+    void* dbase = nullptr;
+    void* hbase = nullptr;
+    if ((rc = scratch_get(ctx, 2, state_bytes + deaths_bytes + slots_bytes, &dbase))) return rc;
+    if ((rc = pinned_get(ctx, slots_bytes + stage_chunk * stage_nbuf, &hbase))) return rc;
+    char* stage = (char*)hbase + slots_bytes;
+    char* dslot_base = (char*)dbase + state_bytes + deaths_bytes;  // [2][R] device egress rows
+    char* hslot_base = (char*)hbase;                                // [2][R] pinned egress rows
+    int64_t* d_deaths = (int64_t*)((char*)dbase + state_bytes);
     double* d[6];
-    for (int k = 0; k < 6; ++k) d[k] = dstate.as<double>() + (size_t)k * m;
-    uint8_t* dal = (uint8_t*)(dstate.as<double>() + 6 * m);
+    for (int k = 0; k < 6; ++k) d[k] = (double*)dbase + (size_t)k * m;
+    uint8_t* dal = (uint8_t*)((double*)dbase + 6 * m);
     double* hs[6] = {x1, x2, x3, p1, p2, p3};
-    int64_t alive0 = 0;
-    for (int64_t i = 0; i < n; ++i) alive0 += alive[i] != 0;
+    std::vector<HostSeg> segs;
     if (n > 0) {
-        for (int k = 0; k < 6; ++k) PT_CUDA(cudaMemcpyAsync(d[k], hs[k], sizeof(double) * n, cudaMemcpyHostToDevice, st));
-        PT_CUDA(cudaMemcpyAsync(dal, alive, n, cudaMemcpyHostToDevice, st));
+        for (int k = 0; k < 6; ++k) segs.push_back(HostSeg{(char*)hs[k], (char*)d[k], sizeof(double) * (size_t)n});
+        segs.push_back(HostSeg{(char*)alive, (char*)dal, (size_t)n});
     }
-    PT_CUDA(cudaMemsetAsync(ddeaths.p, 0, sizeof(int64_t) * (size_t)nsteps, st));
+    const int64_t alive0 = count_nonzero(alive, n);
+    if ((rc = staged_h2d(segs, stage, stage_chunk, stage_nbuf, st))) return rc;
+    PT_CUDA(cudaMemsetAsync(d_deaths, 0, sizeof(int64_t) * (size_t)nsteps, st));
     pt_fast_state* fs = nullptr;
     if (p->precision == PT_PUSH_F32) {
-        rc = pt_fast_state_create(ctx, f, d[0], d[1], d[2], d[3], d[4], d[5], dal, n, &fs);
-        if (rc) return rc;
+        fs = ctx->run_fs;
+        if (fs && fs->n == n) {
+            // reuse the context's state buffers: import this call's particles
+            if (n > 0 && (rc = launch_fast_import(fs, f, d[0], d[1], d[2], d[3], d[4], d[5], dal, st))) return rc;
+            fs->field = f;
+            fs->last_sort = INT64_MIN;
+        } else {
+            if (fs) {
+                cudaStreamSynchronize(st);
+                pt_fast_state_destroy(fs);
+                ctx->run_fs = nullptr;
+            }
+            rc = pt_fast_state_create(ctx, f, d[0], d[1], d[2], d[3], d[4], d[5], dal, n, &fs);
+            if (rc) return rc;
+            ctx->run_fs = fs;
+        }
     }
     cudaEvent_t ev_done[2] = {nullptr, nullptr}, ev_copy[2] = {nullptr, nullptr};
     for (int k = 0; k < 2; ++k) {
@@ -537,7 +563,6 @@ int pt_push_run(pt_ctx* ctx, const pt_field* f, double* x1, double* x2, double* 
             cudaEventDestroy(ev_done[k]);
             cudaEventDestroy(ev_copy[k]);
         }
-        if (fs) pt_fast_state_destroy(fs);
         return code;
     };
     struct Pending {
@@ -549,7 +574,7 @@ int pt_push_run(pt_ctx* ctx, const pt_field* f, double* x1, double* x2, double* 
         if (!q.valid || q.rows == 0) return PT_OK;
         cudaError_t e = cudaEventSynchronize(ev_copy[q.slot]);
         if (e != cudaSuccess) return cuda_fail(e, "cache egress copy");
-        const char* base = (const char*)hslots.p + (size_t)q.slot * R * row_bytes;
+        const char* base = hslot_base + (size_t)q.slot * R * row_bytes;
         for (int64_t r = 0; r < q.rows; ++r)
             if (save(user, q.row_base + r, base + (size_t)r * row_bytes, (int64_t)row_bytes) != 0)
                 return fail(PT_ERR_CALLBACK, "save callback returned non-zero at save " + std::to_string(q.row_base + r));
@@ -561,20 +586,20 @@ int pt_push_run(pt_ctx* ctx, const pt_field* f, double* x1, double* x2, double* 
         const int slot = (int)(chunk & 1);
         const int64_t row_base = s0 / stride;
         const int64_t rows = row_bytes ? ((s0 + steps - 1) / stride - row_base + 1) : 0;
-        void* dslot = row_bytes ? (char*)dslots.p + (size_t)slot * R * row_bytes : nullptr;
+        void* dslot = row_bytes ? dslot_base + (size_t)slot * R * row_bytes : nullptr;
         if (chunk >= 2 && row_bytes) PT_CUDA(cudaStreamWaitEvent(st, ev_copy[slot], 0));
         if (p->precision == PT_PUSH_F64) {
             pt_push_params q = *p;
             rc = pt_push_advance_device(ctx, f, d[0], d[1], d[2], d[3], d[4], d[5], dal, n, &q, s0, steps, dslot,
-                                        row_base, rows, ddeaths.as<int64_t>());
+                                        row_base, rows, d_deaths);
         } else {
-            rc = advance_fast(ctx, f, fs, p, s0, steps, dslot, row_base, rows, ddeaths.as<int64_t>());
+            rc = advance_fast(ctx, f, fs, p, s0, steps, dslot, row_base, rows, d_deaths);
         }
         if (rc) return finish(rc);
         if (row_bytes) {
             PT_CUDA(cudaEventRecord(ev_done[slot], st));
             PT_CUDA(cudaStreamWaitEvent(ctx->copy_stream, ev_done[slot], 0));
-            PT_CUDA(cudaMemcpyAsync((char*)hslots.p + (size_t)slot * R * row_bytes, dslot, (size_t)rows * row_bytes,
+            PT_CUDA(cudaMemcpyAsync(hslot_base + (size_t)slot * R * row_bytes, dslot, (size_t)rows * row_bytes,
                                     cudaMemcpyDeviceToHost, ctx->copy_stream));
             PT_CUDA(cudaEventRecord(ev_copy[slot], ctx->copy_stream));
         }
@@ -588,12 +613,10 @@ int pt_push_run(pt_ctx* ctx, const pt_field* f, double* x1, double* x2, double* 
         rc = launch_fast_export(fs, f, d[0], d[1], d[2], d[3], d[4], d[5], dal, st);
         if (rc) return finish(rc);
     }
-    if (n > 0) {
-        for (int k = 0; k < 6; ++k) PT_CUDA(cudaMemcpyAsync(hs[k], d[k], sizeof(double) * n, cudaMemcpyDeviceToHost, st));
-        PT_CUDA(cudaMemcpyAsync(alive, dal, n, cudaMemcpyDeviceToHost, st));
-    }
+    rc = staged_d2h(segs, stage, stage_chunk, stage_nbuf, st);
+    if (rc) return finish(rc);
     std::vector<int64_t> deaths((size_t)nsteps);
-    PT_CUDA(cudaMemcpyAsync(deaths.data(), ddeaths.p, sizeof(int64_t) * (size_t)nsteps, cudaMemcpyDeviceToHost, st));
+    PT_CUDA(cudaMemcpyAsync(deaths.data(), d_deaths, sizeof(int64_t) * (size_t)nsteps, cudaMemcpyDeviceToHost, st));
     cudaError_t e = cudaStreamSynchronize(st);
     if (e != cudaSuccess) return finish(cuda_fail(e, "pt_push_run"));
     if (alive_count) {

@@ -51,6 +51,8 @@ struct pt_ctx {
     cudaStream_t stream = nullptr;      // stream used by *_device calls
     cudaStream_t copy_stream = nullptr; // egress copies in pt_push_run
     pt::ScratchBuf scratch[4];          // reusable device scratch, grown on demand
+    pt::ScratchBuf pinned;              // pinned host staging of pt_push_run, grown on demand
+    pt_fast_state* run_fs = nullptr;    // FP32-push state reused by pt_push_run
 };
 
 struct pt_field {
@@ -90,8 +92,27 @@ struct pt_fast_state {
 
 namespace pt {
 
+inline size_t align_up(size_t v, size_t a) { return (v + a - 1) / a * a; }
+
 // Grow-only device scratch owned by the context (slot = independent user).
+// Slots: 0 D_mumu, 1 D_pp, 2 pt_push_run state, 3 particle initialisation.
 int scratch_get(pt_ctx* ctx, int slot, size_t bytes, void** out);
+
+// ---------------------------------------------------------------- host I/O
+// Grow-only pinned host buffer of the context.
+int pinned_get(pt_ctx* ctx, size_t bytes, void** out);
+struct HostSeg {
+    char* host;  // pageable host bytes
+    char* dev;   // device bytes
+    size_t bytes;
+};
+// Copy every segment host -> device (or device -> host) on stream s through
+// nbuf pinned chunks of `chunk` bytes at `stage`, filled and drained by host
+// threads while the copy engine moves the previous chunk.  Both return after
+// the last byte has arrived.
+int staged_h2d(const std::vector<HostSeg>& segs, char* stage, size_t chunk, int nbuf, cudaStream_t s);
+int staged_d2h(const std::vector<HostSeg>& segs, char* stage, size_t chunk, int nbuf, cudaStream_t s);
+int64_t count_nonzero(const uint8_t* v, int64_t n);
 
 // ---------------------------------------------------------------- launches
 struct PushArgsRef {

@@ -178,3 +178,32 @@ def test_errors_raise(cuda):
         R.run_push_host(fl, copy_state(pb.state), np.ones(4, np.uint8), R.push_params(pb.dt, 10, 0))
     with pytest.raises(ValueError):
         R.run_push_host(fl, copy_state(pb.state), np.ones(3, np.uint8), R.push_params(pb.dt, 10, 1))
+
+
+@pytest.mark.parametrize("precision", ["f32", "f64"])
+def test_push_run_context_buffers_reused(cuda, precision):
+    """pt_push_run keeps its device state, pinned staging and FP32 state in the
+    context: calls of other sizes in between, and a call after pt_ctx_trim,
+    give the same result as the first call."""
+    pb = small_problem(n=16, n_particles=3000, u_over_c=1e-4)
+    fl = FieldLibrary(pb.fields, pb.grid, "brick_bf16" if precision == "f32" else "ref_f64")
+    params = R.push_params(pb.dt, 200, 4, cache="mu", precision=precision, sort_every=16 if precision == "f32" else 0)
+
+    def run(n):
+        st = {k: v[:n].copy() for k, v in pb.state.items()}
+        col = R.CacheCollector(n, R.n_saves(200, 4), "mu")
+        ac = R.run_push_host(fl, st, np.ones(n, np.uint8), params, col)
+        return col.mu, st, ac
+
+    first = run(3000)
+    small = run(1000)
+    again = run(3000)
+    fl.ctx.trim()
+    after_trim = run(3000)
+    for res in (again, after_trim):
+        assert np.array_equal(res[0], first[0], equal_nan=True)
+        for k in R.KEYS:
+            assert np.array_equal(res[1][k], first[1][k]), k
+        assert np.array_equal(res[2], first[2])
+    # the smaller run is the prefix of the larger one (particles are independent)
+    assert np.array_equal(small[0], first[0][:, :1000], equal_nan=True)
