@@ -30,6 +30,7 @@ namespace pt {
 namespace {
 
 constexpr int kWarp = 32;
+constexpr int kStageWarps = 8;  // warps of a particle slot that stage its series
 
 struct WelfordPart {
     long long count;
@@ -89,6 +90,14 @@ struct DmumuLaunch {
     double* part_sd2;
     WelfordPart* part_w;           // [grid][nl]
 };
+
+// bytes of one particle slot of dmumu_kernel (layout in the kernel)
+size_t dmumu_slot_bytes(int64_t nsave, size_t idx_bytes, int n_bins, int nl_cap)
+{
+    auto a16 = [](size_t v) { return (v + 15) & ~(size_t)15; };
+    return a16((size_t)nsave * sizeof(float)) + a16((size_t)nsave * idx_bytes) +
+           a16(sizeof(int) * (size_t)(kStageWarps * (n_bins + 1) + n_bins + 2)) + a16(16 * (size_t)nl_cap);
+}
 
 template <typename IdxT, bool SMEM_SLOTS>
 __global__ void __launch_bounds__(1024) dmumu_kernel(DmumuLaunch a)
@@ -153,16 +162,23 @@ __global__ void __launch_bounds__(1024) dmumu_kernel(DmumuLaunch a)
     if (L < 1 || L >= a.nsave) L = a.nsave;  // reference: lag >= nsteps -> skipped
     const int64_t lim = a.nsave - L;         // valid starts: s < lim
 
-    // slot layout: series[nsave] float | list[nsave] IdxT | hist[nb+1] int | cur[nb+2] int
-    //              | tot_c[nl] u64 | tot_sd2[nl] f64 (per-particle totals over the bins)
+    // slot layout: series[nsave] float | list[nsave] IdxT | whist[kStageWarps][nb+1] int
+    //              | cur[nb+2] int | tot_c[nl] u64 | tot_sd2[nl] f64 (per-particle totals over the bins)
     unsigned char* sb = slot_base + (size_t)slot * a.slot_bytes;
     float* series = (float*)sb;
     IdxT* list = (IdxT*)(sb + ((a.nsave * sizeof(float) + 15) & ~(size_t)15));
-    int* hist = (int*)((unsigned char*)list + ((a.nsave * sizeof(IdxT) + 15) & ~(size_t)15));
-    int* cur = hist + (nb + 1);
-    unsigned long long* tot_c =
-        (unsigned long long*)((unsigned char*)hist + ((sizeof(int) * (size_t)(2 * nb + 3) + 15) & ~(size_t)15));
+    int* whist = (int*)((unsigned char*)list + ((a.nsave * sizeof(IdxT) + 15) & ~(size_t)15));
+    int* cur = whist + kStageWarps * (nb + 1);
+    unsigned long long* tot_c = (unsigned long long*)((unsigned char*)whist +
+                                                      ((sizeof(int) * (size_t)(kStageWarps * (nb + 1) + nb + 2) + 15) &
+                                                       ~(size_t)15));
     double* tot_sd2 = (double*)(tot_c + nl);
+    // staging is shared by the first `stagers` warps of the slot, each taking a
+    // contiguous range of saves; per-warp bin counts, offset in warp order,
+    // give the same bin-sorted start list (ascending starts within a bin)
+    // as a single warp walking the series
+    const int wis = warp % wps;
+    const int stagers = min(wps, kStageWarps);
 
     long long wc = 0, pn = 0;
     double wm = 0.0, wm2 = 0.0, pss = 0.0;
@@ -174,54 +190,80 @@ __global__ void __launch_bounds__(1024) dmumu_kernel(DmumuLaunch a)
     for (int64_t tile = blockIdx.x; tile < tiles; tile += gridDim.x) {
         const int64_t p = tile * a.ppc + slot;
         const bool have = p < a.n;
-        // ---- stage (first warp of each slot)
-        if (group == 0 && part == 0 && have) {
-            for (int b = lane; b <= nb; b += kWarp) hist[b] = 0;
-            for (int l = lane; l < nl; l += kWarp) {
-                tot_c[l] = 0ull;
-                tot_sd2[l] = 0.0;
-            }
+        // ---- stage: series, per-warp bin counts
+        if (have && wis < stagers) {
+            const int64_t per = ((a.nsave + stagers - 1) / stagers + kWarp - 1) / kWarp * kWarp;
+            const int64_t st_begin = (int64_t)wis * per, st_end = min(a.nsave, st_begin + per);
+            int* my_hist = whist + wis * (nb + 1);
+            for (int b = lane; b <= nb; b += kWarp) my_hist[b] = 0;
+            if (wis == 0)
+                for (int l = lane; l < nl; l += kWarp) {
+                    tot_c[l] = 0ull;
+                    tot_sd2[l] = 0.0;
+                }
             __syncwarp();
             const float* src = a.mu + p * a.sp;
-            for (int64_t s0 = 0; s0 < a.nsave; s0 += kWarp) {
+            for (int64_t s0 = st_begin; s0 < st_end; s0 += kWarp) {
                 const int64_t s = s0 + lane;
-                float v = NAN;
                 int b = -1;
-                if (s < a.nsave) {
-                    v = src[s * a.ss];
+                if (s < st_end) {
+                    const float v = src[s * a.ss];
                     series[s] = v;
                     if (s < scap) b = bin_of(v, s_edges, nb, a.bin_abs);
                 }
                 const unsigned active = __ballot_sync(0xffffffffu, b >= 0);
                 if (b >= 0) {
                     const unsigned same = __match_any_sync(active, b);
-                    if ((same & lt_mask) == 0) hist[b] += __popc(same);
+                    if ((same & lt_mask) == 0) my_hist[b] += __popc(same);
                 }
                 __syncwarp();
             }
-            // exclusive scan of hist[0..nb] into cur[0..nb+1]
-            if (lane == 0) {
-                int run = 0;
-                for (int b = 0; b <= nb; ++b) {
-                    cur[b] = run;
-                    run += hist[b];
+        }
+        __syncthreads();
+        // ---- offsets: bin-major, then stager order within a bin
+        if (have && wis == 0) {
+            int carry = 0;
+            for (int b0 = 0; b0 <= nb; b0 += kWarp) {
+                const int b = b0 + lane;
+                int t = 0;
+                if (b <= nb)
+                    for (int w = 0; w < stagers; ++w) t += whist[w * (nb + 1) + b];
+                int incl = t;
+                for (int d = 1; d < kWarp; d <<= 1) {
+                    const int y = __shfl_up_sync(0xffffffffu, incl, d);
+                    if (lane >= d) incl += y;
                 }
-                cur[nb + 1] = run;
+                if (b <= nb) {
+                    int run = carry + incl - t;
+                    cur[b] = run;
+                    for (int w = 0; w < stagers; ++w) {
+                        const int c = whist[w * (nb + 1) + b];
+                        whist[w * (nb + 1) + b] = run;
+                        run += c;
+                    }
+                }
+                carry += __shfl_sync(0xffffffffu, incl, kWarp - 1);
             }
-            __syncwarp();
-            for (int b = lane; b <= nb; b += kWarp) hist[b] = cur[b];  // hist becomes the scatter cursor
-            __syncwarp();
-            for (int64_t s0 = 0; s0 < scap; s0 += kWarp) {
+            if (lane == 0) cur[nb + 1] = carry;
+        }
+        __syncthreads();
+        // ---- scatter each stager's starts in order
+        if (have && wis < stagers) {
+            const int64_t per = ((a.nsave + stagers - 1) / stagers + kWarp - 1) / kWarp * kWarp;
+            const int64_t st_begin = (int64_t)wis * per, st_end = min(a.nsave, st_begin + per);
+            int* my_hist = whist + wis * (nb + 1);
+            const int64_t end = min(st_end, scap);
+            for (int64_t s0 = st_begin; s0 < end; s0 += kWarp) {
                 const int64_t s = s0 + lane;
                 int b = -1;
-                if (s < scap) b = bin_of(series[s], s_edges, nb, a.bin_abs);
+                if (s < end) b = bin_of(series[s], s_edges, nb, a.bin_abs);
                 const unsigned active = __ballot_sync(0xffffffffu, b >= 0);
                 if (b >= 0) {
                     const unsigned same = __match_any_sync(active, b);
                     const int rank = __popc(same & lt_mask);
-                    list[hist[b] + rank] = (IdxT)s;
+                    list[my_hist[b] + rank] = (IdxT)s;
                     __syncwarp(active);
-                    if (rank == 0) hist[b] += __popc(same);
+                    if (rank == 0) my_hist[b] += __popc(same);
                 }
                 __syncwarp();
             }
@@ -552,8 +594,7 @@ int run_dmumu(pt_ctx* ctx, const DmumuArgs& a, cudaStream_t s)
     // lags per launch: multiple of 32 with the accumulators taking <= ~half the budget
     int nl_cap = (int)std::max<size_t>(32, ((budget / 2) / ((size_t)a.n_bins * 24)) / 32 * 32);
     nl_cap = std::min(nl_cap, 32 * 8);
-    const size_t slot_bytes = align16(a.nsave * sizeof(float)) + align16(a.nsave * idx_bytes) +
-                              align16(sizeof(int) * (size_t)(2 * a.n_bins + 3)) + align16(16 * (size_t)nl_cap);
+    const size_t slot_bytes = dmumu_slot_bytes(a.nsave, idx_bytes, a.n_bins, nl_cap);
     const int lag_batches = (a.n_lags + nl_cap - 1) / nl_cap;
     for (int lb = 0; lb < lag_batches; ++lb) {
         const int lag0 = lb * nl_cap;
@@ -756,8 +797,7 @@ int run_dmumu_noalloc(pt_ctx* ctx, const DmumuArgs& a, cudaStream_t s)
     const size_t edge_bytes = align16(sizeof(double) * (size_t)(a.n_bins + 1));
     int nl_cap = (int)std::max<size_t>(32, ((budget / 2) / ((size_t)a.n_bins * 24)) / 32 * 32);
     nl_cap = std::min(nl_cap, 32 * 8);
-    const size_t slot_bytes = align16(a.nsave * sizeof(float)) + align16(a.nsave * idx_bytes) +
-                              align16(sizeof(int) * (size_t)(2 * a.n_bins + 3)) + align16(16 * (size_t)nl_cap);
+    const size_t slot_bytes = dmumu_slot_bytes(a.nsave, idx_bytes, a.n_bins, nl_cap);
     for (int lag0 = 0; lag0 < a.n_lags; lag0 += nl_cap) {
         const int nl = std::min(nl_cap, a.n_lags - lag0);
         const int groups = (nl + kWarp - 1) / kWarp;

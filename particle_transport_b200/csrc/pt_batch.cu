@@ -110,7 +110,8 @@ int rebuild_tables(pt_batch* b, int fresh)
         b->hist_cap = 0;
         const int64_t want = std::max<int64_t>(key, 2 * b->hist_cap);
         cudaError_t e = cudaMalloc((void**)&b->hist, sizeof(uint32_t) * want);
-        if (e == cudaSuccess) e = cudaMalloc((void**)&b->cursor, sizeof(uint32_t) * want);
+        // cursor[want] followed by the scan's per-tile offsets
+        if (e == cudaSuccess) e = cudaMalloc((void**)&b->cursor, sizeof(uint32_t) * (want + sort_scan_tiles(want)));
         if (e != cudaSuccess) {
             cudaGetLastError();
             return fail(PT_ERR_OOM, "batch sort buckets allocation failed");

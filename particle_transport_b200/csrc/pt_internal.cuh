@@ -213,6 +213,11 @@ struct BatchLaunch {
 };
 int launch_push_batch(const BatchLaunch& L, cudaStream_t s);
 int launch_batch_epoch_end(BatchCampaignDev* camps, int n_camps, int* tile_counter, cudaStream_t s);
+// buckets per tile of the two-level bucket scan of the brick sorts, and the
+// number of tile offsets that follow the cursor array of m buckets
+constexpr int64_t kSortScanTile = 2048;
+inline int64_t sort_scan_tiles(int64_t m) { return (m + kSortScanTile - 1) / kSortScanTile; }
+// cursor must hold max_buckets + sort_scan_tiles(max_buckets) entries
 int launch_batch_sort(const BatchCampaignDev* camps, const int32_t* camp_of, BatchStateDev from, BatchStateDev to,
                       uint32_t* keys, uint32_t* hist, uint32_t* cursor, const int64_t* d_m_buckets,
                       int64_t max_buckets, int num_sms, cudaStream_t s);

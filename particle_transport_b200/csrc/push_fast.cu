@@ -381,34 +381,81 @@ __global__ void sort_key_kernel(const double* __restrict__ xs, const uint8_t* __
     }
 }
 
-// Exclusive scan of hist[0..m) into cursor[0..m) by one block of 1024 threads.
-__global__ void __launch_bounds__(1024) sort_scan_kernel(const uint32_t* __restrict__ hist, uint32_t* cursor,
-                                                         int64_t m)
+// Exclusive scan of hist[0..m) in two levels: sort_scan_tiles_kernel writes
+// each 2048-bucket tile's in-tile exclusive prefix to cursor and the tile's
+// total to tile_off; sort_scan_top_kernel turns tile_off into the tiles'
+// exclusive offsets.  The scatter adds tile_off[key / 2048] to the cursor.
+constexpr int kScanTile = (int)kSortScanTile;
+
+__device__ __forceinline__ uint32_t warp_incl_scan(uint32_t v, int lane)
 {
-    __shared__ uint32_t part[1024];
-    const int t = threadIdx.x;
-    const int64_t per = (m + 1023) / 1024;
-    const int64_t b = t * per, e = min(m, b + per);
-    uint32_t sum = 0;
-    for (int64_t i = b; i < e; ++i) sum += hist[i];
-    part[t] = sum;
-    __syncthreads();
-    for (int off = 1; off < 1024; off <<= 1) {
-        uint32_t v = t >= off ? part[t - off] : 0u;
-        __syncthreads();
-        part[t] += v;
-        __syncthreads();
+    for (int d = 1; d < 32; d <<= 1) {
+        const uint32_t y = __shfl_up_sync(0xffffffffu, v, d);
+        if (lane >= d) v += y;
     }
-    uint32_t run = part[t] - sum;
-    for (int64_t i = b; i < e; ++i) {
-        uint32_t h = hist[i];
-        cursor[i] = run;
-        run += h;
+    return v;
+}
+
+// m_dev, when not null, holds the bucket count (read on the device: the batch
+// sort runs inside CUDA graphs while its bucket count changes)
+__global__ void __launch_bounds__(1024) sort_scan_tiles_kernel(const uint32_t* __restrict__ hist,
+                                                               uint32_t* __restrict__ cursor,
+                                                               uint32_t* __restrict__ tile_off, int64_t m,
+                                                               const int64_t* __restrict__ m_dev)
+{
+    __shared__ uint32_t wsum[32];
+    if (m_dev) m = *m_dev;
+    if ((int64_t)blockIdx.x * kScanTile >= m) return;
+    const int t = threadIdx.x, lane = t & 31, w = t >> 5;
+    const int64_t i0 = (int64_t)blockIdx.x * kScanTile + 2 * t;
+    const uint32_t a = i0 < m ? hist[i0] : 0u;
+    const uint32_t b = i0 + 1 < m ? hist[i0 + 1] : 0u;
+    const uint32_t own = a + b;
+    const uint32_t incl = warp_incl_scan(own, lane);
+    if (lane == 31) wsum[w] = incl;
+    __syncthreads();
+    if (w == 0) {
+        const uint32_t v = wsum[lane];
+        const uint32_t vi = warp_incl_scan(v, lane);
+        wsum[lane] = vi - v;
+        if (lane == 31) tile_off[blockIdx.x] = vi;
+    }
+    __syncthreads();
+    const uint32_t excl = wsum[w] + incl - own;
+    if (i0 < m) cursor[i0] = excl;
+    if (i0 + 1 < m) cursor[i0 + 1] = excl + a;
+}
+
+__global__ void __launch_bounds__(1024) sort_scan_top_kernel(uint32_t* tile_off, int64_t tiles,
+                                                             const int64_t* __restrict__ m_dev)
+{
+    __shared__ uint32_t wsum[32];
+    __shared__ uint32_t carry;
+    const int t = threadIdx.x, lane = t & 31, w = t >> 5;
+    if (m_dev) tiles = (*m_dev + kScanTile - 1) / kScanTile;
+    if (t == 0) carry = 0u;
+    __syncthreads();
+    for (int64_t base = 0; base < tiles; base += 1024) {
+        const int64_t i = base + t;
+        const uint32_t v = i < tiles ? tile_off[i] : 0u;
+        const uint32_t incl = warp_incl_scan(v, lane);
+        if (lane == 31) wsum[w] = incl;
+        __syncthreads();
+        if (w == 0) {
+            const uint32_t x = wsum[lane];
+            wsum[lane] = warp_incl_scan(x, lane) - x;
+        }
+        __syncthreads();
+        const uint32_t excl = carry + wsum[w] + incl - v;
+        __syncthreads();  // every thread has read carry
+        if (i < tiles) tile_off[i] = excl;
+        if (t == 1023) carry = excl + v;
+        __syncthreads();
     }
 }
 
-__global__ void sort_scatter_kernel(const uint32_t* __restrict__ keys, uint32_t* cursor, int64_t n,
-                                    const double* __restrict__ xs, const float* __restrict__ ps,
+__global__ void sort_scatter_kernel(const uint32_t* __restrict__ keys, uint32_t* cursor,
+                                    const uint32_t* __restrict__ tile_off, int64_t n, const double* __restrict__ xs, const float* __restrict__ ps,
                                     const double* __restrict__ p2s, const int32_t* __restrict__ pids,
                                     const uint8_t* __restrict__ as, double* xd, float* pd, double* p2d, int32_t* pidd,
                                     uint8_t* ad)
@@ -425,7 +472,7 @@ __global__ void sort_scatter_kernel(const uint32_t* __restrict__ keys, uint32_t*
         const unsigned same = __match_any_sync(act, key);
         const int leader = __ffs(same) - 1;
         uint32_t first = 0;
-        if (lane == leader) first = atomicAdd(&cursor[key], (uint32_t)__popc(same));
+        if (lane == leader) first = atomicAdd(&cursor[key], (uint32_t)__popc(same)) + tile_off[key / kScanTile];
         first = __shfl_sync(same, first, leader);
         const int64_t d = (int64_t)first + __popc(same & lt);
         xd[d] = xs[i]; xd[n + d] = xs[n + i]; xd[2 * n + d] = xs[2 * n + i];
@@ -540,8 +587,9 @@ int fast_sort(pt_ctx* ctx, pt_fast_state* st, const pt_field* f, cudaStream_t s)
         off += (bytes + 255) & ~(size_t)255;
         return o;
     };
+    const int64_t tiles = (m + kScanTile - 1) / kScanTile;
     const size_t o_keys = take(sizeof(uint32_t) * n), o_hist = take(sizeof(uint32_t) * m),
-                 o_cur = take(sizeof(uint32_t) * m);
+                 o_cur = take(sizeof(uint32_t) * m), o_tiles = take(sizeof(uint32_t) * tiles);
     if (st->sort_tmp_bytes < off) {
         if (st->sort_tmp) cudaFree(st->sort_tmp);
         st->sort_tmp = nullptr;
@@ -568,15 +616,18 @@ int fast_sort(pt_ctx* ctx, pt_fast_state* st, const pt_field* f, cudaStream_t s)
     uint32_t* keys = (uint32_t*)(base + o_keys);
     uint32_t* hist = (uint32_t*)(base + o_hist);
     uint32_t* cur = (uint32_t*)(base + o_cur);
+    uint32_t* tile_off = (uint32_t*)(base + o_tiles);
     PT_CUDA(cudaMemsetAsync(hist, 0, sizeof(uint32_t) * m, s));
     const int gb = grid_for(n, 256, ctx->num_sms);
     sort_key_kernel<<<gb, 256, 0, s>>>(st->x, st->alive, n, f->offs, (int)f->grid.nx, (int)f->grid.ny,
                                        (int)f->grid.nz, nb, keys, hist);
     PT_CHECK_LAUNCH("sort_key_kernel");
-    sort_scan_kernel<<<1, 1024, 0, s>>>(hist, cur, m);
-    PT_CHECK_LAUNCH("sort_scan_kernel");
-    sort_scatter_kernel<<<gb, 256, 0, s>>>(keys, cur, n, st->x, st->p, st->p2, st->pid, st->alive, st->x_alt,
-                                           st->p_alt, st->p2_alt, st->pid_alt, st->alive_alt);
+    sort_scan_tiles_kernel<<<(unsigned)tiles, 1024, 0, s>>>(hist, cur, tile_off, m, nullptr);
+    PT_CHECK_LAUNCH("sort_scan_tiles_kernel");
+    sort_scan_top_kernel<<<1, 1024, 0, s>>>(tile_off, tiles, nullptr);
+    PT_CHECK_LAUNCH("sort_scan_top_kernel");
+    sort_scatter_kernel<<<gb, 256, 0, s>>>(keys, cur, tile_off, n, st->x, st->p, st->p2, st->pid, st->alive,
+                                           st->x_alt, st->p_alt, st->p2_alt, st->pid_alt, st->alive_alt);
     PT_CHECK_LAUNCH("sort_scatter_kernel");
     std::swap(st->x, st->x_alt);
     std::swap(st->p, st->p_alt);
@@ -668,33 +719,6 @@ __global__ void zero_counted_kernel(uint32_t* a, const int64_t* m)
         a[i] = 0u;
 }
 
-// exclusive scan of hist[0..*m) by one block (bucket count read on the device)
-__global__ void __launch_bounds__(1024) scan_counted_kernel(const uint32_t* __restrict__ hist, uint32_t* cursor,
-                                                            const int64_t* m_dev)
-{
-    __shared__ uint32_t part[1024];
-    const int64_t m = *m_dev;
-    const int t = threadIdx.x;
-    const int64_t per = (m + 1023) / 1024;
-    const int64_t b = t * per, e = min(m, b + per);
-    uint32_t sum = 0;
-    for (int64_t i = b; i < e; ++i) sum += hist[i];
-    part[t] = sum;
-    __syncthreads();
-    for (int off = 1; off < 1024; off <<= 1) {
-        uint32_t v = t >= off ? part[t - off] : 0u;
-        __syncthreads();
-        part[t] += v;
-        __syncthreads();
-    }
-    uint32_t run = part[t] - sum;
-    for (int64_t i = b; i < e; ++i) {
-        uint32_t h = hist[i];
-        cursor[i] = run;
-        run += h;
-    }
-}
-
 // Sort key of every occupied slot: the campaign's first bucket + the brick of
 // the particle's cell (the campaign's dead bucket for dead particles).  Free
 // slots (camp_of < 0) take no part.
@@ -732,7 +756,7 @@ __global__ void batch_key_kernel(const BatchCampaignDev* __restrict__ camps, con
 }
 
 __global__ void batch_scatter_kernel(const uint32_t* __restrict__ keys, uint32_t* cursor,
-                                     const BatchCampaignDev* __restrict__ camps, const int32_t* __restrict__ camp_of,
+                                     const uint32_t* __restrict__ tile_off, const BatchCampaignDev* __restrict__ camps, const int32_t* __restrict__ camp_of,
                                      BatchStateDev from, BatchStateDev to)
 {
     const int lane = threadIdx.x & 31;
@@ -749,7 +773,7 @@ __global__ void batch_scatter_kernel(const uint32_t* __restrict__ keys, uint32_t
         const unsigned same = __match_any_sync(act, key);
         const int leader = __ffs(same) - 1;
         uint32_t first = 0;
-        if (lane == leader) first = atomicAdd(&cursor[key], (uint32_t)__popc(same));
+        if (lane == leader) first = atomicAdd(&cursor[key], (uint32_t)__popc(same)) + tile_off[key / kScanTile];
         first = __shfl_sync(same, first, leader);
         const int64_t d = (int64_t)first + __popc(same & lt) + camps[c].shift;
         to.x[d] = from.x[i]; to.x[cap + d] = from.x[cap + i]; to.x[2 * cap + d] = from.x[2 * cap + i];
@@ -834,9 +858,14 @@ int launch_batch_sort(const BatchCampaignDev* camps, const int32_t* camp_of, Bat
     const int gb = grid_for(from.cap, 256, num_sms);
     batch_key_kernel<<<gb, 256, 0, s>>>(camps, camp_of, from, keys, hist);
     PT_CHECK_LAUNCH("batch_key_kernel");
-    scan_counted_kernel<<<1, 1024, 0, s>>>(hist, cursor, d_m);
-    PT_CHECK_LAUNCH("scan_counted_kernel");
-    batch_scatter_kernel<<<gb, 256, 0, s>>>(keys, cursor, camps, camp_of, from, to);
+    uint32_t* tile_off = cursor + max_buckets;
+    const int64_t max_tiles = sort_scan_tiles(max_buckets);
+    sort_scan_tiles_kernel<<<(unsigned)std::max<int64_t>(max_tiles, 1), 1024, 0, s>>>(hist, cursor, tile_off,
+                                                                                    max_buckets, d_m);
+    PT_CHECK_LAUNCH("sort_scan_tiles_kernel");
+    sort_scan_top_kernel<<<1, 1024, 0, s>>>(tile_off, max_tiles, d_m);
+    PT_CHECK_LAUNCH("sort_scan_top_kernel");
+    batch_scatter_kernel<<<gb, 256, 0, s>>>(keys, cursor, tile_off, camps, camp_of, from, to);
     PT_CHECK_LAUNCH("batch_scatter_kernel");
     return PT_OK;
 }
