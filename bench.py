@@ -463,8 +463,31 @@ def run_ours(args, ws, rank, local):
                                     sort_every=args.sort_every, kernel_variant=args.variant), 0, NSTEPS, ps, 0, nsave)
         torch.cuda.synchronize()
         ps_push_s = time.perf_counter() - t0
+        del ens_p
+        # phase-space D_mumu on the device: mu reconstructed (FP32, the reference's
+        # default compute precision) into a device chunk and binned there, 64 log
+        # lags x 50 |mu| bins; no host round trip
+        lags_m = log_spaced_lag_steps(nsave - 1, 64)
+        edges_m, _ = build_mu_edges_full(0.0, 1.0, 50)
+        Bf = [f.float().contiguous() for f in fields[:3]]
+
+        def ps_dmumu_pass(_k):
+            acc = S.new_dmumu_accumulators(len(lags_m), 50, device=dev)
+            S.process_phase_space_chunk_dmumu(ps[:, 0:3], ps[:, 3:6], *Bf, grid, lags_m, edges_m,
+                                              acc["particle_counts"], acc["particle_means"], acc["particle_m2s"],
+                                              acc["pair_sum_squares"], acc["pair_counts"], acc["dmumu_counts"],
+                                              acc["dmumu_sum_delta"], acc["dmumu_sum_delta2"])
+            ps_dmumu_pass.acc = acc
+
+        pms, _ = timed(ps_dmumu_pass, 2, 1, torch)
+        ppairs = int(ps_dmumu_pass.acc["pair_counts"].sum().item())
+        ps_dmumu = {"value": ws * ppairs / max_over_ranks(pms / 2, ws, dev) * 1e3, "unit": "lag-pairs/s",
+                    "pairs_per_pass": ppairs, "ms_per_pass": pms / 2, "particles": npp, "saves": nsave,
+                    "lags": int(len(lags_m)), "mu_bins": 50, "compute_precision": "f32",
+                    "path": "pt_dmumu_accumulate_phase_space_device (reconstruct + bin on the device)",
+                    "compulsory_bytes_per_pass": 24 * npp * nsave}
         mom = ps[:, 3:6, :].contiguous()
-        del ps, ens_p
+        del ps, Bf
         torch.cuda.empty_cache()
         lags_p = log_spaced_lag_steps(nsave - 1, 64)
         p0 = float(torch.linalg.vector_norm(mom[0, :, 0].double()).item())
@@ -492,6 +515,7 @@ def run_ours(args, ws, rank, local):
                "compulsory_bytes_per_pass": 12 * npp * nsave,
                "hbm_frac_of_compulsory": (12 * npp * nsave / dpp_s / 1e9) / peaks["hbm_gbs"],
                "phase_space_push_s": ps_push_s, "phase_space_push_rate": npp * (NSTEPS - 1) / ps_push_s,
+               "phase_space_dmumu": ps_dmumu,
                "energy_histograms": {"snapshots": int(len(snaps)), "bins": 256, "range_GeV": [e_lo, e_hi],
                                      "spacing": "log", "ms_per_pass": hms / 3,
                                      "counted": int(hist_pass.counts.sum().item()),

@@ -258,6 +258,32 @@ int pt_dmumu_accumulate_device(pt_ctx* ctx, const float* d_mu, int64_t n, int64_
                                int64_t* d_pair_n);
 
 /*
+ * Fused phase-space D_mumu: the body of the phase-space branch of the D_mumu
+ * driver (src/compute_delta_mu2_dmumu_full.jl:1137-1164) on the device --
+ * reconstruct_mu_chunk_gpu (src/compute_delta_mu2_curve.jl:186-225) feeding
+ * process_mu_chunk_dmumu_cpu! -- without the mu chunk leaving the device: mu
+ * is reconstructed into a device scratch chunk (at most 1 GiB of particles,
+ * with B read as interleaved node records) and binned there.
+ * d_pos / d_mom: positions (m) and momenta (kg m/s), component c of save s of
+ * particle p at base + s*row_stride + c*comp_stride + p (the Julia
+ * (chunk, 3, nsave) datasets: row_stride = 3*chunk, comp_stride = chunk; the
+ * device phase-space cache [nsave][6][n]: d_mom = d_pos + 3n, row_stride = 6n,
+ * comp_stride = n).  f64 selects the compute precision T of the reference
+ * (0: Float32, the default; 1: Float64); positions, momenta and d_bfield
+ * ({Bx, By, Bz} column-major, nx*ny*nz each) are in T.  mu is bit-identical
+ * to pt_reconstruct_mu at the same precision; the accumulators are those of
+ * pt_dmumu_accumulate_device (device pointers, add-into).  No reference
+ * counterpart as a single function.
+ */
+int pt_dmumu_accumulate_phase_space_device(pt_ctx* ctx, const void* d_pos, const void* d_mom, int64_t n,
+                                           int64_t nsave, int64_t row_stride, int64_t comp_stride,
+                                           const void* const d_bfield[3], const pt_grid* grid, int f64,
+                                           const int64_t* d_lag_steps, int n_lags, const double* d_mu_edges,
+                                           int n_bins, int start_mode, int bin_abs, int64_t* d_counts,
+                                           double* d_sum_d, double* d_sum_d2, int64_t* d_w_count, double* d_w_mean,
+                                           double* d_w_m2, double* d_pair_ss, int64_t* d_pair_n);
+
+/*
  * Same as pt_dmumu_accumulate_device, but allocates no device memory: no
  * cudaMalloc / cudaFree and no allocating library call.  It has no
  * counterpart in the reference.  It is for callers that cannot let a

@@ -55,6 +55,8 @@ def lib():
         L.or_dmumu_accumulate.restype = None
         L.or_dmumu_accumulate.argtypes = [P, i64, i64, i64, i64, P, i32, P, i32, i32, i32, P, P, P, P, P, P, P, P,
                                           i32]
+        L.or_dmumu_accumulate_f64.restype = None
+        L.or_dmumu_accumulate_f64.argtypes = L.or_dmumu_accumulate.argtypes
         L.or_dpp_accumulate.restype = None
         L.or_dpp_accumulate.argtypes = [P, i64, i64, P, i32, d, P, P, P, P, P, i32]
         L.or_energy_snapshots.restype = None
@@ -150,10 +152,12 @@ def reconstruct_mu_f32(pos, mom, bfields, grid, nthreads=0):
 
 
 def dmumu_accumulate(mu, lag_steps, edges, acc, injection=False, bin_abs=True, time_fastest=True, nthreads=0):
-    """mu: (chunk, nsave) if time_fastest else (nsave, chunk) float32.
+    """mu: (chunk, nsave) if time_fastest else (nsave, chunk), float32 (or
+    float64: a mu chunk at compute precision Float64).
     acc: dict with counts/sum_d/sum_d2 shaped (n_lags, n_bins) and the per-lag
     w_count/w_mean/w_m2/pair_ss/pair_n arrays (add-into)."""
-    mu = np.ascontiguousarray(mu, dtype=np.float32)
+    f64 = np.asarray(mu).dtype == np.float64
+    mu = np.ascontiguousarray(mu, dtype=np.float64 if f64 else np.float32)
     if time_fastest:
         chunk, nsave = mu.shape
         sp, ss = nsave, 1
@@ -162,10 +166,10 @@ def dmumu_accumulate(mu, lag_steps, edges, acc, injection=False, bin_abs=True, t
         sp, ss = 1, chunk
     lags = np.ascontiguousarray(lag_steps, dtype=np.int64)
     e = np.ascontiguousarray(edges, dtype=np.float64)
-    lib().or_dmumu_accumulate(_p(mu), chunk, nsave, sp, ss, _p(lags), len(lags), _p(e), len(e) - 1,
-                              int(injection), int(bin_abs), _p(acc["counts"]), _p(acc["sum_d"]),
-                              _p(acc["sum_d2"]), _p(acc["w_count"]), _p(acc["w_mean"]), _p(acc["w_m2"]),
-                              _p(acc["pair_ss"]), _p(acc["pair_n"]), nthreads)
+    fn = lib().or_dmumu_accumulate_f64 if f64 else lib().or_dmumu_accumulate
+    fn(_p(mu), chunk, nsave, sp, ss, _p(lags), len(lags), _p(e), len(e) - 1, int(injection), int(bin_abs),
+       _p(acc["counts"]), _p(acc["sum_d"]), _p(acc["sum_d2"]), _p(acc["w_count"]), _p(acc["w_mean"]), _p(acc["w_m2"]),
+       _p(acc["pair_ss"]), _p(acc["pair_n"]), nthreads)
     return acc
 
 

@@ -369,10 +369,19 @@ void or_combine_welford(int64_t* counts, double* means, double* m2s, int64_t lag
  * Threads keep private accumulators merged in thread order, as the reference
  * does per Threads.threadid().
  */
-void or_dmumu_accumulate(const float* mu, int64_t chunk, int64_t nsave, int64_t sp, int64_t ss,
-                         const int64_t* lag_steps, int n_lags, const double* edges, int n_bins, int injection,
-                         int bin_abs, int64_t* counts, double* sum_d, double* sum_d2, int64_t* w_count,
-                         double* w_mean, double* w_m2, double* pair_ss, int64_t* pair_n, int nthreads)
+/* mu of (particle p, save s): a Float32 chunk (the cache default) or a
+ * Float64 chunk (compute_precision = Float64 in the phase-space path); the
+ * reference reads Float64(mu_chunk[s, p]) either way (dmumu:509-510). */
+static inline double or_mu_at_index(const float* mu32, const double* mu64, int64_t i)
+{
+    return mu32 ? (double)mu32[i] : mu64[i];
+}
+
+static void or_dmumu_core(const float* mu, const double* mu64, int64_t chunk, int64_t nsave, int64_t sp,
+                          int64_t ss, const int64_t* lag_steps, int n_lags, const double* edges, int n_bins,
+                          int injection, int bin_abs, int64_t* counts, double* sum_d, double* sum_d2,
+                          int64_t* w_count, double* w_mean, double* w_m2, double* pair_ss, int64_t* pair_n,
+                          int nthreads)
 {
     int nt = 1;
 #ifdef _OPENMP
@@ -410,8 +419,8 @@ void or_dmumu_accumulate(const float* mu, int64_t chunk, int64_t nsave, int64_t 
             double particle_sumsq = 0.0;
             int64_t valid = 0;
             for (int64_t s = 0; s < last_start; ++s) {
-                double a = (double)mu[p * sp + s * ss];
-                double b = (double)mu[p * sp + (s + lag) * ss];
+                double a = or_mu_at_index(mu, mu64, p * sp + s * ss);
+                double b = or_mu_at_index(mu, mu64, p * sp + (s + lag) * ss);
                 if (!(isfinite(a) && isfinite(b))) continue;
                 double dm = b - a;
                 double dm2 = dm * dm;
@@ -448,6 +457,24 @@ void or_dmumu_accumulate(const float* mu, int64_t chunk, int64_t nsave, int64_t 
         }
     }
     free(lc); free(ld); free(ld2); free(tpc); free(tpm); free(tpm2); free(tss); free(tpn);
+}
+
+void or_dmumu_accumulate(const float* mu, int64_t chunk, int64_t nsave, int64_t sp, int64_t ss,
+                         const int64_t* lag_steps, int n_lags, const double* edges, int n_bins, int injection,
+                         int bin_abs, int64_t* counts, double* sum_d, double* sum_d2, int64_t* w_count,
+                         double* w_mean, double* w_m2, double* pair_ss, int64_t* pair_n, int nthreads)
+{
+    or_dmumu_core(mu, NULL, chunk, nsave, sp, ss, lag_steps, n_lags, edges, n_bins, injection, bin_abs, counts,
+                  sum_d, sum_d2, w_count, w_mean, w_m2, pair_ss, pair_n, nthreads);
+}
+
+void or_dmumu_accumulate_f64(const double* mu, int64_t chunk, int64_t nsave, int64_t sp, int64_t ss,
+                             const int64_t* lag_steps, int n_lags, const double* edges, int n_bins, int injection,
+                             int bin_abs, int64_t* counts, double* sum_d, double* sum_d2, int64_t* w_count,
+                             double* w_mean, double* w_m2, double* pair_ss, int64_t* pair_n, int nthreads)
+{
+    or_dmumu_core(NULL, mu, chunk, nsave, sp, ss, lag_steps, n_lags, edges, n_bins, injection, bin_abs, counts,
+                  sum_d, sum_d2, w_count, w_mean, w_m2, pair_ss, pair_n, nthreads);
 }
 
 /* momentum_magnitude: src/compute_dpp_full.jl:232-234 */

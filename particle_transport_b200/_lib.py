@@ -34,7 +34,7 @@ EXPORTS = (
     "pt_fast_state_sort", "pt_push_advance_fast", "pt_batch_create", "pt_batch_add", "pt_batch_remove",
     "pt_batch_run", "pt_batch_step", "pt_batch_export", "pt_batch_destroy", "pt_dmumu_accumulate",
     "pt_dmumu_accumulate_device",
-    "pt_dmumu_accumulate_device_noalloc", "pt_dpp_accumulate",
+    "pt_dmumu_accumulate_device_noalloc", "pt_dmumu_accumulate_phase_space_device", "pt_dpp_accumulate",
     "pt_dpp_accumulate_device", "pt_energy_snapshots", "pt_energy_histogram_device", "pt_reconstruct_mu",
     "pt_particles_init_device",
 )
@@ -136,6 +136,8 @@ def load():
                                                  P, P, P]),
             "pt_dmumu_accumulate_device_noalloc": (i32, [P, P, i64, i64, i64, i64, P, i32, P, i32, i32, i32, P, P, P,
                                                          P, P, P, P, P]),
+            "pt_dmumu_accumulate_phase_space_device": (i32, [P, P, P, i64, i64, i64, i64, P, C.POINTER(Grid), i32, P,
+                                                             i32, P, i32, i32, i32, P, P, P, P, P, P, P, P]),
             "pt_dpp_accumulate": (i32, [P, P, i64, i64, P, i32, d, P, P, P, P, P]),
             "pt_dpp_accumulate_device": (i32, [P, P, i64, i64, P, i32, d, P, P, P, P, P]),
             "pt_energy_snapshots": (i32, [P, P, i64, i64, P, i32, i64, P]),

@@ -1,10 +1,12 @@
 """Build recipe for libptb200.so (sm_100a).
 
 Each translation unit is compiled by nvcc for ``sm_100a`` only and linked
-in-tree into ``particle_transport_b200/libptb200.so``.  ``push_exact.cu`` and
-``init.cu`` are compiled with ``--fmad=false`` so that the FP64 parity push,
-the mu reconstruction and the particle initialisation keep the reference's
-rounding (no fused multiply-add); the other units keep FMA contraction on.
+in-tree into ``particle_transport_b200/libptb200.so``.  ``push_exact.cu``,
+``lagstats.cu`` and ``init.cu`` are compiled with ``--fmad=false`` so that
+the FP64 parity push, the mu reconstruction (also inside the fused
+phase-space binning), the statistics and the particle initialisation keep
+the reference's rounding (no fused multiply-add; explicit ``fma`` calls
+stay); the other units keep FMA contraction on.
 """
 from __future__ import annotations
 
@@ -25,7 +27,7 @@ UNITS = {
     "push_exact.cu": ["--fmad=false"],
     "init.cu": ["--fmad=false"],
     "push_fast.cu": [],
-    "lagstats.cu": [],
+    "lagstats.cu": ["--fmad=false"],
     "pt_api.cu": [],
     "pt_batch.cu": [],
     "hostio.cu": [],
@@ -48,7 +50,7 @@ def _stale(out: str, deps) -> bool:
 
 def build(force: bool = False, verbose: bool = False, extra=()) -> str:
     os.makedirs(BUILD, exist_ok=True)
-    headers = [os.path.join(CSRC, "pt_internal.cuh"), os.path.join(INCLUDE, "ptb200.h")]
+    headers = [os.path.join(CSRC, h) for h in ("pt_internal.cuh", "exact_mu.cuh")] + [os.path.join(INCLUDE, "ptb200.h")]
     objs = []
     for unit, flags in UNITS.items():
         src = os.path.join(CSRC, unit)

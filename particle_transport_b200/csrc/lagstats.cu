@@ -22,6 +22,7 @@
 // the whole launch; the normalised sums sum(dp/p0) = sum(dp)/p0 and
 // sum((dp/p0)^2) = sum(dp^2)/p0^2 are formed once per lag at the end, which
 // equals the reference's per-pair division up to rounding.
+#include "exact_mu.cuh"
 #include "pt_internal.cuh"
 
 #include <algorithm>
@@ -56,9 +57,8 @@ __device__ __forceinline__ void welford_merge(long long& gc, double& gm, double&
 
 // mu_bin_value + mu_bin_index_full (dmumu:304-318): 0-based bin, n_bins for a
 // finite value outside [edges[0], edges[n_bins]], -1 for a non-finite value.
-__device__ __forceinline__ int bin_of(float mu, const double* __restrict__ edges, int n_bins, int bin_abs)
+__device__ __forceinline__ int bin_of(double v, const double* __restrict__ edges, int n_bins, int bin_abs)
 {
-    double v = (double)mu;
     if (!isfinite(v)) return -1;
     if (bin_abs) v = fabs(v);
     if (v < edges[0] || v > edges[n_bins]) return n_bins;
@@ -73,8 +73,7 @@ __device__ __forceinline__ int bin_of(float mu, const double* __restrict__ edges
 }
 
 struct DmumuLaunch {
-    const float* mu;
-    int64_t n, nsave, sp, ss;
+    int64_t n, nsave;
     int64_t start_cap;         // 1 for the injection estimator, nsave for sliding
     const int64_t* lags;       // this batch's lags
     int nl;                    // lags in this batch
@@ -91,17 +90,30 @@ struct DmumuLaunch {
     WelfordPart* part_w;           // [grid][nl]
 };
 
+// Where dmumu_kernel reads the mu series of particle p: a mu chunk at the
+// compute precision T (the reference's mu_chunk, Float32 by default), element
+// (p, s) at p * sp + s * ss.
+template <typename T_>
+struct CacheSourceT {
+    using T = T_;
+    const T_* mu;
+    int64_t sp, ss;
+    __device__ __forceinline__ T_ operator()(int64_t p, int64_t s) const { return mu[p * sp + s * ss]; }
+};
+using CacheSource = CacheSourceT<float>;
+
 // bytes of one particle slot of dmumu_kernel (layout in the kernel)
-size_t dmumu_slot_bytes(int64_t nsave, size_t idx_bytes, int n_bins, int nl_cap)
+size_t dmumu_slot_bytes(int64_t nsave, size_t mu_bytes, size_t idx_bytes, int n_bins, int nl_cap)
 {
     auto a16 = [](size_t v) { return (v + 15) & ~(size_t)15; };
-    return a16((size_t)nsave * sizeof(float)) + a16((size_t)nsave * idx_bytes) +
+    return a16((size_t)nsave * mu_bytes) + a16((size_t)nsave * idx_bytes) +
            a16(sizeof(int) * (size_t)(kStageWarps * (n_bins + 1) + n_bins + 2)) + a16(16 * (size_t)nl_cap);
 }
 
-template <typename IdxT, bool SMEM_SLOTS>
-__global__ void __launch_bounds__(1024) dmumu_kernel(DmumuLaunch a)
+template <typename IdxT, bool SMEM_SLOTS, class Src>
+__global__ void __launch_bounds__(1024) dmumu_kernel(DmumuLaunch a, Src source)
 {
+    using MuT = typename Src::T;
     extern __shared__ __align__(16) unsigned char smem[];
     const int nb = a.n_bins, nl = a.nl;
     // shared layout: edges | acc_cnt | acc_sd | acc_sd2 | slots
@@ -162,11 +174,11 @@ __global__ void __launch_bounds__(1024) dmumu_kernel(DmumuLaunch a)
     if (L < 1 || L >= a.nsave) L = a.nsave;  // reference: lag >= nsteps -> skipped
     const int64_t lim = a.nsave - L;         // valid starts: s < lim
 
-    // slot layout: series[nsave] float | list[nsave] IdxT | whist[kStageWarps][nb+1] int
+    // slot layout: series[nsave] MuT | list[nsave] IdxT | whist[kStageWarps][nb+1] int
     //              | cur[nb+2] int | tot_c[nl] u64 | tot_sd2[nl] f64 (per-particle totals over the bins)
     unsigned char* sb = slot_base + (size_t)slot * a.slot_bytes;
-    float* series = (float*)sb;
-    IdxT* list = (IdxT*)(sb + ((a.nsave * sizeof(float) + 15) & ~(size_t)15));
+    MuT* series = (MuT*)sb;
+    IdxT* list = (IdxT*)(sb + ((a.nsave * sizeof(MuT) + 15) & ~(size_t)15));
     int* whist = (int*)((unsigned char*)list + ((a.nsave * sizeof(IdxT) + 15) & ~(size_t)15));
     int* cur = whist + kStageWarps * (nb + 1);
     unsigned long long* tot_c = (unsigned long long*)((unsigned char*)whist +
@@ -202,14 +214,13 @@ __global__ void __launch_bounds__(1024) dmumu_kernel(DmumuLaunch a)
                     tot_sd2[l] = 0.0;
                 }
             __syncwarp();
-            const float* src = a.mu + p * a.sp;
             for (int64_t s0 = st_begin; s0 < st_end; s0 += kWarp) {
                 const int64_t s = s0 + lane;
                 int b = -1;
                 if (s < st_end) {
-                    const float v = src[s * a.ss];
+                    const MuT v = source(p, s);
                     series[s] = v;
-                    if (s < scap) b = bin_of(v, s_edges, nb, a.bin_abs);
+                    if (s < scap) b = bin_of((double)v, s_edges, nb, a.bin_abs);
                 }
                 const unsigned active = __ballot_sync(0xffffffffu, b >= 0);
                 if (b >= 0) {
@@ -256,7 +267,7 @@ __global__ void __launch_bounds__(1024) dmumu_kernel(DmumuLaunch a)
             for (int64_t s0 = st_begin; s0 < end; s0 += kWarp) {
                 const int64_t s = s0 + lane;
                 int b = -1;
-                if (s < end) b = bin_of(series[s], s_edges, nb, a.bin_abs);
+                if (s < end) b = bin_of((double)series[s], s_edges, nb, a.bin_abs);
                 const unsigned active = __ballot_sync(0xffffffffu, b >= 0);
                 if (b >= 0) {
                     const unsigned same = __match_any_sync(active, b);
@@ -281,12 +292,12 @@ __global__ void __launch_bounds__(1024) dmumu_kernel(DmumuLaunch a)
                 int e = e0;
                 for (; e + 4 <= e1; e += 4) {
                     int64_t s_[4];
-                    float a_[4], v_[4];
+                    MuT a_[4], v_[4];
 #pragma unroll
                     for (int k = 0; k < 4; ++k) {
                         s_[k] = (int64_t)list[e + k];
                         a_[k] = series[s_[k]];
-                        v_[k] = s_[k] < lim ? series[s_[k] + L] : NAN;
+                        v_[k] = s_[k] < lim ? series[s_[k] + L] : MuT(NAN);
                     }
 #pragma unroll
                     for (int k = 0; k < 4; k += 2) {
@@ -306,8 +317,8 @@ __global__ void __launch_bounds__(1024) dmumu_kernel(DmumuLaunch a)
                 }
                 for (; e < e1; ++e) {
                     const int64_t s = (int64_t)list[e];
-                    const float av = series[s];
-                    const float vv = s < lim ? series[s + L] : NAN;
+                    const MuT av = series[s];
+                    const MuT vv = s < lim ? series[s + L] : MuT(NAN);
                     const double d = (double)vv - (double)av;
                     if (isfinite(d)) {
                         c += 1;
@@ -579,8 +590,13 @@ size_t align16(size_t b) { return (b + 15) & ~(size_t)15; }
 }  // namespace
 
 // ------------------------------------------------------------------ host side
-int run_dmumu(pt_ctx* ctx, const DmumuArgs& a, cudaStream_t s)
+namespace {
+
+// D_mumu over the series that `src` yields (a.mu, a.sp, a.ss are not used here)
+template <class Src>
+int run_dmumu_src(pt_ctx* ctx, const DmumuArgs& a, const Src& src, cudaStream_t s)
 {
+    using MuT = typename Src::T;
     if (a.n <= 0 || a.n_lags <= 0) return PT_OK;
     if (a.n_bins < 1 || a.n_bins > 4096) return fail(PT_ERR_ARG, "n_bins must be in [1, 4096]");
     if (a.nsave < 1) return fail(PT_ERR_ARG, "nsave must be positive");
@@ -594,7 +610,7 @@ int run_dmumu(pt_ctx* ctx, const DmumuArgs& a, cudaStream_t s)
     // lags per launch: multiple of 32 with the accumulators taking <= ~half the budget
     int nl_cap = (int)std::max<size_t>(32, ((budget / 2) / ((size_t)a.n_bins * 24)) / 32 * 32);
     nl_cap = std::min(nl_cap, 32 * 8);
-    const size_t slot_bytes = dmumu_slot_bytes(a.nsave, idx_bytes, a.n_bins, nl_cap);
+    const size_t slot_bytes = dmumu_slot_bytes(a.nsave, sizeof(MuT), idx_bytes, a.n_bins, nl_cap);
     const int lag_batches = (a.n_lags + nl_cap - 1) / nl_cap;
     for (int lb = 0; lb < lag_batches; ++lb) {
         const int lag0 = lb * nl_cap;
@@ -613,8 +629,10 @@ int run_dmumu(pt_ctx* ctx, const DmumuArgs& a, cudaStream_t s)
         size_t smem = fixed + (smem_slots ? (size_t)ppc * slot_bytes : 0);
         const int64_t tiles = (a.n + ppc - 1) / ppc;
         int per_sm = 1;
-        void* kfn = small_idx ? (smem_slots ? (void*)dmumu_kernel<uint16_t, true> : (void*)dmumu_kernel<uint16_t, false>)
-                              : (smem_slots ? (void*)dmumu_kernel<uint32_t, true> : (void*)dmumu_kernel<uint32_t, false>);
+        void* kfn = small_idx ? (smem_slots ? (void*)dmumu_kernel<uint16_t, true, Src>
+                                           : (void*)dmumu_kernel<uint16_t, false, Src>)
+                              : (smem_slots ? (void*)dmumu_kernel<uint32_t, true, Src>
+                                            : (void*)dmumu_kernel<uint32_t, false, Src>);
         PT_CUDA(cudaFuncSetAttribute(kfn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
         cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kfn, threads, smem);
         per_sm = std::max(1, per_sm);
@@ -628,7 +646,7 @@ int run_dmumu(pt_ctx* ctx, const DmumuArgs& a, cudaStream_t s)
         if (rc) return rc;
         char* base = (char*)scratch;
         DmumuLaunch L;
-        L.mu = a.mu; L.n = a.n; L.nsave = a.nsave; L.sp = a.sp; L.ss = a.ss;
+        L.n = a.n; L.nsave = a.nsave;
         L.start_cap = a.injection ? 1 : a.nsave;
         L.lags = a.lags + lag0; L.nl = nl; L.edges = a.edges; L.n_bins = a.n_bins; L.bin_abs = a.bin_abs;
         L.ppc = ppc; L.groups = groups; L.parts = parts; L.slot_bytes = slot_bytes;
@@ -638,11 +656,11 @@ int run_dmumu(pt_ctx* ctx, const DmumuArgs& a, cudaStream_t s)
         L.part_w = (WelfordPart*)(base + 3 * align16(part_acc * 8));
         L.gslots = smem_slots ? nullptr : (char*)L.part_w + align16(sizeof(WelfordPart) * (size_t)grid * nl);
         if (small_idx) {
-            if (smem_slots) dmumu_kernel<uint16_t, true><<<grid, threads, smem, s>>>(L);
-            else dmumu_kernel<uint16_t, false><<<grid, threads, smem, s>>>(L);
+            if (smem_slots) dmumu_kernel<uint16_t, true, Src><<<grid, threads, smem, s>>>(L, src);
+            else dmumu_kernel<uint16_t, false, Src><<<grid, threads, smem, s>>>(L, src);
         } else {
-            if (smem_slots) dmumu_kernel<uint32_t, true><<<grid, threads, smem, s>>>(L);
-            else dmumu_kernel<uint32_t, false><<<grid, threads, smem, s>>>(L);
+            if (smem_slots) dmumu_kernel<uint32_t, true, Src><<<grid, threads, smem, s>>>(L, src);
+            else dmumu_kernel<uint32_t, false, Src><<<grid, threads, smem, s>>>(L, src);
         }
         PT_CHECK_LAUNCH("dmumu_kernel");
         const int fin_threads = 256;
@@ -654,6 +672,85 @@ int run_dmumu(pt_ctx* ctx, const DmumuArgs& a, cudaStream_t s)
         PT_CHECK_LAUNCH("dmumu_finalize_kernel");
     }
     return PT_OK;
+}
+
+}  // namespace
+
+int run_dmumu(pt_ctx* ctx, const DmumuArgs& a, cudaStream_t s)
+{
+    return run_dmumu_src(ctx, a, CacheSource{a.mu, a.sp, a.ss}, s);
+}
+
+namespace {
+
+// (Bx, By, Bz) column-major arrays -> one record per node
+template <typename R>
+__global__ void interleave_b_kernel(const R* __restrict__ bx, const R* __restrict__ by, const R* __restrict__ bz,
+                                    int64_t nodes, exact::Vec4<R>* __restrict__ out)
+{
+    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < nodes; i += (int64_t)gridDim.x * blockDim.x)
+        out[i] = exact::Vec4<R>{bx[i], by[i], bz[i], R(0)};
+}
+
+// mu of particles [p0, p0 + m) at every save, written [s][p - p0] (particle
+// fastest, like the device mu cache); one thread per (particle, save),
+// particles fastest so that the phase-space reads coalesce.
+template <typename R>
+__global__ void __launch_bounds__(256) phase_space_mu_kernel(const R* __restrict__ pos, const R* __restrict__ mom,
+                                                             int64_t row, int64_t comp, int64_t p0, int64_t m,
+                                                             int64_t nsave, const exact::Vec4<R>* __restrict__ B4,
+                                                             pt_grid g, R* __restrict__ mu)
+{
+    const int64_t total = m * nsave;
+    for (int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; t < total; t += (int64_t)gridDim.x * blockDim.x) {
+        const int64_t q = t % m, s = t / m;
+        const R* P = pos + s * row + p0 + q;
+        const R* M = mom + s * row + p0 + q;
+        mu[s * m + q] = exact::phase_space_mu4<R>(P[0], P[comp], P[2 * comp], M[0], M[comp], M[2 * comp], B4, g);
+    }
+}
+
+template <typename R>
+int run_dmumu_phase_space_t(pt_ctx* ctx, const DmumuArgs& a, const R* pos, const R* mom, int64_t row, int64_t comp,
+                            const void* const bfield[3], const pt_grid& g, cudaStream_t s)
+{
+    using V4 = exact::Vec4<R>;
+    const int64_t nodes = g.nx * g.ny * g.nz;
+    // mu chunks of at most 1 GiB
+    const int64_t per = std::max<int64_t>(1, ((int64_t)1 << 30) / ((int64_t)sizeof(R) * a.nsave));
+    const int64_t m_max = std::min<int64_t>(a.n, per);
+    const size_t b4_bytes = align16(sizeof(V4) * (size_t)nodes);
+    void* scratch = nullptr;
+    int rc = scratch_get(ctx, 4, b4_bytes + sizeof(R) * (size_t)m_max * (size_t)a.nsave, &scratch);
+    if (rc) return rc;
+    V4* B4 = (V4*)scratch;
+    R* mu = (R*)((char*)scratch + b4_bytes);
+    const int gb = (int)std::min<int64_t>((nodes + 255) / 256, (int64_t)ctx->num_sms * 16);
+    interleave_b_kernel<R><<<gb, 256, 0, s>>>((const R*)bfield[0], (const R*)bfield[1], (const R*)bfield[2], nodes, B4);
+    PT_CHECK_LAUNCH("interleave_b_kernel");
+    for (int64_t p0 = 0; p0 < a.n; p0 += m_max) {
+        const int64_t m = std::min(m_max, a.n - p0);
+        const int64_t total = m * a.nsave;
+        const int blocks = (int)std::min<int64_t>((total + 255) / 256, (int64_t)ctx->num_sms * 32);
+        phase_space_mu_kernel<R><<<blocks, 256, 0, s>>>(pos, mom, row, comp, p0, m, a.nsave, B4, g, mu);
+        PT_CHECK_LAUNCH("phase_space_mu_kernel");
+        DmumuArgs c = a;
+        c.n = m;
+        rc = run_dmumu_src(ctx, c, CacheSourceT<R>{mu, 1, m}, s);
+        if (rc) return rc;
+    }
+    return PT_OK;
+}
+
+}  // namespace
+
+int run_dmumu_phase_space(pt_ctx* ctx, const DmumuArgs& a, const void* pos, const void* mom, int64_t row,
+                          int64_t comp, const void* const bfield[3], const pt_grid& g, int f64, cudaStream_t s)
+{
+    if (a.n <= 0 || a.n_lags <= 0) return PT_OK;
+    if (f64) return run_dmumu_phase_space_t<double>(ctx, a, (const double*)pos, (const double*)mom, row, comp, bfield,
+                                                    g, s);
+    return run_dmumu_phase_space_t<float>(ctx, a, (const float*)pos, (const float*)mom, row, comp, bfield, g, s);
 }
 
 int run_dpp(pt_ctx* ctx, const DppArgs& a, cudaStream_t s)
@@ -797,7 +894,8 @@ int run_dmumu_noalloc(pt_ctx* ctx, const DmumuArgs& a, cudaStream_t s)
     const size_t edge_bytes = align16(sizeof(double) * (size_t)(a.n_bins + 1));
     int nl_cap = (int)std::max<size_t>(32, ((budget / 2) / ((size_t)a.n_bins * 24)) / 32 * 32);
     nl_cap = std::min(nl_cap, 32 * 8);
-    const size_t slot_bytes = dmumu_slot_bytes(a.nsave, idx_bytes, a.n_bins, nl_cap);
+    const size_t slot_bytes = dmumu_slot_bytes(a.nsave, sizeof(float), idx_bytes, a.n_bins, nl_cap);
+    const CacheSource src{a.mu, a.sp, a.ss};
     for (int lag0 = 0; lag0 < a.n_lags; lag0 += nl_cap) {
         const int nl = std::min(nl_cap, a.n_lags - lag0);
         const int groups = (nl + kWarp - 1) / kWarp;
@@ -818,7 +916,8 @@ int run_dmumu_noalloc(pt_ctx* ctx, const DmumuArgs& a, cudaStream_t s)
         if (cap_grid < 1)
             return fail(PT_ERR_ARG, "pt_dmumu_accumulate_device_noalloc: n_lags x n_bins too large for the " +
                                         std::to_string(kDmumuNoAllocBytes >> 20) + " MiB fixed scratch");
-        void* kfn = small_idx ? (void*)dmumu_kernel<uint16_t, true> : (void*)dmumu_kernel<uint32_t, true>;
+        void* kfn = small_idx ? (void*)dmumu_kernel<uint16_t, true, CacheSource>
+                              : (void*)dmumu_kernel<uint32_t, true, CacheSource>;
         PT_CUDA(cudaFuncSetAttribute(kfn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
         int per_sm = 1;
         cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kfn, threads, smem);
@@ -829,7 +928,7 @@ int run_dmumu_noalloc(pt_ctx* ctx, const DmumuArgs& a, cudaStream_t s)
         const size_t part_acc = (size_t)grid * nl * a.n_bins;
         char* base = (char*)scratch;
         DmumuLaunch L;
-        L.mu = a.mu; L.n = a.n; L.nsave = a.nsave; L.sp = a.sp; L.ss = a.ss;
+        L.n = a.n; L.nsave = a.nsave;
         L.start_cap = a.injection ? 1 : a.nsave;
         L.lags = a.lags + lag0; L.nl = nl; L.edges = a.edges; L.n_bins = a.n_bins; L.bin_abs = a.bin_abs;
         L.ppc = ppc; L.groups = groups; L.parts = parts; L.slot_bytes = slot_bytes;
@@ -840,8 +939,8 @@ int run_dmumu_noalloc(pt_ctx* ctx, const DmumuArgs& a, cudaStream_t s)
         L.gslots = nullptr;
         if (3 * align16(part_acc * 8) + sizeof(WelfordPart) * (size_t)grid * nl > kDmumuNoAllocBytes)
             return fail(PT_ERR_ARG, "internal: no-alloc scratch overflow");
-        if (small_idx) dmumu_kernel<uint16_t, true><<<grid, threads, smem, s>>>(L);
-        else dmumu_kernel<uint32_t, true><<<grid, threads, smem, s>>>(L);
+        if (small_idx) dmumu_kernel<uint16_t, true, CacheSource><<<grid, threads, smem, s>>>(L, src);
+        else dmumu_kernel<uint32_t, true, CacheSource><<<grid, threads, smem, s>>>(L, src);
         PT_CHECK_LAUNCH("dmumu_kernel (no-alloc)");
         const int fin_blocks = (int)((std::max(nl * a.n_bins, nl) + 255) / 256);
         dmumu_finalize_kernel<<<fin_blocks, 256, 0, s>>>(L.part_cnt, L.part_sd, L.part_sd2, L.part_w, grid, nl,

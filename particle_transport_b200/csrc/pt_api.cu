@@ -653,6 +653,31 @@ int pt_dmumu_accumulate_device(pt_ctx* ctx, const float* d_mu, int64_t n, int64_
     return run_dmumu(ctx, a, ctx->stream);
 }
 
+int pt_dmumu_accumulate_phase_space_device(pt_ctx* ctx, const void* d_pos, const void* d_mom, int64_t n,
+                                           int64_t nsave, int64_t row_stride, int64_t comp_stride,
+                                           const void* const d_bfield[3], const pt_grid* grid, int f64,
+                                           const int64_t* d_lags, int n_lags, const double* d_edges, int n_bins,
+                                           int start_mode, int bin_abs, int64_t* d_counts, double* d_sum_d,
+                                           double* d_sum_d2, int64_t* d_w_count, double* d_w_mean, double* d_w_m2,
+                                           double* d_pair_ss, int64_t* d_pair_n)
+{
+    if (!ctx) return fail(PT_ERR_ARG, "ctx is null");
+    int rc = check_grid(grid);
+    if (rc) return rc;
+    if (n < 0 || nsave < 1 || n_lags < 0 || n_bins < 1 || row_stride < 0 || comp_stride < 0)
+        return fail(PT_ERR_ARG, "bad sizes");
+    if (start_mode != PT_START_SLIDING && start_mode != PT_START_INJECTION) return fail(PT_ERR_ARG, "start_mode");
+    if (n == 0 || n_lags == 0) return PT_OK;
+    if (!(d_pos && d_mom && d_bfield && d_bfield[0] && d_bfield[1] && d_bfield[2] && d_lags && d_edges &&
+          d_counts && d_sum_d && d_sum_d2 && d_w_count && d_w_mean && d_w_m2 && d_pair_ss && d_pair_n))
+        return fail(PT_ERR_ARG, "null pointer");
+    PT_CUDA(cudaSetDevice(ctx->device));
+    DmumuArgs a{nullptr, n, nsave, 0, 0, d_lags, n_lags, d_edges, n_bins, start_mode == PT_START_INJECTION,
+                bin_abs != 0, d_counts, d_sum_d, d_sum_d2, d_w_count, d_w_mean, d_w_m2, d_pair_ss, d_pair_n};
+    return run_dmumu_phase_space(ctx, a, d_pos, d_mom, row_stride, comp_stride, d_bfield, *grid, f64 != 0,
+                                 ctx->stream);
+}
+
 int pt_dmumu_accumulate(pt_ctx* ctx, const float* mu, int64_t n, int64_t nsave, int64_t sp, int64_t ss,
                         const int64_t* lags, int n_lags, const double* edges, int n_bins, int start_mode, int bin_abs,
                         int64_t* counts, double* sum_d, double* sum_d2, int64_t* w_count, double* w_mean,

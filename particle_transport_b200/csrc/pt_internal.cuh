@@ -50,7 +50,7 @@ struct pt_ctx {
     cudaStream_t own_stream = nullptr;
     cudaStream_t stream = nullptr;      // stream used by *_device calls
     cudaStream_t copy_stream = nullptr; // egress copies in pt_push_run
-    pt::ScratchBuf scratch[4];          // reusable device scratch, grown on demand
+    pt::ScratchBuf scratch[5];          // reusable device scratch, grown on demand
     pt::ScratchBuf pinned;              // pinned host staging of pt_push_run, grown on demand
     pt_fast_state* run_fs = nullptr;    // FP32-push state reused by pt_push_run
 };
@@ -95,7 +95,8 @@ namespace pt {
 inline size_t align_up(size_t v, size_t a) { return (v + a - 1) / a * a; }
 
 // Grow-only device scratch owned by the context (slot = independent user).
-// Slots: 0 D_mumu, 1 D_pp, 2 pt_push_run state, 3 particle initialisation.
+// Slots: 0 D_mumu, 1 D_pp, 2 pt_push_run state, 3 particle initialisation,
+// 4 phase-space D_mumu (interleaved B + mu chunk).
 int scratch_get(pt_ctx* ctx, int slot, size_t bytes, void** out);
 
 // ---------------------------------------------------------------- host I/O
@@ -253,6 +254,12 @@ struct DmumuArgs {
     int64_t* pair_n;
 };
 int run_dmumu(pt_ctx* ctx, const DmumuArgs& a, cudaStream_t s);
+// D_mumu of a phase-space chunk (a.mu, a.sp, a.ss unused): mu reconstructed
+// on the device into a scratch chunk, then binned; component c of save s of
+// particle p at pos/mom + s * row + c * comp + p, elements and B in the
+// compute precision.
+int run_dmumu_phase_space(pt_ctx* ctx, const DmumuArgs& a, const void* pos, const void* mom, int64_t row,
+                          int64_t comp, const void* const bfield[3], const pt_grid& g, int f64, cudaStream_t s);
 
 struct DppArgs {
     const float* mom;

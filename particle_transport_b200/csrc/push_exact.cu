@@ -5,73 +5,13 @@
 // FMA contraction), division and sqrt are IEEE round-to-nearest, so the FP64
 // results are bit-identical to a Float64 run of the reference on the same
 // inputs.
+#include "exact_mu.cuh"
 #include "pt_internal.cuh"
 
 namespace pt {
 namespace {
 
-// clamp(floor(Int, f), 1, n - 1) as a double (NaN -> 1).
-// src/phase_space_gpu_runner.jl:252-254
-template <typename R>
-__device__ __forceinline__ double cell_index(R f, int64_t n)
-{
-    double c = floor((double)f);
-    double hi = (double)(n - 1);
-    if (!(c >= 1.0)) c = 1.0;
-    if (c > hi) c = hi;
-    return c;
-}
-
-// Cell location of one position, shared by all components sampled there.
-template <typename R>
-struct Cell {
-    int64_t base;  // 0-based linear index of corner (i0, j0, k0)
-    R tx, ty, tz;
-};
-
-template <typename R>
-__device__ __forceinline__ Cell<R> locate(R x, R y, R z, R xmin, R ymin, R zmin, R dx, R dy, R dz, int64_t nx,
-                                          int64_t ny, int64_t nz)
-{
-    // trilinear_sample, src/phase_space_gpu_runner.jl:247-258
-    R fx = (x - xmin) / dx + R(1);
-    R fy = (y - ymin) / dy + R(1);
-    R fz = (z - zmin) / dz + R(1);
-    double ci = cell_index(fx, nx), cj = cell_index(fy, ny), ck = cell_index(fz, nz);
-    Cell<R> c;
-    c.tx = fx - (R)ci;
-    c.ty = fy - (R)cj;
-    c.tz = fz - (R)ck;
-    c.base = ((int64_t)ci - 1) + nx * (((int64_t)cj - 1) + ny * ((int64_t)ck - 1));
-    return c;
-}
-
-// src/phase_space_gpu_runner.jl:260-275
-template <typename R>
-__device__ __forceinline__ R sample(const R* __restrict__ arr, const Cell<R>& c, int64_t sy, int64_t sz)
-{
-    const R* b = arr + c.base;
-    R c000 = __ldg(b), c100 = __ldg(b + 1), c010 = __ldg(b + sy), c110 = __ldg(b + 1 + sy);
-    R c001 = __ldg(b + sz), c101 = __ldg(b + 1 + sz), c011 = __ldg(b + sy + sz), c111 = __ldg(b + 1 + sy + sz);
-    R c00 = c000 * (R(1) - c.tx) + c100 * c.tx;
-    R c10 = c010 * (R(1) - c.tx) + c110 * c.tx;
-    R c01 = c001 * (R(1) - c.tx) + c101 * c.tx;
-    R c11 = c011 * (R(1) - c.tx) + c111 * c.tx;
-    R c0 = c00 * (R(1) - c.ty) + c10 * c.ty;
-    R c1 = c01 * (R(1) - c.ty) + c11 * c.ty;
-    return c0 * (R(1) - c.tz) + c1 * c.tz;
-}
-
-// pitch_mu_from_pB, src/compute_delta_mu2_curve.jl:93-110
-template <typename R>
-__device__ __forceinline__ R pitch_mu(R px, R py, R pz, R bx, R by, R bz)
-{
-    R pn = sqrt(px * px + py * py + pz * pz);
-    R bn = sqrt(bx * bx + by * by + bz * bz);
-    if (!isfinite(pn) || !isfinite(bn) || pn == R(0) || bn == R(0)) return R(NAN);
-    R mu = (px * bx + py * by + pz * bz) / (pn * bn);
-    return mu > R(1) ? R(1) : (mu < R(-1) ? R(-1) : mu);
-}
+using namespace exact;
 
 __device__ __forceinline__ double wrap(double x, double xmin, double xmax)
 {
@@ -201,22 +141,10 @@ __global__ void __launch_bounds__(256) reconstruct_mu_kernel(const R* __restrict
     const int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (t >= chunk * nsave) return;
     const int64_t p = t % chunk, s = t / chunk;
-    const R xmin = (R)g.xmin, ymin = (R)g.ymin, zmin = (R)g.zmin;
-    const R xmax = (R)g.xmax, ymax = (R)g.ymax, zmax = (R)g.zmax;
-    const R dx = (R)g.dx, dy = (R)g.dy, dz = (R)g.dz;
     const R* P = pos + s * 3 * chunk + p;
     const R* M = mom + s * 3 * chunk + p;
-    R xx = P[0], yy = P[chunk], zz = P[2 * chunk];
-    R px = M[0], py = M[chunk], pz = M[2 * chunk];
-    R v = R(NAN);
-    if (!(isnan(xx) || isnan(yy) || isnan(zz) || isnan(px) || isnan(py) || isnan(pz)) && xmin <= xx &&
-        xx <= xmax && ymin <= yy && yy <= ymax && zmin <= zz && zz <= zmax) {
-        Cell<R> c = locate<R>(xx, yy, zz, xmin, ymin, zmin, dx, dy, dz, g.nx, g.ny, g.nz);
-        const int64_t sy = g.nx, sz = g.nx * g.ny;
-        R b0 = sample(bx, c, sy, sz), b1 = sample(by, c, sy, sz), b2 = sample(bz, c, sy, sz);
-        v = pitch_mu<R>(px, py, pz, b0, b1, b2);
-    }
-    mu_out[p * nsave + s] = v;
+    const R* B[3] = {bx, by, bz};
+    mu_out[p * nsave + s] = phase_space_mu<R>(P[0], P[chunk], P[2 * chunk], M[0], M[chunk], M[2 * chunk], B, g);
 }
 
 }  // namespace

@@ -108,6 +108,58 @@ def process_mu_chunk_dmumu(mu_chunk, lag_steps, mu_edges, particle_counts, parti
                   _lib.ptr(edges), n_bins, START[start_mode], int(bool(bin_abs)), *[_lib.ptr(a) for a in accs])
 
 
+def process_phase_space_chunk_dmumu(positions, momenta, Bx, By, Bz, grid, lag_steps, mu_edges, particle_counts,
+                                    particle_means, particle_m2s, pair_sum_squares, pair_counts, dmumu_counts,
+                                    dmumu_sum_delta, dmumu_sum_delta2, start_mode="sliding", bin_abs=True):
+    """Phase-space D_mumu on the device: mu reconstructed from positions and
+    momenta inside the binning kernel (reconstruct_mu_chunk_gpu feeding
+    process_mu_chunk_dmumu_cpu!, src/compute_delta_mu2_dmumu_full.jl:1137-1164).
+
+    positions, momenta: CUDA tensors shaped (nsave, 3, chunk) -- any row and
+    component strides, particles contiguous (e.g. views [:, 0:3] and [:, 3:6]
+    of the device phase-space cache (nsave, 6, n)); float32 (the reference's
+    default compute precision) or float64.  Bx, By, Bz: CUDA tensors (nz, ny,
+    nx) of the same dtype.  Accumulators as for process_mu_chunk_dmumu (CUDA)."""
+    import torch
+
+    start_mode = str(start_mode)
+    if start_mode not in START:
+        raise ValueError(f"Unknown dmumu_start_mode: {start_mode}")
+    if not (_is_cuda(positions) and _is_cuda(momenta)):
+        raise ValueError("positions and momenta must be CUDA tensors")
+    dt = positions.dtype
+    if dt not in (torch.float32, torch.float64) or momenta.dtype != dt:
+        raise ValueError("positions and momenta must share dtype float32 or float64")
+    if positions.dim() != 3 or positions.shape[1] != 3 or tuple(momenta.shape) != tuple(positions.shape):
+        raise ValueError("positions and momenta must be shaped (nsave, 3, chunk)")
+    if positions.stride() != momenta.stride() or positions.stride(2) != 1:
+        raise ValueError("positions and momenta need equal strides and contiguous particles")
+    nsave, _, chunk = positions.shape
+    bs = [b.contiguous() for b in (Bx, By, Bz)]
+    for b in bs:
+        if b.dtype != dt or not b.is_cuda or tuple(b.shape) != grid.shape:
+            raise ValueError("B components must be CUDA tensors of the positions' dtype shaped (nz, ny, nx)")
+    n_lags = len(lag_steps)
+    n_bins = len(mu_edges) - 1
+    for a, nm, t in ((particle_counts, "particle_counts", np.int64), (particle_means, "particle_means", np.float64),
+                     (particle_m2s, "particle_m2s", np.float64), (pair_sum_squares, "pair_sum_squares", np.float64),
+                     (pair_counts, "pair_counts", np.int64)):
+        _check(a, (n_lags,), t, nm)
+    for a, nm, t in ((dmumu_counts, "dmumu_counts", np.int64), (dmumu_sum_delta, "dmumu_sum_delta", np.float64),
+                     (dmumu_sum_delta2, "dmumu_sum_delta2", np.float64)):
+        _check(a, (n_lags, n_bins), t, nm)
+    accs = (dmumu_counts, dmumu_sum_delta, dmumu_sum_delta2, particle_counts, particle_means, particle_m2s,
+            pair_sum_squares, pair_counts)
+    lags = torch.as_tensor(np.asarray(lag_steps, dtype=np.int64), device=positions.device)
+    edges = torch.as_tensor(np.asarray(mu_edges, dtype=np.float64), device=positions.device)
+    ctx = _lib.torch_context(positions)
+    g = grid.to_c()
+    _lib.call("pt_dmumu_accumulate_phase_space_device", ctx.handle, _lib.ptr(positions), _lib.ptr(momenta), chunk,
+              nsave, positions.stride(0), positions.stride(1), _lib.ptr_array(bs), _lib.C.byref(g),
+              int(dt == torch.float64), _lib.ptr(lags), n_lags, _lib.ptr(edges), n_bins, START[start_mode],
+              int(bool(bin_abs)), *[_lib.ptr(a) for a in accs])
+
+
 def new_dpp_accumulators(n_lags: int, device=None):
     if device is not None:
         import torch

@@ -181,3 +181,43 @@ def test_reconstruct_mu_bit_exact(cuda, oracle, dtype):
     g = S.reconstruct_mu_chunk(pos, mom, *pb.fields[:3], pb.grid, dtype=dtype)
     assert np.array_equal(g, o, equal_nan=True)
     assert np.isnan(g[3, 5]) and np.isnan(g[4, 6])
+
+
+@pytest.mark.parametrize("dtype,mode,layout", [(np.float32, "sliding", "julia"), (np.float32, "injection", "cache"),
+                                               (np.float64, "sliding", "cache")])
+def test_phase_space_dmumu_fused_matches_oracle(cuda, oracle, dtype, mode, layout):
+    """Fused phase-space D_mumu = oracle reconstruct_mu at the compute
+    precision, then the oracle binning of that mu chunk."""
+    torch = cuda
+    from helpers import copy_state, fortran_fields, small_problem
+    pb = small_problem(n=12, n_particles=517)
+    st = copy_state(pb.state)
+    f64 = dtype == np.float64
+    (pos, mom), _ = oracle.push_run(fortran_fields(pb.fields), pb.grid, st, np.ones(517, np.uint8), pb.dt, 600, 3,
+                                    cache_mode=2, out_f64=f64)
+    pos[5, 0, 3] = np.nan
+    pos[6, 1, 4] = pb.grid.ymax * 1.01  # outside the box -> NaN mu
+    ff = fortran_fields(pb.fields)[:3]
+    mu = (oracle.reconstruct_mu_f64 if f64 else oracle.reconstruct_mu_f32)(pos, mom, ff, pb.grid)  # (chunk, nsave)
+    nsave = pos.shape[0]
+    lags = log_spaced_lag_steps(nsave - 1, 24)
+    edges, _ = build_mu_edges_full(0.0, 1.0, 16)
+    o = zero_dmumu(len(lags), 16)
+    # the reference bins Float64(mu) of the chunk at the compute precision; a Float32 chunk is exactly the oracle's input
+    oracle.dmumu_accumulate(np.ascontiguousarray(mu, dtype=np.float32) if not f64 else mu, lags, edges, o,
+                            injection=mode == "injection")
+    tdt = torch.float64 if f64 else torch.float32
+    if layout == "julia":
+        P = torch.as_tensor(pos, dtype=tdt, device="cuda")
+        M = torch.as_tensor(mom, dtype=tdt, device="cuda")
+    else:  # the device phase-space cache (nsave, 6, n)
+        cache = torch.cat([torch.as_tensor(pos, dtype=tdt), torch.as_tensor(mom, dtype=tdt)], dim=1).cuda()
+        P, M = cache[:, 0:3], cache[:, 3:6]
+    B = [torch.as_tensor(f, dtype=tdt, device="cuda") for f in pb.fields[:3]]
+    g = S.new_dmumu_accumulators(len(lags), 16, device="cuda")
+    S.process_phase_space_chunk_dmumu(P, M, *B, pb.grid, lags, edges, g["particle_counts"], g["particle_means"],
+                                      g["particle_m2s"], g["pair_sum_squares"], g["pair_counts"], g["dmumu_counts"],
+                                      g["dmumu_sum_delta"], g["dmumu_sum_delta2"], start_mode=mode)
+    g = {k: v.cpu().numpy() for k, v in g.items()}
+    check_dmumu(g, o)
+    assert g["pair_counts"].sum() > 0
