@@ -87,7 +87,10 @@ typedef struct {
     int32_t kernel_variant;   /* F32 form: launch shape, threads per block x resident
                                  blocks per SM: 0 = auto (= 1), 1 = 256 x occupancy,
                                  2 = 256 x 4, 3 = 128 x 8, 4 = 512 x 2, 5 = 256 x 1,
-                                 6 = 512 x 1, 7 = 128 x 3, 8 = 128 x 2              */
+                                 6 = 512 x 1, 7 = 128 x 3, 8 = 128 x 2; BRICK_BF16
+                                 fields: 9 = as 1 with half of the corners fetched
+                                 through the texture path, 10 = as 1 with all of
+                                 them, 11 = as 6 with half (same results)       */
     int32_t reserved;
 } pt_push_params;
 

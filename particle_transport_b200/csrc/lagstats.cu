@@ -101,7 +101,6 @@ struct CacheSourceT {
     __device__ __forceinline__ T_ operator()(int64_t p, int64_t s) const { return mu[p * sp + s * ss]; }
 };
 using CacheSource = CacheSourceT<float>;
-
 // bytes of one particle slot of dmumu_kernel (layout in the kernel)
 size_t dmumu_slot_bytes(int64_t nsave, size_t mu_bytes, size_t idx_bytes, int n_bins, int nl_cap)
 {
@@ -456,24 +455,65 @@ struct DppLaunch {
     const int64_t* lags;
     int nl;
     double p0;
-    int ppc, groups;
+    int ppc, groups, parts;  // particle slots per CTA, 32-lag groups, warps splitting the starts
     size_t slot_bytes;
     char* gslots;
     DppPart* part;  // [grid][nl]
 };
 
+// Warps = (particle slot, 32-lag group, part of the start range).  Lags are
+// dealt to lanes so that lags equal modulo 16 -- whose 8-byte |p| reads hit
+// the same shared-memory banks at every start -- fall into different groups.
 template <bool SMEM_SLOTS>
 __global__ void __launch_bounds__(1024) dpp_kernel(DppLaunch a)
 {
     extern __shared__ __align__(16) unsigned char smem[];
     unsigned char* slot_base = SMEM_SLOTS ? smem : (unsigned char*)(a.gslots + (size_t)blockIdx.x * a.ppc * a.slot_bytes);
+    __shared__ int s_lane_lag[8 * kWarp];
+    __shared__ int s_lag_pos[8 * kWarp];
+    __shared__ unsigned char cnt[8][16];
+    __shared__ int fill[8];
+    for (int i = threadIdx.x; i < 8 * kWarp; i += blockDim.x) s_lane_lag[i] = -1;
+    for (int i = threadIdx.x; i < 8 * 16; i += blockDim.x) cnt[i / 16][i % 16] = 0;
+    if (threadIdx.x < 8) fill[threadIdx.x] = 0;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        // a lag of residue r goes to the group holding fewest lags of that
+        // residue, into lane r or r + 16 (the two half-warps) when free
+        for (int i = 0; i < a.nl; ++i) {
+            const int r = (int)(((a.lags[i] % 16) + 16) % 16);
+            int best = -1;
+            for (int g = 0; g < a.groups; ++g) {
+                if (fill[g] >= kWarp) continue;
+                if (best < 0 || cnt[g][r] < cnt[best][r] || (cnt[g][r] == cnt[best][r] && fill[g] < fill[best]))
+                    best = g;
+            }
+            int lane = -1;
+            for (int h = 0; h < 2 && lane < 0; ++h)
+                if (s_lane_lag[best * kWarp + r + 16 * h] < 0) lane = r + 16 * h;
+            for (int l = 0; l < kWarp && lane < 0; ++l)
+                if (s_lane_lag[best * kWarp + l] < 0) lane = l;
+            const int pos = best * kWarp + lane;
+            fill[best]++;
+            cnt[best][r]++;
+            s_lane_lag[pos] = i;
+            s_lag_pos[i] = pos;
+        }
+    }
+    __syncthreads();
     const int warp = threadIdx.x / kWarp, lane = threadIdx.x % kWarp;
-    const int slot = warp / a.groups, group = warp % a.groups;
-    const int li = group * kWarp + lane;
-    const bool lane_on = li < a.nl;
+    const int wps = a.groups * a.parts;
+    const int slot = warp / wps, group = (warp % wps) / a.parts, part = warp % a.parts;
+    const int li = s_lane_lag[group * kWarp + lane];
+    const bool lane_on = li >= 0;
     int64_t L = lane_on ? a.lags[li] : 0;
     if (L < 1 || L >= a.nsave) L = a.nsave;
     const int64_t lim = a.nsave - L;
+    // the part's starts are a warp-uniform range of the group's longest one
+    // (every lane reads the same series[s], a broadcast); each lane stops at
+    // its own limit
+    const int64_t lim_max = (int64_t)__reduce_max_sync(0xffffffffu, (unsigned)lim);
+    const int64_t s_begin = lim_max * part / a.parts, s_end = lim_max * (part + 1) / a.parts;
     double* series = (double*)(slot_base + (size_t)slot * a.slot_bytes);
     long long c = 0;
     double sdp = 0, sdp2 = 0;
@@ -493,8 +533,10 @@ __global__ void __launch_bounds__(1024) dpp_kernel(DppLaunch a)
             // |p| >= 0 or NaN or +inf, so pe - ps is finite exactly when both
             // ends are finite; the normalised sums are sum(d)/p0 and
             // sum(d^2)/p0^2, formed once per lag in dpp_finalize_kernel.
-            for (int64_t s = 0; s < lim; ++s) {
-                const double d = series[s + L] - series[s];
+            for (int64_t s = s_begin; s < s_end; ++s) {
+                const double ps = series[s];
+                if (s >= lim) continue;  // past this lane's last start
+                const double d = series[s + L] - ps;
                 if (!isfinite(d)) continue;
                 c += 1;
                 sdp += d;
@@ -503,21 +545,23 @@ __global__ void __launch_bounds__(1024) dpp_kernel(DppLaunch a)
         }
         __syncthreads();
     }
-    // CTA epilogue in fixed warp order
-    DppPart* wp = (DppPart*)(SMEM_SLOTS ? smem : smem);
+    // CTA epilogue in fixed (slot, part) order
+    DppPart* wp = (DppPart*)smem;
     __syncthreads();
     wp[warp * kWarp + lane] = DppPart{c, sdp, sdp2};
     __syncthreads();
     const int nwarps = blockDim.x / kWarp;
     for (int l = threadIdx.x; l < a.nl; l += blockDim.x) {
-        const int g = l / kWarp, ln = l % kWarp;
+        const int pos = s_lag_pos[l];
+        const int g = pos / kWarp, ln = pos % kWarp;
         DppPart r{0, 0, 0};
-        for (int sl = 0; sl < a.ppc; ++sl) {
-            const int w = sl * a.groups + g;
-            if (w >= nwarps) break;
-            const DppPart q = wp[w * kWarp + ln];
-            r.count += q.count; r.sdp += q.sdp; r.sdp2 += q.sdp2;
-        }
+        for (int sl = 0; sl < a.ppc; ++sl)
+            for (int q = 0; q < a.parts; ++q) {
+                const int w = sl * wps + g * a.parts + q;
+                if (w >= nwarps) continue;
+                const DppPart v = wp[w * kWarp + ln];
+                r.count += v.count; r.sdp += v.sdp; r.sdp2 += v.sdp2;
+            }
         a.part[(int64_t)blockIdx.x * a.nl + l] = r;
     }
 }
@@ -769,8 +813,10 @@ int run_dpp(pt_ctx* ctx, const DppArgs& a, cudaStream_t s)
         int ppc = smem_slots ? (int)std::min<size_t>((budget - fixed) / slot_bytes, (size_t)(32 / groups))
                              : std::max(1, std::min(8, 32 / groups));
         ppc = std::max(1, ppc);
-        const int threads = ppc * groups * kWarp;
-        const size_t smem = std::max(fixed, smem_slots ? (size_t)ppc * slot_bytes : 0) ;
+        // more warps share each staged series: split its starts over `parts` warps
+        const int parts = std::max(1, std::min(4, 32 / (ppc * groups)));
+        const int threads = ppc * groups * parts * kWarp;
+        const size_t smem = std::max(fixed, smem_slots ? (size_t)ppc * slot_bytes : 0);
         const int64_t tiles = (a.chunk + ppc - 1) / ppc;
         void* kfn = smem_slots ? (void*)dpp_kernel<true> : (void*)dpp_kernel<false>;
         PT_CUDA(cudaFuncSetAttribute(kfn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
@@ -785,7 +831,7 @@ int run_dpp(pt_ctx* ctx, const DppArgs& a, cudaStream_t s)
         if (rc) return rc;
         DppLaunch L;
         L.mom = a.mom; L.chunk = a.chunk; L.nsave = a.nsave; L.lags = a.lags + lag0; L.nl = nl; L.p0 = a.p0;
-        L.ppc = ppc; L.groups = groups; L.slot_bytes = slot_bytes;
+        L.ppc = ppc; L.groups = groups; L.parts = parts; L.slot_bytes = slot_bytes;
         L.part = (DppPart*)scratch;
         L.gslots = smem_slots ? nullptr : (char*)scratch + align16(sizeof(DppPart) * (size_t)grid * nl);
         if (smem_slots) dpp_kernel<true><<<grid, threads, smem, s>>>(L);

@@ -184,6 +184,25 @@ int field_create(pt_ctx* ctx, const double* const comps[6], bool on_device, cons
     for (int c = 0; c < 6; ++c) if (tmp[c]) cudaFree(tmp[c]);
     if (rc) return cleanup(rc);
     if (e != cudaSuccess) return cleanup(cuda_fail(e, "brick conversion"));
+    // the node records as a linear texture of 16-byte texels, so that a push
+    // can fetch part of its corners through the texture path; a field larger
+    // than the device's linear-texture limit simply has none
+    const size_t texels = node_bytes * (size_t)f->n_nodes / 16;
+    int max_texels = 0;
+    cudaDeviceGetAttribute(&max_texels, cudaDevAttrMaxTexture1DLinearWidth, ctx->device);
+    if (texels <= (size_t)max_texels && texels <= (size_t)INT32_MAX) {
+        cudaResourceDesc rd{};
+        rd.resType = cudaResourceTypeLinear;
+        rd.res.linear.devPtr = f->nodes;
+        rd.res.linear.desc = cudaCreateChannelDesc<uint4>();
+        rd.res.linear.sizeInBytes = texels * 16;
+        cudaTextureDesc td{};
+        td.readMode = cudaReadModeElementType;
+        if (cudaCreateTextureObject(&f->tex, &rd, &td, nullptr) != cudaSuccess) {
+            cudaGetLastError();
+            f->tex = 0;
+        }
+    }
     *out = f;
     return PT_OK;
 }
@@ -212,6 +231,7 @@ PushArgsFast fast_args(const pt_field* f, pt_fast_state* st, const pt_push_param
     a.fld.nx = g.nx; a.fld.ny = g.ny; a.fld.nz = g.nz;
     a.fld.bf16 = f->storage != PT_FIELD_BRICK_F32;
     a.fld.layout = field_layout(f->storage);
+    a.fld.tex = f->tex;
     a.wx = (g.xmax - g.xmin) / g.dx;
     a.wy = (g.ymax - g.ymin) / g.dy;
     a.wz = (g.zmax - g.zmin) / g.dz;
@@ -360,6 +380,7 @@ int pt_field_destroy(pt_field* f)
     if (!f) return PT_OK;
     for (int c = 0; c < 6; ++c)
         if (f->comp[c]) cudaFree(f->comp[c]);
+    if (f->tex) cudaDestroyTextureObject(f->tex);
     if (f->nodes) cudaFree(f->nodes);
     if (f->offs) cudaFree(f->offs);
     delete f;

@@ -281,6 +281,7 @@ int pt_batch_add(pt_ctx* ctx, pt_batch* b, const pt_campaign_desc* d, int* id)
     a.fld.nx = g.nx; a.fld.ny = g.ny; a.fld.nz = g.nz;
     a.fld.bf16 = f->storage != PT_FIELD_BRICK_F32;
     a.fld.layout = field_layout(f->storage);
+    a.fld.tex = f->tex;
     a.wx = (g.xmax - g.xmin) / g.dx;
     a.wy = (g.ymax - g.ymin) / g.dy;
     a.wz = (g.zmax - g.zmin) / g.dz;

@@ -67,6 +67,7 @@ struct pt_field {
     int64_t n_nodes = 0;
     uint32_t* offs = nullptr;  // [nx + ny + nz]: offx, offy, offz
     int64_t bytes = 0;
+    cudaTextureObject_t tex = 0;  // brick forms: node records as uint4 texels (0 if over the texture limit)
 };
 
 struct pt_fast_state {
@@ -151,6 +152,7 @@ struct FieldArgsBrick {
     int64_t nx, ny, nz;
     int bf16;    // 1 for the BF16 forms
     int layout;  // LAYOUT_*
+    cudaTextureObject_t tex;  // the node records as a linear uint4 texture (0: none)
 };
 struct PushArgsFast {
     FieldArgsBrick fld;

@@ -71,8 +71,12 @@ __device__ __forceinline__ void acc_bf16x3(float f[6], float w, uint32_t a, uint
 //  LAYOUT_BF16        16-byte node (Bx,By | Bz,ux | uy,uz | pad), 8 x 16-byte loads
 //  LAYOUT_F32         32-byte node (Bx,By,Bz,ux,uy,uz,pad,pad), 8 x 32-byte loads
 //  LAYOUT_BF16_XPAIR  32-byte record = node (i) + node (i+1), 4 x 32-byte loads
-template <int LAYOUT>
-__device__ __forceinline__ void gather6(const void* __restrict__ nodes, const Corners& c, float f[6])
+// TEXC (BF16 only): the odd corners -- TEXC of them -- are fetched through the
+// texture path (tex1Dfetch on the same records), the others with LDG: the two
+// L1TEX data pipes share the gathers.  Same values, same summation order.
+template <int LAYOUT, int TEXC = 0>
+__device__ __forceinline__ void gather6(const void* __restrict__ nodes, cudaTextureObject_t tex, const Corners& c,
+                                        float f[6])
 {
 #pragma unroll
     for (int k = 0; k < 6; ++k) f[k] = 0.0f;
@@ -105,7 +109,11 @@ __device__ __forceinline__ void gather6(const void* __restrict__ nodes, const Co
         const uint4* N = (const uint4*)nodes;
         uint4 v[8];
 #pragma unroll
-        for (int q = 0; q < 8; ++q) v[q] = __ldg(N + c.idx[q]);
+        for (int q = 0; q < 8; ++q) {
+            const bool via_tex = TEXC == 8 || (TEXC == 4 && (q & 1));
+            if (via_tex) v[q] = tex1Dfetch<uint4>(tex, (int)c.idx[q]);
+            else v[q] = __ldg(N + c.idx[q]);
+        }
 #pragma unroll
         for (int q = 0; q < 8; ++q) {
             const float w = c.w[q];
@@ -140,7 +148,7 @@ __device__ __forceinline__ double wrap_cells(double x, double w)
 // (FP64), p/(mc) (FP32) and |p/(mc)|^2 (FP64); pid indexes the cache row.
 // Cache rows of a.n_cache particles: row r at (r - a.row_base) or, with
 // a.ring, at (r % a.rows).
-template <int LAYOUT>
+template <int LAYOUT, int TEXC = 0>
 __device__ __forceinline__ void advance_particle(double& x, double& y, double& z, float& px, float& py, float& pz,
                                                  double& P2, bool& al, const int64_t pid, const PushArgsFast& a,
                                                  const uint32_t* ox, const uint32_t* oy, const uint32_t* oz,
@@ -164,7 +172,7 @@ __device__ __forceinline__ void advance_particle(double& x, double& y, double& z
             float f[6] = {0, 0, 0, 0, 0, 0};
             if (al && (do_push || (is_save && a.cache_mode == PT_CACHE_MU))) {
                 Corners c = locate_brick(x, y, z, ox, oy, oz, nx, ny, nz);
-                gather6<LAYOUT>(a.fld.nodes, c, f);
+                gather6<LAYOUT, TEXC>(a.fld.nodes, a.fld.tex, c, f);
             }
             if (is_save) {
                 const int64_t r = a.ring ? row % a.rows : row - a.row_base;
@@ -235,7 +243,7 @@ __device__ __forceinline__ void advance_particle(double& x, double& y, double& z
     }
 }
 
-template <int LAYOUT, int BLOCK, int MINB>
+template <int LAYOUT, int BLOCK, int MINB, int TEXC = 0>
 __global__ void __launch_bounds__(BLOCK, MINB) push_fast_kernel(PushArgsFast a)
 {
     extern __shared__ uint32_t s_offs[];
@@ -253,7 +261,7 @@ __global__ void __launch_bounds__(BLOCK, MINB) push_fast_kernel(PushArgsFast a)
         float px = a.p[slot], py = a.p[n + slot], pz = a.p[2 * n + slot];
         double P2 = a.p2[slot];
         bool al = a.alive[slot] != 0;
-        advance_particle<LAYOUT>(x, y, z, px, py, pz, P2, al, a.pid[slot], a, ox, oy, oz, a.step_begin, s_end);
+        advance_particle<LAYOUT, TEXC>(x, y, z, px, py, pz, P2, al, a.pid[slot], a, ox, oy, oz, a.step_begin, s_end);
         a.x[slot] = x; a.x[n + slot] = y; a.x[2 * n + slot] = z;
         a.p[slot] = px; a.p[n + slot] = py; a.p[2 * n + slot] = pz;
         a.p2[slot] = P2;
@@ -355,9 +363,21 @@ __global__ void fast_export_kernel(const double* __restrict__ xs, const float* _
 // so that runs of particles in one brick -- the common case once sorted --
 // cost one atomic per warp instead of one per particle.  blockDim must be a
 // multiple of 32 (every lane of a warp runs the same loop trips).
+// sort bucket of a particle: the brick of its cell, dead_key when dead
+__device__ __forceinline__ uint32_t brick_key(double x, double y, double z, uint8_t alive,
+                                              const uint32_t* __restrict__ offs, int nx, int ny, int nz,
+                                              uint32_t dead_key)
+{
+    if (!alive) return dead_key;
+    const int ix = min(max((int)floor(x), 0), nx - 2);
+    const int iy = min(max((int)floor(y), 0), ny - 2);
+    const int iz = min(max((int)floor(z), 0), nz - 2);
+    return (offs[ix] + offs[nx + iy] + offs[nx + ny + iz]) >> 9;
+}
+
 __global__ void sort_key_kernel(const double* __restrict__ xs, const uint8_t* __restrict__ as, int64_t n,
                                 const uint32_t* __restrict__ offs, int nx, int ny, int nz, uint32_t dead_key,
-                                uint32_t* __restrict__ keys, uint32_t* __restrict__ hist)
+                                uint32_t* __restrict__ hist)
 {
     const int lane = threadIdx.x & 31;
     const unsigned lt = (1u << lane) - 1u;
@@ -365,16 +385,10 @@ __global__ void sort_key_kernel(const double* __restrict__ xs, const uint8_t* __
     for (int64_t base = (int64_t)blockIdx.x * blockDim.x + (threadIdx.x & ~31); base < n; base += stride) {
         const int64_t i = base + lane;
         const bool valid = i < n;
-        uint32_t key = dead_key;
-        if (valid && as[i]) {
-            int ix = min(max((int)floor(xs[i]), 0), nx - 2);
-            int iy = min(max((int)floor(xs[n + i]), 0), ny - 2);
-            int iz = min(max((int)floor(xs[2 * n + i]), 0), nz - 2);
-            key = (offs[ix] + offs[nx + iy] + offs[nx + ny + iz]) >> 9;
-        }
+        const uint32_t key =
+            valid ? brick_key(xs[i], xs[n + i], xs[2 * n + i], as[i], offs, nx, ny, nz, dead_key) : dead_key;
         const unsigned act = __ballot_sync(0xffffffffu, valid);
         if (valid) {
-            keys[i] = key;
             const unsigned same = __match_any_sync(act, key);
             if ((same & lt) == 0) atomicAdd(&hist[key], (uint32_t)__popc(same));
         }
@@ -454,11 +468,14 @@ __global__ void __launch_bounds__(1024) sort_scan_top_kernel(uint32_t* tile_off,
     }
 }
 
-__global__ void sort_scatter_kernel(const uint32_t* __restrict__ keys, uint32_t* cursor,
-                                    const uint32_t* __restrict__ tile_off, int64_t n, const double* __restrict__ xs, const float* __restrict__ ps,
+// The whole state of a particle is loaded (and its bucket recomputed from
+// it) before the cursor atomic, so the loads overlap the atomic's round trip.
+__global__ void sort_scatter_kernel(uint32_t* cursor, const uint32_t* __restrict__ tile_off, int64_t n,
+                                    const uint32_t* __restrict__ offs, int nx, int ny, int nz, uint32_t dead_key,
+                                    const double* __restrict__ xs, const float* __restrict__ ps,
                                     const double* __restrict__ p2s, const int32_t* __restrict__ pids,
-                                    const uint8_t* __restrict__ as, double* xd, float* pd, double* p2d, int32_t* pidd,
-                                    uint8_t* ad)
+                                    const uint8_t* __restrict__ as, double* __restrict__ xd, float* __restrict__ pd,
+                                    double* __restrict__ p2d, int32_t* __restrict__ pidd, uint8_t* __restrict__ ad)
 {
     const int lane = threadIdx.x & 31;
     const unsigned lt = (1u << lane) - 1u;
@@ -468,18 +485,23 @@ __global__ void sort_scatter_kernel(const uint32_t* __restrict__ keys, uint32_t*
         const bool valid = i < n;
         const unsigned act = __ballot_sync(0xffffffffu, valid);
         if (!valid) continue;
-        const uint32_t key = keys[i];
+        const double x0 = xs[i], x1 = xs[n + i], x2 = xs[2 * n + i];
+        const float q0 = ps[i], q1 = ps[n + i], q2 = ps[2 * n + i];
+        const double pp = p2s[i];
+        const int32_t id = pids[i];
+        const uint8_t al = as[i];
+        const uint32_t key = brick_key(x0, x1, x2, al, offs, nx, ny, nz, dead_key);
         const unsigned same = __match_any_sync(act, key);
         const int leader = __ffs(same) - 1;
         uint32_t first = 0;
         if (lane == leader) first = atomicAdd(&cursor[key], (uint32_t)__popc(same)) + tile_off[key / kScanTile];
         first = __shfl_sync(same, first, leader);
         const int64_t d = (int64_t)first + __popc(same & lt);
-        xd[d] = xs[i]; xd[n + d] = xs[n + i]; xd[2 * n + d] = xs[2 * n + i];
-        pd[d] = ps[i]; pd[n + d] = ps[n + i]; pd[2 * n + d] = ps[2 * n + i];
-        p2d[d] = p2s[i];
-        pidd[d] = pids[i];
-        ad[d] = as[i];
+        xd[d] = x0; xd[n + d] = x1; xd[2 * n + d] = x2;
+        pd[d] = q0; pd[n + d] = q1; pd[2 * n + d] = q2;
+        p2d[d] = pp;
+        pidd[d] = id;
+        ad[d] = al;
     }
 }
 
@@ -494,14 +516,14 @@ int grid_for(int64_t n, int threads, int num_sms)
 
 // Persistent launch: (SM count) x (resident blocks per SM, optionally capped).
 // The gather is cache-bound, so fewer resident warps can win (less L1 churn).
-template <int LAYOUT, int BLOCK, int MINB>
+template <int LAYOUT, int BLOCK, int MINB, int TEXC = 0>
 int launch_push_fast_shape(const PushArgsFast& a, cudaStream_t s, int cap_per_sm = 0)
 {
     const size_t smem = sizeof(uint32_t) * (size_t)(a.fld.nx + a.fld.ny + a.fld.nz);
     int dev = 0, sms = 148, per_sm = 1;
     cudaGetDevice(&dev);
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-    auto kfn = push_fast_kernel<LAYOUT, BLOCK, MINB>;
+    auto kfn = push_fast_kernel<LAYOUT, BLOCK, MINB, TEXC>;
     if (smem > 48 * 1024) PT_CUDA(cudaFuncSetAttribute(kfn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
     cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kfn, BLOCK, smem);
     per_sm = std::max(per_sm, 1);
@@ -523,6 +545,15 @@ int launch_push_fast_t(const PushArgsFast& a, cudaStream_t s)
     case 6: return launch_push_fast_shape<LAYOUT,512, 1>(a, s, 1);
     case 7: return launch_push_fast_shape<LAYOUT,128, 1>(a, s, 3);
     case 8: return launch_push_fast_shape<LAYOUT,128, 1>(a, s, 2);
+    case 9:   // 256 x occupancy, half of the corners through the texture path
+        if (LAYOUT == LAYOUT_BF16 && a.fld.tex) return launch_push_fast_shape<LAYOUT, 256, 1, 4>(a, s);
+        return launch_push_fast_shape<LAYOUT, 256, 1>(a, s);
+    case 10:  // 256 x occupancy, every corner through the texture path
+        if (LAYOUT == LAYOUT_BF16 && a.fld.tex) return launch_push_fast_shape<LAYOUT, 256, 1, 8>(a, s);
+        return launch_push_fast_shape<LAYOUT, 256, 1>(a, s);
+    case 11:  // 512 x 1, half of the corners through the texture path
+        if (LAYOUT == LAYOUT_BF16 && a.fld.tex) return launch_push_fast_shape<LAYOUT, 512, 1, 4>(a, s, 1);
+        return launch_push_fast_shape<LAYOUT, 512, 1>(a, s, 1);
     case 0:
     case 1:
     default: return launch_push_fast_shape<LAYOUT,256, 1>(a, s);
@@ -579,8 +610,8 @@ int fast_sort(pt_ctx* ctx, pt_fast_state* st, const pt_field* f, cudaStream_t s)
     if (n <= 1) return PT_OK;
     const uint32_t nb = (uint32_t)((f->n_nodes + 511) / 512);
     const int64_t m = (int64_t)nb + 1;  // + dead bucket
-    // scratch: keys[n], hist[m], cursor[m]; the scatter goes to the state's
-    // second buffer set, which then becomes the current one
+    // scratch: hist[m], cursor[m], tile offsets; the scatter goes to the
+    // state's second buffer set, which then becomes the current one
     size_t off = 0;
     auto take = [&](size_t bytes) {
         size_t o = off;
@@ -588,8 +619,8 @@ int fast_sort(pt_ctx* ctx, pt_fast_state* st, const pt_field* f, cudaStream_t s)
         return o;
     };
     const int64_t tiles = (m + kScanTile - 1) / kScanTile;
-    const size_t o_keys = take(sizeof(uint32_t) * n), o_hist = take(sizeof(uint32_t) * m),
-                 o_cur = take(sizeof(uint32_t) * m), o_tiles = take(sizeof(uint32_t) * tiles);
+    const size_t o_hist = take(sizeof(uint32_t) * m), o_cur = take(sizeof(uint32_t) * m),
+                 o_tiles = take(sizeof(uint32_t) * tiles);
     if (st->sort_tmp_bytes < off) {
         if (st->sort_tmp) cudaFree(st->sort_tmp);
         st->sort_tmp = nullptr;
@@ -613,21 +644,20 @@ int fast_sort(pt_ctx* ctx, pt_fast_state* st, const pt_field* f, cudaStream_t s)
         }
     }
     char* base = (char*)st->sort_tmp;
-    uint32_t* keys = (uint32_t*)(base + o_keys);
     uint32_t* hist = (uint32_t*)(base + o_hist);
     uint32_t* cur = (uint32_t*)(base + o_cur);
     uint32_t* tile_off = (uint32_t*)(base + o_tiles);
     PT_CUDA(cudaMemsetAsync(hist, 0, sizeof(uint32_t) * m, s));
     const int gb = grid_for(n, 256, ctx->num_sms);
-    sort_key_kernel<<<gb, 256, 0, s>>>(st->x, st->alive, n, f->offs, (int)f->grid.nx, (int)f->grid.ny,
-                                       (int)f->grid.nz, nb, keys, hist);
+    const int nx = (int)f->grid.nx, ny = (int)f->grid.ny, nz = (int)f->grid.nz;
+    sort_key_kernel<<<gb, 256, 0, s>>>(st->x, st->alive, n, f->offs, nx, ny, nz, nb, hist);
     PT_CHECK_LAUNCH("sort_key_kernel");
     sort_scan_tiles_kernel<<<(unsigned)tiles, 1024, 0, s>>>(hist, cur, tile_off, m, nullptr);
     PT_CHECK_LAUNCH("sort_scan_tiles_kernel");
     sort_scan_top_kernel<<<1, 1024, 0, s>>>(tile_off, tiles, nullptr);
     PT_CHECK_LAUNCH("sort_scan_top_kernel");
-    sort_scatter_kernel<<<gb, 256, 0, s>>>(keys, cur, tile_off, n, st->x, st->p, st->p2, st->pid, st->alive,
-                                           st->x_alt, st->p_alt, st->p2_alt, st->pid_alt, st->alive_alt);
+    sort_scatter_kernel<<<gb, 256, 0, s>>>(cur, tile_off, n, f->offs, nx, ny, nz, nb, st->x, st->p, st->p2, st->pid,
+                                           st->alive, st->x_alt, st->p_alt, st->p2_alt, st->pid_alt, st->alive_alt);
     PT_CHECK_LAUNCH("sort_scatter_kernel");
     std::swap(st->x, st->x_alt);
     std::swap(st->p, st->p_alt);

@@ -85,13 +85,14 @@ def test_fp64_device_api_matches_host(cuda):
         assert np.array_equal(ens.state[k].cpu().numpy(), st_o[k]), k
 
 
-def _fast_mu(pb, storage, nsteps, stride, sort_every=0, u=True):
+def _fast_mu(pb, storage, nsteps, stride, sort_every=0, u=True, variant=0):
     torch = __import__("torch")
     fl = FieldLibrary(pb.fields, pb.grid, storage)
     ens = R.FastEnsemble(fl, pb.state, np.ones(len(pb.state["x1"]), np.uint8))
     nsave = R.n_saves(nsteps, stride)
     cache = torch.full((nsave, ens.n), float("nan"), dtype=torch.float32, device="cuda")
-    params = R.push_params(pb.dt, nsteps, stride, cache="mu", precision="f32", sort_every=sort_every)
+    params = R.push_params(pb.dt, nsteps, stride, cache="mu", precision="f32", sort_every=sort_every,
+                           kernel_variant=variant)
     ens.advance(params, 0, nsteps, cache, 0, nsave)
     st, al = ens.export()
     torch.cuda.synchronize()
@@ -114,6 +115,18 @@ def test_xpair_layout_bit_identical_to_bf16(cuda):
     pb = small_problem(n=16, n_particles=1500, u_over_c=1e-4, energy_GeV=10.0)
     mu_a, st_a, _ = _fast_mu(pb, "brick_bf16", 300, 4, sort_every=32)
     mu_b, st_b, _ = _fast_mu(pb, "brick_bf16x", 300, 4, sort_every=32)
+    assert np.array_equal(mu_a, mu_b, equal_nan=True)
+    for k in R.KEYS:
+        assert np.array_equal(st_a[k], st_b[k]), k
+
+
+@pytest.mark.parametrize("variant", [2, 3, 6, 9, 10, 11])
+def test_launch_shapes_and_texture_fetches_bit_identical(cuda, variant):
+    """Every launch shape, and corner fetches through the texture path
+    (variants 9-11), give the same trajectories as the default shape."""
+    pb = small_problem(n=16, n_particles=1200, u_over_c=1e-4, energy_GeV=10.0)
+    mu_a, st_a, _ = _fast_mu(pb, "brick_bf16", 200, 4, sort_every=32, variant=1)
+    mu_b, st_b, _ = _fast_mu(pb, "brick_bf16", 200, 4, sort_every=32, variant=variant)
     assert np.array_equal(mu_a, mu_b, equal_nan=True)
     for k in R.KEYS:
         assert np.array_equal(st_a[k], st_b[k]), k
