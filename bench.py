@@ -842,51 +842,80 @@ def run_precision(args, dev):
     return out
 
 
-def run_serving(args, dev, n_jobs=16, rate=4.0):
-    """Serving: a Poisson stream (mean 4 jobs/s) of transport jobs against
-    resident 256^3 and 512^3 BF16 libraries (4 modes each), admitted against a
-    150 GB HBM budget, continuously batched; p50/p99 job latency and the
-    aggregate particle-step rate."""
+def run_serving(args, dev, n_jobs=16, rate=4.0, n_cmp=8):
+    """Serving (config 5): a Poisson stream (mean 4 jobs/s) of transport jobs
+    against resident 256^3 and 512^3 libraries (4 modes each), admitted
+    against a 150 GB HBM budget and continuously batched; p50/p99 job latency
+    and the aggregate particle-step rate of the FP32 push over BF16 bricks.
+    Then the FP32 push against the plain FP64 push on one smaller stream
+    (n_cmp jobs, 16k-1M particles, 10-60 T_g0) -- the FP64 server pushes every
+    job with the reference-layout kernel from FP64 libraries of the same
+    fields."""
     import torch
 
     from particle_transport_b200 import fields as F
     from particle_transport_b200.fields import FieldLibrary
     from particle_transport_b200.server import CampaignServer, sample_jobs
 
-    libs, B0 = {}, {}
-    for n in (256, 512):
-        rg = F.gyroradius_m(1.0, 1e-10)
-        grid = F.build_uniform_grid((n - 1) * rg, n, n, n)
-        libs[str(n)] = {}
-        for m in ("total", "alfven", "fast", "slow"):
-            f = F.to_si(F.synthetic_mhd_fields(n, 2, n // 2, 0.5 if n == 256 else 1.0, 1.0, 1e-4, seed=91 + n,
-                                               spectrum="isotropic" if n == 256 else "gs", modes=m, device=dev))
-            if m == "total":
-                B0[str(n)] = F.reference_B0_T(*f[:3])
-            libs[str(n)][m] = FieldLibrary(f, grid, "brick_bf16", B_ref_T=B0[str(n)])
-            del f
+    B0 = {}
+
+    def make_libs(storage):
+        """The 2 x 4 seeded field libraries in one storage (same fields for every storage)."""
+        out = {}
+        for n in (256, 512):
+            rg = F.gyroradius_m(1.0, 1e-10)
+            grid = F.build_uniform_grid((n - 1) * rg, n, n, n)
+            out[str(n)] = {}
+            for m in ("total", "alfven", "fast", "slow"):
+                f = F.to_si(F.synthetic_mhd_fields(n, 2, n // 2, 0.5 if n == 256 else 1.0, 1.0, 1e-4, seed=91 + n,
+                                                   spectrum="isotropic" if n == 256 else "gs", modes=m, device=dev))
+                if m == "total":
+                    B0[str(n)] = F.reference_B0_T(*f[:3])
+                out[str(n)][m] = FieldLibrary(f, grid, storage, B_ref_T=B0[str(n)])
+                del f
+            torch.cuda.empty_cache()
+        return out
+
+    libs = make_libs("brick_bf16")
+
+    def serve(libraries, arrivals, specs, push):
+        srv = CampaignServer(libraries, B0, hbm_budget_bytes=150e9, capacity=1 << 27, max_jobs=len(specs), push=push)
+        torch.cuda.synchronize()
+        t_start = time.perf_counter()
+        nxt = 0
+        while nxt < len(specs) or not srv.idle():
+            now = time.perf_counter() - t_start
+            while nxt < len(specs) and arrivals[nxt] <= now:
+                srv.submit(specs[nxt], arrival=t_start + arrivals[nxt])
+                nxt += 1
+            srv.tick()
+        wall = time.perf_counter() - t_start
+        lat = np.array([r.latency for r in srv.results])
+        steps = sum(r.particle_steps for r in srv.results)
+        busy = srv.device_busy_s()
+        out = {"jobs": len(specs), "p50_s": float(np.percentile(lat, 50)), "p99_s": float(np.percentile(lat, 99)),
+               "mean_s": float(lat.mean()), "wall_s": wall, "particle_steps": int(steps),
+               "aggregate_rate": steps / wall, "device_busy_s": busy, "busy_rate": steps / busy,
+               "admit_host_s": srv.admit_s, "epochs": srv.epochs}
+        srv.close()
         torch.cuda.empty_cache()
+        return out
+
     arrivals, specs = sample_jobs(n_jobs, rate, ["256", "512"], seed=2026)
-    srv = CampaignServer(libs, B0, hbm_budget_bytes=150e9, capacity=1 << 27, max_jobs=n_jobs)
-    torch.cuda.synchronize()
-    t_start = time.perf_counter()
-    nxt = 0
-    while nxt < n_jobs or not srv.idle():
-        now = time.perf_counter() - t_start
-        while nxt < n_jobs and arrivals[nxt] <= now:
-            srv.submit(specs[nxt], arrival=t_start + arrivals[nxt])
-            nxt += 1
-        srv.tick()
-    wall = time.perf_counter() - t_start
-    lat = np.array([r.latency for r in srv.results])
-    steps = sum(r.particle_steps for r in srv.results)
-    busy = srv.device_busy_s()
-    srv.close()
-    return {"jobs": n_jobs, "rate_per_s": rate, "p50_s": float(np.percentile(lat, 50)),
-            "p99_s": float(np.percentile(lat, 99)), "mean_s": float(lat.mean()), "wall_s": wall,
-            "particle_steps": int(steps), "aggregate_rate": steps / wall, "device_busy_s": busy,
-            "busy_rate": steps / busy, "admit_host_s": srv.admit_s, "unit": UNIT, "push": "FP32 / BF16 bricks",
-            "init": "on the device (pt_particles_init_device)", "hbm_budget_GB": 150, "epochs": srv.epochs}
+    main = serve(libs, arrivals, specs, "f32")
+    main.update({"rate_per_s": rate, "unit": UNIT, "push": "FP32 / BF16 bricks",
+                 "init": "on the device (pt_particles_init_device)", "hbm_budget_GB": 150})
+    arr_c, specs_c = sample_jobs(n_cmp, rate, ["256", "512"], seed=7, n_range=(16_384, 1_048_576),
+                                 duration_range=(10.0, 60.0))
+    cmp32 = serve(libs, arr_c, specs_c, "f32")
+    libs64 = make_libs("ref_f64")  # built after the main stream: 29 GB of FP64 fields
+    cmp64 = serve(libs64, arr_c, specs_c, "f64")
+    main["fp32_vs_fp64"] = {"stream": f"{n_cmp} jobs, Poisson {rate}/s, 16k-1M particles, 10-60 T_g0, 1-300 GeV",
+                            "fp32_bf16": cmp32, "fp64_plain": cmp64,
+                            "busy_rate_ratio": cmp32["busy_rate"] / cmp64["busy_rate"]}
+    del libs64
+    torch.cuda.empty_cache()
+    return main
 
 
 def dist_barrier(ws):

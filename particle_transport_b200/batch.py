@@ -110,6 +110,56 @@ class Batch:
             pass
 
 
+class ReferenceBatch:
+    """The plain form of a batch: every campaign is pushed by the FP64
+    reference-layout kernel (pt_push_advance_device), one launch per campaign
+    per epoch, from its own step counter.  Same interface as Batch (add / run /
+    step / remove / close), so that the campaign server can run one job stream
+    through either push."""
+
+    def __init__(self, steps_per_epoch: int = 64, device: int = 0):
+        import torch
+
+        self.K = int(steps_per_epoch)
+        self.device = torch.device("cuda", device)
+        self.campaigns = {}
+        self._next = 0
+
+    def add(self, field: FieldLibrary, state: dict, dt: float, nsteps: int, stride: int, periodic: bool = True,
+            cache=None, alive=None, **_unused) -> int:
+        from .runner import DeviceEnsemble, push_params
+
+        if field.storage != "ref_f64":
+            raise ValueError("ReferenceBatch pushes REF_F64 fields")
+        n = int(len(state["x1"]))
+        ens = DeviceEnsemble(field, state, np.ones(n, np.uint8) if alive is None else alive)
+        params = push_params(dt, nsteps, stride, periodic, cache="mu" if cache is not None else "none",
+                             precision="f64", steps_per_launch=self.K)
+        cid = self._next
+        self._next += 1
+        self.campaigns[cid] = dict(ens=ens, params=params, nsteps=int(nsteps), cache=cache,
+                                   rows=0 if cache is None else int(cache.shape[0]), step=0)
+        return cid
+
+    def run(self, epochs: int, use_graph: bool = True) -> None:
+        for _ in range(int(epochs)):
+            for c in self.campaigns.values():
+                if c["step"] >= c["nsteps"]:
+                    continue
+                count = min(self.K, c["nsteps"] - c["step"])
+                c["ens"].advance(c["params"], c["step"], count, c["cache"], 0, c["rows"])
+                c["step"] += count
+
+    def step(self, cid: int) -> int:
+        return self.campaigns[cid]["step"]
+
+    def remove(self, cid: int) -> None:
+        self.campaigns.pop(cid, None)
+
+    def close(self):
+        self.campaigns.clear()
+
+
 # --------------------------------------------------------------------------
 # autotuner
 # --------------------------------------------------------------------------

@@ -29,7 +29,7 @@ import numpy as np
 
 from . import _lib
 from . import stats as S
-from .batch import Batch
+from .batch import Batch, ReferenceBatch
 from .fields import FieldLibrary, M_P, Q_E
 from .particles import energy_to_gamma, init_particles_device
 from .time_units import build_mu_edges_full, log_spaced_lag_steps, reference_Omega0
@@ -73,8 +73,9 @@ class JobResult:
 class CampaignServer:
     def __init__(self, libraries: dict, B0_ref_T: dict, hbm_budget_bytes: float = 150e9, storage: str = "brick_bf16",
                  steps_per_epoch: int = 64, capacity: int = 1 << 26, max_jobs: int = 256, blocks_per_sm: int = 0,
-                 keep_cache: bool = False, device: int = 0):
-        """libraries: {library: {mode: FieldLibrary}} (brick storage);
+                 keep_cache: bool = False, device: int = 0, push: str = "f32"):
+        """libraries: {library: {mode: FieldLibrary}} (brick storage for the
+        FP32 push; REF_F64 for push="f64", the plain FP64 push);
         B0_ref_T: {library: total-field mean |B|} (time reference of every mode).
         A job's initial state is written on the device from its seed
         (pt_particles_init_device); fixed-mu injection takes the local field
@@ -86,8 +87,14 @@ class CampaignServer:
         self.B0 = B0_ref_T
         self.budget = float(hbm_budget_bytes)
         self.K = int(steps_per_epoch)
-        self.batch = Batch(capacity, max_campaigns=max_jobs, storage=storage, steps_per_epoch=self.K,
-                           blocks_per_sm=blocks_per_sm, device=device)
+        if push not in ("f32", "f64"):
+            raise ValueError("push must be f32 or f64")
+        self.push = push
+        if push == "f64":
+            self.batch = ReferenceBatch(steps_per_epoch=self.K, device=device)
+        else:
+            self.batch = Batch(capacity, max_campaigns=max_jobs, storage=storage, steps_per_epoch=self.K,
+                               blocks_per_sm=blocks_per_sm, device=device)
         self.device = torch.device("cuda", device)
         self.side = torch.cuda.Stream(device=self.device)
         self.side_ctx = _lib.Context(device)

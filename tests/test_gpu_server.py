@@ -25,15 +25,24 @@ def library(cuda):
     return libs, B0
 
 
+@pytest.fixture(scope="module")
+def library64(cuda):
+    pa = small_problem(n=16, n_particles=4, u_over_c=1e-4, seed=3)
+    pb = small_problem(n=16, n_particles=4, u_over_c=2e-4, seed=9)
+    libs = {"16": {"total": FieldLibrary(pa.fields, pa.grid, "ref_f64"),
+                   "alfven": FieldLibrary(pb.fields, pb.grid, "ref_f64")}}
+    return libs, {"16": reference_B0_T(*pa.fields[:3])}
+
+
 JOBS = [JobSpec("16", "total", 1.0, 3000, 6.0, seed=1),
         JobSpec("16", "alfven", 20.0, 777, 3.5, injection="fixed_mu", mu0=0.3, seed=2),
         JobSpec("16", "total", 5.0, 1500, 9.0, seed=3, n_lags=12, n_bins=10),
         JobSpec("16", "alfven", 2.0, 64, 2.0, seed=4)]
 
 
-def run_jobs(library, jobs, budget=150e9, stagger_ticks=0):
+def run_jobs(library, jobs, budget=150e9, stagger_ticks=0, push="f32"):
     libs, B0 = library
-    srv = CampaignServer(libs, B0, hbm_budget_bytes=budget, capacity=20000, max_jobs=8, keep_cache=True)
+    srv = CampaignServer(libs, B0, hbm_budget_bytes=budget, capacity=20000, max_jobs=8, keep_cache=True, push=push)
     pending = list(jobs)
     ids = []
     while pending or not srv.idle():
@@ -82,3 +91,36 @@ def test_budget_holds_jobs_back(library):
     assert all(not (q.admitted <= big.admitted < q.finished) for q in res if q is not big)
     alone = run_jobs(library, [JOBS[2]])[0]
     same([r for r in res if r.spec is JOBS[2]][0], alone)
+
+
+def test_fp64_server_alone_mixed_and_direct(library64):
+    """The plain FP64 push served: each job's result is the same alone and in
+    the mix, and its mu cache is the one a direct FP64 run of the same initial
+    state writes (bit for bit)."""
+    import math
+
+    import torch
+
+    from particle_transport_b200 import runner as R
+    from particle_transport_b200.fields import M_P, Q_E
+    from particle_transport_b200.particles import energy_to_gamma, init_particles_device
+    from particle_transport_b200.time_units import reference_Omega0
+
+    alone = [run_jobs(library64, [j], push="f64")[0] for j in JOBS]
+    mixed = run_jobs(library64, JOBS, stagger_ticks=1, push="f64")
+    for a, m in zip(alone, mixed):
+        same(m, a)
+    libs, B0 = library64
+    j = JOBS[1]
+    fl = libs[j.library][j.mode]
+    st = init_particles_device(fl, j.n_particles, j.energy_GeV, seed=j.seed, injection_mode=j.injection, mu0=j.mu0)
+    dt = (2 * math.pi / j.steps_per_gyroperiod) / reference_Omega0(B0[j.library], energy_to_gamma(j.energy_GeV), Q_E,
+                                                                   M_P)
+    nsteps = int(round(j.duration_gyroperiods * j.steps_per_gyroperiod)) + 1
+    stride = j.steps_per_gyroperiod // j.saves_per_gyroperiod
+    nsave = R.n_saves(nsteps, stride)
+    ens = R.DeviceEnsemble(fl, st, np.ones(j.n_particles, np.uint8))
+    cache = torch.empty((nsave, j.n_particles), dtype=torch.float32, device="cuda")
+    ens.advance(R.push_params(dt, nsteps, stride, cache="mu", precision="f64"), 0, nsteps, cache, 0, nsave)
+    torch.cuda.synchronize()
+    assert np.array_equal(mixed[1].mu, cache.cpu().numpy(), equal_nan=True)
