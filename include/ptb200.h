@@ -218,6 +218,10 @@ typedef struct {
     int32_t cache_ring;        /* 1: save row r goes to row r % cache_rows                   */
     int32_t reserved;
     int64_t* d_deaths;         /* [nsteps] particles killed per step (open boundary), or NULL */
+    float* d_mom_cache;        /* with d_cache: momenta rows [cache_rows][3][n_mom] (Float32, SI, the
+                                  phase-space writer's momenta, src/phase_space_gpu_runner.jl:413-421)
+                                  of particles 0 .. n_mom-1 -- the D_pp subset -- or NULL */
+    int64_t n_mom;
 } pt_campaign_desc;
 
 /* capacity: particle slots; blocks_per_sm: resident blocks of the persistent

@@ -44,9 +44,11 @@ class Batch:
         self.campaigns = {}
 
     def add(self, field: FieldLibrary, state: dict, dt: float, nsteps: int, stride: int, periodic: bool = True,
-            cache=None, ring: bool = False, deaths=None, alive=None) -> int:
+            cache=None, ring: bool = False, deaths=None, alive=None, mom_cache=None) -> int:
         """Add a campaign; state: SI arrays x1..p3 (numpy or CUDA tensors);
-        cache: CUDA float32 tensor [rows][n] for the mu rows (or None)."""
+        cache: CUDA float32 tensor [rows][n] for the mu rows (or None);
+        mom_cache: CUDA float32 tensor [rows][3][n_mom] that receives the
+        momenta of particles 0 .. n_mom-1 at every save (needs cache)."""
         import torch
 
         n = int(len(state["x1"]))
@@ -57,16 +59,24 @@ class Batch:
         if cache is not None:
             if cache.dtype not in (torch.float32, torch.float64) or cache.shape[-1] != n or not cache.is_contiguous():
                 raise ValueError("cache must be a contiguous float tensor [rows][n]")
+        n_mom = 0
+        if mom_cache is not None:
+            if (cache is None or mom_cache.dtype != torch.float32 or mom_cache.dim() != 3 or mom_cache.shape[1] != 3
+                    or mom_cache.shape[0] != cache.shape[0] or not mom_cache.is_contiguous()):
+                raise ValueError("mom_cache must be a contiguous float32 tensor [rows][3][n_mom] beside the mu cache")
+            n_mom = int(mom_cache.shape[2])
         d = _lib.CampaignDesc(field.handle, float(dt), int(nsteps), int(stride), int(bool(periodic)),
                               int(cache is not None and cache.dtype == torch.float64), n,
                               *[st[k].data_ptr() for k in KEYS], al.data_ptr(),
                               cache.data_ptr() if cache is not None else None,
                               int(cache.shape[0]) if cache is not None else 0, int(bool(ring)), 0,
-                              deaths.data_ptr() if deaths is not None else None)
+                              deaths.data_ptr() if deaths is not None else None,
+                              mom_cache.data_ptr() if mom_cache is not None else None, n_mom)
         cid = C.c_int()
         ctx = _lib.torch_context(self.device.index)
         _lib.call("pt_batch_add", ctx.handle, self.handle, C.byref(d), C.byref(cid))
-        self.campaigns[cid.value] = {"field": field, "n": n, "nsteps": int(nsteps), "cache": cache, "deaths": deaths}
+        self.campaigns[cid.value] = {"field": field, "n": n, "nsteps": int(nsteps), "cache": cache, "deaths": deaths,
+                                     "mom_cache": mom_cache}
         return cid.value
 
     def remove(self, cid: int) -> None:
@@ -126,19 +136,38 @@ class ReferenceBatch:
         self._next = 0
 
     def add(self, field: FieldLibrary, state: dict, dt: float, nsteps: int, stride: int, periodic: bool = True,
-            cache=None, alive=None, **_unused) -> int:
+            cache=None, alive=None, mom_cache=None, **_unused) -> int:
+        """As Batch.add.  With mom_cache, the D_pp subset (particles
+        0 .. n_mom-1) is pushed a second time in phase-space mode -- the FP64
+        trajectory of a particle does not depend on the others -- and its
+        momenta rows land in mom_cache when the campaign finishes."""
+        import torch
+
         from .runner import DeviceEnsemble, push_params
 
         if field.storage != "ref_f64":
             raise ValueError("ReferenceBatch pushes REF_F64 fields")
         n = int(len(state["x1"]))
-        ens = DeviceEnsemble(field, state, np.ones(n, np.uint8) if alive is None else alive)
+        al = np.ones(n, np.uint8) if alive is None else alive
+        ens = DeviceEnsemble(field, state, al)
         params = push_params(dt, nsteps, stride, periodic, cache="mu" if cache is not None else "none",
                              precision="f64", steps_per_launch=self.K)
+        sub = None
+        if mom_cache is not None:
+            m = int(mom_cache.shape[2])
+            # a copy: DeviceEnsemble advances its state arrays in place, and a
+            # prefix of the campaign's arrays would alias the main ensemble
+            sub_state = {k: torch.as_tensor(np.asarray(state[k]) if not hasattr(state[k], "is_cuda") else state[k],
+                                            dtype=torch.float64, device=self.device)[:m].clone() for k in KEYS}
+            sub = dict(ens=DeviceEnsemble(field, sub_state, np.asarray(al)[:m].copy()),
+                       params=push_params(dt, nsteps, stride, periodic, cache="phase_space", precision="f64",
+                                          steps_per_launch=self.K),
+                       ps=torch.empty((mom_cache.shape[0], 6, m), dtype=torch.float32, device=self.device),
+                       out=mom_cache)
         cid = self._next
         self._next += 1
         self.campaigns[cid] = dict(ens=ens, params=params, nsteps=int(nsteps), cache=cache,
-                                   rows=0 if cache is None else int(cache.shape[0]), step=0)
+                                   rows=0 if cache is None else int(cache.shape[0]), step=0, sub=sub)
         return cid
 
     def run(self, epochs: int, use_graph: bool = True) -> None:
@@ -148,7 +177,12 @@ class ReferenceBatch:
                     continue
                 count = min(self.K, c["nsteps"] - c["step"])
                 c["ens"].advance(c["params"], c["step"], count, c["cache"], 0, c["rows"])
+                sub = c["sub"]
+                if sub is not None:
+                    sub["ens"].advance(sub["params"], c["step"], count, sub["ps"], 0, c["rows"])
                 c["step"] += count
+                if sub is not None and c["step"] >= c["nsteps"]:
+                    sub["out"].copy_(sub["ps"][:, 3:6, :])
 
     def step(self, cid: int) -> int:
         return self.campaigns[cid]["step"]

@@ -247,6 +247,8 @@ int pt_batch_add(pt_ctx* ctx, pt_batch* b, const pt_campaign_desc* d, int* id)
     if (d->d_cache && d->cache_rows < 1) return fail(PT_ERR_ARG, "cache_rows must be >= 1");
     if (d->d_cache && !d->cache_ring && d->cache_rows < (d->nsteps - 1) / d->stride + 1)
         return fail(PT_ERR_ARG, "a non-ring cache needs one row per save");
+    if (d->d_mom_cache && (!d->d_cache || d->n_mom < 1 || d->n_mom > d->n))
+        return fail(PT_ERR_ARG, "a momenta cache needs the mu cache and 1 <= n_mom <= n");
     int c = -1;
     for (int i = 0; i < b->max_camps; ++i)
         if (!b->h_camps[i].active) {
@@ -303,6 +305,8 @@ int pt_batch_add(pt_ctx* ctx, pt_batch* b, const pt_campaign_desc* d, int* id)
     a.ring = d->cache_ring;
     a.n_cache = d->n;
     a.deaths = d->d_deaths;
+    a.mom_cache = d->d_mom_cache;
+    a.n_mom = d->d_mom_cache ? d->n_mom : 0;
     C.slot0 = slot0;
     C.n = d->n;
     C.step = 0;

@@ -175,6 +175,8 @@ struct PushArgsFast {
     int variant;           // launch shape, see pt_push_params.kernel_variant
     int ring;              // 1: save row r goes to cache row r % rows
     int64_t n_cache;       // particles per cache row
+    float* mom_cache;      // with a mu cache: momenta rows [rows][3][n_mom] of particles pid < n_mom, or null
+    int64_t n_mom;
 };
 int launch_push_fast(const PushArgsFast& a, cudaStream_t s);
 

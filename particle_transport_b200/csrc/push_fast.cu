@@ -182,6 +182,15 @@ __device__ __forceinline__ void advance_particle(double& x, double& y, double& z
                         mu = mu_f32(px, py, pz, f[0], f[1], f[2]);
                     if (a.cache_f64) ((double*)a.cache)[r * n + pid] = (double)mu;
                     else ((float*)a.cache)[r * n + pid] = mu;
+                    if (pid < a.n_mom) {
+                        // momenta of the D_pp subset, as the phase-space writer stores them
+                        const double pm = sqrt(P2) / sqrt((double)px * px + (double)py * py + (double)pz * pz) *
+                                          (M_P * C_LIGHT);
+                        float* M = a.mom_cache + r * 3 * a.n_mom + pid;
+                        M[0] = al ? (float)((double)px * pm) : NAN;
+                        M[a.n_mom] = al ? (float)((double)py * pm) : NAN;
+                        M[2 * a.n_mom] = al ? (float)((double)pz * pm) : NAN;
+                    }
                 } else {
                     double v[6];
                     const double pm = sqrt(P2) / sqrt((double)px * px + (double)py * py + (double)pz * pz) *

@@ -102,7 +102,9 @@ def run_push_host(field: FieldLibrary, state: dict, alive: np.ndarray, params: _
 
 class DeviceEnsemble:
     """FP64 SI state resident on the device (torch tensors) for the
-    reference-layout push (pt_push_advance_device)."""
+    reference-layout push (pt_push_advance_device).  CUDA float64 contiguous
+    state arrays are used as they are, not copied: the push advances them in
+    place."""
 
     def __init__(self, field: FieldLibrary, state: dict, alive):
         import torch

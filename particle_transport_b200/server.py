@@ -50,6 +50,7 @@ class JobSpec:
     n_lags: int = 32
     n_bins: int = 20
     start_mode: str = "sliding"
+    dpp_particles: int = 65536   # D_pp subset: particles 0 .. min(n, this) - 1 (0: no D_pp)
 
 
 @dataclass
@@ -64,6 +65,7 @@ class JobResult:
     lags: np.ndarray = None
     edges: np.ndarray = None
     mu: np.ndarray = None        # the mu cache, when the server keeps it (keep_cache=True)
+    dpp: dict = None             # D_pp sums of the subset on the same lags (counts, sum_delta_p, ...), p0
 
     @property
     def latency(self) -> float:
@@ -116,7 +118,8 @@ class CampaignServer:
         stride = spec.steps_per_gyroperiod // spec.saves_per_gyroperiod
         nsave = (nsteps - 1) // stride + 1
         n = spec.n_particles
-        return n * (2 * 49 + 49) + 4.0 * n * nsave + 64 * spec.n_lags * (spec.n_bins + 1)
+        n_dpp = min(n, max(0, spec.dpp_particles))
+        return n * (2 * 49 + 49) + 4.0 * n * nsave + 12.0 * n_dpp * nsave + 64 * spec.n_lags * (spec.n_bins + 1)
 
     def submit(self, spec: JobSpec, arrival: float = None) -> int:
         jid = self.next_id
@@ -136,9 +139,11 @@ class CampaignServer:
         st = init_particles_device(fl, spec.n_particles, spec.energy_GeV, seed=spec.seed,
                                    injection_mode=spec.injection, mu0=spec.mu0)
         cache = torch.empty((nsave, spec.n_particles), dtype=torch.float32, device=self.device)
-        cid = self.batch.add(fl, st, dt, nsteps, stride, cache=cache)
-        self.active[jid] = dict(spec=spec, cid=cid, cache=cache, nsteps=nsteps, nsave=nsave, arrival=arrival,
-                                admitted=time.perf_counter(), bytes=self.job_bytes(spec))
+        n_dpp = min(spec.n_particles, max(0, spec.dpp_particles))
+        mom = torch.empty((nsave, 3, n_dpp), dtype=torch.float32, device=self.device) if n_dpp else None
+        cid = self.batch.add(fl, st, dt, nsteps, stride, cache=cache, mom_cache=mom)
+        self.active[jid] = dict(spec=spec, cid=cid, cache=cache, mom=mom, nsteps=nsteps, nsave=nsave,
+                                arrival=arrival, admitted=time.perf_counter(), bytes=self.job_bytes(spec))
         self.used += self.job_bytes(spec)
 
     def admit(self) -> int:
@@ -186,10 +191,40 @@ class CampaignServer:
                       *[_lib.ptr(acc[k]) for k in ("dmumu_counts", "dmumu_sum_delta", "dmumu_sum_delta2",
                                                    "particle_counts", "particle_means", "particle_m2s",
                                                    "pair_sum_squares", "pair_counts")])
+            dpp = None
+            if rec["mom"] is not None:
+                # D_pp of the subset with p0 = 1: the kernel normalises once per
+                # lag (sum dp / p0, sum dp^2 / p0 / p0), so dividing by the true
+                # p0 when the result is collected gives the same values without
+                # reading p0 back here
+                mom = rec["mom"]
+                dpp = S.new_dpp_accumulators(len(lags), device=self.device)
+                _lib.call("pt_dpp_accumulate_device", self.side_ctx.handle, _lib.ptr(mom), mom.shape[2],
+                          rec["nsave"], _lib.ptr(d_lags), len(lags), 1.0,
+                          *[_lib.ptr(dpp[k]) for k in ("counts", "sum_delta_p", "sum_delta_p2", "sum_delta_p_norm",
+                                                       "sum_delta_p_norm2")])
             ev = torch.cuda.Event()
             ev.record(self.side)
-        rec.update(acc=acc, lags=lags, edges=edges, ev=ev, keep=(d_lags, d_edges))
+        rec.update(acc=acc, dpp=dpp, lags=lags, edges=edges, ev=ev, keep=(d_lags, d_edges))
         self.binning[jid] = rec
+
+    @staticmethod
+    def _dpp_result(rec):
+        """D_pp sums of a finished job normalised by p0 = |p| of its first
+        particle at the first save (compute_dpp_full.jl:483), as the reference."""
+        if rec["dpp"] is None:
+            return None
+        d = {k: v.cpu().numpy() for k, v in rec["dpp"].items()}
+        m = rec["mom"][0, :, 0].double().cpu().numpy()
+        p0 = math.sqrt(float(m[0]) * float(m[0]) + float(m[1]) * float(m[1]) + float(m[2]) * float(m[2]))
+        if not (math.isfinite(p0) and p0 > 0.0):
+            d["sum_delta_p_norm"] = np.full_like(d["sum_delta_p_norm"], np.nan)
+            d["sum_delta_p_norm2"] = np.full_like(d["sum_delta_p_norm2"], np.nan)
+        else:
+            d["sum_delta_p_norm"] = d["sum_delta_p_norm"] / p0
+            d["sum_delta_p_norm2"] = d["sum_delta_p_norm2"] / p0 / p0
+        d["p0"] = p0
+        return d
 
     def tick(self):
         """One scheduling step; returns the jobs finished in it."""
@@ -217,7 +252,7 @@ class CampaignServer:
                 res = JobResult(jid, spec, rec["arrival"], rec["admitted"], time.perf_counter(),
                                 spec.n_particles * (rec["nsteps"] - 1),
                                 {k: v.cpu().numpy() for k, v in rec["acc"].items()}, rec["lags"], rec["edges"],
-                                rec["cache"].cpu().numpy() if self.keep_cache else None)
+                                rec["cache"].cpu().numpy() if self.keep_cache else None, self._dpp_result(rec))
                 self.batch.remove(rec["cid"])
                 self.used -= rec["bytes"]
                 del self.binning[jid]

@@ -36,7 +36,7 @@ def library64(cuda):
 
 JOBS = [JobSpec("16", "total", 1.0, 3000, 6.0, seed=1),
         JobSpec("16", "alfven", 20.0, 777, 3.5, injection="fixed_mu", mu0=0.3, seed=2),
-        JobSpec("16", "total", 5.0, 1500, 9.0, seed=3, n_lags=12, n_bins=10),
+        JobSpec("16", "total", 5.0, 1500, 9.0, seed=3, n_lags=12, n_bins=10, dpp_particles=500),
         JobSpec("16", "alfven", 2.0, 64, 2.0, seed=4)]
 
 
@@ -65,6 +65,20 @@ def same(a, b):
         assert np.allclose(a.acc[k], b.acc[k], rtol=1e-12, atol=0), k
     sc = 1e-12 * (np.sqrt(np.maximum(b.acc["dmumu_counts"], 1) * b.acc["dmumu_sum_delta2"]) + 1e-30)
     assert np.all(np.abs(a.acc["dmumu_sum_delta"] - b.acc["dmumu_sum_delta"]) <= sc)
+    same_dpp(a.dpp, b.dpp)
+
+
+def same_dpp(a, b):
+    assert (a is None) == (b is None)
+    if b is None:
+        return
+    assert a["p0"] == b["p0"]
+    assert np.array_equal(a["counts"], b["counts"]) and a["counts"].sum() > 0
+    for k in ("sum_delta_p2", "sum_delta_p_norm2"):
+        assert np.allclose(a[k], b[k], rtol=1e-12, atol=0), k
+    for k, k2 in (("sum_delta_p", "sum_delta_p2"), ("sum_delta_p_norm", "sum_delta_p_norm2")):
+        sc = 1e-12 * (np.sqrt(np.maximum(b["counts"], 1) * b[k2]) + 1e-300)
+        assert np.all(np.abs(a[k] - b[k]) <= sc), k
 
 
 def test_job_results_same_alone_and_in_the_mix(library):
@@ -124,3 +138,41 @@ def test_fp64_server_alone_mixed_and_direct(library64):
     ens.advance(R.push_params(dt, nsteps, stride, cache="mu", precision="f64"), 0, nsteps, cache, 0, nsave)
     torch.cuda.synchronize()
     assert np.array_equal(mixed[1].mu, cache.cpu().numpy(), equal_nan=True)
+
+
+def test_dpp_of_served_job_equals_direct_phase_space_run(library):
+    """A served job's D_pp subset: the same momenta as a direct phase-space
+    run of the same initial state, so the same D_pp sums."""
+    import math
+
+    import torch
+
+    from particle_transport_b200 import runner as R
+    from particle_transport_b200 import stats as S
+    from particle_transport_b200.fields import M_P, Q_E
+    from particle_transport_b200.particles import energy_to_gamma, init_particles_device
+    from particle_transport_b200.time_units import reference_Omega0
+
+    j = JOBS[2]
+    res = run_jobs(library, [j])[0]
+    libs, B0 = library
+    fl = libs[j.library][j.mode]
+    st = init_particles_device(fl, j.n_particles, j.energy_GeV, seed=j.seed, injection_mode=j.injection, mu0=j.mu0)
+    dt = (2 * math.pi / j.steps_per_gyroperiod) / reference_Omega0(B0[j.library], energy_to_gamma(j.energy_GeV), Q_E,
+                                                                   M_P)
+    nsteps = int(round(j.duration_gyroperiods * j.steps_per_gyroperiod)) + 1
+    stride = j.steps_per_gyroperiod // j.saves_per_gyroperiod
+    nsave = R.n_saves(nsteps, stride)
+    ens = R.FastEnsemble(fl, st, np.ones(j.n_particles, np.uint8))
+    ps = torch.empty((nsave, 6, j.n_particles), dtype=torch.float32, device="cuda")
+    ens.advance(R.push_params(dt, nsteps, stride, cache="phase_space", precision="f32", sort_every=64), 0, nsteps,
+                ps, 0, nsave)
+    mom = ps[:, 3:6, :j.dpp_particles].contiguous()
+    m0 = mom[0, :, 0].double().cpu().numpy()
+    p0 = math.sqrt(float(m0[0]) * float(m0[0]) + float(m0[1]) * float(m0[1]) + float(m0[2]) * float(m0[2]))
+    acc = S.new_dpp_accumulators(len(res.lags), device="cuda")
+    S.process_momenta_chunk_dpp(mom, res.lags, p0, acc["counts"], acc["sum_delta_p"], acc["sum_delta_p2"],
+                                acc["sum_delta_p_norm"], acc["sum_delta_p_norm2"])
+    direct = {k: v.cpu().numpy() for k, v in acc.items()}
+    direct["p0"] = p0
+    same_dpp(res.dpp, direct)
