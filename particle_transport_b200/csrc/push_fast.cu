@@ -657,7 +657,9 @@ int fast_sort(pt_ctx* ctx, pt_fast_state* st, const pt_field* f, cudaStream_t s)
     uint32_t* cur = (uint32_t*)(base + o_cur);
     uint32_t* tile_off = (uint32_t*)(base + o_tiles);
     PT_CUDA(cudaMemsetAsync(hist, 0, sizeof(uint32_t) * m, s));
-    const int gb = grid_for(n, 256, ctx->num_sms);
+    // one particle per thread: the key and scatter loops are chains of
+    // dependent memory operations, so more of them in flight is what counts
+    const int gb = (int)std::min<int64_t>((n + 255) / 256, INT32_MAX);
     const int nx = (int)f->grid.nx, ny = (int)f->grid.ny, nz = (int)f->grid.nz;
     sort_key_kernel<<<gb, 256, 0, s>>>(st->x, st->alive, n, f->offs, nx, ny, nz, nb, hist);
     PT_CHECK_LAUNCH("sort_key_kernel");
@@ -894,7 +896,7 @@ int launch_batch_sort(const BatchCampaignDev* camps, const int32_t* camp_of, Bat
     const int zb = (int)std::min<int64_t>((max_buckets + 255) / 256, (int64_t)num_sms * 8);
     zero_counted_kernel<<<std::max(zb, 1), 256, 0, s>>>(hist, d_m);
     PT_CHECK_LAUNCH("zero_counted_kernel");
-    const int gb = grid_for(from.cap, 256, num_sms);
+    const int gb = (int)std::min<int64_t>((from.cap + 255) / 256, INT32_MAX);  // one slot per thread
     batch_key_kernel<<<gb, 256, 0, s>>>(camps, camp_of, from, keys, hist);
     PT_CHECK_LAUNCH("batch_key_kernel");
     uint32_t* tile_off = cursor + max_buckets;
