@@ -284,19 +284,21 @@ __global__ void __launch_bounds__(1024) dmumu_kernel(DmumuLaunch a, Src source)
         if (have) {
             long long my_c = 0;
             double my_sd2 = 0.0;
+            // starts and limits fit 32 bits (nsave < 2^31); so does a bin's count
+            const int lim32 = (int)lim;
             for (int b = part; b <= nb; b += a.parts) {
                 const int e0 = cur[b], e1 = cur[b + 1];
-                long long c = 0;
+                int c = 0;
                 double sd0 = 0.0, sd1 = 0.0, sq0 = 0.0, sq1 = 0.0;
                 int e = e0;
                 for (; e + 4 <= e1; e += 4) {
-                    int64_t s_[4];
+                    int s_[4];
                     MuT a_[4], v_[4];
 #pragma unroll
                     for (int k = 0; k < 4; ++k) {
-                        s_[k] = (int64_t)list[e + k];
+                        s_[k] = (int)list[e + k];
                         a_[k] = series[s_[k]];
-                        v_[k] = s_[k] < lim ? series[s_[k] + L] : MuT(NAN);
+                        v_[k] = s_[k] < lim32 ? series[s_[k] + (int)L] : MuT(NAN);
                     }
 #pragma unroll
                     for (int k = 0; k < 4; k += 2) {
@@ -315,9 +317,9 @@ __global__ void __launch_bounds__(1024) dmumu_kernel(DmumuLaunch a, Src source)
                     }
                 }
                 for (; e < e1; ++e) {
-                    const int64_t s = (int64_t)list[e];
+                    const int s = (int)list[e];
                     const MuT av = series[s];
-                    const MuT vv = s < lim ? series[s + L] : MuT(NAN);
+                    const MuT vv = s < lim32 ? series[s + (int)L] : MuT(NAN);
                     const double d = (double)vv - (double)av;
                     if (isfinite(d)) {
                         c += 1;
