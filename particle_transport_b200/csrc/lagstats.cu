@@ -535,15 +535,19 @@ __global__ void __launch_bounds__(1024) dpp_kernel(DppLaunch a)
             // |p| >= 0 or NaN or +inf, so pe - ps is finite exactly when both
             // ends are finite; the normalised sums are sum(d)/p0 and
             // sum(d^2)/p0^2, formed once per lag in dpp_finalize_kernel.
-            for (int64_t s = s_begin; s < s_end; ++s) {
+            // 32-bit indices and a per-tile 32-bit count (nsave < 2^31)
+            const int sb = (int)s_begin, se = (int)s_end, lim32 = (int)lim, L32 = (int)L;
+            int ct = 0;
+            for (int s = sb; s < se; ++s) {
                 const double ps = series[s];
-                if (s >= lim) continue;  // past this lane's last start
-                const double d = series[s + L] - ps;
+                if (s >= lim32) continue;  // past this lane's last start
+                const double d = series[s + L32] - ps;
                 if (!isfinite(d)) continue;
-                c += 1;
+                ct += 1;
                 sdp += d;
                 sdp2 = fma(d, d, sdp2);
             }
+            c += ct;
         }
         __syncthreads();
     }
