@@ -192,6 +192,15 @@ def timed(fn, K, W, torch, per_step=True):
     return evs[0].elapsed_time(evs[K]), steps
 
 
+def host_threads() -> int:
+    """Host threads this process may run on (torchrun sets OMP_NUM_THREADS=1
+    per rank; the CPU baselines pass this count to the oracle explicitly)."""
+    try:
+        return len(os.sched_getaffinity(0))
+    except AttributeError:
+        return os.cpu_count() or 1
+
+
 def cpu_push_rate(fields_host, grid, state, dt, seconds):
     """Oracle FP64 push (restatement of the reference's push) on all host cores."""
     from oracle import build as ob
@@ -199,13 +208,14 @@ def cpu_push_rate(fields_host, grid, state, dt, seconds):
 
     ob.build()
     ff = [np.asfortranarray(f.T) for f in fields_host]
-    nthreads = o.num_threads()
+    nthreads = host_threads()
     n = 4096
     sample = None
     while True:
         st = {k: np.ascontiguousarray(v[:n]).copy() for k, v in state.items()}
         t0 = time.perf_counter()
-        o.push_run(ff, grid, st, np.ones(n, np.uint8), dt, 32001, 8, cache_mode=1, step_begin=0, step_count=64)
+        o.push_run(ff, grid, st, np.ones(n, np.uint8), dt, 32001, 8, cache_mode=1, step_begin=0, step_count=64,
+                   nthreads=nthreads)
         el = time.perf_counter() - t0
         if el * 4 >= seconds or n >= len(state["x1"]):
             sample = (n, 64, el)
@@ -216,7 +226,8 @@ def cpu_push_rate(fields_host, grid, state, dt, seconds):
     st = {k: np.ascontiguousarray(v[:n]).copy() for k, v in state.items()}
     t0 = time.perf_counter()
     for r in range(reps):
-        o.push_run(ff, grid, st, np.ones(n, np.uint8), dt, 32001, 8, cache_mode=1, step_begin=64 * r, step_count=64)
+        o.push_run(ff, grid, st, np.ones(n, np.uint8), dt, 32001, 8, cache_mode=1, step_begin=64 * r, step_count=64,
+                   nthreads=nthreads)
     el = time.perf_counter() - t0
     return {"value": n * 64 * reps / el, "unit": UNIT, "cores": nthreads, "kind": "port",
             "sample": f"{n} particles x {64 * reps} FP64 steps (mu cache every 8) of the same workload, "
@@ -233,13 +244,13 @@ def cpu_lag_rate(mu_chunk, lags, edges, seconds):
                "w_count": np.zeros(nl, np.int64), "w_mean": np.zeros(nl), "w_m2": np.zeros(nl),
                "pair_ss": np.zeros(nl), "pair_n": np.zeros(nl, np.int64)}
         t0 = time.perf_counter()
-        o.dmumu_accumulate(mu_chunk[:n], lags, edges, acc)
+        o.dmumu_accumulate(mu_chunk[:n], lags, edges, acc, nthreads=host_threads())
         el = time.perf_counter() - t0
         if el * 2 >= seconds or n >= mu_chunk.shape[0]:
             break
         n = min(mu_chunk.shape[0], int(n * max(2.0, min(16.0, seconds / 2 / max(el, 1e-3)))))
     pairs = int(acc["pair_n"].sum())
-    return {"value": pairs / el, "unit": "lag-pairs/s", "cores": o.num_threads(), "kind": "port",
+    return {"value": pairs / el, "unit": "lag-pairs/s", "cores": host_threads(), "kind": "port",
             "sample": f"{n} particles x {mu_chunk.shape[1]} saves x {len(lags)} lags ({pairs} pairs), {el:.1f} s"}
 
 
@@ -254,13 +265,13 @@ def cpu_dpp_rate(mom, lags, p0, seconds):
                                                                                "sum_dpn2")}}
         sub = np.ascontiguousarray(mom[:, :, :n])
         t0 = time.perf_counter()
-        o.dpp_accumulate(sub, lags, p0, acc)
+        o.dpp_accumulate(sub, lags, p0, acc, nthreads=host_threads())
         el = time.perf_counter() - t0
         if el * 2 >= seconds or n >= mom.shape[2]:
             break
         n = min(mom.shape[2], int(n * max(2.0, min(16.0, seconds / 2 / max(el, 1e-3)))))
     pairs = int(acc["counts"].sum())
-    return {"value": pairs / el, "unit": "lag-pairs/s", "cores": o.num_threads(), "kind": "port",
+    return {"value": pairs / el, "unit": "lag-pairs/s", "cores": host_threads(), "kind": "port",
             "sample": f"{n} particles x {mom.shape[0]} saves x {nl} lags ({pairs} pairs), {el:.1f} s"}
 
 
@@ -282,13 +293,14 @@ def run_reference(args, ws, rank):
     fields_host = [f.cpu().numpy() for f in fields]
     del fields
     ff = [np.asfortranarray(f.T) for f in fields_host]
-    nthreads = o.num_threads()
+    nthreads = host_threads()
     # size one step (a sample of the particles over 64 pushes) at ~3 s
     n = 4096
     while True:
         st = {k: np.ascontiguousarray(v[:n]).copy() for k, v in state.items()}
         t0 = time.perf_counter()
-        o.push_run(ff, grid, st, np.ones(n, np.uint8), dt, 32001, 8, cache_mode=1, step_begin=0, step_count=64)
+        o.push_run(ff, grid, st, np.ones(n, np.uint8), dt, 32001, 8, cache_mode=1, step_begin=0, step_count=64,
+                   nthreads=nthreads)
         el = time.perf_counter() - t0
         if el >= 1.5 or n >= args.particles:
             break
@@ -296,10 +308,12 @@ def run_reference(args, ws, rank):
     st = {k: np.ascontiguousarray(v[:n]).copy() for k, v in state.items()}
     al = np.ones(n, np.uint8)
     for w in range(args.warmup):
-        o.push_run(ff, grid, st, al, dt, 32001, 8, cache_mode=1, step_begin=64 * w, step_count=64)
+        o.push_run(ff, grid, st, al, dt, 32001, 8, cache_mode=1, step_begin=64 * w, step_count=64,
+                   nthreads=nthreads)
     t0 = time.perf_counter()
     for k in range(args.steps):
-        o.push_run(ff, grid, st, al, dt, 32001, 8, cache_mode=1, step_begin=64 * (args.warmup + k), step_count=64)
+        o.push_run(ff, grid, st, al, dt, 32001, 8, cache_mode=1, step_begin=64 * (args.warmup + k), step_count=64,
+                   nthreads=nthreads)
     el = time.perf_counter() - t0
     value = n * 64 * args.steps / el
     sample = f"{n} of {args.particles} particles per step x 64 FP64 pushes (mu cache every 8)"
