@@ -65,7 +65,7 @@ def parse():
     ap.add_argument("--lag-particles", type=int, default=1_048_576)
     ap.add_argument("--dpp-particles", type=int, default=262_144)
     ap.add_argument("--e2e-gyroperiods", type=int, default=8)
-    ap.add_argument("--skip", default="", help="comma list of legs to skip: fp64,lag,dpp,e2e,cpu,batch,serve")
+    ap.add_argument("--skip", default="", help="comma list of legs to skip: fp32b,fp64,lag,dpp,e2e,cpu,batch,serve")
     ap.add_argument("--cpu-seconds", type=float, default=10.0)
     ap.add_argument("--precision", action="store_true",
                     help="run only the plain-vs-precision study (256^3, 3 energies) and print its JSON line")
@@ -395,6 +395,29 @@ def run_ours(args, ws, rank, local):
                 "algorithmic_bytes_per_launch": bpl, "launch_ms": launch_ms,
                 "sort_ms_per_step": float(np.mean(steps_ms)) - launch_ms}
 
+    # ---------------- the same push over FP32 bricks (the field's second storage)
+    fp32b = None
+    if "fp32b" not in skip and args.storage != "brick_f32":
+        f32 = FieldLibrary(fields, grid, "brick_f32", B_ref_T=B0)
+        ens32 = R.FastEnsemble(f32, state, alive)
+        p32 = R.push_params(dt, NSTEPS, STRIDE, cache="mu", precision="f32", sort_every=args.sort_every,
+                            kernel_variant=args.variant)
+        at32 = [0]
+
+        def f32_step(k):
+            ens32.advance(p32, at32[0], 64, ring, at32[0] // STRIDE, 8)
+            at32[0] += 64
+
+        K32 = max(2, K // 2)
+        ms32, _ = timed(f32_step, K32, max(3, min(W, 3)), torch)
+        ms32 = max_over_ranks(ms32, ws, dev)
+        fp32b = {"value": ws * n * 64 * K32 / (ms32 / 1e3), "unit": UNIT, "ms_per_step": ms32 / K32, "steps": K32,
+                 "field": "brick_f32", "field_bytes": f32.device_bytes,
+                 "gather_bytes_per_particle_step": GATHER_BYTES["brick_f32"]}
+        ens32.close()
+        del ens32, f32
+        torch.cuda.empty_cache()
+
     # ---------------- FP64 plain push on the same particles
     fp64 = None
     if "fp64" not in skip:
@@ -599,7 +622,8 @@ def run_ours(args, ws, rank, local):
                            "kernel_variant": args.variant,
                            "l2": "inputs larger than L2 (field and state exceed 126 MB); no flush",
                            "parallelism": f"particle-sharded replicas x{ws}"},
-                "roofline": roofline, "fp64_push": fp64, "lag_pairs": lag, "dpp": dpp, "e2e": e2e,
+                "roofline": roofline, "fp32_bricks": fp32b, "fp64_push": fp64, "lag_pairs": lag, "dpp": dpp,
+                "e2e": e2e,
                 "cpu_baseline": cpu,
                 "clocks": clocks, "gpu_launches": launches["push"] + launches["sort"], "batched": batched,
                 "job_latency": ({"p50_s": serving["p50_s"], "p99_s": serving["p99_s"]} if serving else None),
