@@ -336,9 +336,15 @@ int pt_dpp_accumulate_device(pt_ctx* ctx, const float* d_mom, int64_t chunk, int
  */
 int pt_energy_snapshots(pt_ctx* ctx, const float* mom, int64_t chunk, int64_t nsave, const int64_t* snap_steps,
                         int n_snap, int64_t particle_offset, double* out);
+/* Same on the device: d_mom and d_snap_steps are device arrays, d_out the
+ * device (n_snap, n_total) array; enqueued on the context stream.  A snapshot
+ * index outside [0, nsave) gives NaN (the device indices are not checked on
+ * the host). */
+int pt_energy_snapshots_device(pt_ctx* ctx, const float* d_mom, int64_t chunk, int64_t nsave,
+                               const int64_t* d_snap_steps, int n_snap, int64_t particle_offset, double* d_out);
 /* On-device histogram of the snapshot energies into n_hist log-spaced bins on
  * [e_min, e_max] GeV (counts[n_snap][n_hist], add-into; out-of-range and NaN
- * energies are not counted).  No reference counterpart: the reference stores
+ * energies, and snapshot indices outside [0, nsave), are not counted).  No reference counterpart: the reference stores
  * the raw energies and bins them in Python (scripts/plot_energy_distribution.py:167-174). */
 int pt_energy_histogram_device(pt_ctx* ctx, const float* d_mom, int64_t chunk, int64_t nsave,
                                const int64_t* d_snap_steps, int n_snap, double e_min, double e_max, int n_hist,

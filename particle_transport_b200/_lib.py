@@ -35,7 +35,8 @@ EXPORTS = (
     "pt_batch_run", "pt_batch_step", "pt_batch_export", "pt_batch_destroy", "pt_dmumu_accumulate",
     "pt_dmumu_accumulate_device",
     "pt_dmumu_accumulate_device_noalloc", "pt_dmumu_accumulate_phase_space_device", "pt_dpp_accumulate",
-    "pt_dpp_accumulate_device", "pt_energy_snapshots", "pt_energy_histogram_device", "pt_reconstruct_mu",
+    "pt_dpp_accumulate_device", "pt_energy_snapshots", "pt_energy_snapshots_device",
+    "pt_energy_histogram_device", "pt_reconstruct_mu",
     "pt_particles_init_device",
 )
 
@@ -141,6 +142,7 @@ def load():
             "pt_dpp_accumulate": (i32, [P, P, i64, i64, P, i32, d, P, P, P, P, P]),
             "pt_dpp_accumulate_device": (i32, [P, P, i64, i64, P, i32, d, P, P, P, P, P]),
             "pt_energy_snapshots": (i32, [P, P, i64, i64, P, i32, i64, P]),
+            "pt_energy_snapshots_device": (i32, [P, P, i64, i64, P, i32, i64, P]),
             "pt_energy_histogram_device": (i32, [P, P, i64, i64, P, i32, d, d, i32, P]),
             "pt_reconstruct_mu": (i32, [P, P, P, i64, i64, P, C.POINTER(Grid), i32, P]),
             "pt_particles_init_device": (i32, [P, P, C.POINTER(InitParams), P, P, P, P, P, P]),

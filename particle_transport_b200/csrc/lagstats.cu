@@ -601,20 +601,28 @@ __device__ __forceinline__ double kinetic_gev(double pmag)
     return __ddiv_rn(__dmul_rn(__dmul_rn(__dadd_rn(gamma, -1.0), M_P), C_LIGHT * C_LIGHT), gev_to_j);
 }
 
-__global__ void energy_snap_kernel(const float* __restrict__ mom, int64_t chunk, const int64_t* __restrict__ snaps,
-                                   int n_snap, int64_t offset, double* __restrict__ out)
+// snapshot indices outside [0, nsave) (possible for the device entry point,
+// whose indices the host cannot see) give NaN instead of a stray read
+__global__ void energy_snap_kernel(const float* __restrict__ mom, int64_t chunk, int64_t nsave,
+                                   const int64_t* __restrict__ snaps, int n_snap, int64_t offset,
+                                   double* __restrict__ out)
 {
     const int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (t >= chunk * n_snap) return;
     const int64_t p = t % chunk;
     const int j = (int)(t / chunk);
-    const float* m = mom + snaps[j] * 3 * chunk + p;
+    const int64_t sj = snaps[j];
+    if (sj < 0 || sj >= nsave) {
+        out[(offset + p) * n_snap + j] = NAN;
+        return;
+    }
+    const float* m = mom + sj * 3 * chunk + p;
     out[(offset + p) * n_snap + j] = kinetic_gev(pmag_exact(m[0], m[chunk], m[2 * chunk]));
 }
 
-__global__ void energy_hist_kernel(const float* __restrict__ mom, int64_t chunk, const int64_t* __restrict__ snaps,
-                                   int n_snap, double log_emin, double inv_dlog, int n_hist,
-                                   unsigned long long* __restrict__ counts)
+__global__ void energy_hist_kernel(const float* __restrict__ mom, int64_t chunk, int64_t nsave,
+                                   const int64_t* __restrict__ snaps, int n_snap, double log_emin, double inv_dlog,
+                                   int n_hist, unsigned long long* __restrict__ counts)
 {
     extern __shared__ unsigned long long h[];
     for (int i = threadIdx.x; i < n_snap * n_hist; i += blockDim.x) h[i] = 0ull;
@@ -623,7 +631,9 @@ __global__ void energy_hist_kernel(const float* __restrict__ mom, int64_t chunk,
          t += (int64_t)gridDim.x * blockDim.x) {
         const int64_t p = t % chunk;
         const int j = (int)(t / chunk);
-        const float* m = mom + snaps[j] * 3 * chunk + p;
+        const int64_t sj = snaps[j];
+        if (sj < 0 || sj >= nsave) continue;  // not a save of this chunk: counted nowhere
+        const float* m = mom + sj * 3 * chunk + p;
         const double e = kinetic_gev(pmag_exact(m[0], m[chunk], m[2 * chunk]));
         if (!(e > 0.0) || !isfinite(e)) continue;
         const double f = (log(e) - log_emin) * inv_dlog;
@@ -853,10 +863,9 @@ int run_dpp(pt_ctx* ctx, const DppArgs& a, cudaStream_t s)
 int launch_energy_snapshots(const float* mom, int64_t chunk, int64_t nsave, const int64_t* snaps, int n_snap,
                             int64_t offset, double* out, cudaStream_t s)
 {
-    (void)nsave;
     const int64_t total = chunk * n_snap;
     if (total <= 0) return PT_OK;
-    energy_snap_kernel<<<(unsigned)((total + 255) / 256), 256, 0, s>>>(mom, chunk, snaps, n_snap, offset, out);
+    energy_snap_kernel<<<(unsigned)((total + 255) / 256), 256, 0, s>>>(mom, chunk, nsave, snaps, n_snap, offset, out);
     PT_CHECK_LAUNCH("energy_snap_kernel");
     return PT_OK;
 }
@@ -864,7 +873,6 @@ int launch_energy_snapshots(const float* mom, int64_t chunk, int64_t nsave, cons
 int launch_energy_histogram(const float* mom, int64_t chunk, int64_t nsave, const int64_t* snaps, int n_snap,
                             double e_min, double e_max, int n_hist, int64_t* counts, cudaStream_t s)
 {
-    (void)nsave;
     const int64_t total = chunk * n_snap;
     if (total <= 0) return PT_OK;
     const size_t smem = sizeof(unsigned long long) * (size_t)n_snap * n_hist;
@@ -874,7 +882,7 @@ int launch_energy_histogram(const float* mom, int64_t chunk, int64_t nsave, cons
     const double log_emin = log(e_min);
     const double inv_dlog = (double)n_hist / (log(e_max) - log_emin);
     const int blocks = (int)std::min<int64_t>((total + 255) / 256, 148 * 4);
-    energy_hist_kernel<<<blocks, 256, smem, s>>>(mom, chunk, snaps, n_snap, log_emin, inv_dlog, n_hist,
+    energy_hist_kernel<<<blocks, 256, smem, s>>>(mom, chunk, nsave, snaps, n_snap, log_emin, inv_dlog, n_hist,
                                                  (unsigned long long*)counts);
     PT_CHECK_LAUNCH("energy_hist_kernel");
     return PT_OK;

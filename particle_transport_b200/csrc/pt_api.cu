@@ -823,6 +823,17 @@ int pt_energy_snapshots(pt_ctx* ctx, const float* mom, int64_t chunk, int64_t ns
     return PT_OK;
 }
 
+int pt_energy_snapshots_device(pt_ctx* ctx, const float* d_mom, int64_t chunk, int64_t nsave,
+                               const int64_t* d_snap_steps, int n_snap, int64_t particle_offset, double* d_out)
+{
+    if (!ctx) return fail(PT_ERR_ARG, "ctx is null");
+    if (chunk < 0 || nsave < 1 || n_snap < 0 || particle_offset < 0) return fail(PT_ERR_ARG, "bad sizes");
+    if (chunk == 0 || n_snap == 0) return PT_OK;
+    if (!(d_mom && d_snap_steps && d_out)) return fail(PT_ERR_ARG, "null pointer");
+    PT_CUDA(cudaSetDevice(ctx->device));
+    return launch_energy_snapshots(d_mom, chunk, nsave, d_snap_steps, n_snap, particle_offset, d_out, ctx->stream);
+}
+
 int pt_energy_histogram_device(pt_ctx* ctx, const float* d_mom, int64_t chunk, int64_t nsave,
                                const int64_t* d_snaps, int n_snap, double e_min, double e_max, int n_hist,
                                int64_t* d_counts)

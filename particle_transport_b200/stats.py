@@ -199,8 +199,23 @@ def process_momenta_chunk_dpp(momenta, lag_steps, p0, counts, sum_delta_p, sum_d
 
 def fill_energy_snapshots(energy_snapshots, momenta, snapshot_indices, particle_offset: int = 0):
     """energy_snapshots: float64 (n_particles, n_snap); snapshot_indices are
-    0-based save indices; writes rows particle_offset .. + chunk."""
+    0-based save indices; writes rows particle_offset .. + chunk.  With CUDA
+    tensors (momenta and energy_snapshots) it runs on the device without a
+    host round trip (pt_energy_snapshots_device)."""
     nsave, _, chunk = momenta.shape
+    if _is_cuda(momenta):
+        import torch
+
+        snaps = torch.as_tensor(np.asarray(snapshot_indices, dtype=np.int64), device=momenta.device)
+        if not (_is_cuda(energy_snapshots) and energy_snapshots.dtype == torch.float64
+                and energy_snapshots.is_contiguous() and energy_snapshots.shape[1] == len(snaps)
+                and energy_snapshots.shape[0] >= particle_offset + chunk):
+            raise ValueError("energy_snapshots must be a contiguous CUDA float64 tensor (n_particles, n_snap)")
+        _check(momenta, momenta.shape, np.float32, "momenta")
+        ctx = _lib.torch_context(momenta)
+        _lib.call("pt_energy_snapshots_device", ctx.handle, _lib.ptr(momenta), chunk, nsave, _lib.ptr(snaps),
+                  len(snaps), int(particle_offset), _lib.ptr(energy_snapshots))
+        return
     snaps = np.ascontiguousarray(snapshot_indices, dtype=np.int64)
     if energy_snapshots.shape[1] != len(snaps) or energy_snapshots.shape[0] < particle_offset + chunk:
         raise ValueError("energy_snapshots has the wrong shape")

@@ -150,6 +150,26 @@ def test_energy_snapshots_bit_exact(cuda, oracle):
     assert np.array_equal(g, o, equal_nan=True)
 
 
+def test_energy_snapshots_device_bit_exact(cuda, oracle):
+    torch = cuda
+    rng = np.random.default_rng(0)
+    mom = np.ascontiguousarray(rng.normal(scale=5e-19, size=(50, 3, 300)).astype(np.float32))
+    mom[3, :, 7] = np.nan
+    snaps = np.array([0, 3, 25, 49])
+    o = np.full((600, 4), np.nan)
+    oracle.energy_snapshots(mom, snaps, o, particle_offset=300)
+    g = torch.full((600, 4), float("nan"), dtype=torch.float64, device="cuda")
+    S.fill_energy_snapshots(g, torch.as_tensor(mom, device="cuda"), snaps, particle_offset=300)
+    assert np.array_equal(g.cpu().numpy(), o, equal_nan=True)
+    # an index outside the chunk's saves yields NaN, not a stray read
+    g2 = torch.zeros((300, 2), dtype=torch.float64, device="cuda")
+    S.fill_energy_snapshots(g2, torch.as_tensor(mom, device="cuda"), [1, 50])
+    h = g2.cpu().numpy()
+    o1 = np.full((300, 1), np.nan)
+    oracle.energy_snapshots(mom, np.array([1]), o1)
+    assert np.all(np.isnan(h[:, 1])) and np.array_equal(h[:, 0], o1[:, 0], equal_nan=True)
+
+
 def test_energy_histogram(cuda, oracle):
     torch = cuda
     rng = np.random.default_rng(1)
