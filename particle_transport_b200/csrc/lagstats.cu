@@ -115,7 +115,7 @@ __global__ void __launch_bounds__(1024) dmumu_kernel(DmumuLaunch a, Src source)
     using MuT = typename Src::T;
     extern __shared__ __align__(16) unsigned char smem[];
     const int nb = a.n_bins, nl = a.nl;
-    // shared layout: edges | acc_cnt | acc_sd | acc_sd2 | slots
+    // shared layout: edges | acc_cnt | acc_sd | acc_sd2 ([bin][lag] each) | slots
     double* s_edges = (double*)smem;
     size_t off = ((size_t)(nb + 1) * sizeof(double) + 15) & ~(size_t)15;
     unsigned long long* acc_cnt = (unsigned long long*)(smem + off);
@@ -329,7 +329,7 @@ __global__ void __launch_bounds__(1024) dmumu_kernel(DmumuLaunch a, Src source)
                 }
                 const double sd = sd0 + sd1, sd2 = sq0 + sq1;
                 if (b < nb && c > 0 && lane_on) {
-                    const int ai = li * nb + b;
+                    const int ai = b * nl + li;  // [bin][lag]: the lanes of a flush hit consecutive words
                     atomicAdd(&acc_cnt[ai], (unsigned long long)c);
                     atomicAdd(&acc_sd[ai], sd);
                     atomicAdd(&acc_sd2[ai], sd2);
@@ -364,9 +364,10 @@ __global__ void __launch_bounds__(1024) dmumu_kernel(DmumuLaunch a, Src source)
     // ---- CTA epilogue: (bin, lag) accumulators and Welford triples
     const int64_t cta = blockIdx.x;
     for (int i = threadIdx.x; i < nl * nb; i += blockDim.x) {
-        a.part_cnt[cta * nl * nb + i] = acc_cnt[i];
-        a.part_sd[cta * nl * nb + i] = acc_sd[i];
-        a.part_sd2[cta * nl * nb + i] = acc_sd2[i];
+        const int j = (i % nb) * nl + i / nb;  // partials are [lag][bin], the shared sums [bin][lag]
+        a.part_cnt[cta * nl * nb + i] = acc_cnt[j];
+        a.part_sd[cta * nl * nb + i] = acc_sd[j];
+        a.part_sd2[cta * nl * nb + i] = acc_sd2[j];
     }
     __syncthreads();
     // reuse the accumulator region to gather per-warp Welford triples
