@@ -65,7 +65,7 @@ def parse():
     ap.add_argument("--lag-particles", type=int, default=1_048_576)
     ap.add_argument("--dpp-particles", type=int, default=262_144)
     ap.add_argument("--e2e-gyroperiods", type=int, default=8)
-    ap.add_argument("--skip", default="", help="comma list of legs to skip: fp32b,fp64,lag,dpp,e2e,cpu,batch,serve")
+    ap.add_argument("--skip", default="", help="comma list of legs to skip: fp32b,fp64,lag,dpp,e2e,cpu,batch,serve,config1")
     ap.add_argument("--cpu-seconds", type=float, default=10.0)
     ap.add_argument("--precision", action="store_true",
                     help="run only the plain-vs-precision study (256^3, 3 energies) and print its JSON line")
@@ -603,6 +603,8 @@ def run_ours(args, ws, rank, local):
     torch.cuda.empty_cache()
     serving = run_serving(args, dev) if ("serve" not in skip and ws == 1) else None
     torch.cuda.empty_cache()
+    config1 = run_config1(args, rank) if ("config1" not in skip and rank == 0) else None
+    torch.cuda.empty_cache()
 
     # ---------------- CPU baseline (oracle, host cores)
     cpu = None
@@ -627,7 +629,7 @@ def run_ours(args, ws, rank, local):
                 "cpu_baseline": cpu,
                 "clocks": clocks, "gpu_launches": launches["push"] + launches["sort"], "batched": batched,
                 "job_latency": ({"p50_s": serving["p50_s"], "p99_s": serving["p99_s"]} if serving else None),
-                "serving": serving}
+                "serving": serving, "config1_end_to_end": config1}
         print(json.dumps(line), flush=True)
 
 
@@ -635,6 +637,76 @@ def run_ours(args, ws, rank, local):
 # push_fast_kernel launch of this workload, from a 1-pass ncu capture of the
 # same command; keyed by (storage, grid, particles)
 TRAFFIC = {("brick_bf16", 512, 16_777_216): 12.57e9 + 5.02e9}
+
+
+def run_config1(args, rank):
+    """The reference's CPU-runnable configuration end to end, through the host
+    API the Julia seams call: 64^3 (dB/B0 = 0.5, |k| = 2..32, E = 0), 4096
+    protons at 1 GeV, 64 steps/T_g0 for 50 T_g0 (3200 pushes), mu cache every
+    4 steps (801 saves) handed to the host row by row, then D_mumu on 20 log
+    lags x 20 |mu| bins of the host mu cache.  The GPU path (pt_push_run FP64
+    and FP32/BF16, pt_dmumu_accumulate) against the oracle on all host cores
+    (the same FP64 push and binning, the reference's arithmetic)."""
+    from oracle import build as ob
+    from oracle import oracle as o
+    from particle_transport_b200 import fields as F
+    from particle_transport_b200 import runner as R
+    from particle_transport_b200 import stats as S
+    from particle_transport_b200.fields import FieldLibrary
+    from particle_transport_b200.particles import energy_to_gamma, init_particles
+    from particle_transport_b200.time_units import build_mu_edges_full, log_spaced_lag_steps, reference_Omega0
+
+    ob.build()
+    n, np_, spg, dur, stride = 64, 4096, 64, 50, 4
+    fields = [np.ascontiguousarray(f.numpy()) for f in F.to_si(F.synthetic_mhd_fields(n, 2, 32, 0.5, 1.0, 0.0, seed=1))]
+    rg = F.gyroradius_m(1.0, 1e-10)
+    grid = F.build_uniform_grid((n - 1) * rg, n, n, n)
+    B0 = F.reference_B0_T(*fields[:3])
+    dt = (2 * math.pi / spg) / reference_Omega0(B0, energy_to_gamma(1.0), F.Q_E, F.M_P)
+    state = init_particles(np_, grid, 1.0, seed=1)
+    nsteps = spg * dur + 1
+    nsave = R.n_saves(nsteps, stride)
+    lags = log_spaced_lag_steps(nsave - 1, 20)
+    edges, _ = build_mu_edges_full(0.0, 1.0, 20)
+
+    def gpu(storage, precision):
+        fl = FieldLibrary(fields, grid, storage, B_ref_T=B0)
+        best = None
+        for _ in range(3):  # the first call also sets up the context buffers
+            st = {k: v.copy() for k, v in state.items()}
+            t0 = time.perf_counter()
+            col = R.CacheCollector(np_, nsave, "mu")
+            R.run_push_host(fl, st, np.ones(np_, np.uint8),
+                            R.push_params(dt, nsteps, stride, cache="mu", precision=precision,
+                                          sort_every=64 if precision == "f32" else 0), col)
+            acc = S.new_dmumu_accumulators(len(lags), 20)
+            S.process_mu_chunk_dmumu(col.mu, lags, edges, acc["particle_counts"], acc["particle_means"],
+                                     acc["particle_m2s"], acc["pair_sum_squares"], acc["pair_counts"],
+                                     acc["dmumu_counts"], acc["dmumu_sum_delta"], acc["dmumu_sum_delta2"],
+                                     layout="particle_fastest")
+            el = time.perf_counter() - t0
+            best = el if best is None else min(best, el)
+        fl.close()
+        return best
+
+    out = {"workload": "64^3, 4096 protons at 1 GeV, 3200 pushes, 801 mu saves, D_mumu 20 lags x 20 bins; "
+                       "host state and host mu cache (pt_push_run + pt_dmumu_accumulate)",
+           "gpu_f64_s": gpu("ref_f64", "f64"), "gpu_f32_bf16_s": gpu("brick_bf16", "f32")}
+    nt = host_threads()
+    st = {k: v.copy() for k, v in state.items()}
+    t0 = time.perf_counter()
+    mu, _ = o.push_run([np.asfortranarray(f.T) for f in fields], grid, st, np.ones(np_, np.uint8), dt, nsteps,
+                       stride, cache_mode=1, nthreads=nt)
+    acc = {"counts": np.zeros((len(lags), 20), np.int64), "sum_d": np.zeros((len(lags), 20)),
+           "sum_d2": np.zeros((len(lags), 20)), "w_count": np.zeros(len(lags), np.int64),
+           "w_mean": np.zeros(len(lags)), "w_m2": np.zeros(len(lags)), "pair_ss": np.zeros(len(lags)),
+           "pair_n": np.zeros(len(lags), np.int64)}
+    o.dmumu_accumulate(mu, lags, edges, acc, time_fastest=False, nthreads=nt)
+    out["cpu_oracle_s"] = time.perf_counter() - t0
+    out["cpu_cores"] = nt
+    out["speedup_f64"] = out["cpu_oracle_s"] / out["gpu_f64_s"]
+    out["speedup_f32_bf16"] = out["cpu_oracle_s"] / out["gpu_f32_bf16_s"]
+    return out
 
 
 def run_batched(args, dev, rank):
