@@ -22,6 +22,8 @@
 // the whole launch; the normalised sums sum(dp/p0) = sum(dp)/p0 and
 // sum((dp/p0)^2) = sum(dp^2)/p0^2 are formed once per lag at the end, which
 // equals the reference's per-pair division up to rounding.
+#include <math_constants.h>
+
 #include "exact_mu.cuh"
 #include "pt_internal.cuh"
 
@@ -302,30 +304,30 @@ __global__ void __launch_bounds__(1024) dmumu_kernel(DmumuLaunch a, Src source)
                     }
 #pragma unroll
                     for (int k = 0; k < 4; k += 2) {
-                        const double d0 = (double)v_[k] - (double)a_[k];
-                        const double d1 = (double)v_[k + 1] - (double)a_[k + 1];
-                        if (isfinite(d0)) {
-                            c += 1;
-                            sd0 += d0;
-                            sq0 = fma(d0, d0, sq0);
-                        }
-                        if (isfinite(d1)) {
-                            c += 1;
-                            sd1 += d1;
-                            sq1 = fma(d1, d1, sq1);
-                        }
+                        // branch-free: an invalid pair adds 0 (and 0 * 0), which
+                        // leaves the sums bit-identical to skipping it
+                        double d0 = (double)v_[k] - (double)a_[k];
+                        double d1 = (double)v_[k + 1] - (double)a_[k + 1];
+                        const bool ok0 = isfinite(d0), ok1 = isfinite(d1);
+                        d0 = ok0 ? d0 : 0.0;
+                        d1 = ok1 ? d1 : 0.0;
+                        c += (int)ok0 + (int)ok1;
+                        sd0 += d0;
+                        sq0 = fma(d0, d0, sq0);
+                        sd1 += d1;
+                        sq1 = fma(d1, d1, sq1);
                     }
                 }
                 for (; e < e1; ++e) {
                     const int s = (int)list[e];
                     const MuT av = series[s];
                     const MuT vv = s < lim32 ? series[s + (int)L] : MuT(NAN);
-                    const double d = (double)vv - (double)av;
-                    if (isfinite(d)) {
-                        c += 1;
-                        sd0 += d;
-                        sq0 = fma(d, d, sq0);
-                    }
+                    double d = (double)vv - (double)av;
+                    const bool ok = isfinite(d);
+                    d = ok ? d : 0.0;
+                    c += (int)ok;
+                    sd0 += d;
+                    sq0 = fma(d, d, sq0);
                 }
                 const double sd = sd0 + sd1, sd2 = sq0 + sq1;
                 if (b < nb && c > 0 && lane_on) {
@@ -541,10 +543,13 @@ __global__ void __launch_bounds__(1024) dpp_kernel(DppLaunch a)
             int ct = 0;
             for (int s = sb; s < se; ++s) {
                 const double ps = series[s];
-                if (s >= lim32) continue;  // past this lane's last start
-                const double d = series[s + L32] - ps;
-                if (!isfinite(d)) continue;
-                ct += 1;
+                // past this lane's last start the end is not read; an invalid
+                // pair adds 0 (branch-free), which leaves the sums unchanged
+                const double pe = s < lim32 ? series[s + L32] : CUDART_NAN;
+                double d = pe - ps;
+                const bool ok = isfinite(d);
+                d = ok ? d : 0.0;
+                ct += (int)ok;
                 sdp += d;
                 sdp2 = fma(d, d, sdp2);
             }
