@@ -636,7 +636,7 @@ def run_ours(args, ws, rank, local):
 # DRAM bytes (dram__bytes_read.sum + dram__bytes_write.sum) of one 64-step
 # push_fast_kernel launch of this workload, from a 1-pass ncu capture of the
 # same command; keyed by (storage, grid, particles)
-TRAFFIC = {("brick_bf16", 512, 16_777_216): 12.57e9 + 5.02e9}
+TRAFFIC = {("brick_bf16", 512, 16_777_216): 12.89e9 + 5.02e9}
 
 
 def run_config1(args, rank):
