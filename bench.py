@@ -366,7 +366,7 @@ def run_ours(args, ws, rank, local):
             ens.sort()
             last_sort[0] = s0
             if k >= 0:
-                launches["sort"] += 3
+                launches["sort"] += 4  # sort_key, sort_scan_tiles, sort_scan_top, sort_scatter
         if k >= 0:
             e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
             e0.record()
