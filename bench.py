@@ -988,8 +988,9 @@ def run_serving(args, dev, n_jobs=16, rate=4.0, n_cmp=8):
 
     libs = make_libs("brick_bf16")
 
-    def serve(libraries, arrivals, specs, push):
-        srv = CampaignServer(libraries, B0, hbm_budget_bytes=150e9, capacity=1 << 27, max_jobs=len(specs), push=push)
+    def serve(libraries, arrivals, specs, push, schedule="srpt"):
+        srv = CampaignServer(libraries, B0, hbm_budget_bytes=150e9, capacity=1 << 27, max_jobs=len(specs), push=push,
+                             schedule=schedule)
         torch.cuda.synchronize()
         t_start = time.perf_counter()
         nxt = 0
@@ -1014,7 +1015,10 @@ def run_serving(args, dev, n_jobs=16, rate=4.0, n_cmp=8):
     arrivals, specs = sample_jobs(n_jobs, rate, ["256", "512"], seed=2026)
     main = serve(libs, arrivals, specs, "f32")
     main.update({"rate_per_s": rate, "unit": UNIT, "push": "FP32 / BF16 bricks",
-                 "init": "on the device (pt_particles_init_device)", "hbm_budget_GB": 150})
+                 "init": "on the device (pt_particles_init_device)", "hbm_budget_GB": 150,
+                 "schedule": "srpt: least work left first, epochs filled to 262144 particles"})
+    every = serve(libs, arrivals, specs, "f32", schedule="all")
+    main["schedule_all"] = {k: every[k] for k in ("p50_s", "p99_s", "mean_s", "wall_s", "busy_rate", "epochs")}
     arr_c, specs_c = sample_jobs(n_cmp, rate, ["256", "512"], seed=7, n_range=(16_384, 1_048_576),
                                  duration_range=(10.0, 60.0))
     cmp32 = serve(libs, arr_c, specs_c, "f32")

@@ -232,6 +232,15 @@ int pt_batch_add(pt_ctx* ctx, pt_batch* batch, const pt_campaign_desc* campaign,
 int pt_batch_remove(pt_ctx* ctx, pt_batch* batch, int id);
 /* Run `epochs` epochs on the context stream (asynchronous). */
 int pt_batch_run(pt_ctx* ctx, pt_batch* batch, int64_t epochs, int use_graph);
+/* Choose which campaigns the following epochs advance: exactly ids[0 .. n_ids)
+ * (n_ids = -1: every campaign).  A paused campaign keeps its slots, step
+ * counter and caches as they are; the sort leaves its slots alone, and it
+ * continues from the same step when it runs again, so its trajectory is the
+ * one it would have had running throughout.  New campaigns (pt_batch_add)
+ * run.  The campaign server uses this to give its epochs to the jobs with
+ * the least work left.  No reference counterpart (the reference has no
+ * serving mode). */
+int pt_batch_set_running(pt_ctx* ctx, pt_batch* batch, const int* ids, int n_ids);
 /* Next step of campaign `id` (synchronises the context stream). */
 int pt_batch_step(pt_ctx* ctx, pt_batch* batch, int id, int64_t* step);
 /* Copy campaign `id`'s state back to SI device arrays (n each). */

@@ -88,6 +88,17 @@ class Batch:
         ctx = _lib.torch_context(self.device.index)
         _lib.call("pt_batch_run", ctx.handle, self.handle, int(epochs), int(bool(use_graph)))
 
+    def set_running(self, ids=None) -> None:
+        """Advance only campaigns `ids` in the following epochs (None: all).
+        Paused campaigns keep their slots and step counters and resume where
+        they stopped, with the same trajectory."""
+        ctx = _lib.torch_context(self.device.index)
+        if ids is None:
+            _lib.call("pt_batch_set_running", ctx.handle, self.handle, None, -1)
+            return
+        arr = (C.c_int * max(len(ids), 1))(*[int(i) for i in ids])
+        _lib.call("pt_batch_set_running", ctx.handle, self.handle, C.cast(arr, C.c_void_p), len(ids))
+
     def step(self, cid: int) -> int:
         v = C.c_int64()
         ctx = _lib.torch_context(self.device.index)
@@ -134,6 +145,7 @@ class ReferenceBatch:
         self.device = torch.device("cuda", device)
         self.campaigns = {}
         self._next = 0
+        self._running = None  # None: all campaigns
 
     def add(self, field: FieldLibrary, state: dict, dt: float, nsteps: int, stride: int, periodic: bool = True,
             cache=None, alive=None, mom_cache=None, **_unused) -> int:
@@ -172,8 +184,8 @@ class ReferenceBatch:
 
     def run(self, epochs: int, use_graph: bool = True) -> None:
         for _ in range(int(epochs)):
-            for c in self.campaigns.values():
-                if c["step"] >= c["nsteps"]:
+            for cid, c in self.campaigns.items():
+                if c["step"] >= c["nsteps"] or (self._running is not None and cid not in self._running):
                     continue
                 count = min(self.K, c["nsteps"] - c["step"])
                 c["ens"].advance(c["params"], c["step"], count, c["cache"], 0, c["rows"])
@@ -183,6 +195,14 @@ class ReferenceBatch:
                 c["step"] += count
                 if sub is not None and c["step"] >= c["nsteps"]:
                     sub["out"].copy_(sub["ps"][:, 3:6, :])
+
+    def set_running(self, ids=None) -> None:
+        """As Batch.set_running: only campaigns `ids` advance (None: all)."""
+        if ids is not None:
+            for i in ids:
+                if i not in self.campaigns:
+                    raise ValueError(f"no such campaign {i}")
+        self._running = None if ids is None else set(int(i) for i in ids)
 
     def step(self, cid: int) -> int:
         return self.campaigns[cid]["step"]

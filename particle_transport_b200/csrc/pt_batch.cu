@@ -20,10 +20,11 @@ struct pt_batch {
     int grid = 148;
     BatchStateDev buf[2]{};   // ping-pong state
     int cur = 0;              // buffer holding the current state
-    int32_t* camp_of = nullptr;
+    int sort_grid = 1;        // blocks of the sort's tile kernels (a power of two >= the tiles, with slack)
     BatchCampaignDev* d_camps = nullptr;
     std::vector<BatchCampaignDev> h_camps;
     std::vector<const pt_field*> fields;
+    std::vector<int> home;    // buffer holding a paused campaign's slots (the sort moves running ones only)
     BatchTile* d_tiles = nullptr;
     int* d_ntiles = nullptr;
     int* d_counter = nullptr;
@@ -94,13 +95,13 @@ int rebuild_tables(pt_batch* b, int fresh)
     std::vector<BatchTile> tiles;
     for (int c = 0; c < b->max_camps; ++c) {
         BatchCampaignDev& C = b->h_camps[c];
-        if (!C.active) continue;
+        if (!C.active || !C.running) continue;
         C.key_base = key;
         key += C.n_bricks + 1;
         C.shift = C.slot0 - dense;
         dense += C.n;
-        for (int64_t s = 0; s < C.n; s += 256)
-            tiles.push_back(BatchTile{c, (int32_t)std::min<int64_t>(256, C.n - s), C.slot0 + s});
+        for (int64_t s = 0; s < C.n; s += kBatchTile)
+            tiles.push_back(BatchTile{c, (int32_t)std::min<int64_t>(kBatchTile, C.n - s), C.slot0 + s});
     }
     if (key > UINT32_MAX) return fail(PT_ERR_ARG, "too many sort buckets in the batch");
     if (key > b->hist_cap) {
@@ -120,8 +121,19 @@ int rebuild_tables(pt_batch* b, int fresh)
         drop_graphs(b);
     }
     const int nt = (int)tiles.size();
-    const int64_t max_tiles = b->cap / 256 + b->max_camps + 1;
+    const int64_t max_tiles = b->cap / kBatchTile + b->max_camps + 1;
     if (nt > max_tiles) return fail(PT_ERR_ARG, "internal: tile table overflow");
+    {
+        // the sort kernels run one block per tile; their grid is part of the
+        // captured graphs, so it changes (and the graphs are captured again)
+        // only when the tiles outgrow it or fall below a quarter of it
+        int want = 1;
+        while (want < nt && want < (1 << 30)) want <<= 1;
+        if (want > b->sort_grid || 4 * want < b->sort_grid) {
+            b->sort_grid = want;
+            drop_graphs(b);
+        }
+    }
     cudaStream_t s = b->ctx->stream;
     PT_CUDA(cudaMemcpyAsync(b->d_camps, b->h_camps.data(), sizeof(BatchCampaignDev) * b->max_camps,
                             cudaMemcpyHostToDevice, s));
@@ -136,8 +148,8 @@ int enqueue_epoch(pt_batch* b, cudaStream_t s)
 {
     int cur = b->cur;
     if (b->sort) {
-        int rc = launch_batch_sort(b->d_camps, b->camp_of, b->buf[cur], b->buf[1 - cur], b->keys, b->hist, b->cursor,
-                                   b->d_m, b->hist_cap, b->ctx->num_sms, s);
+        int rc = launch_batch_sort(b->d_camps, b->d_tiles, b->d_ntiles, b->sort_grid, b->buf[cur], b->buf[1 - cur],
+                                   b->keys, b->hist, b->cursor, b->d_m, b->hist_cap, b->ctx->num_sms, s);
         if (rc) return rc;
         cur = 1 - cur;
     }
@@ -192,14 +204,14 @@ int pt_batch_create(pt_ctx* ctx, int64_t capacity, int max_campaigns, int storag
     b->sort = sort ? 1 : 0;
     b->h_camps.assign(max_campaigns, BatchCampaignDev{});
     b->fields.assign(max_campaigns, nullptr);
+    b->home.assign(max_campaigns, 0);
     b->free_ranges.push_back({0, capacity});
     int rc = alloc_state(b->buf[0], capacity);
     if (!rc && b->sort) rc = alloc_state(b->buf[1], capacity);
-    const int64_t max_tiles = capacity / 256 + max_campaigns + 1;
+    const int64_t max_tiles = capacity / kBatchTile + max_campaigns + 1;
     cudaError_t e = cudaSuccess;
     if (!rc) {
-        e = cudaMalloc((void**)&b->camp_of, sizeof(int32_t) * capacity);
-        if (e == cudaSuccess) e = cudaMalloc((void**)&b->d_camps, sizeof(BatchCampaignDev) * max_campaigns);
+        e = cudaMalloc((void**)&b->d_camps, sizeof(BatchCampaignDev) * max_campaigns);
         if (e == cudaSuccess) e = cudaMalloc((void**)&b->d_tiles, sizeof(BatchTile) * max_tiles);
         if (e == cudaSuccess) e = cudaMalloc((void**)&b->d_ntiles, sizeof(int));
         if (e == cudaSuccess) e = cudaMalloc((void**)&b->d_counter, sizeof(int));
@@ -215,8 +227,7 @@ int pt_batch_create(pt_ctx* ctx, int64_t capacity, int max_campaigns, int storag
         cudaStream_t s = ctx->stream;
         const int zero = 0;
         const int64_t zero64 = 0;
-        e = cudaMemsetAsync(b->camp_of, 0xff, sizeof(int32_t) * capacity, s);  // -1: free slot
-        if (e == cudaSuccess) e = cudaMemsetAsync(b->d_camps, 0, sizeof(BatchCampaignDev) * max_campaigns, s);
+        e = cudaMemsetAsync(b->d_camps, 0, sizeof(BatchCampaignDev) * max_campaigns, s);
         if (e == cudaSuccess) e = cudaMemcpyAsync(b->d_ntiles, &zero, sizeof(int), cudaMemcpyHostToDevice, s);
         if (e == cudaSuccess) e = cudaMemcpyAsync(b->d_counter, &zero, sizeof(int), cudaMemcpyHostToDevice, s);
         if (e == cudaSuccess) e = cudaMemcpyAsync(b->d_m, &zero64, sizeof(int64_t), cudaMemcpyHostToDevice, s);
@@ -272,9 +283,6 @@ int pt_batch_add(pt_ctx* ctx, pt_batch* b, const pt_campaign_desc* d, int* id)
     int rc = launch_batch_import(b->buf[b->cur], slot0, d->n, f, d->d_x1, d->d_x2, d->d_x3, d->d_p1, d->d_p2,
                                  d->d_p3, d->d_alive, ctx->num_sms, s);
     if (rc) return rc;
-    // camp_of[slot0 .. slot0 + n) = c
-    std::vector<int32_t> tag((size_t)d->n, c);
-    PT_CUDA(cudaMemcpyAsync(b->camp_of + slot0, tag.data(), sizeof(int32_t) * d->n, cudaMemcpyHostToDevice, s));
     BatchCampaignDev C{};
     const pt_grid& g = f->grid;
     PushArgsFast& a = C.a;
@@ -313,7 +321,9 @@ int pt_batch_add(pt_ctx* ctx, pt_batch* b, const pt_campaign_desc* d, int* id)
     C.K = b->K;
     C.n_bricks = (f->n_nodes + 511) / 512;
     C.active = 1;
+    C.running = 1;
     b->h_camps[c] = C;
+    b->home[c] = b->cur;
     b->fields[c] = f;
     const int words = (int)(g.nx + g.ny + g.nz);
     if (words > b->smem_words) {
@@ -332,7 +342,6 @@ int pt_batch_remove(pt_ctx* ctx, pt_batch* b, int id)
     if (id < 0 || id >= b->max_camps || !b->h_camps[id].active) return fail(PT_ERR_ARG, "no such campaign");
     BatchCampaignDev& C = b->h_camps[id];
     PT_CUDA(cudaStreamSynchronize(ctx->stream));  // the step counter on the host mirror is stale: keep device's
-    PT_CUDA(cudaMemsetAsync(b->camp_of + C.slot0, 0xff, sizeof(int32_t) * C.n, ctx->stream));
     b->free_ranges.push_back({C.slot0, C.n});
     std::sort(b->free_ranges.begin(), b->free_ranges.end());
     std::vector<std::pair<int64_t, int64_t>> merged;
@@ -373,6 +382,46 @@ int pt_batch_run(pt_ctx* ctx, pt_batch* b, int64_t epochs, int use_graph)
     return PT_OK;
 }
 
+int pt_batch_set_running(pt_ctx* ctx, pt_batch* b, const int* ids, int n_ids)
+{
+    if (!ctx || !b) return fail(PT_ERR_ARG, "null argument");
+    if (n_ids > 0 && !ids) return fail(PT_ERR_ARG, "null ids");
+    std::vector<char> want((size_t)b->max_camps, n_ids < 0 ? 1 : 0);
+    for (int k = 0; k < n_ids; ++k) {
+        const int id = ids[k];
+        if (id < 0 || id >= b->max_camps || !b->h_camps[id].active) return fail(PT_ERR_ARG, "no such campaign");
+        want[id] = 1;
+    }
+    bool changed = false;
+    cudaStream_t s = ctx->stream;
+    for (int c = 0; c < b->max_camps; ++c) {
+        BatchCampaignDev& C = b->h_camps[c];
+        if (!C.active || (int)want[c] == C.running) continue;
+        changed = true;
+        if (!want[c]) {
+            // paused: its slots stay in the buffer of the current parity
+            b->home[c] = b->cur;
+        } else if (b->sort && b->home[c] != b->cur) {
+            // resumed after the epochs flipped the parity: bring its slots over
+            const BatchStateDev& from = b->buf[b->home[c]];
+            const BatchStateDev& to = b->buf[b->cur];
+            const int64_t cap = b->cap, o = C.slot0, n = C.n;
+            for (int k = 0; k < 3; ++k) {
+                PT_CUDA(cudaMemcpyAsync(to.x + k * cap + o, from.x + k * cap + o, sizeof(double) * n,
+                                        cudaMemcpyDeviceToDevice, s));
+                PT_CUDA(cudaMemcpyAsync(to.p + k * cap + o, from.p + k * cap + o, sizeof(float) * n,
+                                        cudaMemcpyDeviceToDevice, s));
+            }
+            PT_CUDA(cudaMemcpyAsync(to.p2 + o, from.p2 + o, sizeof(double) * n, cudaMemcpyDeviceToDevice, s));
+            PT_CUDA(cudaMemcpyAsync(to.pid + o, from.pid + o, sizeof(int32_t) * n, cudaMemcpyDeviceToDevice, s));
+            PT_CUDA(cudaMemcpyAsync(to.alive + o, from.alive + o, n, cudaMemcpyDeviceToDevice, s));
+        }
+        if (want[c]) b->home[c] = b->cur;
+        C.running = want[c];
+    }
+    return changed ? rebuild_tables(b, -1) : PT_OK;
+}
+
 int pt_batch_step(pt_ctx* ctx, pt_batch* b, int id, int64_t* step)
 {
     if (!ctx || !b || !step) return fail(PT_ERR_ARG, "null argument");
@@ -389,7 +438,8 @@ int pt_batch_export(pt_ctx* ctx, pt_batch* b, int id, double* x1, double* x2, do
     if (id < 0 || id >= b->max_camps || !b->h_camps[id].active) return fail(PT_ERR_ARG, "no such campaign");
     if (!(x1 && x2 && x3 && p1 && p2 && p3 && alive)) return fail(PT_ERR_ARG, "null state");
     const BatchCampaignDev& C = b->h_camps[id];
-    return launch_batch_export(b->buf[b->cur], C.slot0, C.n, b->fields[id], x1, x2, x3, p1, p2, p3, alive,
+    const int buf = C.running ? b->cur : b->home[id];
+    return launch_batch_export(b->buf[buf], C.slot0, C.n, b->fields[id], x1, x2, x3, p1, p2, p3, alive,
                                ctx->num_sms, ctx->stream);
 }
 
@@ -400,7 +450,7 @@ int pt_batch_destroy(pt_batch* b)
     drop_graphs(b);
     free_state(b->buf[0]);
     free_state(b->buf[1]);
-    for (void* p : {(void*)b->camp_of, (void*)b->d_camps, (void*)b->d_tiles, (void*)b->d_ntiles, (void*)b->d_counter,
+    for (void* p : {(void*)b->d_camps, (void*)b->d_tiles, (void*)b->d_ntiles, (void*)b->d_counter,
                     (void*)b->keys, (void*)b->hist, (void*)b->cursor, (void*)b->d_m})
         if (p) cudaFree(p);
     if (b->cap_stream) cudaStreamDestroy(b->cap_stream);

@@ -190,9 +190,10 @@ struct BatchCampaignDev {
     int64_t key_base;  // first sort bucket
     int64_t n_bricks;  // bricks of the campaign's field (bucket n_bricks = dead)
     int64_t shift;     // arena slot = dense sort position + shift
-    int32_t active;    // holds particles (keyed by the sort)
-    int32_t pad;
+    int32_t active;    // holds particles
+    int32_t running;   // pushed, sorted and stepped by the epochs (0: paused, slots held as they are)
 };
+constexpr int kBatchTile = 256;  // particles per tile of a batch (= block size of its kernels)
 struct BatchTile {
     int32_t campaign;
     int32_t count;
@@ -223,9 +224,9 @@ int launch_batch_epoch_end(BatchCampaignDev* camps, int n_camps, int* tile_count
 constexpr int64_t kSortScanTile = 2048;
 inline int64_t sort_scan_tiles(int64_t m) { return (m + kSortScanTile - 1) / kSortScanTile; }
 // cursor must hold max_buckets + sort_scan_tiles(max_buckets) entries
-int launch_batch_sort(const BatchCampaignDev* camps, const int32_t* camp_of, BatchStateDev from, BatchStateDev to,
-                      uint32_t* keys, uint32_t* hist, uint32_t* cursor, const int64_t* d_m_buckets,
-                      int64_t max_buckets, int num_sms, cudaStream_t s);
+int launch_batch_sort(const BatchCampaignDev* camps, const BatchTile* tiles, const int* n_tiles, int grid,
+                      BatchStateDev from, BatchStateDev to, uint32_t* keys, uint32_t* hist, uint32_t* cursor,
+                      const int64_t* d_m, int64_t max_buckets, int num_sms, cudaStream_t s);
 int launch_batch_import(BatchStateDev st, int64_t slot0, int64_t n, const pt_field* f, const double* x1,
                         const double* x2, const double* x3, const double* p1, const double* p2, const double* p3,
                         const uint8_t* alive, int num_sms, cudaStream_t s);

@@ -749,7 +749,8 @@ __global__ void __launch_bounds__(256, 1) push_batch_kernel(BatchLaunch L)
 __global__ void batch_epoch_end_kernel(BatchCampaignDev* camps, int n, int* tile_counter)
 {
     const int c = blockIdx.x * blockDim.x + threadIdx.x;
-    if (c < n && camps[c].active) camps[c].step = min(camps[c].step + camps[c].K, camps[c].a.nsteps);
+    if (c < n && camps[c].active && camps[c].running)
+        camps[c].step = min(camps[c].step + camps[c].K, camps[c].a.nsteps);
     if (c == 0) *tile_counter = 0;
 }
 
@@ -760,23 +761,27 @@ __global__ void zero_counted_kernel(uint32_t* a, const int64_t* m)
         a[i] = 0u;
 }
 
-// Sort key of every occupied slot: the campaign's first bucket + the brick of
-// the particle's cell (the campaign's dead bucket for dead particles).  Free
-// slots (camp_of < 0) take no part.
-__global__ void batch_key_kernel(const BatchCampaignDev* __restrict__ camps, const int32_t* __restrict__ camp_of,
-                                 BatchStateDev st, uint32_t* __restrict__ keys, uint32_t* __restrict__ hist)
+// Sort key of every particle of a running campaign -- the slots the tile
+// table covers, one block per tile: the campaign's first bucket + the brick
+// of the particle's cell (the campaign's dead bucket for dead particles).
+// Free slots and paused campaigns hold no tiles and take no part, so the
+// cost follows the particles in flight, not the arena's capacity.
+__global__ void __launch_bounds__(kBatchTile) batch_key_kernel(const BatchCampaignDev* __restrict__ camps,
+                                                               const BatchTile* __restrict__ tiles,
+                                                               const int* __restrict__ n_tiles, BatchStateDev st,
+                                                               uint32_t* __restrict__ keys, uint32_t* __restrict__ hist)
 {
     const int lane = threadIdx.x & 31;
     const unsigned lt = (1u << lane) - 1u;
     const int64_t cap = st.cap;
-    const int64_t stride = (int64_t)gridDim.x * blockDim.x;
-    for (int64_t base = (int64_t)blockIdx.x * blockDim.x + (threadIdx.x & ~31); base < cap; base += stride) {
-        const int64_t i = base + lane;
-        const int c = i < cap ? camp_of[i] : -1;
-        const bool valid = c >= 0;
+    const int nt = *n_tiles;
+    for (int t = blockIdx.x; t < nt; t += gridDim.x) {
+        const BatchTile T = tiles[t];
+        const bool valid = (int)threadIdx.x < T.count;
+        const int64_t i = T.begin + threadIdx.x;
         uint32_t key = 0;
         if (valid) {
-            const BatchCampaignDev& C = camps[c];
+            const BatchCampaignDev& C = camps[T.campaign];
             key = (uint32_t)(C.key_base + C.n_bricks);
             if (st.alive[i]) {
                 const int nx = (int)C.a.fld.nx, ny = (int)C.a.fld.ny, nz = (int)C.a.fld.nz;
@@ -796,27 +801,30 @@ __global__ void batch_key_kernel(const BatchCampaignDev* __restrict__ camps, con
     }
 }
 
-__global__ void batch_scatter_kernel(const uint32_t* __restrict__ keys, uint32_t* cursor,
-                                     const uint32_t* __restrict__ tile_off, const BatchCampaignDev* __restrict__ camps, const int32_t* __restrict__ camp_of,
-                                     BatchStateDev from, BatchStateDev to)
+__global__ void __launch_bounds__(kBatchTile) batch_scatter_kernel(const uint32_t* __restrict__ keys, uint32_t* cursor,
+                                                                   const uint32_t* __restrict__ tile_off,
+                                                                   const BatchCampaignDev* __restrict__ camps,
+                                                                   const BatchTile* __restrict__ tiles,
+                                                                   const int* __restrict__ n_tiles,
+                                                                   BatchStateDev from, BatchStateDev to)
 {
     const int lane = threadIdx.x & 31;
     const unsigned lt = (1u << lane) - 1u;
     const int64_t cap = from.cap;
-    const int64_t stride = (int64_t)gridDim.x * blockDim.x;
-    for (int64_t base = (int64_t)blockIdx.x * blockDim.x + (threadIdx.x & ~31); base < cap; base += stride) {
-        const int64_t i = base + lane;
-        const int c = i < cap ? camp_of[i] : -1;
-        const bool valid = c >= 0;
+    const int nt = *n_tiles;
+    for (int t = blockIdx.x; t < nt; t += gridDim.x) {
+        const BatchTile T = tiles[t];
+        const bool valid = (int)threadIdx.x < T.count;
         const unsigned act = __ballot_sync(0xffffffffu, valid);
         if (!valid) continue;
+        const int64_t i = T.begin + threadIdx.x;
         const uint32_t key = keys[i];
         const unsigned same = __match_any_sync(act, key);
         const int leader = __ffs(same) - 1;
         uint32_t first = 0;
         if (lane == leader) first = atomicAdd(&cursor[key], (uint32_t)__popc(same)) + tile_off[key / kScanTile];
         first = __shfl_sync(same, first, leader);
-        const int64_t d = (int64_t)first + __popc(same & lt) + camps[c].shift;
+        const int64_t d = (int64_t)first + __popc(same & lt) + camps[T.campaign].shift;
         to.x[d] = from.x[i]; to.x[cap + d] = from.x[cap + i]; to.x[2 * cap + d] = from.x[2 * cap + i];
         to.p[d] = from.p[i]; to.p[cap + d] = from.p[cap + i]; to.p[2 * cap + d] = from.p[2 * cap + i];
         to.p2[d] = from.p2[i];
@@ -889,15 +897,15 @@ int launch_batch_epoch_end(BatchCampaignDev* camps, int n_camps, int* tile_count
     return PT_OK;
 }
 
-int launch_batch_sort(const BatchCampaignDev* camps, const int32_t* camp_of, BatchStateDev from, BatchStateDev to,
-                      uint32_t* keys, uint32_t* hist, uint32_t* cursor, const int64_t* d_m, int64_t max_buckets,
-                      int num_sms, cudaStream_t s)
+int launch_batch_sort(const BatchCampaignDev* camps, const BatchTile* tiles, const int* n_tiles, int grid,
+                      BatchStateDev from, BatchStateDev to, uint32_t* keys, uint32_t* hist, uint32_t* cursor,
+                      const int64_t* d_m, int64_t max_buckets, int num_sms, cudaStream_t s)
 {
     const int zb = (int)std::min<int64_t>((max_buckets + 255) / 256, (int64_t)num_sms * 8);
     zero_counted_kernel<<<std::max(zb, 1), 256, 0, s>>>(hist, d_m);
     PT_CHECK_LAUNCH("zero_counted_kernel");
-    const int gb = (int)std::min<int64_t>((from.cap + 255) / 256, INT32_MAX);  // one slot per thread
-    batch_key_kernel<<<gb, 256, 0, s>>>(camps, camp_of, from, keys, hist);
+    const int gb = std::max(grid, 1);  // one block per tile of the table (tile-stride beyond)
+    batch_key_kernel<<<gb, kBatchTile, 0, s>>>(camps, tiles, n_tiles, from, keys, hist);
     PT_CHECK_LAUNCH("batch_key_kernel");
     uint32_t* tile_off = cursor + max_buckets;
     const int64_t max_tiles = sort_scan_tiles(max_buckets);
@@ -906,7 +914,7 @@ int launch_batch_sort(const BatchCampaignDev* camps, const int32_t* camp_of, Bat
     PT_CHECK_LAUNCH("sort_scan_tiles_kernel");
     sort_scan_top_kernel<<<1, 1024, 0, s>>>(tile_off, max_tiles, d_m);
     PT_CHECK_LAUNCH("sort_scan_top_kernel");
-    batch_scatter_kernel<<<gb, 256, 0, s>>>(keys, cursor, tile_off, camps, camp_of, from, to);
+    batch_scatter_kernel<<<gb, kBatchTile, 0, s>>>(keys, cursor, tile_off, camps, tiles, n_tiles, from, to);
     PT_CHECK_LAUNCH("batch_scatter_kernel");
     return PT_OK;
 }

@@ -7,8 +7,16 @@ any time (submit); each scheduler tick
   1. admits waiting jobs, in arrival order, while the HBM budget and the
      batch's slot arena have room (the job's particle state, mu cache and
      accumulators are charged against the budget);
-  2. runs one epoch (steps_per_epoch pushes of every admitted job, one
-     persistent launch replayed from a CUDA graph);
+  2. picks the jobs this epoch advances and runs one epoch (steps_per_epoch
+     pushes of each of them, one persistent launch replayed from a CUDA
+     graph).  With schedule="srpt" (the default) those are the jobs with the
+     least work left (particles x steps to go), taken in that order until
+     they hold fill_particles particles (262,144 by default: 1024 tiles,
+     which keep every SM busy at ~75 % of the full-batch rate) while the
+     others wait with their state on the device
+     (pt_batch_set_running); small jobs then finish in a few epochs instead
+     of sharing every epoch with the largest ones.  schedule="all" advances
+     every admitted job in every epoch;
   3. for each job that reached its last step, launches its lag-pair binning
      on a side stream -- overlapping the next epoch -- and, once that
      finished, computes the products, records the latency and frees the job.
@@ -75,7 +83,8 @@ class JobResult:
 class CampaignServer:
     def __init__(self, libraries: dict, B0_ref_T: dict, hbm_budget_bytes: float = 150e9, storage: str = "brick_bf16",
                  steps_per_epoch: int = 64, capacity: int = 1 << 26, max_jobs: int = 256, blocks_per_sm: int = 0,
-                 keep_cache: bool = False, device: int = 0, push: str = "f32"):
+                 keep_cache: bool = False, device: int = 0, push: str = "f32", schedule: str = "srpt",
+                 fill_particles: int = 1 << 18):
         """libraries: {library: {mode: FieldLibrary}} (brick storage for the
         FP32 push; REF_F64 for push="f64", the plain FP64 push);
         B0_ref_T: {library: total-field mean |B|} (time reference of every mode).
@@ -91,6 +100,11 @@ class CampaignServer:
         self.K = int(steps_per_epoch)
         if push not in ("f32", "f64"):
             raise ValueError("push must be f32 or f64")
+        if schedule not in ("srpt", "all"):
+            raise ValueError("schedule must be srpt or all")
+        self.schedule = schedule
+        self.fill = int(fill_particles)
+        self._running_ids = None  # campaign ids set running in the batch (None: all)
         self.push = push
         if push == "f64":
             self.batch = ReferenceBatch(steps_per_epoch=self.K, device=device)
@@ -142,6 +156,7 @@ class CampaignServer:
         n_dpp = min(spec.n_particles, max(0, spec.dpp_particles))
         mom = torch.empty((nsave, 3, n_dpp), dtype=torch.float32, device=self.device) if n_dpp else None
         cid = self.batch.add(fl, st, dt, nsteps, stride, cache=cache, mom_cache=mom)
+        self._running_ids = None  # a new campaign runs until the next selection
         self.active[jid] = dict(spec=spec, cid=cid, cache=cache, mom=mom, nsteps=nsteps, nsave=nsave,
                                 arrival=arrival, admitted=time.perf_counter(), bytes=self.job_bytes(spec))
         self.used += self.job_bytes(spec)
@@ -226,19 +241,41 @@ class CampaignServer:
         d["p0"] = p0
         return d
 
+    def _work_left(self, rec) -> int:
+        """Particle-steps a job still has to push."""
+        return rec["spec"].n_particles * max(rec["nsteps"] - rec.get("epochs", 0) * self.K, 0)
+
+    def _select(self):
+        """Jobs the next epoch advances (see the module docstring)."""
+        if self.schedule == "all":
+            return list(self.active)
+        order = sorted(self.active, key=lambda j: (self._work_left(self.active[j]), j))
+        run, fill = [], 0
+        for jid in order:
+            if run and fill >= self.fill:
+                break
+            run.append(jid)
+            fill += self.active[jid]["spec"].n_particles
+        ids = sorted(self.active[j]["cid"] for j in run)
+        if ids != self._running_ids:
+            self.batch.set_running(ids)
+            self._running_ids = ids
+        return run
+
     def tick(self):
         """One scheduling step; returns the jobs finished in it."""
         self.admit()
         if self.active:
+            run = self._select()
             ev0, ev1 = self.torch.cuda.Event(enable_timing=True), self.torch.cuda.Event(enable_timing=True)
             ev0.record()
             self.batch.run(1)
             ev1.record()
             self._epoch_events.append((ev0, ev1))
             self.epochs += 1
-            for jid in list(self.active):
+            for jid in run:
                 rec = self.active[jid]
-                # every job advances K steps per epoch from its admission
+                # a job advances K steps in every epoch it is selected for
                 rec.setdefault("epochs", 0)
                 rec["epochs"] += 1
                 if rec["epochs"] * self.K >= rec["nsteps"]:
@@ -254,6 +291,7 @@ class CampaignServer:
                                 {k: v.cpu().numpy() for k, v in rec["acc"].items()}, rec["lags"], rec["edges"],
                                 rec["cache"].cpu().numpy() if self.keep_cache else None, self._dpp_result(rec))
                 self.batch.remove(rec["cid"])
+                self._running_ids = None
                 self.used -= rec["bytes"]
                 del self.binning[jid]
                 self.results.append(res)

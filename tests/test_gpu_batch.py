@@ -113,6 +113,47 @@ def test_batch_join_and_leave(cuda):
     b.close()
 
 
+@pytest.mark.parametrize("sort", [True, False])
+def test_batch_pause_and_resume(cuda, sort):
+    """Campaigns paused for some epochs (pt_batch_set_running) and resumed --
+    after an odd number of epochs, so that the sort buffers changed parity
+    while they waited -- end with the caches and states of their runs alone."""
+    torch = cuda
+    cs = campaigns(torch)
+    ref = [run_alone(torch, c) for c in cs]
+    K = 32
+    b = Batch(5000, max_campaigns=8, steps_per_epoch=K, sort=sort)
+    caches = [new_cache(torch, c) for c in cs]
+    ids = [b.add(c["field"], c["state"], c["dt"], c["nsteps"], c["stride"], cache=ch) for c, ch in zip(cs, caches)]
+    b.run(1)
+    b.set_running([ids[1], ids[3]])
+    st0 = {k: v.cpu().numpy() for k, v in b.export(ids[0])[0].items()}
+    b.run(3)
+    assert b.step(ids[0]) == K and b.step(ids[2]) == K
+    assert b.step(ids[1]) == min(4 * K, cs[1]["nsteps"])
+    # a paused campaign exports the state it stopped with
+    st0b = {k: v.cpu().numpy() for k, v in b.export(ids[0])[0].items()}
+    for k in st0:
+        assert np.array_equal(st0[k], st0b[k]), k
+    b.set_running([ids[0]])
+    b.run(2)
+    b.set_running([ids[2], ids[0]])
+    b.run(1)
+    b.set_running(None)
+    b.run(max(math.ceil(c["nsteps"] / K) for c in cs))
+    for c, cid, ch, (mu_ref, st_ref) in zip(cs, ids, caches, ref):
+        assert b.step(cid) == c["nsteps"]
+        assert np.array_equal(ch.cpu().numpy(), mu_ref, equal_nan=True)
+        st, _ = b.export(cid)
+        for k in st:
+            assert np.array_equal(st[k].cpu().numpy(), st_ref[k]), k
+    from particle_transport_b200._lib import PtError
+    b.remove(ids[3])
+    with pytest.raises(PtError, match="no such campaign"):
+        b.set_running([ids[3]])
+    b.close()
+
+
 def test_batch_ring_cache(cuda):
     torch = cuda
     c = campaigns(torch)[1]

@@ -40,9 +40,10 @@ JOBS = [JobSpec("16", "total", 1.0, 3000, 6.0, seed=1),
         JobSpec("16", "alfven", 2.0, 64, 2.0, seed=4)]
 
 
-def run_jobs(library, jobs, budget=150e9, stagger_ticks=0, push="f32"):
+def run_jobs(library, jobs, budget=150e9, stagger_ticks=0, push="f32", schedule="srpt", fill=1 << 22):
     libs, B0 = library
-    srv = CampaignServer(libs, B0, hbm_budget_bytes=budget, capacity=20000, max_jobs=8, keep_cache=True, push=push)
+    srv = CampaignServer(libs, B0, hbm_budget_bytes=budget, capacity=20000, max_jobs=8, keep_cache=True, push=push,
+                         schedule=schedule, fill_particles=fill)
     pending = list(jobs)
     ids = []
     while pending or not srv.idle():
@@ -89,6 +90,26 @@ def test_job_results_same_alone_and_in_the_mix(library):
         assert m.particle_steps > 0 and m.latency > 0
     # the products are populated: pair counts equal sum over lags of valid starts
     assert all(r.acc["pair_counts"].sum() > 0 for r in mixed)
+
+
+@pytest.mark.parametrize("schedule,fill", [("srpt", 1000), ("srpt", 1), ("all", 0)])
+def test_schedules_give_the_same_results(library, schedule, fill):
+    """Least-work-first epochs that hold back all but a few jobs (fill of
+    1000 or 1 particles: the waiting jobs are paused in the batch) and the
+    every-job schedule give every job the results of its run alone."""
+    alone = [run_jobs(library, [j])[0] for j in JOBS]
+    mixed = run_jobs(library, JOBS, stagger_ticks=1, schedule=schedule, fill=fill)
+    for a, m in zip(alone, mixed):
+        same(m, a)
+
+
+def test_srpt_finishes_small_jobs_first(library):
+    """With one job running at a time, jobs submitted together finish in the
+    order of their work (particles x steps)."""
+    res = run_jobs(library, JOBS, schedule="srpt", fill=1)
+    by_finish = [r.job_id for r in sorted(res, key=lambda r: r.finished)]
+    by_work = [r.job_id for r in sorted(res, key=lambda r: r.particle_steps)]
+    assert by_finish == by_work
 
 
 def test_budget_holds_jobs_back(library):
