@@ -4,6 +4,7 @@
 
 #include <algorithm>
 #include <cmath>
+#include <cstring>
 #include <new>
 #include <string>
 #include <vector>
@@ -38,6 +39,17 @@ struct pt_batch {
     cudaStream_t cap_stream = nullptr;
     cudaGraphExec_t graph[2] = {nullptr, nullptr};
     bool graph_dirty = true;
+    // pinned staging of the campaign and tile tables (rebuild_tables)
+    static constexpr int kStages = 4;
+    struct Stage {
+        void* host = nullptr;
+        size_t bytes = 0;
+        cudaEvent_t ev = nullptr;
+        bool pending = false;  // an upload from it is enqueued
+    } stage[kStages];
+    int stage_next = 0;
+    BatchCampaignDev* d_stage = nullptr;
+    std::vector<BatchTile> tile_scratch;
 };
 
 namespace {
@@ -78,21 +90,18 @@ void drop_graphs(pt_batch* b)
     b->graph_dirty = true;
 }
 
-// Recompute sort buckets and tile table after the campaign set changed.  The
-// step counters live on the device (advanced by every epoch): they are read
-// back first so that uploading the table does not rewind running campaigns;
-// `fresh` is a campaign just added (its step stays 0).
+// Recompute sort buckets and tile table after the campaign set changed and
+// upload them behind the epochs already enqueued, without waiting for them.
+// The step counters are advanced on the device by every epoch, so the host
+// table's steps are stale: batch_apply_kernel installs the new table but
+// keeps each running campaign's device step (`fresh`, a campaign just added,
+// takes its step 0 from the table).  The table goes through a ring of pinned
+// staging buffers; one is written again only after its upload has run.
 int rebuild_tables(pt_batch* b, int fresh)
 {
-    {
-        std::vector<BatchCampaignDev> dev((size_t)b->max_camps);
-        PT_CUDA(cudaStreamSynchronize(b->ctx->stream));
-        PT_CUDA(cudaMemcpy(dev.data(), b->d_camps, sizeof(BatchCampaignDev) * b->max_camps, cudaMemcpyDeviceToHost));
-        for (int i = 0; i < b->max_camps; ++i)
-            if (i != fresh && b->h_camps[i].active) b->h_camps[i].step = dev[i].step;
-    }
     int64_t key = 0, dense = 0;
-    std::vector<BatchTile> tiles;
+    std::vector<BatchTile>& tiles = b->tile_scratch;
+    tiles.clear();
     for (int c = 0; c < b->max_camps; ++c) {
         BatchCampaignDev& C = b->h_camps[c];
         if (!C.active || !C.running) continue;
@@ -105,11 +114,11 @@ int rebuild_tables(pt_batch* b, int fresh)
     }
     if (key > UINT32_MAX) return fail(PT_ERR_ARG, "too many sort buckets in the batch");
     if (key > b->hist_cap) {
+        const int64_t want = std::max<int64_t>(key, 2 * b->hist_cap);
         if (b->hist) cudaFree(b->hist);
         if (b->cursor) cudaFree(b->cursor);
         b->hist = b->cursor = nullptr;
         b->hist_cap = 0;
-        const int64_t want = std::max<int64_t>(key, 2 * b->hist_cap);
         cudaError_t e = cudaMalloc((void**)&b->hist, sizeof(uint32_t) * want);
         // cursor[want] followed by the scan's per-tile offsets
         if (e == cudaSuccess) e = cudaMalloc((void**)&b->cursor, sizeof(uint32_t) * (want + sort_scan_tiles(want)));
@@ -134,13 +143,43 @@ int rebuild_tables(pt_batch* b, int fresh)
             drop_graphs(b);
         }
     }
+    // staging layout: campaigns | n_tiles (int) | buckets (int64) | tiles
+    const size_t camps_bytes = sizeof(BatchCampaignDev) * (size_t)b->max_camps;
+    const size_t o_nt = (camps_bytes + 15) & ~(size_t)15, o_m = o_nt + 16, o_tiles = o_m + 16;
+    const size_t need = o_tiles + sizeof(BatchTile) * (size_t)nt;
+    pt_batch::Stage& S = b->stage[b->stage_next];
+    b->stage_next = (b->stage_next + 1) % pt_batch::kStages;
+    if (S.pending) {
+        PT_CUDA(cudaEventSynchronize(S.ev));
+        S.pending = false;
+    }
+    if (S.bytes < need) {
+        if (S.host) cudaFreeHost(S.host);
+        S.host = nullptr;
+        S.bytes = 0;
+        const size_t want = std::max(need + need / 2, (size_t)1 << 16);
+        cudaError_t e = cudaMallocHost(&S.host, want);
+        if (e != cudaSuccess) {
+            cudaGetLastError();
+            S.host = nullptr;
+            return fail(PT_ERR_OOM, "pinned staging allocation of the batch tables failed");
+        }
+        S.bytes = want;
+    }
+    char* h = (char*)S.host;
+    std::memcpy(h, b->h_camps.data(), camps_bytes);
+    std::memcpy(h + o_nt, &nt, sizeof(int));
+    std::memcpy(h + o_m, &key, sizeof(int64_t));
+    if (nt) std::memcpy(h + o_tiles, tiles.data(), sizeof(BatchTile) * (size_t)nt);
     cudaStream_t s = b->ctx->stream;
-    PT_CUDA(cudaMemcpyAsync(b->d_camps, b->h_camps.data(), sizeof(BatchCampaignDev) * b->max_camps,
-                            cudaMemcpyHostToDevice, s));
-    if (nt) PT_CUDA(cudaMemcpyAsync(b->d_tiles, tiles.data(), sizeof(BatchTile) * nt, cudaMemcpyHostToDevice, s));
-    PT_CUDA(cudaMemcpyAsync(b->d_ntiles, &nt, sizeof(int), cudaMemcpyHostToDevice, s));
-    PT_CUDA(cudaMemcpyAsync(b->d_m, &key, sizeof(int64_t), cudaMemcpyHostToDevice, s));
-    PT_CUDA(cudaStreamSynchronize(s));  // host vectors are reused right away
+    PT_CUDA(cudaMemcpyAsync(b->d_stage, h, camps_bytes, cudaMemcpyHostToDevice, s));
+    if (nt) PT_CUDA(cudaMemcpyAsync(b->d_tiles, h + o_tiles, sizeof(BatchTile) * nt, cudaMemcpyHostToDevice, s));
+    PT_CUDA(cudaMemcpyAsync(b->d_ntiles, h + o_nt, sizeof(int), cudaMemcpyHostToDevice, s));
+    PT_CUDA(cudaMemcpyAsync(b->d_m, h + o_m, sizeof(int64_t), cudaMemcpyHostToDevice, s));
+    int rc = launch_batch_apply(b->d_camps, b->d_stage, b->max_camps, fresh, s);
+    if (rc) return rc;
+    PT_CUDA(cudaEventRecord(S.ev, s));
+    S.pending = true;
     return PT_OK;
 }
 
@@ -212,12 +251,15 @@ int pt_batch_create(pt_ctx* ctx, int64_t capacity, int max_campaigns, int storag
     cudaError_t e = cudaSuccess;
     if (!rc) {
         e = cudaMalloc((void**)&b->d_camps, sizeof(BatchCampaignDev) * max_campaigns);
+        if (e == cudaSuccess) e = cudaMalloc((void**)&b->d_stage, sizeof(BatchCampaignDev) * max_campaigns);
         if (e == cudaSuccess) e = cudaMalloc((void**)&b->d_tiles, sizeof(BatchTile) * max_tiles);
         if (e == cudaSuccess) e = cudaMalloc((void**)&b->d_ntiles, sizeof(int));
         if (e == cudaSuccess) e = cudaMalloc((void**)&b->d_counter, sizeof(int));
         if (e == cudaSuccess) e = cudaMalloc((void**)&b->d_m, sizeof(int64_t));
         if (e == cudaSuccess && b->sort) e = cudaMalloc((void**)&b->keys, sizeof(uint32_t) * capacity);
         if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&b->cap_stream, cudaStreamNonBlocking);
+        for (auto& st : b->stage)
+            if (e == cudaSuccess) e = cudaEventCreateWithFlags(&st.ev, cudaEventDisableTiming);
         if (e != cudaSuccess) {
             cudaGetLastError();
             rc = fail(PT_ERR_OOM, "batch allocation failed");
@@ -341,7 +383,6 @@ int pt_batch_remove(pt_ctx* ctx, pt_batch* b, int id)
     if (!ctx || !b) return fail(PT_ERR_ARG, "null argument");
     if (id < 0 || id >= b->max_camps || !b->h_camps[id].active) return fail(PT_ERR_ARG, "no such campaign");
     BatchCampaignDev& C = b->h_camps[id];
-    PT_CUDA(cudaStreamSynchronize(ctx->stream));  // the step counter on the host mirror is stale: keep device's
     b->free_ranges.push_back({C.slot0, C.n});
     std::sort(b->free_ranges.begin(), b->free_ranges.end());
     std::vector<std::pair<int64_t, int64_t>> merged;
@@ -450,7 +491,11 @@ int pt_batch_destroy(pt_batch* b)
     drop_graphs(b);
     free_state(b->buf[0]);
     free_state(b->buf[1]);
-    for (void* p : {(void*)b->d_camps, (void*)b->d_tiles, (void*)b->d_ntiles, (void*)b->d_counter,
+    for (auto& st : b->stage) {
+        if (st.host) cudaFreeHost(st.host);
+        if (st.ev) cudaEventDestroy(st.ev);
+    }
+    for (void* p : {(void*)b->d_stage, (void*)b->d_camps, (void*)b->d_tiles, (void*)b->d_ntiles, (void*)b->d_counter,
                     (void*)b->keys, (void*)b->hist, (void*)b->cursor, (void*)b->d_m})
         if (p) cudaFree(p);
     if (b->cap_stream) cudaStreamDestroy(b->cap_stream);

@@ -218,6 +218,8 @@ struct BatchLaunch {
     int grid;
 };
 int launch_push_batch(const BatchLaunch& L, cudaStream_t s);
+int launch_batch_apply(BatchCampaignDev* camps, const BatchCampaignDev* staged, int n_camps, int fresh,
+                       cudaStream_t s);
 int launch_batch_epoch_end(BatchCampaignDev* camps, int n_camps, int* tile_counter, cudaStream_t s);
 // buckets per tile of the two-level bucket scan of the brick sorts, and the
 // number of tile offsets that follow the cursor array of m buckets

@@ -754,6 +754,19 @@ __global__ void batch_epoch_end_kernel(BatchCampaignDev* camps, int n, int* tile
     if (c == 0) *tile_counter = 0;
 }
 
+// Install a new campaign table uploaded by the host while keeping the step
+// counter of every campaign that was already running on the device (the
+// host's copy of it is stale); `fresh` takes the table's step (0).
+__global__ void batch_apply_kernel(BatchCampaignDev* camps, const BatchCampaignDev* __restrict__ staged, int n,
+                                   int fresh)
+{
+    const int c = blockIdx.x * blockDim.x + threadIdx.x;
+    if (c >= n) return;
+    BatchCampaignDev v = staged[c];
+    if (c != fresh && v.active && camps[c].active) v.step = camps[c].step;
+    camps[c] = v;
+}
+
 __global__ void zero_counted_kernel(uint32_t* a, const int64_t* m)
 {
     const int64_t mm = *m;
@@ -887,6 +900,14 @@ int launch_push_batch(const BatchLaunch& L, cudaStream_t s)
     else if (L.layout == LAYOUT_BF16_XPAIR) push_batch_kernel<LAYOUT_BF16_XPAIR><<<L.grid, 256, smem, s>>>(L);
     else push_batch_kernel<LAYOUT_BF16><<<L.grid, 256, smem, s>>>(L);
     PT_CHECK_LAUNCH("push_batch_kernel");
+    return PT_OK;
+}
+
+int launch_batch_apply(BatchCampaignDev* camps, const BatchCampaignDev* staged, int n_camps, int fresh,
+                       cudaStream_t s)
+{
+    batch_apply_kernel<<<(std::max(n_camps, 1) + 127) / 128, 128, 0, s>>>(camps, staged, n_camps, fresh);
+    PT_CHECK_LAUNCH("batch_apply_kernel");
     return PT_OK;
 }
 

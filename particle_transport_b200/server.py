@@ -29,6 +29,7 @@ The reference has no serving mode; it runs campaigns back to back
 """
 from __future__ import annotations
 
+import collections
 import math
 import time
 from dataclasses import dataclass, field as dfield
@@ -84,7 +85,7 @@ class CampaignServer:
     def __init__(self, libraries: dict, B0_ref_T: dict, hbm_budget_bytes: float = 150e9, storage: str = "brick_bf16",
                  steps_per_epoch: int = 64, capacity: int = 1 << 26, max_jobs: int = 256, blocks_per_sm: int = 0,
                  keep_cache: bool = False, device: int = 0, push: str = "f32", schedule: str = "srpt",
-                 fill_particles: int = 1 << 18):
+                 fill_particles: int = 1 << 18, max_epochs_in_flight: int = 2):
         """libraries: {library: {mode: FieldLibrary}} (brick storage for the
         FP32 push; REF_F64 for push="f64", the plain FP64 push);
         B0_ref_T: {library: total-field mean |B|} (time reference of every mode).
@@ -104,6 +105,11 @@ class CampaignServer:
             raise ValueError("schedule must be srpt or all")
         self.schedule = schedule
         self.fill = int(fill_particles)
+        # epochs enqueued but not finished on the device: the scheduler stays
+        # this close to the device, so its choices (and new jobs) take effect
+        # within a few epochs instead of behind a long launch queue
+        self.depth = max(1, int(max_epochs_in_flight))
+        self._inflight = collections.deque()
         self._running_ids = None  # campaign ids set running in the batch (None: all)
         self.push = push
         if push == "f64":
@@ -196,8 +202,11 @@ class CampaignServer:
         with torch.cuda.stream(self.side):
             self.side.wait_event(done)
             acc = S.new_dmumu_accumulators(len(lags), spec.n_bins, device=self.device)
-            d_lags = torch.as_tensor(lags, device=self.device)
-            d_edges = torch.as_tensor(edges, device=self.device)
+            # pinned sources and non-blocking copies: a pageable copy would
+            # wait here for the side stream, i.e. for the binning of every
+            # job before this one, and stall the epochs behind it
+            d_lags = torch.as_tensor(lags).pin_memory().to(self.device, non_blocking=True)
+            d_edges = torch.as_tensor(edges).pin_memory().to(self.device, non_blocking=True)
             self.side_ctx.use_stream(self.side)
             cache = rec["cache"]
             _lib.call("pt_dmumu_accumulate_device", self.side_ctx.handle, _lib.ptr(cache), spec.n_particles,
@@ -230,7 +239,7 @@ class CampaignServer:
         if rec["dpp"] is None:
             return None
         d = {k: v.cpu().numpy() for k, v in rec["dpp"].items()}
-        m = rec["mom"][0, :, 0].double().cpu().numpy()
+        m = rec["mom"][0, :, 0].cpu().double().numpy()
         p0 = math.sqrt(float(m[0]) * float(m[0]) + float(m[1]) * float(m[1]) + float(m[2]) * float(m[2]))
         if not (math.isfinite(p0) and p0 > 0.0):
             d["sum_delta_p_norm"] = np.full_like(d["sum_delta_p_norm"], np.nan)
@@ -265,12 +274,15 @@ class CampaignServer:
     def tick(self):
         """One scheduling step; returns the jobs finished in it."""
         self.admit()
-        if self.active:
+        while self._inflight and self._inflight[0].query():
+            self._inflight.popleft()
+        if self.active and len(self._inflight) < self.depth:
             run = self._select()
             ev0, ev1 = self.torch.cuda.Event(enable_timing=True), self.torch.cuda.Event(enable_timing=True)
             ev0.record()
             self.batch.run(1)
             ev1.record()
+            self._inflight.append(ev1)
             self._epoch_events.append((ev0, ev1))
             self.epochs += 1
             for jid in run:
@@ -286,10 +298,14 @@ class CampaignServer:
             rec = self.binning[jid]
             if rec["ev"].query():
                 spec = rec["spec"]
+                # read back on the side stream, which has finished this job's
+                # work: a copy on the main stream would wait for the epochs
+                with self.torch.cuda.stream(self.side):
+                    acc = {k: v.cpu().numpy() for k, v in rec["acc"].items()}
+                    mu = rec["cache"].cpu().numpy() if self.keep_cache else None
+                    dpp = self._dpp_result(rec)
                 res = JobResult(jid, spec, rec["arrival"], rec["admitted"], time.perf_counter(),
-                                spec.n_particles * (rec["nsteps"] - 1),
-                                {k: v.cpu().numpy() for k, v in rec["acc"].items()}, rec["lags"], rec["edges"],
-                                rec["cache"].cpu().numpy() if self.keep_cache else None, self._dpp_result(rec))
+                                spec.n_particles * (rec["nsteps"] - 1), acc, rec["lags"], rec["edges"], mu, dpp)
                 self.batch.remove(rec["cid"])
                 self._running_ids = None
                 self.used -= rec["bytes"]
