@@ -14,6 +14,7 @@ _HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(_HERE, "libptb200.so")
 
 PT_OK = 0
+PT_ERR_ARG = -1
 PT_ERR = {-1: "PT_ERR_ARG", -2: "PT_ERR_CUDA", -3: "PT_ERR_OOM", -4: "PT_ERR_TIMEOUT", -5: "PT_ERR_CALLBACK",
           -6: "PT_ERR_STATE"}
 

@@ -209,12 +209,22 @@ class CampaignServer:
             d_edges = torch.as_tensor(edges).pin_memory().to(self.device, non_blocking=True)
             self.side_ctx.use_stream(self.side)
             cache = rec["cache"]
-            _lib.call("pt_dmumu_accumulate_device", self.side_ctx.handle, _lib.ptr(cache), spec.n_particles,
-                      rec["nsave"], 1, spec.n_particles, _lib.ptr(d_lags), len(lags), _lib.ptr(d_edges),
-                      spec.n_bins, S.START[spec.start_mode], 1,
-                      *[_lib.ptr(acc[k]) for k in ("dmumu_counts", "dmumu_sum_delta", "dmumu_sum_delta2",
-                                                   "particle_counts", "particle_means", "particle_m2s",
-                                                   "pair_sum_squares", "pair_counts")])
+            args = (self.side_ctx.handle, _lib.ptr(cache), spec.n_particles, rec["nsave"], 1, spec.n_particles,
+                    _lib.ptr(d_lags), len(lags), _lib.ptr(d_edges), spec.n_bins, S.START[spec.start_mode], 1,
+                    *[_lib.ptr(acc[k]) for k in ("dmumu_counts", "dmumu_sum_delta", "dmumu_sum_delta2",
+                                                 "particle_counts", "particle_means", "particle_m2s",
+                                                 "pair_sum_squares", "pair_counts")])
+            # the entry that allocates nothing: a scratch regrowth in the
+            # allocating one would free memory, and cudaFree waits for the
+            # whole device -- the epochs and every earlier job's binning.
+            # All binning runs on this one side stream, so its calls never
+            # overlap on the fixed scratch.  Series too long to stage on chip
+            # take the allocating entry.
+            rc = _lib.load().pt_dmumu_accumulate_device_noalloc(*args)
+            if rc == _lib.PT_ERR_ARG:
+                _lib.call("pt_dmumu_accumulate_device", *args)
+            else:
+                _lib.check(rc, "pt_dmumu_accumulate_device_noalloc")
             dpp = None
             if rec["mom"] is not None:
                 # D_pp of the subset with p0 = 1: the kernel normalises once per
