@@ -713,14 +713,15 @@ def run_batched(args, dev, rank):
     """Batched campaigns: 12 campaigns (4 modes x 1/10/100 GeV) on a resident
     256^3 FP32 field library, N log-uniform in [65536, 4194304], 20-500 T_g0
     at 64 steps per T_g0 of each energy, one persistent launch per epoch
-    (CUDA graph), launch shape picked by the autotuner; then D_mumu per
+    (CUDA graph); steps per epoch, blocks per SM and each campaign's re-sort
+    cadence (by particle speed) picked by the tuner; then D_mumu per
     campaign (32 log lags x 20 |mu| bins) from its full mu cache (a save
     every 32 steps)."""
     import torch
 
     from particle_transport_b200 import fields as F
     from particle_transport_b200 import stats as S
-    from particle_transport_b200.batch import Batch, autotune
+    from particle_transport_b200.batch import Batch, tune_batch
     from particle_transport_b200.fields import FieldLibrary
     from particle_transport_b200.particles import energy_to_gamma, init_particles
     from particle_transport_b200.time_units import build_mu_edges_full, log_spaced_lag_steps, reference_Omega0
@@ -749,15 +750,16 @@ def run_batched(args, dev, rank):
                               nsteps=int(round(64 * dur)) + 1, stride=32, mode=m, E=E))
     ntot = sum(len(c["state"]["x1"]) for c in camps)
     t0 = time.perf_counter()
-    best, timings = autotune(camps, "brick_f32", ntot, epochs=2, use_cache=False)
+    tune = tune_batch(camps, "brick_f32", ntot, use_cache=False)
     tune_s = time.perf_counter() - t0
-    K, bps = best
+    K, bps = tune["K"], tune["blocks_per_sm"]
     b = Batch(ntot, max_campaigns=len(camps), storage="brick_f32", steps_per_epoch=K, blocks_per_sm=bps)
     caches = []
-    for c in camps:
+    for c, se in zip(camps, tune["sort_every"]):
         nsave = (c["nsteps"] - 1) // c["stride"] + 1
         caches.append(torch.empty((nsave, len(c["state"]["x1"])), dtype=torch.float32, device=dev))
-        c["id"] = b.add(c["field"], c["state"], c["dt"], c["nsteps"], c["stride"], cache=caches[-1])
+        c["id"] = b.add(c["field"], c["state"], c["dt"], c["nsteps"], c["stride"], cache=caches[-1], sort_every=se)
+        c["sort_every"] = se
     epochs = max(math.ceil(c["nsteps"] / K) for c in camps)
     b.run(1)  # graph capture + first epoch
     torch.cuda.synchronize()
@@ -786,11 +788,13 @@ def run_batched(args, dev, rank):
     lag_s = e0.elapsed_time(e1) / 1e3
     pairs = int(sum(int(c["pairs"].sum().item()) for c in camps))
     return {"campaigns": len(camps), "particles": ntot, "epochs": epochs, "steps_per_epoch": K,
-            "blocks_per_sm": bps, "autotune": {"candidates": timings, "seconds": tune_s},
+            "blocks_per_sm": bps,
+            "autotune": {"cadence_steps_by_speed_class": {str(k): v for k, v in tune["cadence_steps"].items()},
+                         "trials": {k: round(v, 1) for k, v in tune["timings"].items()}, "seconds": tune_s},
             "value": steps_timed / push_s, "unit": UNIT, "push_s": push_s,
             "lag_pairs_per_s": pairs / lag_s, "lag_s": lag_s, "field": "256^3 FP32 bricks x 4 modes",
             "per_campaign": [{"mode": c["mode"], "E_GeV": c["E"], "n": len(c["state"]["x1"]),
-                              "T_g0": (c["nsteps"] - 1) / 64} for c in camps]}
+                              "T_g0": (c["nsteps"] - 1) / 64, "sort_every_epochs": c["sort_every"]} for c in camps]}
 
 
 def run_precision(args, dev):

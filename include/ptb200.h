@@ -188,8 +188,8 @@ int pt_push_advance_fast(pt_ctx* ctx, const pt_field* field, pt_fast_state* st, 
  * holding many campaigns (mode x energy, or jobs of a server), each with its
  * own field, dt, step count, save stride and mu cache.  One persistent
  * kernel advances every campaign by steps_per_epoch steps per epoch
- * (finished campaigns idle); with sort = 1 the slots are re-sorted by brick
- * within each campaign before every epoch.  Epochs run as CUDA graphs (one
+ * (finished campaigns idle); with sort = 1 each campaign's slots are
+ * re-sorted by brick before every sort_every-th epoch it runs.  Epochs run as CUDA graphs (one
  * per sort buffer parity) when use_graph = 1.  Campaigns can be added and
  * removed between epochs.  A particle's trajectory and cache rows are
  * bit-identical to a single-campaign pt_push_advance_fast run.
@@ -216,7 +216,10 @@ typedef struct {
     void* d_cache;             /* mu rows [cache_rows][n] (NULL: no cache)                   */
     int64_t cache_rows;
     int32_t cache_ring;        /* 1: save row r goes to row r % cache_rows                   */
-    int32_t reserved;
+    int32_t sort_every;        /* re-sort this campaign's slots by brick before every sort_every-th
+                                  epoch it runs (0 or 1: every epoch); batches made with sort = 0
+                                  never sort.  Fast particles lose their brick order within a few
+                                  steps and gain from frequent sorts, slow ones do not.          */
     int64_t* d_deaths;         /* [nsteps] particles killed per step (open boundary), or NULL */
     float* d_mom_cache;        /* with d_cache: momenta rows [cache_rows][3][n_mom] (Float32, SI, the
                                   phase-space writer's momenta, src/phase_space_gpu_runner.jl:413-421)

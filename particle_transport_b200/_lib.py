@@ -74,7 +74,7 @@ class CampaignDesc(C.Structure):
         ("periodic", C.c_int32), ("cache_f64", C.c_int32), ("n", C.c_int64),
         ("d_x1", C.c_void_p), ("d_x2", C.c_void_p), ("d_x3", C.c_void_p), ("d_p1", C.c_void_p),
         ("d_p2", C.c_void_p), ("d_p3", C.c_void_p), ("d_alive", C.c_void_p),
-        ("d_cache", C.c_void_p), ("cache_rows", C.c_int64), ("cache_ring", C.c_int32), ("reserved", C.c_int32),
+        ("d_cache", C.c_void_p), ("cache_rows", C.c_int64), ("cache_ring", C.c_int32), ("sort_every", C.c_int32),
         ("d_deaths", C.c_void_p), ("d_mom_cache", C.c_void_p), ("n_mom", C.c_int64),
     ]
 

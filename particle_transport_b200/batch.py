@@ -8,9 +8,12 @@ all of them by steps_per_epoch steps from their own device-resident step
 counters; epochs replay as CUDA graphs.  Campaigns are added and removed
 between epochs.
 
-The autotuner times candidate (steps per epoch = sort cadence, resident
-blocks per SM) pairs on a throw-away copy of the campaigns and caches the
-winner per (device, storage, particle count, field size) in a JSON file.
+The tuner (tune_batch) picks a re-sort cadence per speed class of
+campaigns (particles that cross a brick every few steps want frequent
+sorts, slow ones do not), the steps per epoch and the resident blocks per
+SM, timing each on throw-away copies of the campaigns, and caches the result
+in a JSON file; autotune sweeps (steps per epoch, blocks per SM) pairs with
+a sort before every epoch.
 """
 from __future__ import annotations
 
@@ -23,7 +26,7 @@ import time
 import numpy as np
 
 from . import _lib
-from .fields import STORAGE, FieldLibrary
+from .fields import C_LIGHT, M_P, STORAGE, FieldLibrary
 
 KEYS = ("x1", "x2", "x3", "p1", "p2", "p3")
 
@@ -44,11 +47,13 @@ class Batch:
         self.campaigns = {}
 
     def add(self, field: FieldLibrary, state: dict, dt: float, nsteps: int, stride: int, periodic: bool = True,
-            cache=None, ring: bool = False, deaths=None, alive=None, mom_cache=None) -> int:
+            cache=None, ring: bool = False, deaths=None, alive=None, mom_cache=None, sort_every: int = 1) -> int:
         """Add a campaign; state: SI arrays x1..p3 (numpy or CUDA tensors);
         cache: CUDA float32 tensor [rows][n] for the mu rows (or None);
         mom_cache: CUDA float32 tensor [rows][3][n_mom] that receives the
-        momenta of particles 0 .. n_mom-1 at every save (needs cache)."""
+        momenta of particles 0 .. n_mom-1 at every save (needs cache);
+        sort_every: re-sort the campaign by brick before every sort_every-th
+        epoch it runs (see sort_cadence for a choice by particle speed)."""
         import torch
 
         n = int(len(state["x1"]))
@@ -69,7 +74,7 @@ class Batch:
                               int(cache is not None and cache.dtype == torch.float64), n,
                               *[st[k].data_ptr() for k in KEYS], al.data_ptr(),
                               cache.data_ptr() if cache is not None else None,
-                              int(cache.shape[0]) if cache is not None else 0, int(bool(ring)), 0,
+                              int(cache.shape[0]) if cache is not None else 0, int(bool(ring)), int(sort_every),
                               deaths.data_ptr() if deaths is not None else None,
                               mom_cache.data_ptr() if mom_cache is not None else None, n_mom)
         cid = C.c_int()
@@ -217,7 +222,7 @@ class ReferenceBatch:
 # --------------------------------------------------------------------------
 # autotuner
 # --------------------------------------------------------------------------
-CANDIDATES = ((64, 2), (128, 2), (32, 2), (64, 1), (64, 3))
+CANDIDATES = ((64, 2), (128, 2), (32, 2), (16, 2), (64, 1), (64, 3))
 
 
 def _cache_path():
@@ -276,3 +281,114 @@ def autotune(campaigns, storage: str, capacity: int, epochs: int = 2, candidates
     except Exception:
         pass
     return best, timings
+
+
+# --------------------------------------------------------------------------
+# sort cadence by particle speed
+# --------------------------------------------------------------------------
+def cells_per_step(field: FieldLibrary, state: dict, dt: float) -> float:
+    """Distance the campaign's particles cover per step, in cells, from the
+    speed of its first particle (a campaign is mono-energetic)."""
+    pm = math.sqrt(sum(float(state[k][0]) ** 2 for k in ("p1", "p2", "p3")))
+    gamma = math.sqrt(1.0 + (pm / (M_P * C_LIGHT)) ** 2)
+    g = field.grid
+    return pm / (gamma * M_P) * dt / min(g.dx, g.dy, g.dz)
+
+
+def speed_class(cps: float) -> int:
+    """Campaigns whose particles cover cells per step within a factor of 2
+    share a class (and a tuned sort cadence)."""
+    return int(math.floor(math.log2(max(cps, 1e-9))))
+
+
+def sort_cadence(cps: float) -> int:
+    """Default re-sort cadence, in steps, for particles covering cps cells per
+    step, from the cadences tune_batch picked on a B200 at 256^3 (FP32 bricks,
+    64 steps per gyroperiod): 64 steps at 1 GeV (0.1 cell per step) and 10 GeV
+    (1 cell; 32-128 within 3 %), 16 steps at 100 GeV (10 cells, 54 % faster
+    than 64): the particles of a warp leave each other's bricks within a few
+    steps, and a sort brings them back together."""
+    if cps >= 4.0:
+        return 16
+    if cps >= 2.0:
+        return 32
+    return 64
+
+
+def _trial(campaigns, storage, capacity, K, bps, sort_every, steps):
+    """Particle-steps/s of `steps` steps (rounded to whole epochs) of a fresh
+    batch of the campaigns, after one warm-up epoch."""
+    import torch
+
+    b = Batch(capacity, max_campaigns=max(len(campaigns), 1), storage=storage, steps_per_epoch=K, sort=True,
+              blocks_per_sm=bps)
+    for c, se in zip(campaigns, sort_every):
+        b.add(c["field"], c["state"], c["dt"], c["nsteps"], c["stride"], c.get("periodic", True), sort_every=se)
+    epochs = max(1, steps // K)
+    b.run(1)  # warm-up (graph capture)
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    b.run(epochs)
+    torch.cuda.synchronize()
+    el = time.perf_counter() - t0
+    b.close()
+    return sum(len(c["state"]["x1"]) for c in campaigns) * K * epochs / el
+
+
+def tune_batch(campaigns, storage: str, capacity: int, cadences=(16, 32, 64, 128), blocks=(1, 2, 3),
+               steps: int = 256, use_cache: bool = True) -> dict:
+    """Launch shape and per-campaign sort cadence of a batch.
+
+    1. Campaigns are grouped by speed class.  For each class alone, every
+       cadence in `cadences` is timed as an epoch of that many steps with a
+       sort before each; the fastest is the class's cadence.
+    2. The batch's steps per epoch K is the shortest cadence picked; each
+       campaign re-sorts every (its class's cadence / K) epochs.
+    3. Resident blocks per SM of the persistent kernel: each of `blocks` is
+       timed on the whole batch with those cadences.
+    Every trial runs `steps` steps (whole epochs) of a fresh batch without
+    caches.  The result is cached in a JSON file keyed by device, storage,
+    particle count, grid and speed classes.  Returns {"K", "blocks_per_sm",
+    "sort_every" (one per campaign, in epochs), "cadence_steps" (per class),
+    "timings"}."""
+    n_total = sum(len(c["state"]["x1"]) for c in campaigns)
+    grid_n = max(c["field"].grid.nx for c in campaigns)
+    cls = [speed_class(cells_per_step(c["field"], c["state"], c["dt"])) for c in campaigns]
+    key = tune_key(storage, n_total, grid_n) + "|classes" + ",".join(str(v) for v in sorted(set(cls)))
+    path = _cache_path()
+    table = {}
+    if use_cache and os.path.exists(path):
+        try:
+            table = json.load(open(path))
+        except Exception:
+            table = {}
+    if key in table and "cadence_steps" in table[key]:
+        hit = table[key]
+        cad = {int(k): int(v) for k, v in hit["cadence_steps"].items()}
+        K = int(hit["K"])
+        return {"K": K, "blocks_per_sm": int(hit["blocks_per_sm"]), "sort_every": [cad[c] // K for c in cls],
+                "cadence_steps": cad, "timings": hit["timings"], "cached": True}
+    timings = {}
+    cad = {}
+    for c in sorted(set(cls)):
+        sub = [campaigns[i] for i in range(len(campaigns)) if cls[i] == c]
+        rates = {}
+        for cs in cadences:
+            rates[cs] = _trial(sub, storage, capacity, cs, 2, [1] * len(sub), steps)
+            timings[f"class{c}:{cs}"] = rates[cs]
+        cad[c] = max(rates, key=rates.get)
+    K = min(cad.values())
+    sort_every = [cad[c] // K for c in cls]
+    rates = {}
+    for bps in blocks:
+        rates[bps] = _trial(campaigns, storage, capacity, K, bps, sort_every, steps)
+        timings[f"all:{K}x{bps}"] = rates[bps]
+    bps = max(rates, key=rates.get)
+    table[key] = {"K": K, "blocks_per_sm": bps, "cadence_steps": {str(k): v for k, v in cad.items()},
+                  "timings": timings}
+    try:
+        json.dump(table, open(path, "w"), indent=1)
+    except Exception:
+        pass
+    return {"K": K, "blocks_per_sm": bps, "sort_every": sort_every, "cadence_steps": cad, "timings": timings,
+            "cached": False}

@@ -19,13 +19,11 @@ struct pt_batch {
     int K = 64;
     int sort = 1;
     int grid = 148;
-    BatchStateDev buf[2]{};   // ping-pong state
-    int cur = 0;              // buffer holding the current state
+    BatchStateDev buf[2]{};   // ping-pong state (each campaign's current buffer is its device-side par)
     int sort_grid = 1;        // blocks of the sort's tile kernels (a power of two >= the tiles, with slack)
     BatchCampaignDev* d_camps = nullptr;
     std::vector<BatchCampaignDev> h_camps;
     std::vector<const pt_field*> fields;
-    std::vector<int> home;    // buffer holding a paused campaign's slots (the sort moves running ones only)
     BatchTile* d_tiles = nullptr;
     int* d_ntiles = nullptr;
     int* d_counter = nullptr;
@@ -37,7 +35,7 @@ struct pt_batch {
     int smem_words = 1;
     std::vector<std::pair<int64_t, int64_t>> free_ranges;  // (start, length), sorted
     cudaStream_t cap_stream = nullptr;
-    cudaGraphExec_t graph[2] = {nullptr, nullptr};
+    cudaGraphExec_t graph = nullptr;
     bool graph_dirty = true;
     // pinned staging of the campaign and tile tables (rebuild_tables)
     static constexpr int kStages = 4;
@@ -82,11 +80,10 @@ int alloc_state(BatchStateDev& s, int64_t cap)
 
 void drop_graphs(pt_batch* b)
 {
-    for (auto& g : b->graph)
-        if (g) {
-            cudaGraphExecDestroy(g);
-            g = nullptr;
-        }
+    if (b->graph) {
+        cudaGraphExecDestroy(b->graph);
+        b->graph = nullptr;
+    }
     b->graph_dirty = true;
 }
 
@@ -99,7 +96,7 @@ void drop_graphs(pt_batch* b)
 // staging buffers; one is written again only after its upload has run.
 int rebuild_tables(pt_batch* b, int fresh)
 {
-    int64_t key = 0, dense = 0;
+    int64_t key = 0;
     std::vector<BatchTile>& tiles = b->tile_scratch;
     tiles.clear();
     for (int c = 0; c < b->max_camps; ++c) {
@@ -107,8 +104,6 @@ int rebuild_tables(pt_batch* b, int fresh)
         if (!C.active || !C.running) continue;
         C.key_base = key;
         key += C.n_bricks + 1;
-        C.shift = C.slot0 - dense;
-        dense += C.n;
         for (int64_t s = 0; s < C.n; s += kBatchTile)
             tiles.push_back(BatchTile{c, (int32_t)std::min<int64_t>(kBatchTile, C.n - s), C.slot0 + s});
     }
@@ -183,37 +178,36 @@ int rebuild_tables(pt_batch* b, int fresh)
     return PT_OK;
 }
 
+// One epoch: re-sort the campaigns due for it (each into its other buffer),
+// push every running campaign K steps from its own buffer, advance the
+// device-side counters.  Every decision is made on the device from the
+// campaign table, so one captured graph replays every epoch.
 int enqueue_epoch(pt_batch* b, cudaStream_t s)
 {
-    int cur = b->cur;
     if (b->sort) {
-        int rc = launch_batch_sort(b->d_camps, b->d_tiles, b->d_ntiles, b->sort_grid, b->buf[cur], b->buf[1 - cur],
-                                   b->keys, b->hist, b->cursor, b->d_m, b->hist_cap, b->ctx->num_sms, s);
+        int rc = launch_batch_sort(b->d_camps, b->max_camps, b->d_tiles, b->d_ntiles, b->sort_grid, b->buf[0],
+                                   b->buf[1], b->keys, b->hist, b->cursor, b->d_m, b->hist_cap, b->ctx->num_sms, s);
         if (rc) return rc;
-        cur = 1 - cur;
     }
-    BatchLaunch L{b->d_camps, b->d_tiles, b->d_ntiles, b->d_counter, b->buf[cur],
+    BatchLaunch L{b->d_camps, b->d_tiles, b->d_ntiles, b->d_counter, {b->buf[0], b->buf[1]}, b->sort,
                   field_layout(b->storage), b->smem_words, b->grid};
     int rc = launch_push_batch(L, s);
     if (rc) return rc;
-    return launch_batch_epoch_end(b->d_camps, b->max_camps, b->d_counter, s);
+    return launch_batch_epoch_end(b->d_camps, b->max_camps, b->d_counter, b->sort, s);
 }
 
-int capture(pt_batch* b, int parity)
+int capture(pt_batch* b)
 {
-    const int saved = b->cur;
-    b->cur = parity;
     cudaGraph_t g = nullptr;
     PT_CUDA(cudaStreamBeginCapture(b->cap_stream, cudaStreamCaptureModeThreadLocal));
     int rc = enqueue_epoch(b, b->cap_stream);
     cudaError_t e = cudaStreamEndCapture(b->cap_stream, &g);
-    b->cur = saved;
     if (rc) {
         if (g) cudaGraphDestroy(g);
         return rc;
     }
     if (e != cudaSuccess) return cuda_fail(e, "cudaStreamEndCapture");
-    e = cudaGraphInstantiate(&b->graph[parity], g, 0);
+    e = cudaGraphInstantiate(&b->graph, g, 0);
     cudaGraphDestroy(g);
     if (e != cudaSuccess) return cuda_fail(e, "cudaGraphInstantiate");
     return PT_OK;
@@ -243,7 +237,6 @@ int pt_batch_create(pt_ctx* ctx, int64_t capacity, int max_campaigns, int storag
     b->sort = sort ? 1 : 0;
     b->h_camps.assign(max_campaigns, BatchCampaignDev{});
     b->fields.assign(max_campaigns, nullptr);
-    b->home.assign(max_campaigns, 0);
     b->free_ranges.push_back({0, capacity});
     int rc = alloc_state(b->buf[0], capacity);
     if (!rc && b->sort) rc = alloc_state(b->buf[1], capacity);
@@ -302,6 +295,7 @@ int pt_batch_add(pt_ctx* ctx, pt_batch* b, const pt_campaign_desc* d, int* id)
         return fail(PT_ERR_ARG, "a non-ring cache needs one row per save");
     if (d->d_mom_cache && (!d->d_cache || d->n_mom < 1 || d->n_mom > d->n))
         return fail(PT_ERR_ARG, "a momenta cache needs the mu cache and 1 <= n_mom <= n");
+    if (d->sort_every < 0) return fail(PT_ERR_ARG, "sort_every must be >= 0");
     int c = -1;
     for (int i = 0; i < b->max_camps; ++i)
         if (!b->h_camps[i].active) {
@@ -322,7 +316,8 @@ int pt_batch_add(pt_ctx* ctx, pt_batch* b, const pt_campaign_desc* d, int* id)
                                         [](const std::pair<int64_t, int64_t>& r) { return r.second == 0; }),
                          b->free_ranges.end());
     cudaStream_t s = ctx->stream;
-    int rc = launch_batch_import(b->buf[b->cur], slot0, d->n, f, d->d_x1, d->d_x2, d->d_x3, d->d_p1, d->d_p2,
+    // a new campaign starts in buffer 0
+    int rc = launch_batch_import(b->buf[0], slot0, d->n, f, d->d_x1, d->d_x2, d->d_x3, d->d_p1, d->d_p2,
                                  d->d_p3, d->d_alive, ctx->num_sms, s);
     if (rc) return rc;
     BatchCampaignDev C{};
@@ -362,10 +357,12 @@ int pt_batch_add(pt_ctx* ctx, pt_batch* b, const pt_campaign_desc* d, int* id)
     C.step = 0;
     C.K = b->K;
     C.n_bricks = (f->n_nodes + 511) / 512;
+    C.epochs = 0;
+    C.sort_every = b->sort ? std::max(d->sort_every, 1) : 0;
+    C.par = 0;
     C.active = 1;
     C.running = 1;
     b->h_camps[c] = C;
-    b->home[c] = b->cur;
     b->fields[c] = f;
     const int words = (int)(g.nx + g.ny + g.nz);
     if (words > b->smem_words) {
@@ -404,21 +401,16 @@ int pt_batch_run(pt_ctx* ctx, pt_batch* b, int64_t epochs, int use_graph)
     if (use_graph) {
         if (b->graph_dirty) {
             drop_graphs(b);
-            int rc = capture(b, 0);
-            if (!rc && b->sort) rc = capture(b, 1);
+            int rc = capture(b);
             if (rc) return rc;
             b->graph_dirty = false;
         }
-        for (int64_t e = 0; e < epochs; ++e) {
-            PT_CUDA(cudaGraphLaunch(b->graph[b->sort ? b->cur : 0], s));
-            if (b->sort) b->cur = 1 - b->cur;
-        }
+        for (int64_t e = 0; e < epochs; ++e) PT_CUDA(cudaGraphLaunch(b->graph, s));
         return PT_OK;
     }
     for (int64_t e = 0; e < epochs; ++e) {
         int rc = enqueue_epoch(b, s);
         if (rc) return rc;
-        if (b->sort) b->cur = 1 - b->cur;
     }
     return PT_OK;
 }
@@ -434,31 +426,13 @@ int pt_batch_set_running(pt_ctx* ctx, pt_batch* b, const int* ids, int n_ids)
         want[id] = 1;
     }
     bool changed = false;
-    cudaStream_t s = ctx->stream;
     for (int c = 0; c < b->max_camps; ++c) {
         BatchCampaignDev& C = b->h_camps[c];
         if (!C.active || (int)want[c] == C.running) continue;
-        changed = true;
-        if (!want[c]) {
-            // paused: its slots stay in the buffer of the current parity
-            b->home[c] = b->cur;
-        } else if (b->sort && b->home[c] != b->cur) {
-            // resumed after the epochs flipped the parity: bring its slots over
-            const BatchStateDev& from = b->buf[b->home[c]];
-            const BatchStateDev& to = b->buf[b->cur];
-            const int64_t cap = b->cap, o = C.slot0, n = C.n;
-            for (int k = 0; k < 3; ++k) {
-                PT_CUDA(cudaMemcpyAsync(to.x + k * cap + o, from.x + k * cap + o, sizeof(double) * n,
-                                        cudaMemcpyDeviceToDevice, s));
-                PT_CUDA(cudaMemcpyAsync(to.p + k * cap + o, from.p + k * cap + o, sizeof(float) * n,
-                                        cudaMemcpyDeviceToDevice, s));
-            }
-            PT_CUDA(cudaMemcpyAsync(to.p2 + o, from.p2 + o, sizeof(double) * n, cudaMemcpyDeviceToDevice, s));
-            PT_CUDA(cudaMemcpyAsync(to.pid + o, from.pid + o, sizeof(int32_t) * n, cudaMemcpyDeviceToDevice, s));
-            PT_CUDA(cudaMemcpyAsync(to.alive + o, from.alive + o, n, cudaMemcpyDeviceToDevice, s));
-        }
-        if (want[c]) b->home[c] = b->cur;
+        // a paused campaign's slots stay in the buffer they are in (its
+        // device-side par); neither the sort nor the push touches them
         C.running = want[c];
+        changed = true;
     }
     return changed ? rebuild_tables(b, -1) : PT_OK;
 }
@@ -479,9 +453,8 @@ int pt_batch_export(pt_ctx* ctx, pt_batch* b, int id, double* x1, double* x2, do
     if (id < 0 || id >= b->max_camps || !b->h_camps[id].active) return fail(PT_ERR_ARG, "no such campaign");
     if (!(x1 && x2 && x3 && p1 && p2 && p3 && alive)) return fail(PT_ERR_ARG, "null state");
     const BatchCampaignDev& C = b->h_camps[id];
-    const int buf = C.running ? b->cur : b->home[id];
-    return launch_batch_export(b->buf[buf], C.slot0, C.n, b->fields[id], x1, x2, x3, p1, p2, p3, alive,
-                               ctx->num_sms, ctx->stream);
+    return launch_batch_export(b->buf[0], b->buf[1], b->d_camps, id, C.slot0, C.n, b->fields[id], x1, x2, x3, p1, p2,
+                               p3, alive, ctx->num_sms, ctx->stream);
 }
 
 int pt_batch_destroy(pt_batch* b)

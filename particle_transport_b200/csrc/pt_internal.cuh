@@ -183,16 +183,28 @@ int launch_push_fast(const PushArgsFast& a, cudaStream_t s);
 // ---------------------------------------------------------------- batches
 // A batch is an arena of particle slots shared by many campaigns (each a
 // contiguous slot range with its own field, dt, step counter and cache).
+// Campaigns sort on their own cadence (every sort_every-th epoch they run),
+// so each keeps its slots in its own buffer of the ping-pong pair (par); the
+// fields step, epochs and par are owned by the device (advanced by the
+// epochs), the others by the host.
 struct BatchCampaignDev {
-    PushArgsFast a;    // per-campaign constants (state pointers unused)
-    int64_t slot0, n;  // slot range in the arena
-    int64_t step, K;   // next step; steps per epoch
-    int64_t key_base;  // first sort bucket
-    int64_t n_bricks;  // bricks of the campaign's field (bucket n_bricks = dead)
-    int64_t shift;     // arena slot = dense sort position + shift
-    int32_t active;    // holds particles
-    int32_t running;   // pushed, sorted and stepped by the epochs (0: paused, slots held as they are)
+    PushArgsFast a;      // per-campaign constants (state pointers unused)
+    int64_t slot0, n;    // slot range in the arena (the same in both buffers)
+    int64_t step, K;     // next step; steps per epoch
+    int64_t key_base;    // first sort bucket
+    int64_t n_bricks;    // bricks of the campaign's field (bucket n_bricks = dead)
+    int64_t dense_base;  // sort position of the campaign's first bucket in the current epoch
+    int64_t epochs;      // epochs run so far
+    int32_t sort_every;  // re-sorted before every sort_every-th epoch it runs (0: never)
+    int32_t par;         // buffer (0/1) holding the campaign's slots
+    int32_t active;      // holds particles
+    int32_t running;     // pushed, sorted and stepped by the epochs (0: paused, slots held as they are)
 };
+// Whether campaign C is re-sorted before its next epoch.
+__host__ __device__ inline bool batch_sort_due(const BatchCampaignDev& C)
+{
+    return C.active && C.running && C.sort_every > 0 && C.step < C.a.nsteps && C.epochs % C.sort_every == 0;
+}
 constexpr int kBatchTile = 256;  // particles per tile of a batch (= block size of its kernels)
 struct BatchTile {
     int32_t campaign;
@@ -212,7 +224,8 @@ struct BatchLaunch {
     const BatchTile* tiles;
     const int* n_tiles;
     int* tile_counter;
-    BatchStateDev st;
+    BatchStateDev st[2];
+    int sorted;        // the epoch re-sorted the due campaigns into their other buffer
     int layout;        // LAYOUT_* shared by the batch's fields
     int smem_words;    // max (nx + ny + nz) over the batch's fields
     int grid;
@@ -220,20 +233,22 @@ struct BatchLaunch {
 int launch_push_batch(const BatchLaunch& L, cudaStream_t s);
 int launch_batch_apply(BatchCampaignDev* camps, const BatchCampaignDev* staged, int n_camps, int fresh,
                        cudaStream_t s);
-int launch_batch_epoch_end(BatchCampaignDev* camps, int n_camps, int* tile_counter, cudaStream_t s);
+int launch_batch_epoch_end(BatchCampaignDev* camps, int n_camps, int* tile_counter, int sorted, cudaStream_t s);
 // buckets per tile of the two-level bucket scan of the brick sorts, and the
 // number of tile offsets that follow the cursor array of m buckets
 constexpr int64_t kSortScanTile = 2048;
 inline int64_t sort_scan_tiles(int64_t m) { return (m + kSortScanTile - 1) / kSortScanTile; }
 // cursor must hold max_buckets + sort_scan_tiles(max_buckets) entries
-int launch_batch_sort(const BatchCampaignDev* camps, const BatchTile* tiles, const int* n_tiles, int grid,
-                      BatchStateDev from, BatchStateDev to, uint32_t* keys, uint32_t* hist, uint32_t* cursor,
+int launch_batch_sort(BatchCampaignDev* camps, int n_camps, const BatchTile* tiles, const int* n_tiles, int grid,
+                      BatchStateDev st0, BatchStateDev st1, uint32_t* keys, uint32_t* hist, uint32_t* cursor,
                       const int64_t* d_m, int64_t max_buckets, int num_sms, cudaStream_t s);
 int launch_batch_import(BatchStateDev st, int64_t slot0, int64_t n, const pt_field* f, const double* x1,
                         const double* x2, const double* x3, const double* p1, const double* p2, const double* p3,
                         const uint8_t* alive, int num_sms, cudaStream_t s);
-int launch_batch_export(BatchStateDev st, int64_t slot0, int64_t n, const pt_field* f, double* x1, double* x2,
-                        double* x3, double* p1, double* p2, double* p3, uint8_t* alive, int num_sms, cudaStream_t s);
+// reads the campaign's buffer parity from camps[id] on the device
+int launch_batch_export(BatchStateDev st0, BatchStateDev st1, const BatchCampaignDev* camps, int id, int64_t slot0,
+                        int64_t n, const pt_field* f, double* x1, double* x2, double* x3, double* p1, double* p2,
+                        double* p3, uint8_t* alive, int num_sms, cudaStream_t s);
 int launch_fast_import(pt_fast_state* st, const pt_field* f, const double* x1, const double* x2, const double* x3,
                        const double* p1, const double* p2, const double* p3, const uint8_t* alive, cudaStream_t s);
 int launch_fast_export(const pt_fast_state* st, const pt_field* f, double* x1, double* x2, double* x3, double* p1,

@@ -692,7 +692,7 @@ __global__ void __launch_bounds__(256, 1) push_batch_kernel(BatchLaunch L)
 {
     extern __shared__ uint32_t s_offs[];
     __shared__ PushArgsFast s_a;
-    __shared__ int s_tile, s_camp;
+    __shared__ int s_tile, s_camp, s_buf;
     __shared__ const uint32_t* s_loaded;
     __shared__ long long s_begin, s_end;
     if (threadIdx.x == 0) {
@@ -700,7 +700,7 @@ __global__ void __launch_bounds__(256, 1) push_batch_kernel(BatchLaunch L)
         s_loaded = nullptr;
     }
     const int n_tiles = *L.n_tiles;
-    const int64_t cap = L.st.cap;
+    const int64_t cap = L.st[0].cap;
     for (;;) {
         __syncthreads();
         if (threadIdx.x == 0) s_tile = atomicAdd(L.tile_counter, 1);
@@ -716,6 +716,8 @@ __global__ void __launch_bounds__(256, 1) push_batch_kernel(BatchLaunch L)
             if (threadIdx.x == 0) {
                 s_begin = C->step;
                 s_end = min(C->step + C->K, C->a.nsteps);
+                // a campaign re-sorted in this epoch now sits in its other buffer
+                s_buf = (L.sorted && batch_sort_due(*C)) ? 1 - C->par : C->par;
             }
             __syncthreads();
             if (threadIdx.x == 0) s_camp = T.campaign;
@@ -732,38 +734,49 @@ __global__ void __launch_bounds__(256, 1) push_batch_kernel(BatchLaunch L)
             const uint32_t* ox = s_offs;
             const uint32_t* oy = s_offs + s_a.fld.nx;
             const uint32_t* oz = s_offs + s_a.fld.nx + s_a.fld.ny;
+            const BatchStateDev st = s_buf ? L.st[1] : L.st[0];
             const int64_t slot = T.begin + threadIdx.x;
-            double x = L.st.x[slot], y = L.st.x[cap + slot], z = L.st.x[2 * cap + slot];
-            float px = L.st.p[slot], py = L.st.p[cap + slot], pz = L.st.p[2 * cap + slot];
-            double P2 = L.st.p2[slot];
-            bool al = L.st.alive[slot] != 0;
-            advance_particle<LAYOUT>(x, y, z, px, py, pz, P2, al, L.st.pid[slot], s_a, ox, oy, oz, sb, se);
-            L.st.x[slot] = x; L.st.x[cap + slot] = y; L.st.x[2 * cap + slot] = z;
-            L.st.p[slot] = px; L.st.p[cap + slot] = py; L.st.p[2 * cap + slot] = pz;
-            L.st.p2[slot] = P2;
-            L.st.alive[slot] = al ? 1 : 0;
+            double x = st.x[slot], y = st.x[cap + slot], z = st.x[2 * cap + slot];
+            float px = st.p[slot], py = st.p[cap + slot], pz = st.p[2 * cap + slot];
+            double P2 = st.p2[slot];
+            bool al = st.alive[slot] != 0;
+            advance_particle<LAYOUT>(x, y, z, px, py, pz, P2, al, st.pid[slot], s_a, ox, oy, oz, sb, se);
+            st.x[slot] = x; st.x[cap + slot] = y; st.x[2 * cap + slot] = z;
+            st.p[slot] = px; st.p[cap + slot] = py; st.p[2 * cap + slot] = pz;
+            st.p2[slot] = P2;
+            st.alive[slot] = al ? 1 : 0;
         }
     }
 }
 
-__global__ void batch_epoch_end_kernel(BatchCampaignDev* camps, int n, int* tile_counter)
+__global__ void batch_epoch_end_kernel(BatchCampaignDev* camps, int n, int* tile_counter, int sorted)
 {
     const int c = blockIdx.x * blockDim.x + threadIdx.x;
-    if (c < n && camps[c].active && camps[c].running)
-        camps[c].step = min(camps[c].step + camps[c].K, camps[c].a.nsteps);
+    if (c < n && camps[c].active && camps[c].running) {
+        BatchCampaignDev& C = camps[c];
+        if (sorted && batch_sort_due(C)) C.par ^= 1;
+        C.epochs += 1;
+        C.step = min(C.step + C.K, C.a.nsteps);
+    }
     if (c == 0) *tile_counter = 0;
 }
 
-// Install a new campaign table uploaded by the host while keeping the step
-// counter of every campaign that was already running on the device (the
-// host's copy of it is stale); `fresh` takes the table's step (0).
+// Install a new campaign table uploaded by the host while keeping the fields
+// the epochs advance on the device (step, epochs, buffer parity) of every
+// campaign already in the batch -- the host's copies of them are stale;
+// `fresh`, a campaign just added, takes the table's (0, 0, buffer 0).
 __global__ void batch_apply_kernel(BatchCampaignDev* camps, const BatchCampaignDev* __restrict__ staged, int n,
                                    int fresh)
 {
     const int c = blockIdx.x * blockDim.x + threadIdx.x;
     if (c >= n) return;
     BatchCampaignDev v = staged[c];
-    if (c != fresh && v.active && camps[c].active) v.step = camps[c].step;
+    const BatchCampaignDev& old = camps[c];
+    if (c != fresh && v.active && old.active) {
+        v.step = old.step;
+        v.epochs = old.epochs;
+        v.par = old.par;
+    }
     camps[c] = v;
 }
 
@@ -774,27 +787,31 @@ __global__ void zero_counted_kernel(uint32_t* a, const int64_t* m)
         a[i] = 0u;
 }
 
-// Sort key of every particle of a running campaign -- the slots the tile
-// table covers, one block per tile: the campaign's first bucket + the brick
-// of the particle's cell (the campaign's dead bucket for dead particles).
-// Free slots and paused campaigns hold no tiles and take no part, so the
-// cost follows the particles in flight, not the arena's capacity.
+// Sort key of every particle of a campaign due for a re-sort -- the slots
+// the tile table covers, one block per tile: the campaign's first bucket +
+// the brick of the particle's cell (the campaign's dead bucket for dead
+// particles).  Free slots and paused campaigns hold no tiles, and campaigns
+// not due skip their tiles, so the cost follows the particles sorted, not
+// the arena's capacity.
 __global__ void __launch_bounds__(kBatchTile) batch_key_kernel(const BatchCampaignDev* __restrict__ camps,
                                                                const BatchTile* __restrict__ tiles,
-                                                               const int* __restrict__ n_tiles, BatchStateDev st,
-                                                               uint32_t* __restrict__ keys, uint32_t* __restrict__ hist)
+                                                               const int* __restrict__ n_tiles, BatchStateDev st0,
+                                                               BatchStateDev st1, uint32_t* __restrict__ keys,
+                                                               uint32_t* __restrict__ hist)
 {
     const int lane = threadIdx.x & 31;
     const unsigned lt = (1u << lane) - 1u;
-    const int64_t cap = st.cap;
+    const int64_t cap = st0.cap;
     const int nt = *n_tiles;
     for (int t = blockIdx.x; t < nt; t += gridDim.x) {
         const BatchTile T = tiles[t];
+        const BatchCampaignDev& C = camps[T.campaign];
+        if (!batch_sort_due(C)) continue;  // uniform over the block
+        const BatchStateDev st = C.par ? st1 : st0;
         const bool valid = (int)threadIdx.x < T.count;
         const int64_t i = T.begin + threadIdx.x;
         uint32_t key = 0;
         if (valid) {
-            const BatchCampaignDev& C = camps[T.campaign];
             key = (uint32_t)(C.key_base + C.n_bricks);
             if (st.alive[i]) {
                 const int nx = (int)C.a.fld.nx, ny = (int)C.a.fld.ny, nz = (int)C.a.fld.nz;
@@ -814,19 +831,35 @@ __global__ void __launch_bounds__(kBatchTile) batch_key_kernel(const BatchCampai
     }
 }
 
+// Sort position of each due campaign's first bucket, read before the
+// scatter's cursor atomics move it: a campaign's particles land at
+// slot0 + (sort position - dense_base) in its other buffer.
+__global__ void batch_base_kernel(BatchCampaignDev* camps, int n, const uint32_t* __restrict__ cursor,
+                                  const uint32_t* __restrict__ tile_off)
+{
+    const int c = blockIdx.x * blockDim.x + threadIdx.x;
+    if (c >= n || !batch_sort_due(camps[c])) return;
+    const int64_t k = camps[c].key_base;
+    camps[c].dense_base = (int64_t)cursor[k] + tile_off[k / kScanTile];
+}
+
 __global__ void __launch_bounds__(kBatchTile) batch_scatter_kernel(const uint32_t* __restrict__ keys, uint32_t* cursor,
                                                                    const uint32_t* __restrict__ tile_off,
                                                                    const BatchCampaignDev* __restrict__ camps,
                                                                    const BatchTile* __restrict__ tiles,
                                                                    const int* __restrict__ n_tiles,
-                                                                   BatchStateDev from, BatchStateDev to)
+                                                                   BatchStateDev st0, BatchStateDev st1)
 {
     const int lane = threadIdx.x & 31;
     const unsigned lt = (1u << lane) - 1u;
-    const int64_t cap = from.cap;
+    const int64_t cap = st0.cap;
     const int nt = *n_tiles;
     for (int t = blockIdx.x; t < nt; t += gridDim.x) {
         const BatchTile T = tiles[t];
+        const BatchCampaignDev& C = camps[T.campaign];
+        if (!batch_sort_due(C)) continue;  // uniform over the block
+        const BatchStateDev from = C.par ? st1 : st0, to = C.par ? st0 : st1;
+        const int64_t base = C.slot0 - C.dense_base;
         const bool valid = (int)threadIdx.x < T.count;
         const unsigned act = __ballot_sync(0xffffffffu, valid);
         if (!valid) continue;
@@ -837,7 +870,7 @@ __global__ void __launch_bounds__(kBatchTile) batch_scatter_kernel(const uint32_
         uint32_t first = 0;
         if (lane == leader) first = atomicAdd(&cursor[key], (uint32_t)__popc(same)) + tile_off[key / kScanTile];
         first = __shfl_sync(same, first, leader);
-        const int64_t d = (int64_t)first + __popc(same & lt) + camps[T.campaign].shift;
+        const int64_t d = (int64_t)first + __popc(same & lt) + base;
         to.x[d] = from.x[i]; to.x[cap + d] = from.x[cap + i]; to.x[2 * cap + d] = from.x[2 * cap + i];
         to.p[d] = from.p[i]; to.p[cap + d] = from.p[cap + i]; to.p[2 * cap + d] = from.p[2 * cap + i];
         to.p2[d] = from.p2[i];
@@ -869,10 +902,12 @@ __global__ void batch_import_kernel(BatchStateDev st, int64_t slot0, int64_t n, 
     }
 }
 
-__global__ void batch_export_kernel(BatchStateDev st, int64_t slot0, int64_t n, double xmin, double ymin, double zmin,
+__global__ void batch_export_kernel(BatchStateDev st0, BatchStateDev st1, const BatchCampaignDev* __restrict__ camps,
+                                    int id, int64_t slot0, int64_t n, double xmin, double ymin, double zmin,
                                     double dx, double dy, double dz, double* x1, double* x2, double* x3, double* p1,
                                     double* p2, double* p3, uint8_t* alive)
 {
+    const BatchStateDev st = camps[id].par ? st1 : st0;
     const int64_t cap = st.cap;
     for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
         const int64_t s = slot0 + i;
@@ -896,9 +931,9 @@ int launch_push_batch(const BatchLaunch& L, cudaStream_t s)
                 : (L.layout == LAYOUT_BF16_XPAIR ? (void*)push_batch_kernel<LAYOUT_BF16_XPAIR>
                                                  : (void*)push_batch_kernel<LAYOUT_BF16>);
     if (smem > 48 * 1024) PT_CUDA(cudaFuncSetAttribute(kfn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-    if (L.layout == LAYOUT_F32) push_batch_kernel<LAYOUT_F32><<<L.grid, 256, smem, s>>>(L);
-    else if (L.layout == LAYOUT_BF16_XPAIR) push_batch_kernel<LAYOUT_BF16_XPAIR><<<L.grid, 256, smem, s>>>(L);
-    else push_batch_kernel<LAYOUT_BF16><<<L.grid, 256, smem, s>>>(L);
+    if (L.layout == LAYOUT_F32) push_batch_kernel<LAYOUT_F32><<<L.grid, kBatchTile, smem, s>>>(L);
+    else if (L.layout == LAYOUT_BF16_XPAIR) push_batch_kernel<LAYOUT_BF16_XPAIR><<<L.grid, kBatchTile, smem, s>>>(L);
+    else push_batch_kernel<LAYOUT_BF16><<<L.grid, kBatchTile, smem, s>>>(L);
     PT_CHECK_LAUNCH("push_batch_kernel");
     return PT_OK;
 }
@@ -911,22 +946,22 @@ int launch_batch_apply(BatchCampaignDev* camps, const BatchCampaignDev* staged, 
     return PT_OK;
 }
 
-int launch_batch_epoch_end(BatchCampaignDev* camps, int n_camps, int* tile_counter, cudaStream_t s)
+int launch_batch_epoch_end(BatchCampaignDev* camps, int n_camps, int* tile_counter, int sorted, cudaStream_t s)
 {
-    batch_epoch_end_kernel<<<(std::max(n_camps, 1) + 127) / 128, 128, 0, s>>>(camps, n_camps, tile_counter);
+    batch_epoch_end_kernel<<<(std::max(n_camps, 1) + 127) / 128, 128, 0, s>>>(camps, n_camps, tile_counter, sorted);
     PT_CHECK_LAUNCH("batch_epoch_end_kernel");
     return PT_OK;
 }
 
-int launch_batch_sort(const BatchCampaignDev* camps, const BatchTile* tiles, const int* n_tiles, int grid,
-                      BatchStateDev from, BatchStateDev to, uint32_t* keys, uint32_t* hist, uint32_t* cursor,
+int launch_batch_sort(BatchCampaignDev* camps, int n_camps, const BatchTile* tiles, const int* n_tiles, int grid,
+                      BatchStateDev st0, BatchStateDev st1, uint32_t* keys, uint32_t* hist, uint32_t* cursor,
                       const int64_t* d_m, int64_t max_buckets, int num_sms, cudaStream_t s)
 {
     const int zb = (int)std::min<int64_t>((max_buckets + 255) / 256, (int64_t)num_sms * 8);
     zero_counted_kernel<<<std::max(zb, 1), 256, 0, s>>>(hist, d_m);
     PT_CHECK_LAUNCH("zero_counted_kernel");
     const int gb = std::max(grid, 1);  // one block per tile of the table (tile-stride beyond)
-    batch_key_kernel<<<gb, kBatchTile, 0, s>>>(camps, tiles, n_tiles, from, keys, hist);
+    batch_key_kernel<<<gb, kBatchTile, 0, s>>>(camps, tiles, n_tiles, st0, st1, keys, hist);
     PT_CHECK_LAUNCH("batch_key_kernel");
     uint32_t* tile_off = cursor + max_buckets;
     const int64_t max_tiles = sort_scan_tiles(max_buckets);
@@ -935,7 +970,9 @@ int launch_batch_sort(const BatchCampaignDev* camps, const BatchTile* tiles, con
     PT_CHECK_LAUNCH("sort_scan_tiles_kernel");
     sort_scan_top_kernel<<<1, 1024, 0, s>>>(tile_off, max_tiles, d_m);
     PT_CHECK_LAUNCH("sort_scan_top_kernel");
-    batch_scatter_kernel<<<gb, kBatchTile, 0, s>>>(keys, cursor, tile_off, camps, tiles, n_tiles, from, to);
+    batch_base_kernel<<<(std::max(n_camps, 1) + 127) / 128, 128, 0, s>>>(camps, n_camps, cursor, tile_off);
+    PT_CHECK_LAUNCH("batch_base_kernel");
+    batch_scatter_kernel<<<gb, kBatchTile, 0, s>>>(keys, cursor, tile_off, camps, tiles, n_tiles, st0, st1);
     PT_CHECK_LAUNCH("batch_scatter_kernel");
     return PT_OK;
 }
@@ -952,13 +989,15 @@ int launch_batch_import(BatchStateDev st, int64_t slot0, int64_t n, const pt_fie
     return PT_OK;
 }
 
-int launch_batch_export(BatchStateDev st, int64_t slot0, int64_t n, const pt_field* f, double* x1, double* x2,
-                        double* x3, double* p1, double* p2, double* p3, uint8_t* alive, int num_sms, cudaStream_t s)
+int launch_batch_export(BatchStateDev st0, BatchStateDev st1, const BatchCampaignDev* camps, int id, int64_t slot0,
+                        int64_t n, const pt_field* f, double* x1, double* x2, double* x3, double* p1, double* p2,
+                        double* p3, uint8_t* alive, int num_sms, cudaStream_t s)
 {
     if (n <= 0) return PT_OK;
     const pt_grid& g = f->grid;
-    batch_export_kernel<<<grid_for(n, 256, num_sms), 256, 0, s>>>(st, slot0, n, g.xmin, g.ymin, g.zmin, g.dx, g.dy,
-                                                                 g.dz, x1, x2, x3, p1, p2, p3, alive);
+    batch_export_kernel<<<grid_for(n, 256, num_sms), 256, 0, s>>>(st0, st1, camps, id, slot0, n, g.xmin, g.ymin,
+                                                                 g.zmin, g.dx, g.dy, g.dz, x1, x2, x3, p1, p2, p3,
+                                                                 alive);
     PT_CHECK_LAUNCH("batch_export_kernel");
     return PT_OK;
 }

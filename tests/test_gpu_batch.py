@@ -12,7 +12,7 @@ import pytest
 
 from helpers import small_problem
 from particle_transport_b200 import runner as R
-from particle_transport_b200.batch import Batch, autotune
+from particle_transport_b200.batch import Batch, autotune, tune_batch
 from particle_transport_b200.fields import FieldLibrary
 from particle_transport_b200.particles import energy_to_gamma, init_particles
 from particle_transport_b200.time_units import reference_Omega0
@@ -53,14 +53,20 @@ def new_cache(torch, c):
                       dtype=torch.float32, device="cuda")
 
 
-@pytest.mark.parametrize("sort,graph,K", [(True, True, 64), (True, False, 32), (False, True, 50)])
-def test_batch_bit_identical_to_single_runs(cuda, sort, graph, K):
+@pytest.mark.parametrize("sort,graph,K,every", [(True, True, 64, (1, 1, 1, 1)), (True, False, 32, (1, 1, 1, 1)),
+                                               (False, True, 50, (1, 1, 1, 1)), (True, True, 16, (1, 3, 2, 5)),
+                                               (True, False, 16, (4, 1, 0, 2))])
+def test_batch_bit_identical_to_single_runs(cuda, sort, graph, K, every):
+    """Every campaign ends with the cache and state of its run alone, with a
+    sort before every epoch, on per-campaign cadences (each campaign then
+    holds its slots in its own buffer of the pair), or without sorting."""
     torch = cuda
     cs = campaigns(torch)
     ref = [run_alone(torch, c) for c in cs]
     b = Batch(5000, max_campaigns=8, steps_per_epoch=K, sort=sort)
     caches = [new_cache(torch, c) for c in cs]
-    ids = [b.add(c["field"], c["state"], c["dt"], c["nsteps"], c["stride"], cache=ch) for c, ch in zip(cs, caches)]
+    ids = [b.add(c["field"], c["state"], c["dt"], c["nsteps"], c["stride"], cache=ch, sort_every=e)
+           for c, ch, e in zip(cs, caches, every)]
     epochs = max(math.ceil(c["nsteps"] / K) for c in cs)
     b.run(epochs, use_graph=graph)
     for c, cid, ch, (mu_ref, st_ref) in zip(cs, ids, caches, ref):
@@ -191,3 +197,25 @@ def test_autotune_picks_a_candidate(cuda, tmp_path, monkeypatch):
     assert best in ((64, 2), (32, 1)) and len(timings) == 2
     best2, _ = autotune(cs, "brick_bf16", 5000, epochs=1, candidates=((64, 2), (32, 1)))
     assert best2 == best  # served from the cache file
+
+
+def test_tune_batch_picks_cadences(cuda, tmp_path, monkeypatch):
+    torch = cuda
+    monkeypatch.setenv("PTB200_TUNE_CACHE", str(tmp_path))
+    cs = campaigns(torch)
+    t = tune_batch(cs, "brick_bf16", 5000, cadences=(16, 32), blocks=(1, 2), steps=64)
+    assert t["K"] in (16, 32) and t["blocks_per_sm"] in (1, 2) and not t["cached"]
+    assert len(t["sort_every"]) == len(cs) and all(v >= 1 for v in t["sort_every"])
+    assert all(v in (16, 32) for v in t["cadence_steps"].values())
+    t2 = tune_batch(cs, "brick_bf16", 5000, cadences=(16, 32), blocks=(1, 2), steps=64)
+    assert t2["cached"] and t2["K"] == t["K"] and t2["sort_every"] == t["sort_every"]
+    # the tuned batch gives every campaign the result of its run alone
+    ref = [run_alone(torch, c) for c in cs]
+    b = Batch(5000, max_campaigns=8, steps_per_epoch=t["K"], blocks_per_sm=t["blocks_per_sm"])
+    caches = [new_cache(torch, c) for c in cs]
+    for c, ch, e in zip(cs, caches, t["sort_every"]):
+        b.add(c["field"], c["state"], c["dt"], c["nsteps"], c["stride"], cache=ch, sort_every=e)
+    b.run(max(math.ceil(c["nsteps"] / t["K"]) for c in cs))
+    for ch, (mu_ref, _) in zip(caches, ref):
+        assert np.array_equal(ch.cpu().numpy(), mu_ref, equal_nan=True)
+    b.close()
