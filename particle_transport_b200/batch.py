@@ -291,8 +291,13 @@ def cells_per_step(field: FieldLibrary, state: dict, dt: float) -> float:
     speed of its first particle (a campaign is mono-energetic)."""
     pm = math.sqrt(sum(float(state[k][0]) ** 2 for k in ("p1", "p2", "p3")))
     gamma = math.sqrt(1.0 + (pm / (M_P * C_LIGHT)) ** 2)
+    return cells_per_step_gamma(field, gamma, dt)
+
+
+def cells_per_step_gamma(field: FieldLibrary, gamma: float, dt: float) -> float:
+    """Distance a particle of Lorentz factor gamma covers per step, in cells."""
     g = field.grid
-    return pm / (gamma * M_P) * dt / min(g.dx, g.dy, g.dz)
+    return C_LIGHT * math.sqrt(max(1.0 - 1.0 / (gamma * gamma), 0.0)) * dt / min(g.dx, g.dy, g.dz)
 
 
 def speed_class(cps: float) -> int:

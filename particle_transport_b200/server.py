@@ -38,7 +38,7 @@ import numpy as np
 
 from . import _lib
 from . import stats as S
-from .batch import Batch, ReferenceBatch
+from .batch import Batch, ReferenceBatch, cells_per_step_gamma, sort_cadence
 from .fields import FieldLibrary, M_P, Q_E
 from .particles import energy_to_gamma, init_particles_device
 from .time_units import build_mu_edges_full, log_spaced_lag_steps, reference_Omega0
@@ -161,7 +161,10 @@ class CampaignServer:
         cache = torch.empty((nsave, spec.n_particles), dtype=torch.float32, device=self.device)
         n_dpp = min(spec.n_particles, max(0, spec.dpp_particles))
         mom = torch.empty((nsave, 3, n_dpp), dtype=torch.float32, device=self.device) if n_dpp else None
-        cid = self.batch.add(fl, st, dt, nsteps, stride, cache=cache, mom_cache=mom)
+        # re-sort cadence by particle speed: fast particles leave their
+        # bricks within a few steps (taken from the energy: no device read)
+        every = max(1, sort_cadence(cells_per_step_gamma(fl, g0, dt)) // self.K)
+        cid = self.batch.add(fl, st, dt, nsteps, stride, cache=cache, mom_cache=mom, sort_every=every)
         self._running_ids = None  # a new campaign runs until the next selection
         self.active[jid] = dict(spec=spec, cid=cid, cache=cache, mom=mom, nsteps=nsteps, nsave=nsave,
                                 arrival=arrival, admitted=time.perf_counter(), bytes=self.job_bytes(spec))

@@ -4,7 +4,7 @@ from types import SimpleNamespace
 
 import numpy as np
 
-from particle_transport_b200.batch import cells_per_step, sort_cadence, speed_class
+from particle_transport_b200.batch import cells_per_step, cells_per_step_gamma, sort_cadence, speed_class
 from particle_transport_b200.fields import C_LIGHT, M_P, Q_E
 from particle_transport_b200.particles import energy_to_gamma
 
@@ -17,6 +17,7 @@ def test_cells_per_step_of_a_proton():
     fld = SimpleNamespace(grid=SimpleNamespace(dx=1e5, dy=2e5, dz=3e5))
     v = C_LIGHT * math.sqrt(1 - 1 / g ** 2)
     assert math.isclose(cells_per_step(fld, state, 1e-3), v * 1e-3 / 1e5, rel_tol=1e-12)
+    assert math.isclose(cells_per_step_gamma(fld, g, 1e-3), v * 1e-3 / 1e5, rel_tol=1e-12)
 
 
 def test_speed_classes_and_default_cadence():
