@@ -107,7 +107,7 @@ using CacheSource = CacheSourceT<float>;
 size_t dmumu_slot_bytes(int64_t nsave, size_t mu_bytes, size_t idx_bytes, int n_bins, int nl_cap)
 {
     auto a16 = [](size_t v) { return (v + 15) & ~(size_t)15; };
-    return a16((size_t)nsave * mu_bytes) + a16((size_t)nsave * idx_bytes) +
+    return a16((size_t)(nsave + 1) * mu_bytes) + a16((size_t)nsave * idx_bytes) +
            a16(sizeof(int) * (size_t)(kStageWarps * (n_bins + 1) + n_bins + 2)) + a16(16 * (size_t)nl_cap);
 }
 
@@ -172,14 +172,15 @@ __global__ void __launch_bounds__(1024) dmumu_kernel(DmumuLaunch a, Src source)
     const int li = s_lane_lag[group * kWarp + lane];
     const bool lane_on = li >= 0;
     int64_t L = lane_on ? a.lags[li] : 0;
-    if (L < 1 || L >= a.nsave) L = a.nsave;  // reference: lag >= nsteps -> skipped
-    const int64_t lim = a.nsave - L;         // valid starts: s < lim
+    if (L < 1 || L >= a.nsave) L = a.nsave;  // reference: lag >= nsteps -> skipped (valid starts: s < nsave - L)
 
-    // slot layout: series[nsave] MuT | list[nsave] IdxT | whist[kStageWarps][nb+1] int
+    // slot layout: series[nsave + 1] MuT | list[nsave] IdxT | whist[kStageWarps][nb+1] int
     //              | cur[nb+2] int | tot_c[nl] u64 | tot_sd2[nl] f64 (per-particle totals over the bins)
+    // The series holds the finite mu values and NaN for the others, and
+    // series[nsave] = NaN: a lag partner past the end of the series reads it.
     unsigned char* sb = slot_base + (size_t)slot * a.slot_bytes;
     MuT* series = (MuT*)sb;
-    IdxT* list = (IdxT*)(sb + ((a.nsave * sizeof(MuT) + 15) & ~(size_t)15));
+    IdxT* list = (IdxT*)(sb + (((a.nsave + 1) * sizeof(MuT) + 15) & ~(size_t)15));
     int* whist = (int*)((unsigned char*)list + ((a.nsave * sizeof(IdxT) + 15) & ~(size_t)15));
     int* cur = whist + kStageWarps * (nb + 1);
     unsigned long long* tot_c = (unsigned long long*)((unsigned char*)whist +
@@ -209,18 +210,20 @@ __global__ void __launch_bounds__(1024) dmumu_kernel(DmumuLaunch a, Src source)
             const int64_t st_begin = (int64_t)wis * per, st_end = min(a.nsave, st_begin + per);
             int* my_hist = whist + wis * (nb + 1);
             for (int b = lane; b <= nb; b += kWarp) my_hist[b] = 0;
-            if (wis == 0)
+            if (wis == 0) {
                 for (int l = lane; l < nl; l += kWarp) {
                     tot_c[l] = 0ull;
                     tot_sd2[l] = 0.0;
                 }
+                if (lane == 0) series[a.nsave] = MuT(NAN);
+            }
             __syncwarp();
             for (int64_t s0 = st_begin; s0 < st_end; s0 += kWarp) {
                 const int64_t s = s0 + lane;
                 int b = -1;
                 if (s < st_end) {
                     const MuT v = source(p, s);
-                    series[s] = v;
+                    series[s] = isfinite(v) ? v : MuT(NAN);
                     if (s < scap) b = bin_of((double)v, s_edges, nb, a.bin_abs);
                 }
                 const unsigned active = __ballot_sync(0xffffffffu, b >= 0);
@@ -286,32 +289,34 @@ __global__ void __launch_bounds__(1024) dmumu_kernel(DmumuLaunch a, Src source)
         if (have) {
             long long my_c = 0;
             double my_sd2 = 0.0;
-            // starts and limits fit 32 bits (nsave < 2^31); so does a bin's count
-            const int lim32 = (int)lim;
+            // starts, lags and nsave fit 32 bits (nsave < 2^31); so does a bin's count
+            const unsigned n32 = (unsigned)a.nsave, L32 = (unsigned)L;
             for (int b = part; b <= nb; b += a.parts) {
                 const int e0 = cur[b], e1 = cur[b + 1];
                 int c = 0;
                 double sd0 = 0.0, sd1 = 0.0, sq0 = 0.0, sq1 = 0.0;
                 int e = e0;
+                // Branch-free pairs.  A start in the list has a finite mu; its
+                // partner series[s + L] is NaN when the particle's mu is not
+                // finite there, and s + L past the series end reads the NaN pad
+                // (idle lanes have L = nsave).  An invalid partner is replaced by
+                // the start's own value, so the pair adds +0 and 0 * 0 -- the
+                // sums are bit-identical to skipping it (they are never -0).
                 for (; e + 4 <= e1; e += 4) {
-                    int s_[4];
                     MuT a_[4], v_[4];
 #pragma unroll
                     for (int k = 0; k < 4; ++k) {
-                        s_[k] = (int)list[e + k];
-                        a_[k] = series[s_[k]];
-                        v_[k] = s_[k] < lim32 ? series[s_[k] + (int)L] : MuT(NAN);
+                        const unsigned s = (unsigned)list[e + k];
+                        a_[k] = series[s];
+                        v_[k] = series[min(s + L32, n32)];
                     }
 #pragma unroll
                     for (int k = 0; k < 4; k += 2) {
-                        // branch-free: an invalid pair adds 0 (and 0 * 0), which
-                        // leaves the sums bit-identical to skipping it
-                        double d0 = (double)v_[k] - (double)a_[k];
-                        double d1 = (double)v_[k + 1] - (double)a_[k + 1];
-                        const bool ok0 = isfinite(d0), ok1 = isfinite(d1);
-                        d0 = ok0 ? d0 : 0.0;
-                        d1 = ok1 ? d1 : 0.0;
+                        const bool ok0 = v_[k] == v_[k], ok1 = v_[k + 1] == v_[k + 1];
+                        const MuT w0 = ok0 ? v_[k] : a_[k], w1 = ok1 ? v_[k + 1] : a_[k + 1];
                         c += (int)ok0 + (int)ok1;
+                        const double d0 = (double)w0 - (double)a_[k];
+                        const double d1 = (double)w1 - (double)a_[k + 1];
                         sd0 += d0;
                         sq0 = fma(d0, d0, sq0);
                         sd1 += d1;
@@ -319,12 +324,11 @@ __global__ void __launch_bounds__(1024) dmumu_kernel(DmumuLaunch a, Src source)
                     }
                 }
                 for (; e < e1; ++e) {
-                    const int s = (int)list[e];
+                    const unsigned s = (unsigned)list[e];
                     const MuT av = series[s];
-                    const MuT vv = s < lim32 ? series[s + (int)L] : MuT(NAN);
-                    double d = (double)vv - (double)av;
-                    const bool ok = isfinite(d);
-                    d = ok ? d : 0.0;
+                    const MuT vv = series[min(s + L32, n32)];
+                    const bool ok = vv == vv;
+                    const double d = (double)(ok ? vv : av) - (double)av;
                     c += (int)ok;
                     sd0 += d;
                     sq0 = fma(d, d, sq0);
