@@ -152,5 +152,64 @@ __device__ __forceinline__ R phase_space_mu4(R xx, R yy, R zz, R px, R py, R pz,
     return v;
 }
 
+// B of the 8 corners of one cell as one record: corner-major in the order of
+// lerp8 (c000, c100, c010, c110, c001, c101, c011, c111), (Bx, By, Bz) within
+// a corner.  Indexed by the cell's base node (i0, j0, k0), so a sample reads
+// one contiguous 24-value record instead of 8 node records spread over 4 rows
+// of the grid.  The values and the arithmetic are those of sample().
+template <typename R>
+struct alignas(32) CellB {
+    R v[24];
+};
+
+template <typename R>
+__device__ __forceinline__ void load_cell(const CellB<R>* p, R out[24])
+{
+    if constexpr (sizeof(R) == 4) {
+        // three 32-byte read-only loads (the record is 96 bytes, 32-byte aligned)
+        const char* b = (const char*)p;
+#pragma unroll
+        for (int q = 0; q < 3; ++q) {
+            uint32_t w[8];
+            asm volatile("ld.global.nc.v8.u32 {%0, %1, %2, %3, %4, %5, %6, %7}, [%8];"
+                         : "=r"(w[0]), "=r"(w[1]), "=r"(w[2]), "=r"(w[3]), "=r"(w[4]), "=r"(w[5]), "=r"(w[6]),
+                           "=r"(w[7])
+                         : "l"(b + 32 * q));
+#pragma unroll
+            for (int k = 0; k < 8; ++k) out[8 * q + k] = __uint_as_float(w[k]);
+        }
+    } else {
+        const double2* b = (const double2*)p;
+#pragma unroll
+        for (int q = 0; q < 12; ++q) {
+            const double2 v = __ldg(b + q);
+            out[2 * q] = v.x;
+            out[2 * q + 1] = v.y;
+        }
+    }
+}
+
+// phase_space_mu() with B read from cell records
+template <typename R>
+__device__ __forceinline__ R phase_space_mu_cell(R xx, R yy, R zz, R px, R py, R pz,
+                                                 const CellB<R>* __restrict__ cells, const pt_grid& g)
+{
+    const R xmin = (R)g.xmin, ymin = (R)g.ymin, zmin = (R)g.zmin;
+    const R xmax = (R)g.xmax, ymax = (R)g.ymax, zmax = (R)g.zmax;
+    const R dx = (R)g.dx, dy = (R)g.dy, dz = (R)g.dz;
+    R v = R(NAN);
+    if (!(isnan(xx) || isnan(yy) || isnan(zz) || isnan(px) || isnan(py) || isnan(pz)) && xmin <= xx &&
+        xx <= xmax && ymin <= yy && yy <= ymax && zmin <= zz && zz <= zmax) {
+        Cell<R> c = locate<R>(xx, yy, zz, xmin, ymin, zmin, dx, dy, dz, g.nx, g.ny, g.nz);
+        R r[24];
+        load_cell(cells + c.base, r);
+        const R b0 = lerp8(r[0], r[3], r[6], r[9], r[12], r[15], r[18], r[21], c);
+        const R b1 = lerp8(r[1], r[4], r[7], r[10], r[13], r[16], r[19], r[22], c);
+        const R b2 = lerp8(r[2], r[5], r[8], r[11], r[14], r[17], r[20], r[23], c);
+        v = pitch_mu<R>(px, py, pz, b0, b1, b2);
+    }
+    return v;
+}
+
 }  // namespace exact
 }  // namespace pt

@@ -25,6 +25,9 @@
 #include <math_constants.h>
 
 #include "exact_mu.cuh"
+
+#include <cstdlib>
+#include <cstring>
 #include "pt_internal.cuh"
 
 #include <algorithm>
@@ -762,21 +765,52 @@ __global__ void interleave_b_kernel(const R* __restrict__ bx, const R* __restric
         out[i] = exact::Vec4<R>{bx[i], by[i], bz[i], R(0)};
 }
 
+// (Bx, By, Bz) column-major arrays -> one 8-corner record per cell, indexed
+// by the cell's base node (nodes on the last x, y or z plane are no base and
+// their records are left unwritten: a sample never reads them).  Thread per
+// record: the corner reads of neighbouring threads coalesce, and so do the
+// record writes.
+template <typename R>
+__global__ void cell_b_kernel(const R* __restrict__ bx, const R* __restrict__ by, const R* __restrict__ bz, int64_t nx,
+                              int64_t ny, int64_t nz, exact::CellB<R>* __restrict__ out)
+{
+    const int64_t nodes = nx * ny * nz, sy = nx, sz = nx * ny;
+    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < nodes; i += (int64_t)gridDim.x * blockDim.x) {
+        const int64_t ix = i % nx, iy = (i / nx) % ny, iz = i / sz;
+        if (ix >= nx - 1 || iy >= ny - 1 || iz >= nz - 1) continue;
+        const int64_t off[8] = {0, 1, sy, 1 + sy, sz, 1 + sz, sy + sz, 1 + sy + sz};
+        exact::CellB<R> r;
+#pragma unroll
+        for (int q = 0; q < 8; ++q) {
+            r.v[3 * q] = bx[i + off[q]];
+            r.v[3 * q + 1] = by[i + off[q]];
+            r.v[3 * q + 2] = bz[i + off[q]];
+        }
+        out[i] = r;
+    }
+}
+
 // mu of particles [p0, p0 + m) at every save, written [s][p - p0] (particle
 // fastest, like the device mu cache); one thread per (particle, save),
-// particles fastest so that the phase-space reads coalesce.
-template <typename R>
+// particles fastest so that the phase-space reads coalesce.  B comes from
+// cell records (CELLS) or node records.
+template <typename R, bool CELLS>
 __global__ void __launch_bounds__(256) phase_space_mu_kernel(const R* __restrict__ pos, const R* __restrict__ mom,
                                                              int64_t row, int64_t comp, int64_t p0, int64_t m,
-                                                             int64_t nsave, const exact::Vec4<R>* __restrict__ B4,
-                                                             pt_grid g, R* __restrict__ mu)
+                                                             int64_t nsave, const void* __restrict__ Bsrc, pt_grid g,
+                                                             R* __restrict__ mu)
 {
     const int64_t total = m * nsave;
     for (int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; t < total; t += (int64_t)gridDim.x * blockDim.x) {
         const int64_t q = t % m, s = t / m;
         const R* P = pos + s * row + p0 + q;
         const R* M = mom + s * row + p0 + q;
-        mu[s * m + q] = exact::phase_space_mu4<R>(P[0], P[comp], P[2 * comp], M[0], M[comp], M[2 * comp], B4, g);
+        if constexpr (CELLS)
+            mu[s * m + q] = exact::phase_space_mu_cell<R>(P[0], P[comp], P[2 * comp], M[0], M[comp], M[2 * comp],
+                                                          (const exact::CellB<R>*)Bsrc, g);
+        else
+            mu[s * m + q] = exact::phase_space_mu4<R>(P[0], P[comp], P[2 * comp], M[0], M[comp], M[2 * comp],
+                                                      (const exact::Vec4<R>*)Bsrc, g);
     }
 }
 
@@ -785,24 +819,51 @@ int run_dmumu_phase_space_t(pt_ctx* ctx, const DmumuArgs& a, const R* pos, const
                             const void* const bfield[3], const pt_grid& g, cudaStream_t s)
 {
     using V4 = exact::Vec4<R>;
+    using CB = exact::CellB<R>;
     const int64_t nodes = g.nx * g.ny * g.nz;
     // mu chunks of at most 1 GiB
     const int64_t per = std::max<int64_t>(1, ((int64_t)1 << 30) / ((int64_t)sizeof(R) * a.nsave));
     const int64_t m_max = std::min<int64_t>(a.n, per);
-    const size_t b4_bytes = align16(sizeof(V4) * (size_t)nodes);
+    const size_t mu_bytes = sizeof(R) * (size_t)m_max * (size_t)a.nsave;
+    // B as cell records when they take at most half of the free device
+    // memory: a sample then reads one 96-byte (FP32) record instead of 8
+    // node records from 4 grid rows, ~4x fewer DRAM bytes on the random
+    // gathers of particles in id order; otherwise as node records
+    size_t free_b = 0, total_b = 0;
+    if (cudaMemGetInfo(&free_b, &total_b) != cudaSuccess) {
+        cudaGetLastError();
+        free_b = 0;
+    }
+    const size_t cell_bytes = align16(sizeof(CB) * (size_t)nodes);
+    bool cells = cell_bytes + mu_bytes <= free_b / 2;
+    // PTB200_PHASE_SPACE_B = "nodes" or "cells" overrides the choice (same results)
+    if (const char* e = std::getenv("PTB200_PHASE_SPACE_B")) {
+        if (!std::strcmp(e, "nodes")) cells = false;
+        else if (!std::strcmp(e, "cells")) cells = true;
+    }
+    const size_t b_bytes = cells ? cell_bytes : align16(sizeof(V4) * (size_t)nodes);
     void* scratch = nullptr;
-    int rc = scratch_get(ctx, 4, b4_bytes + sizeof(R) * (size_t)m_max * (size_t)a.nsave, &scratch);
+    int rc = scratch_get(ctx, 4, b_bytes + mu_bytes, &scratch);
     if (rc) return rc;
-    V4* B4 = (V4*)scratch;
-    R* mu = (R*)((char*)scratch + b4_bytes);
+    R* mu = (R*)((char*)scratch + b_bytes);
     const int gb = (int)std::min<int64_t>((nodes + 255) / 256, (int64_t)ctx->num_sms * 16);
-    interleave_b_kernel<R><<<gb, 256, 0, s>>>((const R*)bfield[0], (const R*)bfield[1], (const R*)bfield[2], nodes, B4);
-    PT_CHECK_LAUNCH("interleave_b_kernel");
+    if (cells) {
+        cell_b_kernel<R><<<gb, 256, 0, s>>>((const R*)bfield[0], (const R*)bfield[1], (const R*)bfield[2], g.nx, g.ny,
+                                            g.nz, (CB*)scratch);
+        PT_CHECK_LAUNCH("cell_b_kernel");
+    } else {
+        interleave_b_kernel<R><<<gb, 256, 0, s>>>((const R*)bfield[0], (const R*)bfield[1], (const R*)bfield[2], nodes,
+                                                  (V4*)scratch);
+        PT_CHECK_LAUNCH("interleave_b_kernel");
+    }
     for (int64_t p0 = 0; p0 < a.n; p0 += m_max) {
         const int64_t m = std::min(m_max, a.n - p0);
         const int64_t total = m * a.nsave;
         const int blocks = (int)std::min<int64_t>((total + 255) / 256, (int64_t)ctx->num_sms * 32);
-        phase_space_mu_kernel<R><<<blocks, 256, 0, s>>>(pos, mom, row, comp, p0, m, a.nsave, B4, g, mu);
+        if (cells)
+            phase_space_mu_kernel<R, true><<<blocks, 256, 0, s>>>(pos, mom, row, comp, p0, m, a.nsave, scratch, g, mu);
+        else
+            phase_space_mu_kernel<R, false><<<blocks, 256, 0, s>>>(pos, mom, row, comp, p0, m, a.nsave, scratch, g, mu);
         PT_CHECK_LAUNCH("phase_space_mu_kernel");
         DmumuArgs c = a;
         c.n = m;

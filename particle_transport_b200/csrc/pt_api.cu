@@ -40,9 +40,10 @@ int scratch_get(pt_ctx* ctx, int slot, size_t bytes, void** out)
         }
         b.ptr = nullptr;
         b.bytes = 0;
-        // generous first size and 1.5x growth: a regrowth frees the old
-        // buffer, and cudaFree waits for every stream of the device
-        size_t want = std::max(bytes + bytes / 2, (size_t)16 << 20);
+        // generous first size and 1.5x growth (at most 256 MiB of slack): a
+        // regrowth frees the old buffer, and cudaFree waits for every stream
+        // of the device
+        size_t want = std::max(bytes + std::min(bytes / 2, (size_t)256 << 20), (size_t)16 << 20);
         cudaError_t e = cudaMalloc(&b.ptr, want);
         if (e != cudaSuccess) {
             cudaGetLastError();

@@ -203,12 +203,15 @@ def test_reconstruct_mu_bit_exact(cuda, oracle, dtype):
     assert np.isnan(g[3, 5]) and np.isnan(g[4, 6])
 
 
+@pytest.mark.parametrize("b_layout", ["cells", "nodes"])
 @pytest.mark.parametrize("dtype,mode,layout", [(np.float32, "sliding", "julia"), (np.float32, "injection", "cache"),
                                                (np.float64, "sliding", "cache")])
-def test_phase_space_dmumu_fused_matches_oracle(cuda, oracle, dtype, mode, layout):
+def test_phase_space_dmumu_fused_matches_oracle(cuda, oracle, dtype, mode, layout, b_layout, monkeypatch):
     """Fused phase-space D_mumu = oracle reconstruct_mu at the compute
-    precision, then the oracle binning of that mu chunk."""
+    precision, then the oracle binning of that mu chunk -- with B read from
+    8-corner cell records and from node records."""
     torch = cuda
+    monkeypatch.setenv("PTB200_PHASE_SPACE_B", b_layout)
     from helpers import copy_state, fortran_fields, small_problem
     pb = small_problem(n=12, n_particles=517)
     st = copy_state(pb.state)
