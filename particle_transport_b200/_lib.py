@@ -18,7 +18,7 @@ PT_ERR_ARG = -1
 PT_ERR = {-1: "PT_ERR_ARG", -2: "PT_ERR_CUDA", -3: "PT_ERR_OOM", -4: "PT_ERR_TIMEOUT", -5: "PT_ERR_CALLBACK",
           -6: "PT_ERR_STATE"}
 
-PT_FIELD_REF_F64, PT_FIELD_BRICK_F32, PT_FIELD_BRICK_BF16, PT_FIELD_BRICK_BF16_XPAIR = 0, 1, 2, 3
+PT_FIELD_REF_F64, PT_FIELD_BRICK_F32, PT_FIELD_BRICK_BF16, PT_FIELD_BRICK_BF16_XPAIR, PT_FIELD_BRICK_F64 = 0, 1, 2, 3, 4
 PT_CACHE_NONE, PT_CACHE_MU, PT_CACHE_PHASE_SPACE = 0, 1, 2
 PT_PUSH_F64, PT_PUSH_F32 = 0, 1
 PT_START_SLIDING, PT_START_INJECTION = 0, 1

@@ -162,13 +162,16 @@ class ReferenceBatch:
 
         from .runner import DeviceEnsemble, push_params
 
-        if field.storage != "ref_f64":
-            raise ValueError("ReferenceBatch pushes REF_F64 fields")
+        if field.storage not in ("ref_f64", "brick_f64"):
+            raise ValueError("ReferenceBatch pushes ref_f64 or brick_f64 fields")
+        # over FP64 bricks the slots are re-sorted by brick every 64 steps
+        # (same results: the FP64 push of a particle does not depend on its slot)
+        sort_every = 64 if field.storage == "brick_f64" else 0
         n = int(len(state["x1"]))
         al = np.ones(n, np.uint8) if alive is None else alive
         ens = DeviceEnsemble(field, state, al)
         params = push_params(dt, nsteps, stride, periodic, cache="mu" if cache is not None else "none",
-                             precision="f64", steps_per_launch=self.K)
+                             precision="f64", steps_per_launch=self.K, sort_every=sort_every)
         sub = None
         if mom_cache is not None:
             m = int(mom_cache.shape[2])
@@ -178,7 +181,7 @@ class ReferenceBatch:
                                             dtype=torch.float64, device=self.device)[:m].clone() for k in KEYS}
             sub = dict(ens=DeviceEnsemble(field, sub_state, np.asarray(al)[:m].copy()),
                        params=push_params(dt, nsteps, stride, periodic, cache="phase_space", precision="f64",
-                                          steps_per_launch=self.K),
+                                          steps_per_launch=self.K, sort_every=sort_every),
                        ps=torch.empty((mom_cache.shape[0], 6, m), dtype=torch.float32, device=self.device),
                        out=mom_cache)
         cid = self._next

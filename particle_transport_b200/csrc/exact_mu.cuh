@@ -48,6 +48,32 @@ __device__ __forceinline__ Cell<R> locate(R x, R y, R z, R xmin, R ymin, R zmin,
     return c;
 }
 
+// locate() with the cell's 0-based node indices instead of its linear base
+template <typename R>
+struct Cell3 {
+    int i, j, k;
+    Cell<R> t;  // tx, ty, tz (base unused)
+};
+
+template <typename R>
+__device__ __forceinline__ Cell3<R> locate3(R x, R y, R z, R xmin, R ymin, R zmin, R dx, R dy, R dz, int64_t nx,
+                                            int64_t ny, int64_t nz)
+{
+    R fx = (x - xmin) / dx + R(1);
+    R fy = (y - ymin) / dy + R(1);
+    R fz = (z - zmin) / dz + R(1);
+    double ci = cell_index(fx, nx), cj = cell_index(fy, ny), ck = cell_index(fz, nz);
+    Cell3<R> c;
+    c.t.tx = fx - (R)ci;
+    c.t.ty = fy - (R)cj;
+    c.t.tz = fz - (R)ck;
+    c.t.base = 0;
+    c.i = (int)ci - 1;
+    c.j = (int)cj - 1;
+    c.k = (int)ck - 1;
+    return c;
+}
+
 // src/phase_space_gpu_runner.jl:260-275
 template <typename R>
 __device__ __forceinline__ R sample(const R* __restrict__ arr, const Cell<R>& c, int64_t sy, int64_t sz)

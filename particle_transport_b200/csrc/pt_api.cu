@@ -118,10 +118,9 @@ int field_create(pt_ctx* ctx, const double* const comps[6], bool on_device, cons
     if (rc) return rc;
     for (int c = 0; c < 6; ++c)
         if (!comps[c]) return fail(PT_ERR_ARG, "field component is null");
-    if (storage < PT_FIELD_REF_F64 || storage > PT_FIELD_BRICK_BF16_XPAIR)
-        return fail(PT_ERR_ARG, "unknown field storage");
-    if (storage != PT_FIELD_REF_F64 && !(B_ref > 0 && std::isfinite(B_ref)))
-        return fail(PT_ERR_ARG, "B_ref_T must be finite and positive for brick storage");
+    if (storage < PT_FIELD_REF_F64 || storage > PT_FIELD_BRICK_F64) return fail(PT_ERR_ARG, "unknown field storage");
+    if (fast_storage(storage) && !(B_ref > 0 && std::isfinite(B_ref)))
+        return fail(PT_ERR_ARG, "B_ref_T must be finite and positive for the FP32-push brick storages");
     if (grid->nx > 4096 || grid->ny > 4096 || grid->nz > 4096) return fail(PT_ERR_ARG, "grid axis above 4096 nodes");
     PT_CUDA(cudaSetDevice(ctx->device));
     pt_field* f = new (std::nothrow) pt_field();
@@ -217,9 +216,9 @@ int check_params(const pt_push_params* p, const pt_field* f)
     if (p->nsteps < 1) return fail(PT_ERR_ARG, "nsteps must be >= 1");
     if (p->stride < 1) return fail(PT_ERR_ARG, "stride must be >= 1");
     if (p->cache_mode < PT_CACHE_NONE || p->cache_mode > PT_CACHE_PHASE_SPACE) return fail(PT_ERR_ARG, "cache_mode");
-    if (p->precision == PT_PUSH_F64 && f->storage != PT_FIELD_REF_F64)
-        return fail(PT_ERR_ARG, "the FP64 push needs a REF_F64 field");
-    if (p->precision == PT_PUSH_F32 && f->storage == PT_FIELD_REF_F64)
+    if (p->precision == PT_PUSH_F64 && f->storage != PT_FIELD_REF_F64 && f->storage != PT_FIELD_BRICK_F64)
+        return fail(PT_ERR_ARG, "the FP64 push needs a REF_F64 or BRICK_F64 field");
+    if (p->precision == PT_PUSH_F32 && !fast_storage(f->storage))
         return fail(PT_ERR_ARG, "the FP32 push needs a brick field (BRICK_F32 or BRICK_BF16)");
     if (p->precision != PT_PUSH_F64 && p->precision != PT_PUSH_F32) return fail(PT_ERR_ARG, "precision");
     return PT_OK;
@@ -254,6 +253,86 @@ PushArgsFast fast_args(const pt_field* f, pt_fast_state* st, const pt_push_param
 }
 
 }  // namespace
+
+// The FP64 push over a BRICK_F64 field.  Without a sort cadence it runs on
+// the caller's arrays (slot = particle).  With one (sort_every > 0) the state
+// is copied into slots of a context-owned buffer pair, re-sorted by brick at
+// the start and every sort_every steps, pushed there (cache columns by
+// particle id), and scattered back to the caller's order at the end.
+static int advance_exact_brick(pt_ctx* ctx, const pt_field* f, double* d_x1, double* d_x2, double* d_x3, double* d_p1,
+                               double* d_p2, double* d_p3, uint8_t* d_alive, int64_t n, const pt_push_params* p,
+                               int64_t step_begin, int64_t step_count, void* d_cache, int64_t row_base, int64_t rows,
+                               int64_t* d_deaths)
+{
+    if (n <= 0 || step_count <= 0) return PT_OK;
+    PushArgsExactBrick a{};
+    a.nodes = f->nodes;
+    a.offs = f->offs;
+    a.g = f->grid;
+    a.n = n; a.dt = p->dt; a.nsteps = p->nsteps; a.stride = p->stride;
+    a.periodic = p->periodic; a.cache_mode = p->cache_mode; a.cache_f64 = p->cache_f64;
+    a.cache = d_cache; a.row_base = row_base; a.rows = rows; a.deaths = d_deaths;
+    const int64_t K = p->steps_per_launch > 0 ? p->steps_per_launch : 64;
+    const int64_t end = step_begin + step_count;
+    cudaStream_t s = ctx->stream;
+    double* user[6] = {d_x1, d_x2, d_x3, d_p1, d_p2, d_p3};
+    if (p->sort_every <= 0) {
+        for (int k = 0; k < 3; ++k) {
+            a.x[k] = user[k];
+            a.p[k] = user[3 + k];
+        }
+        a.alive = d_alive;
+        a.pid = nullptr;
+        for (int64_t s0 = step_begin; s0 < end; s0 += K) {
+            a.step_begin = s0;
+            a.step_count = std::min(K, end - s0);
+            int rc = launch_push_exact_brick(a, s);
+            if (rc) return rc;
+        }
+        return PT_OK;
+    }
+    if (n > INT32_MAX) return fail(PT_ERR_ARG, "particle count above 2^31 for the sorted FP64 push");
+    // slot buffers: 2 x ([6][n] doubles, pid[n], alive[n]), then the sort's buckets
+    const int64_t m = (f->n_nodes + 511) / 512 + 1;
+    auto a256 = [](size_t v) { return (v + 255) & ~(size_t)255; };
+    const size_t xs_b = a256(sizeof(double) * 6 * (size_t)n), pid_b = a256(sizeof(int32_t) * (size_t)n),
+                 al_b = a256((size_t)n), set_b = xs_b + pid_b + al_b;
+    const size_t hist_b = a256(sizeof(uint32_t) * (size_t)m),
+                 cur_b = a256(sizeof(uint32_t) * (size_t)(m + sort_scan_tiles(m)));
+    void* base = nullptr;
+    int rc = scratch_get(ctx, 5, 2 * set_b + hist_b + cur_b, &base);
+    if (rc) return rc;
+    char* b0 = (char*)base;
+    double* xs[2] = {(double*)b0, (double*)(b0 + set_b)};
+    int32_t* pid[2] = {(int32_t*)(b0 + xs_b), (int32_t*)(b0 + set_b + xs_b)};
+    uint8_t* al[2] = {(uint8_t*)(b0 + xs_b + pid_b), (uint8_t*)(b0 + set_b + xs_b + pid_b)};
+    uint32_t* hist = (uint32_t*)(b0 + 2 * set_b);
+    uint32_t* cursor = (uint32_t*)(b0 + 2 * set_b + hist_b);
+    if ((rc = launch_exact_import(user, d_alive, n, xs[0], pid[0], al[0], ctx->num_sms, s))) return rc;
+    int cur = 0;
+    int64_t last_sort = INT64_MIN;
+    for (int64_t s0 = step_begin; s0 < end;) {
+        if (last_sort == INT64_MIN || s0 - last_sort >= p->sort_every) {
+            rc = launch_exact_sort(xs[cur], pid[cur], al[cur], n, f, xs[1 - cur], pid[1 - cur], al[1 - cur], hist,
+                                   cursor, ctx->num_sms, s);
+            if (rc) return rc;
+            cur = 1 - cur;
+            last_sort = s0;
+        }
+        const int64_t c = std::min(std::min(K, end - s0), last_sort + p->sort_every - s0);
+        for (int k = 0; k < 3; ++k) {
+            a.x[k] = xs[cur] + (size_t)k * n;
+            a.p[k] = xs[cur] + (size_t)(3 + k) * n;
+        }
+        a.alive = al[cur];
+        a.pid = pid[cur];
+        a.step_begin = s0;
+        a.step_count = c;
+        if ((rc = launch_push_exact_brick(a, s))) return rc;
+        s0 += c;
+    }
+    return launch_exact_export(xs[cur], pid[cur], al[cur], n, user, d_alive, ctx->num_sms, s);
+}
 
 // Advance the fast state over [s0, s0 + count), splitting launches at the
 // re-sort cadence (sort_every steps) and at steps_per_launch.
@@ -405,6 +484,9 @@ int pt_push_advance_device(pt_ctx* ctx, const pt_field* f, double* d_x1, double*
         return fail(PT_ERR_ARG, "step range outside [0, nsteps)");
     if (n > 0 && !(d_x1 && d_x2 && d_x3 && d_p1 && d_p2 && d_p3 && d_alive)) return fail(PT_ERR_ARG, "null state");
     if (p->cache_mode != PT_CACHE_NONE && rows > 0 && !d_cache) return fail(PT_ERR_ARG, "null cache");
+    if (f->storage == PT_FIELD_BRICK_F64)
+        return advance_exact_brick(ctx, f, d_x1, d_x2, d_x3, d_p1, d_p2, d_p3, d_alive, n, p, step_begin, step_count,
+                                   d_cache, row_base, rows, d_deaths);
     PushArgsRef a{};
     for (int c = 0; c < 6; ++c) a.f[c] = f->comp[c];
     a.g = f->grid;
@@ -428,7 +510,7 @@ int pt_fast_state_create(pt_ctx* ctx, const pt_field* f, const double* d_x1, con
                          int64_t n, pt_fast_state** out)
 {
     if (!ctx || !f || !out) return fail(PT_ERR_ARG, "null argument");
-    if (f->storage == PT_FIELD_REF_F64) return fail(PT_ERR_ARG, "fast state needs a brick field");
+    if (!fast_storage(f->storage)) return fail(PT_ERR_ARG, "fast state needs an FP32-push brick field");
     if (n < 0 || n > INT32_MAX) return fail(PT_ERR_ARG, "particle count out of range");
     pt_fast_state* st = new (std::nothrow) pt_fast_state();
     if (!st) return fail(PT_ERR_OOM, "host allocation failed");

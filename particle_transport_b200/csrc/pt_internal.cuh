@@ -50,7 +50,7 @@ struct pt_ctx {
     cudaStream_t own_stream = nullptr;
     cudaStream_t stream = nullptr;      // stream used by *_device calls
     cudaStream_t copy_stream = nullptr; // egress copies in pt_push_run
-    pt::ScratchBuf scratch[5];          // reusable device scratch, grown on demand
+    pt::ScratchBuf scratch[6];          // reusable device scratch, grown on demand
     pt::ScratchBuf pinned;              // pinned host staging of pt_push_run, grown on demand
     pt_fast_state* run_fs = nullptr;    // FP32-push state reused by pt_push_run
 };
@@ -134,16 +134,57 @@ struct PushArgsRef {
 };
 int launch_push_ref(const PushArgsRef& a, cudaStream_t s);
 
+// The same FP64 push over a BRICK_F64 field: the corner values are read from
+// 64-byte node records (2 loads per corner) instead of 6 arrays, and the
+// state may be in brick-sorted slot order with pid[slot] the particle's cache
+// column.  Same arithmetic, so the results are bit-identical.
+struct PushArgsExactBrick {
+    const void* nodes;
+    const uint32_t* offs;  // [nx + ny + nz] per-axis node offsets
+    pt_grid g;
+    double* x[3];
+    double* p[3];
+    uint8_t* alive;
+    const int32_t* pid;    // cache column of each slot (null: the slot itself)
+    int64_t n;
+    double dt;
+    int64_t nsteps, stride;
+    int periodic, cache_mode, cache_f64;
+    int64_t step_begin, step_count;
+    void* cache;
+    int64_t row_base, rows;
+    int64_t* deaths;
+};
+int launch_push_exact_brick(const PushArgsExactBrick& a, cudaStream_t s);
+// FP64 SI state in slots: xs = [6][n] (x1, x2, x3, p1, p2, p3), pid[n], alive[n]
+// brick re-sort into xd/pidd/ad (hist: n_bricks + 1 buckets; cursor: the
+// buckets then sort_scan_tiles() tile offsets)
+int launch_exact_sort(const double* xs, const int32_t* pids, const uint8_t* as, int64_t n, const pt_field* f,
+                      double* xd, int32_t* pidd, uint8_t* ad, uint32_t* hist, uint32_t* cursor, int num_sms,
+                      cudaStream_t s);
+// caller arrays -> slots (pid = slot), and slots -> caller arrays by pid
+int launch_exact_import(double* const src[6], const uint8_t* alive, int64_t n, double* xs, int32_t* pids,
+                        uint8_t* as, int num_sms, cudaStream_t s);
+int launch_exact_export(const double* xs, const int32_t* pids, const uint8_t* as, int64_t n, double* const dst[6],
+                        uint8_t* alive, int num_sms, cudaStream_t s);
+
 // node record layouts of the brick forms
-enum { LAYOUT_BF16 = 0, LAYOUT_F32 = 1, LAYOUT_BF16_XPAIR = 2 };
+enum { LAYOUT_BF16 = 0, LAYOUT_F32 = 1, LAYOUT_BF16_XPAIR = 2, LAYOUT_F64 = 3 };
 inline int field_layout(int storage)
 {
-    return storage == PT_FIELD_BRICK_F32 ? LAYOUT_F32 : (storage == PT_FIELD_BRICK_BF16_XPAIR ? LAYOUT_BF16_XPAIR
-                                                                                               : LAYOUT_BF16);
+    return storage == PT_FIELD_BRICK_F32         ? LAYOUT_F32
+           : storage == PT_FIELD_BRICK_BF16_XPAIR ? LAYOUT_BF16_XPAIR
+           : storage == PT_FIELD_BRICK_F64        ? LAYOUT_F64
+                                                  : LAYOUT_BF16;
 }
 inline size_t record_bytes(int storage)
 {
-    return storage == PT_FIELD_BRICK_BF16 ? 16 : 32;
+    return storage == PT_FIELD_BRICK_BF16 ? 16 : (storage == PT_FIELD_BRICK_F64 ? 64 : 32);
+}
+// brick forms read by the FP32 push
+inline bool fast_storage(int storage)
+{
+    return storage == PT_FIELD_BRICK_F32 || storage == PT_FIELD_BRICK_BF16 || storage == PT_FIELD_BRICK_BF16_XPAIR;
 }
 
 struct FieldArgsBrick {

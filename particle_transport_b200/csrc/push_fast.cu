@@ -301,6 +301,13 @@ __global__ void brick_convert_kernel(const double* __restrict__ bx, const double
          t += (int64_t)gridDim.x * blockDim.x) {
         const int64_t i = t % nx, j = (t / nx) % ny, k = t / (nx * ny);
         const uint32_t node = offs[i] + offs[nx + j] + offs[nx + ny + k];
+        if (layout == LAYOUT_F64) {
+            // SI values as they are (the FP64 push reads them unchanged)
+            double4* N = (double4*)nodes;
+            N[2 * (size_t)node] = make_double4(bx[t], by[t], bz[t], ux[t]);
+            N[2 * (size_t)node + 1] = make_double4(uy[t], uz[t], 0.0, 0.0);
+            continue;
+        }
         float v[6];
         comps(t, v);
         if (layout == LAYOUT_BF16) {
@@ -514,6 +521,94 @@ __global__ void sort_scatter_kernel(uint32_t* cursor, const uint32_t* __restrict
     }
 }
 
+// ---- brick sort of an FP64 SI state (the FP64 push over BRICK_F64 fields):
+// xs = [6][n] (x1, x2, x3, p1, p2, p3), pid, alive.  The bucket is the
+// brick of the cell holding the position; it only orders the slots.
+__device__ __forceinline__ uint32_t exact_brick_key(const double* __restrict__ xs, int64_t n, int64_t i, uint8_t al,
+                                                    double x0, double y0, double z0, double idx, double idy,
+                                                    double idz, const uint32_t* __restrict__ offs, int nx, int ny,
+                                                    int nz, uint32_t dead_key)
+{
+    return brick_key((xs[i] - x0) * idx, (xs[n + i] - y0) * idy, (xs[2 * n + i] - z0) * idz, al, offs, nx, ny, nz,
+                     dead_key);
+}
+
+__global__ void exact_key_kernel(const double* __restrict__ xs, const uint8_t* __restrict__ as, int64_t n, double x0,
+                                 double y0, double z0, double idx, double idy, double idz,
+                                 const uint32_t* __restrict__ offs, int nx, int ny, int nz, uint32_t dead_key,
+                                 uint32_t* __restrict__ hist)
+{
+    const int lane = threadIdx.x & 31;
+    const unsigned lt = (1u << lane) - 1u;
+    const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    const bool valid = i < n;
+    const uint32_t key =
+        valid ? exact_brick_key(xs, n, i, as[i], x0, y0, z0, idx, idy, idz, offs, nx, ny, nz, dead_key) : dead_key;
+    const unsigned act = __ballot_sync(0xffffffffu, valid);
+    if (valid) {
+        const unsigned same = __match_any_sync(act, key);
+        if ((same & lt) == 0) atomicAdd(&hist[key], (uint32_t)__popc(same));
+    }
+}
+
+__global__ void exact_scatter_kernel(uint32_t* cursor, const uint32_t* __restrict__ tile_off, int64_t n, double x0,
+                                     double y0, double z0, double idx, double idy, double idz,
+                                     const uint32_t* __restrict__ offs, int nx, int ny, int nz, uint32_t dead_key,
+                                     const double* __restrict__ xs, const int32_t* __restrict__ pids,
+                                     const uint8_t* __restrict__ as, double* __restrict__ xd,
+                                     int32_t* __restrict__ pidd, uint8_t* __restrict__ ad)
+{
+    const int lane = threadIdx.x & 31;
+    const unsigned lt = (1u << lane) - 1u;
+    const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    const bool valid = i < n;
+    const unsigned act = __ballot_sync(0xffffffffu, valid);
+    if (!valid) return;
+    double v[6];
+#pragma unroll
+    for (int k = 0; k < 6; ++k) v[k] = xs[k * n + i];
+    const int32_t id = pids[i];
+    const uint8_t al = as[i];
+    const uint32_t key = exact_brick_key(xs, n, i, al, x0, y0, z0, idx, idy, idz, offs, nx, ny, nz, dead_key);
+    const unsigned same = __match_any_sync(act, key);
+    const int leader = __ffs(same) - 1;
+    uint32_t first = 0;
+    if (lane == leader) first = atomicAdd(&cursor[key], (uint32_t)__popc(same)) + tile_off[key / kScanTile];
+    first = __shfl_sync(same, first, leader);
+    const int64_t d = (int64_t)first + __popc(same & lt);
+#pragma unroll
+    for (int k = 0; k < 6; ++k) xd[k * n + d] = v[k];
+    pidd[d] = id;
+    ad[d] = al;
+}
+
+__global__ void exact_import_kernel(const double* __restrict__ s0, const double* __restrict__ s1,
+                                    const double* __restrict__ s2, const double* __restrict__ s3,
+                                    const double* __restrict__ s4, const double* __restrict__ s5,
+                                    const uint8_t* __restrict__ alive, int64_t n, double* __restrict__ xs,
+                                    int32_t* __restrict__ pids, uint8_t* __restrict__ as)
+{
+    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+        xs[i] = s0[i]; xs[n + i] = s1[i]; xs[2 * n + i] = s2[i];
+        xs[3 * n + i] = s3[i]; xs[4 * n + i] = s4[i]; xs[5 * n + i] = s5[i];
+        pids[i] = (int32_t)i;
+        as[i] = alive[i];
+    }
+}
+
+__global__ void exact_export_kernel(const double* __restrict__ xs, const int32_t* __restrict__ pids,
+                                    const uint8_t* __restrict__ as, int64_t n, double* __restrict__ d0,
+                                    double* __restrict__ d1, double* __restrict__ d2, double* __restrict__ d3,
+                                    double* __restrict__ d4, double* __restrict__ d5, uint8_t* __restrict__ alive)
+{
+    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+        const int64_t q = pids[i];
+        d0[q] = xs[i]; d1[q] = xs[n + i]; d2[q] = xs[2 * n + i];
+        d3[q] = xs[3 * n + i]; d4[q] = xs[4 * n + i]; d5[q] = xs[5 * n + i];
+        alive[q] = as[i];
+    }
+}
+
 int grid_for(int64_t n, int threads, int num_sms)
 {
     int64_t b = (n + threads - 1) / threads;
@@ -675,6 +770,54 @@ int fast_sort(pt_ctx* ctx, pt_fast_state* st, const pt_field* f, cudaStream_t s)
     std::swap(st->p2, st->p2_alt);
     std::swap(st->pid, st->pid_alt);
     std::swap(st->alive, st->alive_alt);
+    return PT_OK;
+}
+
+int launch_exact_sort(const double* xs, const int32_t* pids, const uint8_t* as, int64_t n, const pt_field* f,
+                      double* xd, int32_t* pidd, uint8_t* ad, uint32_t* hist, uint32_t* cursor, int num_sms,
+                      cudaStream_t s)
+{
+    if (n <= 0) return PT_OK;
+    const pt_grid& g = f->grid;
+    const uint32_t nb = (uint32_t)((f->n_nodes + 511) / 512);
+    const int64_t m = (int64_t)nb + 1;  // + dead bucket
+    const int64_t tiles = sort_scan_tiles(m);
+    uint32_t* tile_off = cursor + m;
+    PT_CUDA(cudaMemsetAsync(hist, 0, sizeof(uint32_t) * m, s));
+    const int gb = (int)std::min<int64_t>((n + 255) / 256, INT32_MAX);
+    const int nx = (int)g.nx, ny = (int)g.ny, nz = (int)g.nz;
+    const double idx = 1.0 / g.dx, idy = 1.0 / g.dy, idz = 1.0 / g.dz;
+    exact_key_kernel<<<gb, 256, 0, s>>>(xs, as, n, g.xmin, g.ymin, g.zmin, idx, idy, idz, f->offs, nx, ny, nz, nb,
+                                        hist);
+    PT_CHECK_LAUNCH("exact_key_kernel");
+    sort_scan_tiles_kernel<<<(unsigned)tiles, 1024, 0, s>>>(hist, cursor, tile_off, m, nullptr);
+    PT_CHECK_LAUNCH("sort_scan_tiles_kernel");
+    sort_scan_top_kernel<<<1, 1024, 0, s>>>(tile_off, tiles, nullptr);
+    PT_CHECK_LAUNCH("sort_scan_top_kernel");
+    exact_scatter_kernel<<<gb, 256, 0, s>>>(cursor, tile_off, n, g.xmin, g.ymin, g.zmin, idx, idy, idz, f->offs, nx, ny,
+                                            nz, nb, xs, pids, as, xd, pidd, ad);
+    PT_CHECK_LAUNCH("exact_scatter_kernel");
+    (void)num_sms;
+    return PT_OK;
+}
+
+int launch_exact_import(double* const src[6], const uint8_t* alive, int64_t n, double* xs, int32_t* pids,
+                        uint8_t* as, int num_sms, cudaStream_t s)
+{
+    if (n <= 0) return PT_OK;
+    exact_import_kernel<<<grid_for(n, 256, num_sms), 256, 0, s>>>(src[0], src[1], src[2], src[3], src[4], src[5],
+                                                                 alive, n, xs, pids, as);
+    PT_CHECK_LAUNCH("exact_import_kernel");
+    return PT_OK;
+}
+
+int launch_exact_export(const double* xs, const int32_t* pids, const uint8_t* as, int64_t n, double* const dst[6],
+                        uint8_t* alive, int num_sms, cudaStream_t s)
+{
+    if (n <= 0) return PT_OK;
+    exact_export_kernel<<<grid_for(n, 256, num_sms), 256, 0, s>>>(xs, pids, as, n, dst[0], dst[1], dst[2], dst[3],
+                                                                 dst[4], dst[5], alive);
+    PT_CHECK_LAUNCH("exact_export_kernel");
     return PT_OK;
 }
 

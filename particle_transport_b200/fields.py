@@ -30,7 +30,10 @@ PC_TO_M = 3.085677581e16
 GEV_TO_J = 1e9 * 1.602176634e-19
 
 STORAGE = {"ref_f64": _lib.PT_FIELD_REF_F64, "brick_f32": _lib.PT_FIELD_BRICK_F32,
-           "brick_bf16": _lib.PT_FIELD_BRICK_BF16, "brick_bf16x": _lib.PT_FIELD_BRICK_BF16_XPAIR}
+           "brick_bf16": _lib.PT_FIELD_BRICK_BF16, "brick_bf16x": _lib.PT_FIELD_BRICK_BF16_XPAIR,
+           "brick_f64": _lib.PT_FIELD_BRICK_F64}
+# storages the FP64 (exact) push reads
+F64_STORAGE = ("ref_f64", "brick_f64")
 
 
 @dataclass
@@ -193,8 +196,9 @@ class FieldLibrary:
     fields: six SI arrays (Bx, By, Bz, ux, uy, uz), each C-ordered (nz, ny, nx)
     float64 -- numpy (uploaded from the host) or CUDA torch tensors (converted
     on the device).  storage: "ref_f64" (reference layout, FP64 push),
-    "brick_f32" or "brick_bf16" (Morton bricks, FP32 push); B_ref_T scales the
-    brick forms (defaults to the mean |B| of the field)."""
+    "brick_f64" (Morton bricks of FP64 SI node records, FP64 push, the same
+    results), "brick_f32" or "brick_bf16" (Morton bricks, FP32 push); B_ref_T
+    scales the FP32-push brick forms (defaults to the mean |B| of the field)."""
 
     def __init__(self, fields, grid: UniformGrid, storage: str = "ref_f64", B_ref_T: float | None = None,
                  device: int = 0):

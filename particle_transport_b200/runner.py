@@ -19,7 +19,7 @@ from types import SimpleNamespace
 import numpy as np
 
 from . import _lib
-from .fields import FieldLibrary, reference_B0_T
+from .fields import F64_STORAGE, FieldLibrary, reference_B0_T
 from .particles import energy_to_gamma, energy_to_speed, init_particles
 from .time_units import (campaign_time_reference, reference_Omega0, resolve_save_stride,
                          resolve_trajectory_time_grid, sampled_step_indices)
@@ -101,16 +101,17 @@ def run_push_host(field: FieldLibrary, state: dict, alive: np.ndarray, params: _
 
 
 class DeviceEnsemble:
-    """FP64 SI state resident on the device (torch tensors) for the
-    reference-layout push (pt_push_advance_device).  CUDA float64 contiguous
-    state arrays are used as they are, not copied: the push advances them in
-    place."""
+    """FP64 SI state resident on the device (torch tensors) for the FP64 push
+    (pt_push_advance_device) over a ref_f64 or brick_f64 field.  CUDA float64
+    contiguous state arrays are used as they are, not copied: the push
+    advances them in place (over brick_f64 with a sort cadence, through a
+    brick-sorted copy that is scattered back after each call)."""
 
     def __init__(self, field: FieldLibrary, state: dict, alive):
         import torch
 
-        if field.storage != "ref_f64":
-            raise ValueError("DeviceEnsemble runs the FP64 push on a ref_f64 field")
+        if field.storage not in F64_STORAGE:
+            raise ValueError("DeviceEnsemble runs the FP64 push on a ref_f64 or brick_f64 field")
         self.field = field
         self.state = {k: torch.as_tensor(state[k], dtype=torch.float64, device="cuda").contiguous() for k in KEYS}
         self.alive = torch.as_tensor(alive, dtype=torch.uint8, device="cuda").contiguous()
@@ -130,8 +131,8 @@ class FastEnsemble:
     def __init__(self, field: FieldLibrary, state: dict, alive):
         import torch
 
-        if field.storage == "ref_f64":
-            raise ValueError("FastEnsemble needs a brick field (brick_f32 or brick_bf16)")
+        if field.storage in F64_STORAGE:
+            raise ValueError("FastEnsemble needs an FP32-push brick field (brick_f32 or brick_bf16)")
         self.field = field
         st = {k: torch.as_tensor(state[k], dtype=torch.float64, device="cuda").contiguous() for k in KEYS}
         al = torch.as_tensor(alive, dtype=torch.uint8, device="cuda").contiguous()

@@ -16,7 +16,13 @@ from particle_transport_b200.fields import FieldLibrary
 pytestmark = pytest.mark.gpu
 
 
-def run_both(pb, nsteps, stride, cache, periodic=True, f64_out=False, alive=None):
+# the FP64 push over the reference layout, over FP64 bricks with the slots in
+# particle order, and over FP64 bricks re-sorted by brick every 16 steps:
+# every one must be bit-identical to the oracle
+F64_FORMS = [("ref_f64", 0), ("brick_f64", 0), ("brick_f64", 16)]
+
+
+def run_both(pb, nsteps, stride, cache, periodic=True, f64_out=False, alive=None, storage="ref_f64", sort_every=0):
     from oracle import oracle as o
     n = len(pb.state["x1"])
     alive0 = np.ones(n, np.uint8) if alive is None else alive.copy()
@@ -24,18 +30,21 @@ def run_both(pb, nsteps, stride, cache, periodic=True, f64_out=False, alive=None
     al_o = alive0.copy()
     out_o, ac_o = o.push_run(fortran_fields(pb.fields), pb.grid, st_o, al_o, pb.dt, nsteps, stride, periodic=periodic,
                              cache_mode={"mu": 1, "phase_space": 2}[cache], out_f64=f64_out)
-    fl = FieldLibrary(pb.fields, pb.grid, "ref_f64")
+    fl = FieldLibrary(pb.fields, pb.grid, storage)
     st_g = copy_state(pb.state)
     al_g = alive0.copy()
     col = R.CacheCollector(n, R.n_saves(nsteps, stride), cache, f64_out)
-    params = R.push_params(pb.dt, nsteps, stride, periodic=periodic, cache=cache, cache_f64=f64_out)
+    params = R.push_params(pb.dt, nsteps, stride, periodic=periodic, cache=cache, cache_f64=f64_out,
+                           sort_every=sort_every)
     ac_g = R.run_push_host(fl, st_g, al_g, params, col)
     return (out_o, ac_o, st_o, al_o), (col, ac_g, st_g, al_g)
 
 
-def test_fp64_mu_cache_bit_exact(cuda):
+@pytest.mark.parametrize("storage,sort_every", F64_FORMS)
+def test_fp64_mu_cache_bit_exact(cuda, storage, sort_every):
     pb = small_problem(n=16, n_particles=700, u_over_c=1e-4)
-    (mu_o, ac_o, st_o, al_o), (col, ac_g, st_g, al_g) = run_both(pb, 641, 4, "mu")
+    (mu_o, ac_o, st_o, al_o), (col, ac_g, st_g, al_g) = run_both(pb, 641, 4, "mu", storage=storage,
+                                                                 sort_every=sort_every)
     assert np.array_equal(col.mu, mu_o, equal_nan=True)
     for k in R.KEYS:
         assert np.array_equal(st_g[k], st_o[k]), k
@@ -43,37 +52,42 @@ def test_fp64_mu_cache_bit_exact(cuda):
     assert np.array_equal(al_g, al_o)
 
 
+@pytest.mark.parametrize("storage,sort_every", F64_FORMS)
 @pytest.mark.parametrize("f64_out", [False, True])
-def test_fp64_phase_space_bit_exact(cuda, f64_out):
+def test_fp64_phase_space_bit_exact(cuda, f64_out, storage, sort_every):
     pb = small_problem(n=12, n_particles=300, energy_GeV=10.0, u_over_c=1e-4)
-    ((pos_o, mom_o), ac_o, st_o, _), (col, ac_g, st_g, _) = run_both(pb, 257, 8, "phase_space", f64_out=f64_out)
+    ((pos_o, mom_o), ac_o, st_o, _), (col, ac_g, st_g, _) = run_both(pb, 257, 8, "phase_space", f64_out=f64_out,
+                                                                     storage=storage, sort_every=sort_every)
     assert np.array_equal(col.positions, pos_o, equal_nan=True)
     assert np.array_equal(col.momenta, mom_o, equal_nan=True)
     for k in R.KEYS:
         assert np.array_equal(st_g[k], st_o[k]), k
 
 
-def test_fp64_open_boundary_bit_exact(cuda):
+@pytest.mark.parametrize("storage,sort_every", F64_FORMS)
+def test_fp64_open_boundary_bit_exact(cuda, storage, sort_every):
     pb = small_problem(n=10, n_particles=400, energy_GeV=30.0, u_over_c=1e-4)
     alive = np.ones(400, np.uint8)
     alive[::17] = 0  # some particles dead on entry
-    (mu_o, ac_o, st_o, al_o), (col, ac_g, st_g, al_g) = run_both(pb, 400, 3, "mu", periodic=False, alive=alive)
+    (mu_o, ac_o, st_o, al_o), (col, ac_g, st_g, al_g) = run_both(pb, 400, 3, "mu", periodic=False, alive=alive,
+                                                                 storage=storage, sort_every=sort_every)
     assert ac_o[-1] < ac_o[0]  # particles left the box
     assert np.array_equal(ac_g, ac_o)
     assert np.array_equal(al_g, al_o)
     assert np.array_equal(col.mu, mu_o, equal_nan=True)
 
 
-def test_fp64_device_api_matches_host(cuda):
+@pytest.mark.parametrize("storage,sort_every", F64_FORMS)
+def test_fp64_device_api_matches_host(cuda, storage, sort_every):
     torch = cuda
     pb = small_problem(n=16, n_particles=512)
     nsteps, stride = 333, 4
     (mu_o, _, st_o, _), _ = run_both(pb, nsteps, stride, "mu")
-    fl = FieldLibrary(pb.fields, pb.grid, "ref_f64")
+    fl = FieldLibrary(pb.fields, pb.grid, storage)
     ens = R.DeviceEnsemble(fl, pb.state, np.ones(512, np.uint8))
     nsave = R.n_saves(nsteps, stride)
     cache = torch.full((nsave, 512), float("nan"), dtype=torch.float32, device="cuda")
-    params = R.push_params(pb.dt, nsteps, stride, cache="mu", steps_per_launch=16)
+    params = R.push_params(pb.dt, nsteps, stride, cache="mu", steps_per_launch=16, sort_every=sort_every)
     s = 0
     for chunk in (5, 100, 1, 227):  # uneven chunks, each a separate call
         ens.advance(params, s, chunk, cache, 0, nsave)
@@ -191,6 +205,12 @@ def test_errors_raise(cuda):
         R.run_push_host(fl, copy_state(pb.state), np.ones(4, np.uint8), R.push_params(pb.dt, 10, 0))
     with pytest.raises(ValueError):
         R.run_push_host(fl, copy_state(pb.state), np.ones(3, np.uint8), R.push_params(pb.dt, 10, 1))
+    # FP64 bricks are for the FP64 push only
+    f64b = FieldLibrary(pb.fields, pb.grid, "brick_f64")
+    with pytest.raises(PtError, match="brick field"):
+        R.run_push_host(f64b, copy_state(pb.state), np.ones(4, np.uint8), R.push_params(pb.dt, 10, 1, precision="f32"))
+    with pytest.raises(ValueError, match="FP32-push brick field"):
+        R.FastEnsemble(f64b, pb.state, np.ones(4, np.uint8))
 
 
 @pytest.mark.parametrize("precision", ["f32", "f64"])

@@ -26,6 +26,15 @@ def library(cuda):
 
 
 @pytest.fixture(scope="module")
+def library64b(cuda):
+    pa = small_problem(n=16, n_particles=4, u_over_c=1e-4, seed=3)
+    pb = small_problem(n=16, n_particles=4, u_over_c=2e-4, seed=9)
+    libs = {"16": {"total": FieldLibrary(pa.fields, pa.grid, "brick_f64"),
+                   "alfven": FieldLibrary(pb.fields, pb.grid, "brick_f64")}}
+    return libs, {"16": reference_B0_T(*pa.fields[:3])}
+
+
+@pytest.fixture(scope="module")
 def library64(cuda):
     pa = small_problem(n=16, n_particles=4, u_over_c=1e-4, seed=3)
     pb = small_problem(n=16, n_particles=4, u_over_c=2e-4, seed=9)
@@ -197,3 +206,13 @@ def test_dpp_of_served_job_equals_direct_phase_space_run(library):
     direct = {k: v.cpu().numpy() for k, v in acc.items()}
     direct["p0"] = p0
     same_dpp(res.dpp, direct)
+
+
+def test_fp64_server_over_bricks_same_as_reference_layout(library64, library64b):
+    """The FP64 server over FP64 bricks (brick-sorted slots) returns what it
+    returns over the reference layout: mu caches bit for bit, the same
+    products."""
+    ref = run_jobs(library64, JOBS, stagger_ticks=1, push="f64")
+    brk = run_jobs(library64b, JOBS, stagger_ticks=1, push="f64")
+    for a, b in zip(ref, brk):
+        same(b, a)
