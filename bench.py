@@ -1050,11 +1050,17 @@ def run_serving(args, dev, n_jobs=16, rate=4.0, n_cmp=8):
     cmp32 = serve(libs, arr_c, specs_c, "f32")
     libs64 = make_libs("ref_f64")  # built after the main stream: 29 GB of FP64 fields
     cmp64 = serve(libs64, arr_c, specs_c, "f64")
-    main["fp32_vs_fp64"] = {"stream": f"{n_cmp} jobs, Poisson {rate}/s, 16k-1M particles, 10-60 T_g0, 1-300 GeV",
-                            "fp32_bf16": cmp32, "fp64_plain": cmp64,
-                            "busy_rate_ratio": cmp32["busy_rate"] / cmp64["busy_rate"]}
     del libs64
     torch.cuda.empty_cache()
+    libs64b = make_libs("brick_f64")  # the same fields as FP64 bricks (38 GB)
+    cmp64b = serve(libs64b, arr_c, specs_c, "f64")
+    del libs64b
+    torch.cuda.empty_cache()
+    main["fp32_vs_fp64"] = {"stream": f"{n_cmp} jobs, Poisson {rate}/s, 16k-1M particles, 10-60 T_g0, 1-300 GeV",
+                            "fp32_bf16": cmp32, "fp64_plain": cmp64,
+                            "fp64_bricks": dict(cmp64b, note="the same FP64 push (bit-identical results) over "
+                                                              "FP64 bricks with brick-sorted slots"),
+                            "busy_rate_ratio": cmp32["busy_rate"] / cmp64["busy_rate"]}
     return main
 
 

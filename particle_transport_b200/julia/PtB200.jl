@@ -10,6 +10,7 @@ const LIB = get(ENV, "PTB200_LIB", joinpath(@__DIR__, "..", "libptb200.so"))
 const PT_FIELD_REF_F64 = Cint(0)
 const PT_FIELD_BRICK_F32 = Cint(1)
 const PT_FIELD_BRICK_BF16 = Cint(2)
+const PT_FIELD_BRICK_F64 = Cint(4)   # FP64 push, bit-identical to PT_FIELD_REF_F64
 const PT_CACHE_MU = Cint(1)
 const PT_CACHE_PHASE_SPACE = Cint(2)
 const PT_PUSH_F64 = Cint(0)
