@@ -64,7 +64,9 @@ def parse():
     ap.add_argument("--variant", type=int, default=1, help="push launch shape (pt_push_params.kernel_variant)")
     ap.add_argument("--lag-particles", type=int, default=1_048_576)
     ap.add_argument("--dpp-particles", type=int, default=262_144)
-    ap.add_argument("--e2e-gyroperiods", type=int, default=8)
+    ap.add_argument("--e2e-gyroperiods", type=int, default=32,
+                    help="T_g0 per pt_push_run call in the e2e leg (the reference pushes a whole campaign, "
+                         "500 T_g0 at 512^3, per call)")
     ap.add_argument("--skip", default="", help="comma list of legs to skip: fp32b,fp64,lag,dpp,e2e,cpu,batch,serve,config1")
     ap.add_argument("--cpu-seconds", type=float, default=10.0)
     ap.add_argument("--precision", action="store_true",
@@ -612,6 +614,7 @@ def run_ours(args, ws, rank, local):
         el = max_over_ranks(el * 1e3, ws, dev) / 1e3
         nsave_e = (ns - 1) // STRIDE + 1
         e2e = {"value": ws * n * (ns - 1) * ncall / el, "unit": UNIT,
+               "step": "one pt_push_run call: host state in, mu rows and state out",
                "h2d_bytes_per_step": int(n * (6 * 8 + 1)),
                "d2h_bytes_per_step": int(n * (6 * 8 + 1) + nsave_e * n * 4 + 8 * ns),
                "call": f"pt_push_run over {G} T_g0 ({ns - 1} pushes, {nsave_e} mu rows) per call, host state",

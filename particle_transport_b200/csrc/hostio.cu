@@ -10,6 +10,7 @@
 #include "pt_internal.cuh"
 
 #include <atomic>
+#include <cstdlib>
 #include <condition_variable>
 #include <cstring>
 #include <deque>
@@ -53,8 +54,14 @@ class HostPool {
   private:
     HostPool()
     {
+        // workers besides the calling thread: 7 (at most hardware threads - 1),
+        // or PTB200_HOST_THREADS - 1
         const unsigned hw = std::thread::hardware_concurrency();
-        const int k = (int)std::min<unsigned>(7u, hw > 1 ? hw - 1 : 0u);
+        int k = (int)std::min<unsigned>(7u, hw > 1 ? hw - 1 : 0u);
+        if (const char* e = std::getenv("PTB200_HOST_THREADS")) {
+            const int t = std::atoi(e);
+            if (t >= 1) k = std::min(t - 1, 63);
+        }
         for (int i = 0; i < k; ++i) workers_.emplace_back([this] { loop(); });
     }
     ~HostPool()
