@@ -335,13 +335,17 @@ class CampaignServer:
     def idle(self) -> bool:
         return not (self.queue or self.active or self.binning)
 
-    def run_until_idle(self, max_ticks: int = 10 ** 7):
-        for _ in range(max_ticks):
-            if self.idle():
+    def run_until_idle(self, timeout_s: float = None):
+        """Tick until every submitted job has returned its results (or
+        timeout_s seconds passed); returns the results so far."""
+        t0 = time.perf_counter()
+        while not self.idle():
+            if timeout_s is not None and time.perf_counter() - t0 > timeout_s:
                 break
-            if not self.active and not self.queue:
-                time.sleep(1e-4)
+            epochs = self.epochs
             self.tick()
+            if self.epochs == epochs:
+                time.sleep(5e-5)  # nothing to enqueue now: epochs in flight, or binning to finish
         return self.results
 
     def close(self):

@@ -216,3 +216,15 @@ def test_fp64_server_over_bricks_same_as_reference_layout(library64, library64b)
     brk = run_jobs(library64b, JOBS, stagger_ticks=1, push="f64")
     for a, b in zip(ref, brk):
         same(b, a)
+
+
+def test_run_until_idle_returns_every_job(library):
+    libs, B0 = library
+    srv = CampaignServer(libs, B0, capacity=20000, max_jobs=8, keep_cache=True, fill_particles=1000)
+    for j in JOBS:
+        srv.submit(j)
+    res = srv.run_until_idle(timeout_s=120)
+    srv.close()
+    assert sorted(r.job_id for r in res) == list(range(len(JOBS)))
+    alone = run_jobs(library, [JOBS[1]])[0]
+    same([r for r in res if r.job_id == 1][0], alone)
