@@ -440,7 +440,7 @@ def run_ours(args, ws, rank, local):
                 "field": "reference layout, six FP64 arrays", "speedup_mixed_vs_fp64": value / v64}
         del dens, fr
         torch.cuda.empty_cache()
-        # the same FP64 push over FP64 bricks: 64-byte SI node records in Morton
+        # the same FP64 push over FP64 bricks: SI node values in Morton
         # bricks, slots re-sorted by brick every 64 steps; bit-identical results
         # (the cache and state of every particle; tested against the oracle)
         fb64 = FieldLibrary(fields, grid, "brick_f64")
@@ -456,7 +456,7 @@ def run_ours(args, ws, rank, local):
         ms64b = max_over_ranks(ms64b, ws, dev)
         v64b = ws * n * 64 * K64 / (ms64b / 1e3)
         fp64["bricks"] = {"value": v64b, "unit": UNIT, "ms_per_step": ms64b / K64, "steps": K64,
-                          "field": "FP64 bricks (Morton 8^3, 64-byte SI node records), slots re-sorted by brick "
+                          "field": "FP64 bricks (Morton 8^3, SI node values in a 32-byte and a 16-byte plane), slots re-sorted by brick "
                                    "every 64 steps (imported, sorted and scattered back within each call)",
                           "field_bytes": fb64.device_bytes, "speedup_vs_reference_layout": v64b / v64,
                           "speedup_mixed_vs_fp64_bricks": value / v64b}

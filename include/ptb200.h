@@ -50,9 +50,10 @@ enum {
     PT_FIELD_BRICK_BF16 = 2, /* Morton 8^3 bricks, 6 comps interleaved per node, bfloat16     */
     PT_FIELD_BRICK_BF16_XPAIR = 3, /* as BF16, each 32-byte record holds a node and its +x neighbour:
                                       the 8 corners of a cell are 4 x 32-byte loads          */
-    PT_FIELD_BRICK_F64 = 4 /* Morton 8^3 bricks of 64-byte Float64 node records (Bx, By, Bz, ux,
-                              uy, uz, 0, 0) in SI units: the FP64 push reads the same values as
-                              from REF_F64 (bit-identical results) with 2 loads per corner */
+    PT_FIELD_BRICK_F64 = 4 /* Morton 8^3 bricks of Float64 SI values in two planes: (Bx, By, Bz, ux)
+                              32 bytes and (uy, uz) 16 bytes per node.  The FP64 push reads the
+                              same values as from REF_F64 (bit-identical results), 2 loads per
+                              corner                                                       */
 };
 
 /* cache written at every save step (pre-push state) */

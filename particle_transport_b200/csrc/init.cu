@@ -53,7 +53,7 @@ __device__ inline double node_B(const InitArgs& a, int64_t i, int64_t j, int64_t
 {
     if (a.storage == PT_FIELD_REF_F64) return a.B[c][(k * a.g.ny + j) * a.g.nx + i];
     const uint32_t node = a.offs[i] + a.offs[a.g.nx + j] + a.offs[a.g.nx + a.g.ny + k];
-    if (a.storage == PT_FIELD_BRICK_F64) return ((const double*)a.nodes)[8 * (size_t)node + c];  // SI, as REF_F64
+    if (a.storage == PT_FIELD_BRICK_F64) return ((const double*)a.nodes)[4 * (size_t)node + c];  // SI head plane
     if (a.storage == PT_FIELD_BRICK_F32) return (double)((const float*)a.nodes)[8 * (size_t)node + c];
     const size_t words = a.storage == PT_FIELD_BRICK_BF16 ? 4 : 8;  // 16 B records or 32 B x-pair records
     const uint32_t w = ((const uint32_t*)a.nodes)[words * node + (c >> 1)];

@@ -181,7 +181,7 @@ int field_create(pt_ctx* ctx, const double* const comps[6], bool on_device, cons
     }
     const double* src[6];
     for (int c = 0; c < 6; ++c) src[c] = on_device ? comps[c] : tmp[c];
-    rc = launch_brick_convert(src, *grid, B_ref, field_layout(storage), f->nodes, f->offs, s);
+    rc = launch_brick_convert(src, *grid, B_ref, field_layout(storage), f->nodes, f->offs, f->n_nodes, s);
     e = cudaStreamSynchronize(s);
     for (int c = 0; c < 6; ++c) if (tmp[c]) cudaFree(tmp[c]);
     if (rc) return cleanup(rc);
@@ -267,6 +267,7 @@ static int advance_exact_brick(pt_ctx* ctx, const pt_field* f, double* d_x1, dou
     if (n <= 0 || step_count <= 0) return PT_OK;
     PushArgsExactBrick a{};
     a.nodes = f->nodes;
+    a.tail = (const char*)f->nodes + 32 * (size_t)f->n_nodes;
     a.offs = f->offs;
     a.g = f->grid;
     a.n = n; a.dt = p->dt; a.nsteps = p->nsteps; a.stride = p->stride;

@@ -135,11 +135,12 @@ struct PushArgsRef {
 int launch_push_ref(const PushArgsRef& a, cudaStream_t s);
 
 // The same FP64 push over a BRICK_F64 field: the corner values are read from
-// 64-byte node records (2 loads per corner) instead of 6 arrays, and the
+// node records in two planes (2 loads per corner) instead of 6 arrays, and the
 // state may be in brick-sorted slot order with pid[slot] the particle's cache
 // column.  Same arithmetic, so the results are bit-identical.
 struct PushArgsExactBrick {
-    const void* nodes;
+    const void* nodes;     // head plane: (Bx, By, Bz, ux) per node, 32 bytes
+    const void* tail;      // tail plane: (uy, uz) per node, 16 bytes
     const uint32_t* offs;  // [nx + ny + nz] per-axis node offsets
     pt_grid g;
     double* x[3];
@@ -179,7 +180,7 @@ inline int field_layout(int storage)
 }
 inline size_t record_bytes(int storage)
 {
-    return storage == PT_FIELD_BRICK_BF16 ? 16 : (storage == PT_FIELD_BRICK_F64 ? 64 : 32);
+    return storage == PT_FIELD_BRICK_BF16 ? 16 : (storage == PT_FIELD_BRICK_F64 ? 48 : 32);
 }
 // brick forms read by the FP32 push
 inline bool fast_storage(int storage)
@@ -297,7 +298,7 @@ int launch_fast_export(const pt_fast_state* st, const pt_field* f, double* x1, d
 int fast_sort(pt_ctx* ctx, pt_fast_state* st, const pt_field* f, cudaStream_t s);
 
 int launch_brick_convert(const double* const comps[6], const pt_grid& g, double B_ref, int layout, void* nodes,
-                         const uint32_t* offs, cudaStream_t s);
+                         const uint32_t* offs, int64_t n_nodes, cudaStream_t s);
 
 struct DmumuArgs {
     const float* mu;

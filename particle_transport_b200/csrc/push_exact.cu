@@ -142,8 +142,8 @@ __global__ void __launch_bounds__(256) push_ref_kernel(PushArgsRef a)
     a.alive[p] = al ? 1 : 0;
 }
 
-// First 32 bytes of a 64-byte FP64 node record: (Bx, By, Bz, ux), one 256-bit
-// read-only load; the record is 64-byte aligned.
+// Head record (Bx, By, Bz, ux) of an FP64 node: one 256-bit read-only load
+// (32-byte aligned).
 __device__ __forceinline__ double4 ld_node_head(const double* r)
 {
     uint32_t w[8];
@@ -155,7 +155,8 @@ __device__ __forceinline__ double4 ld_node_head(const double* r)
 }
 
 // push_ref_kernel over a BRICK_F64 field: the 8 corners of the cell are
-// node records (ox[i] + oy[j] + oz[k] in the Morton brick order); each
+// node records (ox[i] + oy[j] + oz[k] in the Morton brick order) in a head
+// plane (Bx, By, Bz, ux) and a tail plane (uy, uz); each
 // component is interpolated by the lerps of sample() in the same order, so
 // every value equals the reference-layout kernel's.  Slots may be in brick
 // order; the cache column of slot p is pid[p].
@@ -172,6 +173,7 @@ __global__ void __launch_bounds__(256) push_exact_brick_kernel(PushArgsExactBric
     const uint32_t* oy = s_offs + nx;
     const uint32_t* oz = s_offs + nx + ny;
     const double* N = (const double*)a.nodes;
+    const double2* T = (const double2*)a.tail;
     const int64_t q = a.pid ? (int64_t)a.pid[p] : p;
     double xx = a.x[0][p], yy = a.x[1][p], zz = a.x[2][p];
     double px = a.p[0][p], py = a.p[1][p], pz = a.p[2][p];
@@ -198,14 +200,14 @@ __global__ void __launch_bounds__(256) push_exact_brick_kernel(PushArgsExactBric
                                     x0 + y0 + z1, x1 + y0 + z1, x0 + y1 + z1, x1 + y1 + z1};
             double4 h[8];
 #pragma unroll
-            for (int k = 0; k < 8; ++k) h[k] = ld_node_head(N + 8 * (size_t)nd[k]);
+            for (int k = 0; k < 8; ++k) h[k] = ld_node_head(N + 4 * (size_t)nd[k]);
             bx = lerp8(h[0].x, h[1].x, h[2].x, h[3].x, h[4].x, h[5].x, h[6].x, h[7].x, c.t);
             by = lerp8(h[0].y, h[1].y, h[2].y, h[3].y, h[4].y, h[5].y, h[6].y, h[7].y, c.t);
             bz = lerp8(h[0].z, h[1].z, h[2].z, h[3].z, h[4].z, h[5].z, h[6].z, h[7].z, c.t);
             if (do_push) {
                 double2 u[8];
 #pragma unroll
-                for (int k = 0; k < 8; ++k) u[k] = __ldg((const double2*)(N + 8 * (size_t)nd[k] + 4));
+                for (int k = 0; k < 8; ++k) u[k] = __ldg(T + nd[k]);
                 vfx = lerp8(h[0].w, h[1].w, h[2].w, h[3].w, h[4].w, h[5].w, h[6].w, h[7].w, c.t);
                 vfy = lerp8(u[0].x, u[1].x, u[2].x, u[3].x, u[4].x, u[5].x, u[6].x, u[7].x, c.t);
                 vfz = lerp8(u[0].y, u[1].y, u[2].y, u[3].y, u[4].y, u[5].y, u[6].y, u[7].y, c.t);

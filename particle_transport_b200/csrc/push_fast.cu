@@ -283,7 +283,7 @@ __global__ void brick_convert_kernel(const double* __restrict__ bx, const double
                                      const double* __restrict__ bz, const double* __restrict__ ux,
                                      const double* __restrict__ uy, const double* __restrict__ uz, int64_t nx,
                                      int64_t ny, int64_t nz, double inv_b, double inv_c, int layout, void* nodes,
-                                     const uint32_t* __restrict__ offs)
+                                     const uint32_t* __restrict__ offs, int64_t n_nodes)
 {
     const int64_t total = nx * ny * nz;
     auto comps = [&](int64_t t, float v[6]) {
@@ -302,10 +302,10 @@ __global__ void brick_convert_kernel(const double* __restrict__ bx, const double
         const int64_t i = t % nx, j = (t / nx) % ny, k = t / (nx * ny);
         const uint32_t node = offs[i] + offs[nx + j] + offs[nx + ny + k];
         if (layout == LAYOUT_F64) {
-            // SI values as they are (the FP64 push reads them unchanged)
-            double4* N = (double4*)nodes;
-            N[2 * (size_t)node] = make_double4(bx[t], by[t], bz[t], ux[t]);
-            N[2 * (size_t)node + 1] = make_double4(uy[t], uz[t], 0.0, 0.0);
+            // SI values as they are (the FP64 push reads them unchanged): the
+            // head plane (Bx, By, Bz, ux), then the tail plane (uy, uz)
+            ((double4*)nodes)[node] = make_double4(bx[t], by[t], bz[t], ux[t]);
+            ((double2*)((double4*)nodes + n_nodes))[node] = make_double2(uy[t], uz[t]);
             continue;
         }
         float v[6];
@@ -675,13 +675,14 @@ int launch_push_fast(const PushArgsFast& a, cudaStream_t s)
 }
 
 int launch_brick_convert(const double* const comps[6], const pt_grid& g, double B_ref, int layout, void* nodes,
-                         const uint32_t* offs, cudaStream_t s)
+                         const uint32_t* offs, int64_t n_nodes, cudaStream_t s)
 {
     const int64_t total = g.nx * g.ny * g.nz;
     const int threads = 256;
     int blocks = (int)std::min<int64_t>((total + threads - 1) / threads, 148 * 32);
     brick_convert_kernel<<<blocks, threads, 0, s>>>(comps[0], comps[1], comps[2], comps[3], comps[4], comps[5],
-                                                    g.nx, g.ny, g.nz, 1.0 / B_ref, 1.0 / C_LIGHT, layout, nodes, offs);
+                                                    g.nx, g.ny, g.nz, 1.0 / B_ref, 1.0 / C_LIGHT, layout, nodes, offs,
+                                                    n_nodes);
     PT_CHECK_LAUNCH("brick_convert_kernel");
     return PT_OK;
 }
