@@ -467,120 +467,115 @@ struct DppLaunch {
     const int64_t* lags;
     int nl;
     double p0;
-    int ppc, groups, parts;  // particle slots per CTA, 32-lag groups, warps splitting the starts
+    int ppc, wps;  // particle slots per CTA, warps per slot
     size_t slot_bytes;
     char* gslots;
     DppPart* part;  // [grid][nl]
 };
 
-// Warps = (particle slot, 32-lag group, part of the start range).  Lags are
-// dealt to lanes so that lags equal modulo 16 -- whose 8-byte |p| reads hit
-// the same shared-memory banks at every start -- fall into different groups.
+// Warps = (particle slot, lag subset): warp w of a slot owns lags w, w + wps,
+// w + 2 wps, ... and takes kDppLags of them at a time; its lanes take the
+// starts s = lane, lane + 32, ...  A warp's 8-byte |p| reads are then
+// consecutive (no shared-memory bank conflicts, whatever the lags), and
+// |p|[s] is read once for the lags of a pass.  The series of a slot holds |p| at saves 0..nsave-1 and
+// NaN at index nsave, so the end of a pair past the series reads NaN (an
+// invalid pair) with no bounds test.  A lag's sums are warp-reduced once per
+// particle and added by lane 0 into the slot's accumulator for that lag (one
+// writer per (slot, lag)); the CTA adds its slots in slot order at the end.
+// lags of a warp per pass over the starts (|p|[s] read once for them); 4 was
+// measured slower: a pass runs to the range of its smallest lag
+constexpr int kDppLags = 2;
+
 template <bool SMEM_SLOTS>
 __global__ void __launch_bounds__(1024) dpp_kernel(DppLaunch a)
 {
     extern __shared__ __align__(16) unsigned char smem[];
-    unsigned char* slot_base = SMEM_SLOTS ? smem : (unsigned char*)(a.gslots + (size_t)blockIdx.x * a.ppc * a.slot_bytes);
-    __shared__ int s_lane_lag[8 * kWarp];
-    __shared__ int s_lag_pos[8 * kWarp];
-    __shared__ unsigned char cnt[8][16];
-    __shared__ int fill[8];
-    for (int i = threadIdx.x; i < 8 * kWarp; i += blockDim.x) s_lane_lag[i] = -1;
-    for (int i = threadIdx.x; i < 8 * 16; i += blockDim.x) cnt[i / 16][i % 16] = 0;
-    if (threadIdx.x < 8) fill[threadIdx.x] = 0;
-    __syncthreads();
-    if (threadIdx.x == 0) {
-        // a lag of residue r goes to the group holding fewest lags of that
-        // residue, into lane r or r + 16 (the two half-warps) when free
-        for (int i = 0; i < a.nl; ++i) {
-            const int r = (int)(((a.lags[i] % 16) + 16) % 16);
-            int best = -1;
-            for (int g = 0; g < a.groups; ++g) {
-                if (fill[g] >= kWarp) continue;
-                if (best < 0 || cnt[g][r] < cnt[best][r] || (cnt[g][r] == cnt[best][r] && fill[g] < fill[best]))
-                    best = g;
-            }
-            int lane = -1;
-            for (int h = 0; h < 2 && lane < 0; ++h)
-                if (s_lane_lag[best * kWarp + r + 16 * h] < 0) lane = r + 16 * h;
-            for (int l = 0; l < kWarp && lane < 0; ++l)
-                if (s_lane_lag[best * kWarp + l] < 0) lane = l;
-            const int pos = best * kWarp + lane;
-            fill[best]++;
-            cnt[best][r]++;
-            s_lane_lag[pos] = i;
-            s_lag_pos[i] = pos;
-        }
-    }
-    __syncthreads();
+    // shared layout: acc[ppc][nl] | slots (when on chip)
+    DppPart* acc = (DppPart*)smem;
+    const size_t acc_bytes = ((size_t)a.ppc * a.nl * sizeof(DppPart) + 15) & ~(size_t)15;
+    unsigned char* slot_base =
+        SMEM_SLOTS ? smem + acc_bytes : (unsigned char*)(a.gslots + (size_t)blockIdx.x * a.ppc * a.slot_bytes);
+    for (int i = threadIdx.x; i < a.ppc * a.nl; i += blockDim.x) acc[i] = DppPart{0, 0.0, 0.0};
     const int warp = threadIdx.x / kWarp, lane = threadIdx.x % kWarp;
-    const int wps = a.groups * a.parts;
-    const int slot = warp / wps, group = (warp % wps) / a.parts, part = warp % a.parts;
-    const int li = s_lane_lag[group * kWarp + lane];
-    const bool lane_on = li >= 0;
-    int64_t L = lane_on ? a.lags[li] : 0;
-    if (L < 1 || L >= a.nsave) L = a.nsave;
-    const int64_t lim = a.nsave - L;
-    // the part's starts are a warp-uniform range of the group's longest one
-    // (every lane reads the same series[s], a broadcast); each lane stops at
-    // its own limit
-    const int64_t lim_max = (int64_t)__reduce_max_sync(0xffffffffu, (unsigned)lim);
-    const int64_t s_begin = lim_max * part / a.parts, s_end = lim_max * (part + 1) / a.parts;
+    const int slot = warp / a.wps, w = warp % a.wps;
+    const int nsave = (int)a.nsave;  // nsave < 2^31
     double* series = (double*)(slot_base + (size_t)slot * a.slot_bytes);
-    long long c = 0;
-    double sdp = 0, sdp2 = 0;
     const int64_t tiles = (a.chunk + a.ppc - 1) / a.ppc;
+    __syncthreads();
     for (int64_t tile = blockIdx.x; tile < tiles; tile += gridDim.x) {
         // cooperative staging: thread t -> (save, particle slot)
         const int64_t p0i = tile * a.ppc;
         const int np = (int)(a.chunk - p0i < (int64_t)a.ppc ? a.chunk - p0i : (int64_t)a.ppc);
-        for (int64_t t = threadIdx.x; t < (int64_t)np * a.nsave; t += blockDim.x) {
+        for (int64_t t = threadIdx.x; t < (int64_t)np * (a.nsave + 1); t += blockDim.x) {
             const int sl = (int)(t % np);
             const int64_t s = t / np;
-            const float* m = a.mom + s * 3 * a.chunk + p0i + sl;
-            ((double*)(slot_base + (size_t)sl * a.slot_bytes))[s] = pmag_exact(m[0], m[a.chunk], m[2 * a.chunk]);
+            double v = CUDART_NAN;  // the pad at index nsave
+            if (s < a.nsave) {
+                const float* m = a.mom + s * 3 * a.chunk + p0i + sl;
+                v = pmag_exact(m[0], m[a.chunk], m[2 * a.chunk]);
+            }
+            ((double*)(slot_base + (size_t)sl * a.slot_bytes))[s] = v;
         }
         __syncthreads();
         if (slot < np) {
             // |p| >= 0 or NaN or +inf, so pe - ps is finite exactly when both
-            // ends are finite; the normalised sums are sum(d)/p0 and
-            // sum(d^2)/p0^2, formed once per lag in dpp_finalize_kernel.
-            // 32-bit indices and a per-tile 32-bit count (nsave < 2^31)
-            const int sb = (int)s_begin, se = (int)s_end, lim32 = (int)lim, L32 = (int)L;
-            int ct = 0;
-            for (int s = sb; s < se; ++s) {
-                const double ps = series[s];
-                // past this lane's last start the end is not read; an invalid
-                // pair adds 0 (branch-free), which leaves the sums unchanged
-                const double pe = s < lim32 ? series[s + L32] : CUDART_NAN;
-                double d = pe - ps;
-                const bool ok = isfinite(d);
-                d = ok ? d : 0.0;
-                ct += (int)ok;
-                sdp += d;
-                sdp2 = fma(d, d, sdp2);
+            // ends are finite; an invalid pair adds 0 (branch-free), which
+            // leaves the sums unchanged.  The normalised sums are sum(d)/p0
+            // and sum(d^2)/p0^2, formed once per lag in dpp_finalize_kernel.
+            for (int l0 = w; l0 < a.nl; l0 += kDppLags * a.wps) {
+                int L[kDppLags], cnt[kDppLags];
+                double sd[kDppLags], sq[kDppLags];
+                int lmin = nsave;
+#pragma unroll
+                for (int k = 0; k < kDppLags; ++k) {
+                    const int l = l0 + k * a.wps;
+                    int v = l < a.nl ? (int)a.lags[l] : nsave;
+                    if (v < 1 || v >= nsave) v = nsave;  // reference: lag >= nsteps -> skipped
+                    L[k] = v;
+                    lmin = min(lmin, v);
+                    cnt[k] = 0;
+                    sd[k] = 0.0;
+                    sq[k] = 0.0;
+                }
+                const int lim = nsave - lmin;
+                for (int s = lane; s < lim; s += kWarp) {
+                    const double ps = series[s];
+#pragma unroll
+                    for (int k = 0; k < kDppLags; ++k) {
+                        const double pe = series[min((unsigned)s + (unsigned)L[k], (unsigned)nsave)];
+                        double d = pe - ps;
+                        const bool ok = isfinite(d);
+                        d = ok ? d : 0.0;
+                        cnt[k] += (int)ok;
+                        sd[k] += d;
+                        sq[k] = fma(d, d, sq[k]);
+                    }
+                }
+#pragma unroll
+                for (int k = 0; k < kDppLags; ++k) {
+#pragma unroll
+                    for (int o = 16; o > 0; o >>= 1) {
+                        cnt[k] += __shfl_xor_sync(0xffffffffu, cnt[k], o);
+                        sd[k] += __shfl_xor_sync(0xffffffffu, sd[k], o);
+                        sq[k] += __shfl_xor_sync(0xffffffffu, sq[k], o);
+                    }
+                    const int l = l0 + k * a.wps;
+                    if (lane == 0 && l < a.nl) {
+                        DppPart& A = acc[slot * a.nl + l];
+                        A.count += cnt[k]; A.sdp += sd[k]; A.sdp2 += sq[k];
+                    }
+                }
             }
-            c += ct;
         }
         __syncthreads();
     }
-    // CTA epilogue in fixed (slot, part) order
-    DppPart* wp = (DppPart*)smem;
-    __syncthreads();
-    wp[warp * kWarp + lane] = DppPart{c, sdp, sdp2};
-    __syncthreads();
-    const int nwarps = blockDim.x / kWarp;
+    // CTA epilogue: slots added in slot order
     for (int l = threadIdx.x; l < a.nl; l += blockDim.x) {
-        const int pos = s_lag_pos[l];
-        const int g = pos / kWarp, ln = pos % kWarp;
         DppPart r{0, 0, 0};
-        for (int sl = 0; sl < a.ppc; ++sl)
-            for (int q = 0; q < a.parts; ++q) {
-                const int w = sl * wps + g * a.parts + q;
-                if (w >= nwarps) continue;
-                const DppPart v = wp[w * kWarp + ln];
-                r.count += v.count; r.sdp += v.sdp; r.sdp2 += v.sdp2;
-            }
+        for (int sl = 0; sl < a.ppc; ++sl) {
+            const DppPart v = acc[sl * a.nl + l];
+            r.count += v.count; r.sdp += v.sdp; r.sdp2 += v.sdp2;
+        }
         a.part[(int64_t)blockIdx.x * a.nl + l] = r;
     }
 }
@@ -890,20 +885,20 @@ int run_dpp(pt_ctx* ctx, const DppArgs& a, cudaStream_t s)
     int max_smem = 0;
     cudaDeviceGetAttribute(&max_smem, cudaDevAttrMaxSharedMemoryPerBlockOptin, ctx->device);
     const size_t budget = (size_t)std::min(max_smem, 200 * 1024);
-    const size_t slot_bytes = align16(sizeof(double) * a.nsave);
+    if (a.nsave >= INT32_MAX) return fail(PT_ERR_ARG, "nsave must be below 2^31");
+    const size_t slot_bytes = align16(sizeof(double) * (size_t)(a.nsave + 1));  // + NaN pad
     const int nl_cap = 32 * 8;
     for (int lag0 = 0; lag0 < a.n_lags; lag0 += nl_cap) {
         const int nl = std::min(nl_cap, a.n_lags - lag0);
-        const int groups = (nl + kWarp - 1) / kWarp;
-        const size_t fixed = sizeof(DppPart) * 1024;
-        bool smem_slots = slot_bytes <= budget - fixed;
-        int ppc = smem_slots ? (int)std::min<size_t>((budget - fixed) / slot_bytes, (size_t)(32 / groups))
-                             : std::max(1, std::min(8, 32 / groups));
+        // particle slots per CTA (series on chip when they fit) and warps per
+        // slot (each takes ceil(nl / wps) lags, two at a time)
+        const size_t acc_per_slot = sizeof(DppPart) * (size_t)nl;
+        bool smem_slots = align16(acc_per_slot) + slot_bytes <= budget;
+        int ppc = smem_slots ? (int)std::min<size_t>(budget / (slot_bytes + acc_per_slot), 8) : 4;
         ppc = std::max(1, ppc);
-        // more warps share each staged series: split its starts over `parts` warps
-        const int parts = std::max(1, std::min(4, 32 / (ppc * groups)));
-        const int threads = ppc * groups * parts * kWarp;
-        const size_t smem = std::max(fixed, smem_slots ? (size_t)ppc * slot_bytes : 0);
+        const int wps = std::max(1, std::min(32 / ppc, (nl + kDppLags - 1) / kDppLags));
+        const int threads = ppc * wps * kWarp;
+        const size_t smem = align16(acc_per_slot * ppc) + (smem_slots ? (size_t)ppc * slot_bytes : 0);
         const int64_t tiles = (a.chunk + ppc - 1) / ppc;
         void* kfn = smem_slots ? (void*)dpp_kernel<true> : (void*)dpp_kernel<false>;
         PT_CUDA(cudaFuncSetAttribute(kfn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
@@ -918,7 +913,7 @@ int run_dpp(pt_ctx* ctx, const DppArgs& a, cudaStream_t s)
         if (rc) return rc;
         DppLaunch L;
         L.mom = a.mom; L.chunk = a.chunk; L.nsave = a.nsave; L.lags = a.lags + lag0; L.nl = nl; L.p0 = a.p0;
-        L.ppc = ppc; L.groups = groups; L.parts = parts; L.slot_bytes = slot_bytes;
+        L.ppc = ppc; L.wps = wps; L.slot_bytes = slot_bytes;
         L.part = (DppPart*)scratch;
         L.gslots = smem_slots ? nullptr : (char*)scratch + align16(sizeof(DppPart) * (size_t)grid * nl);
         if (smem_slots) dpp_kernel<true><<<grid, threads, smem, s>>>(L);

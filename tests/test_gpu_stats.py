@@ -114,7 +114,8 @@ def test_dmumu_rejects_bad_lags(cuda):
         gpu_dmumu(mu, np.array([0, 1]), edges)
 
 
-@pytest.mark.parametrize("chunk,nsave,n_lags", [(500, 201, 24), (37, 1000, 40), (2, 30001, 5)])
+@pytest.mark.parametrize("chunk,nsave,n_lags", [(500, 201, 24), (37, 1000, 40), (2, 30001, 5), (64, 1500, 300),
+                                                 (16, 6000, 500)])
 def test_dpp_matches_oracle(cuda, oracle, chunk, nsave, n_lags):
     rng = np.random.default_rng(chunk)
     p = 5.4e-19 * (1 + 1e-3 * np.cumsum(rng.normal(size=(nsave, 1, chunk)), axis=0))
