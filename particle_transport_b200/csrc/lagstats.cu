@@ -529,8 +529,9 @@ __global__ void __launch_bounds__(1024) dpp_kernel(DppLaunch a)
 #pragma unroll
                 for (int k = 0; k < kDppLags; ++k) {
                     const int l = l0 + k * a.wps;
-                    int v = l < a.nl ? (int)a.lags[l] : nsave;
-                    if (v < 1 || v >= nsave) v = nsave;  // reference: lag >= nsteps -> skipped
+                    // the range test in 64 bits, before the narrowing
+                    const int64_t v64 = l < a.nl ? a.lags[l] : a.nsave;
+                    const int v = (v64 < 1 || v64 >= a.nsave) ? nsave : (int)v64;  // lag >= nsteps -> skipped
                     L[k] = v;
                     lmin = min(lmin, v);
                     cnt[k] = 0;

@@ -61,7 +61,8 @@ def test_empty_inputs_are_no_ops(cuda):
 def test_dmumu_all_nan_and_lags_beyond_series(cuda, oracle):
     mu = random_mu_cache(64, 50, seed=1)
     mu[::3] = np.nan  # every third particle dead from the start
-    lags = np.array([1, 49, 50, 51, 1000])  # 50 and beyond: no pair (lag >= nsave is skipped)
+    # 50 and beyond: no pair (lag >= nsave is skipped), past 2^32 too
+    lags = np.array([1, 49, 50, 51, 1000, 2 ** 32 + 3], dtype=np.int64)
     edges, _ = build_mu_edges_full(0.0, 1.0, 10)
     o = zero_dmumu(len(lags), 10)
     oracle.dmumu_accumulate(mu, lags, edges, o)
@@ -96,7 +97,9 @@ def test_dpp_nan_and_long_lags(cuda, oracle):
     mom = (5e-19 * (1 + 1e-3 * rng.normal(size=(300, 3, 40)))).astype(np.float32)
     mom[:, :, 7] = np.nan
     mom[100:, :, 3] = np.nan
-    lags = np.array([1, 2, 299, 300, 400])
+    # lags at and past the series end are skipped (one beyond 2^32 too: the
+    # range test must come before any narrowing of the lag)
+    lags = np.array([1, 2, 299, 300, 400, 2 ** 32 + 5], dtype=np.int64)
     o = zero_dpp(len(lags))
     oracle.dpp_accumulate(mom, lags, 5e-19, o)
     g = S.new_dpp_accumulators(len(lags))
