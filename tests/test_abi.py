@@ -37,3 +37,28 @@ def test_no_cpu_fallback_in_product():
                 src = open(os.path.join(root, f)).read()
                 assert "import oracle" not in src and "from oracle" not in src, f
                 assert "libptoracle" not in src, f
+
+
+def test_header_is_plain_c(tmp_path):
+    """A C host (Julia's ccall, cgo, ctypes) sees the header as C: it compiles
+    as pedantic C99, and the structs the host fills keep their field names."""
+    import shutil
+    import subprocess
+
+    import pytest
+
+    cc = shutil.which("gcc") or shutil.which("cc")
+    if not cc:
+        pytest.skip("no C compiler")
+    src = tmp_path / "use_header.c"
+    src.write_text('#include "ptb200.h"\n'
+                   "int main(void) {\n"
+                   "    pt_campaign_desc d = {0};\n"
+                   "    pt_push_params p = {0};\n"
+                   "    d.sort_every = 2; d.n_mom = 1; p.sort_every = 64;\n"
+                   "    return PT_FIELD_BRICK_F64 - 4 + (int)(d.sort_every - 2) + (int)(p.sort_every - 64);\n"
+                   "}\n")
+    out = subprocess.run([cc, "-std=c99", "-Wall", "-Wextra", "-pedantic", "-Werror",
+                          "-I" + os.path.dirname(HEADER), "-c", str(src), "-o", str(tmp_path / "use_header.o")],
+                         capture_output=True, text=True)
+    assert out.returncode == 0, out.stderr
