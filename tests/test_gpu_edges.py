@@ -11,7 +11,7 @@ from helpers import copy_state, fortran_fields, random_mu_cache, small_problem, 
 from particle_transport_b200 import runner as R
 from particle_transport_b200 import stats as S
 from particle_transport_b200.fields import FieldLibrary
-from particle_transport_b200.time_units import build_mu_edges_full, log_spaced_lag_steps
+from particle_transport_b200.time_units import build_mu_edges_full
 
 pytestmark = pytest.mark.gpu
 

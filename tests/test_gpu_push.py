@@ -4,7 +4,6 @@ FP64 form: bit-identical to the oracle (and so to a Float64 run of the
 reference) -- trajectories, mu cache, phase-space cache and alive counts.
 FP32 form over Morton bricks: bounded deviation over the first gyroperiod,
 exact |p| conservation with E = 0, results independent of the brick sort."""
-import math
 
 import numpy as np
 import pytest

@@ -5,7 +5,7 @@ from types import SimpleNamespace
 import numpy as np
 
 from particle_transport_b200.batch import cells_per_step, cells_per_step_gamma, sort_cadence, speed_class
-from particle_transport_b200.fields import C_LIGHT, M_P, Q_E
+from particle_transport_b200.fields import C_LIGHT, M_P
 from particle_transport_b200.particles import energy_to_gamma
 
 
