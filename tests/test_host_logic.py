@@ -1,0 +1,101 @@
+"""Host logic of the batch tuner and of the server's admission (no GPU).
+
+tune_batch times real batches on a B200; here its timing trial is replaced
+by a synthetic rate model, so the selection logic itself is checked: speed
+classes, the cadence per class, K = the shortest cadence, each campaign's
+sort_every, the blocks-per-SM choice and the JSON cache.  The server admits
+waiting jobs in arrival order while the HBM budget has room, and holds every
+later job behind one that does not fit."""
+import math
+from types import SimpleNamespace
+
+import numpy as np
+
+from particle_transport_b200 import batch as B
+from particle_transport_b200.fields import C_LIGHT, M_P
+from particle_transport_b200.particles import energy_to_gamma
+from particle_transport_b200.server import CampaignServer, JobSpec
+
+
+def campaign(E_GeV, n, dx=1.0):
+    g = energy_to_gamma(E_GeV)
+    p = g * M_P * C_LIGHT * math.sqrt(1 - 1 / g ** 2)
+    fld = SimpleNamespace(grid=SimpleNamespace(dx=dx, dy=dx, dz=dx, nx=64))
+    # a fixed number of steps per gyroperiod: dt grows with gamma; a 1 GeV
+    # particle covers 0.1 cell per step, a 100 GeV one about 11
+    g1 = energy_to_gamma(1.0)
+    v1 = C_LIGHT * math.sqrt(1 - 1 / g1 ** 2)
+    dt = 0.1 * dx / v1 * (g / g1)
+    state = {"x1": np.zeros(n), "p1": np.array([p]), "p2": np.array([0.0]), "p3": np.array([0.0])}
+    return dict(field=fld, state=state, dt=dt, nsteps=1000, stride=8, E=E_GeV)
+
+
+def test_tune_batch_selection_and_cache(tmp_path, monkeypatch):
+    monkeypatch.setenv("PTB200_TUNE_CACHE", str(tmp_path))
+    calls = []
+
+    def fake_trial(camps, storage, capacity, K, bps, sort_every, steps):
+        calls.append((len(camps), K, bps, tuple(sort_every)))
+        # slow particles prefer long cadences, fast ones short; 2 blocks per SM best
+        cps = B.cells_per_step(camps[0]["field"], camps[0]["state"], camps[0]["dt"])
+        best = 128 if cps < 0.5 else (16 if cps > 4 else 64)
+        rate = 1e10 / (1 + abs(math.log2(K / best)))
+        return rate * (1.0 if bps == 2 else 0.9)
+
+    monkeypatch.setattr(B, "_trial", fake_trial)
+    camps = [campaign(1.0, 1000), campaign(100.0, 2000), campaign(1.0, 500), campaign(100.0, 700)]
+    t = B.tune_batch(camps, "brick_f32", 10_000, use_cache=True)
+    cls = [B.speed_class(B.cells_per_step(c["field"], c["state"], c["dt"])) for c in camps]
+    assert cls[0] == cls[2] and cls[1] == cls[3] and cls[0] < cls[1]
+    assert t["cadence_steps"] == {cls[0]: 128, cls[1]: 16}
+    assert t["K"] == 16 and t["blocks_per_sm"] == 2 and not t["cached"]
+    assert t["sort_every"] == [8, 1, 8, 1]  # 128 / 16 and 16 / 16 epochs
+    # each class timed alone at every cadence, then the whole batch at each block count
+    assert sum(1 for c in calls if c[0] == 2) == 2 * 4 and sum(1 for c in calls if c[0] == 4) == 3
+    n_calls = len(calls)
+    t2 = B.tune_batch(camps, "brick_f32", 10_000, use_cache=True)
+    assert t2["cached"] and len(calls) == n_calls  # served from the JSON file
+    assert (t2["K"], t2["blocks_per_sm"], t2["sort_every"]) == (t["K"], t["blocks_per_sm"], t["sort_every"])
+
+
+def admission_server(budget):
+    srv = CampaignServer.__new__(CampaignServer)
+    srv.budget = budget
+    srv.used = 0.0
+    srv.queue = []
+    srv.active = {}
+    srv.admit_s = 0.0
+    admitted = []
+
+    def fake_admit(jid, spec, arrival):
+        admitted.append(jid)
+        srv.active[jid] = {"bytes": srv.job_bytes(spec)}
+        srv.used += srv.job_bytes(spec)
+
+    srv._admit = fake_admit
+    return srv, admitted
+
+
+def test_admission_in_order_under_the_budget():
+    small = JobSpec("256", "total", 1.0, 10_000, 10.0)
+    big = JobSpec("256", "total", 1.0, 4_000_000, 300.0)
+    s_b, b_b = CampaignServer.job_bytes(small), CampaignServer.job_bytes(big)
+    srv, admitted = admission_server(budget=b_b + 1.5 * s_b)
+    for i, spec in enumerate([small, big, small, small]):
+        srv.queue.append((i, spec, 0.0))
+    assert srv.admit() == 2
+    # job 2 no longer fits beside the big job and the first small one; job 3,
+    # which would fit, waits behind it (no overtaking)
+    assert admitted == [0, 1] and [q[0] for q in srv.queue] == [2, 3]
+    # the big job leaves: its bytes return to the budget, the rest are admitted
+    srv.used -= b_b
+    assert srv.admit() == 2 and admitted == [0, 1, 2, 3] and srv.queue == []
+
+
+def test_admission_holds_later_jobs_behind_one_that_does_not_fit():
+    small = JobSpec("256", "total", 1.0, 10_000, 10.0)
+    big = JobSpec("256", "total", 1.0, 4_000_000, 300.0)
+    srv, admitted = admission_server(budget=CampaignServer.job_bytes(big) * 0.5)
+    srv.queue = [(0, big, 0.0), (1, small, 0.0)]
+    assert srv.admit() == 0 and admitted == []  # FIFO: the small job does not overtake
+    assert [q[0] for q in srv.queue] == [0, 1]
