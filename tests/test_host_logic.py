@@ -84,8 +84,8 @@ def test_admission_in_order_under_the_budget():
     for i, spec in enumerate([small, big, small, small]):
         srv.queue.append((i, spec, 0.0))
     assert srv.admit() == 2
-    # job 2 no longer fits beside the big job and the first small one; job 3,
-    # which would fit, waits behind it (no overtaking)
+    # job 2 no longer fits beside the big job and the first small one; job 3
+    # waits behind it
     assert admitted == [0, 1] and [q[0] for q in srv.queue] == [2, 3]
     # the big job leaves: its bytes return to the budget, the rest are admitted
     srv.used -= b_b
