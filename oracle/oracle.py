@@ -66,6 +66,16 @@ def lib():
         L.or_num_threads.restype = i32
         L.or_init_particles.restype = i64
         L.or_init_particles.argtypes = [i64, C.c_uint64, d, i32, i32, d, P, P, C.POINTER(Grid), P, P, P, P, P, P]
+        L.or_dmumu_arrays_full.restype = None
+        L.or_dmumu_arrays_full.argtypes = [P, P, P, P, P, i32, i32, i64, P]
+        L.or_average_over_tau_full.restype = None
+        L.or_average_over_tau_full.argtypes = [P, P, i32, i32, i64, P, P]
+        L.or_sem_from_stats.restype = d
+        L.or_sem_from_stats.argtypes = [i64, d]
+        L.or_output_table.restype = None
+        L.or_output_table.argtypes = [P, i32, P, P, P, P, P, P, P]
+        L.or_dpp_arrays.restype = None
+        L.or_dpp_arrays.argtypes = [P, P, P, P, P, P, P, i32, P]
         _lib = L
     return _lib
 
@@ -208,3 +218,60 @@ def init_particles(n, seed, energy_GeV, grid, injection="isotropic", mu0=0.0, po
                                   _ptr_array(bs) if bs else None, C.byref(g),
                                   *[_p(out[k]) for k in ("x1", "x2", "x3", "p1", "p2", "p3")])
     return out, int(bad)
+
+
+DMUMU_ARRAY_KEYS = ("mean_delta", "mean_delta2", "drift_norm", "dmumu_raw_norm", "dmumu_centered_norm",
+                    "dmumu_raw_per_s", "dmumu_centered_per_s")
+DPP_ARRAY_KEYS = ("mean_delta_p", "mean_delta_p2", "mean_delta_p_norm", "mean_delta_p_norm2", "dpp_raw_per_s",
+                  "dpp_centered_per_s", "dpp_raw_norm", "dpp_centered_norm")
+TABLE_KEYS = ("tau_s", "tau_norm", "tau_gyroperiods", "delta_mu2_particle_std", "delta_mu2_particle_sem",
+              "delta_mu2_pair_mean")
+
+
+def _f64(a):
+    return np.ascontiguousarray(a, dtype=np.float64)
+
+
+def _i64(a):
+    return np.ascontiguousarray(a, dtype=np.int64)
+
+
+def dmumu_arrays_full(counts, sum_d, sum_d2, tau_s, tau_norm, min_count_per_cell):
+    """compute_dmumu_arrays_full on (n_lags, n_bins) arrays (the Julia
+    (n_bins, n_lags) arrays in C order); returns a dict of the seven arrays."""
+    counts = _i64(counts)
+    n_lags, n_bins = counts.shape
+    out = np.empty((7, n_lags, n_bins))
+    lib().or_dmumu_arrays_full(_p(counts), _p(_f64(sum_d)), _p(_f64(sum_d2)), _p(_f64(tau_s)), _p(_f64(tau_norm)),
+                               n_lags, n_bins, int(min_count_per_cell), _p(out))
+    return dict(zip(DMUMU_ARRAY_KEYS, out))
+
+
+def average_over_tau_full(values, counts, min_count_per_cell):
+    counts = _i64(counts)
+    n_lags, n_bins = counts.shape
+    unw, cw = np.empty(n_bins), np.empty(n_bins)
+    lib().or_average_over_tau_full(_p(_f64(values)), _p(counts), n_lags, n_bins, int(min_count_per_cell), _p(unw),
+                                   _p(cw))
+    return unw, cw
+
+
+def sem_from_stats(count, m2):
+    return float(lib().or_sem_from_stats(int(count), float(m2)))
+
+
+def output_table(lag_steps, t_s, t_norm, particle_counts, particle_m2s, pair_sum_squares, pair_counts):
+    """The computed columns of build_output_dataframe."""
+    lags = _i64(lag_steps)
+    out = np.empty((6, len(lags)))
+    lib().or_output_table(_p(lags), len(lags), _p(_f64(t_s)), _p(_f64(t_norm)), _p(_i64(particle_counts)),
+                          _p(_f64(particle_m2s)), _p(_f64(pair_sum_squares)), _p(_i64(pair_counts)), _p(out))
+    return dict(zip(TABLE_KEYS, out))
+
+
+def dpp_arrays(counts, sum_dp, sum_dp2, sum_dpn, sum_dpn2, tau_s, tau_norm):
+    counts = _i64(counts)
+    out = np.empty((8, len(counts)))
+    lib().or_dpp_arrays(_p(counts), _p(_f64(sum_dp)), _p(_f64(sum_dp2)), _p(_f64(sum_dpn)), _p(_f64(sum_dpn2)),
+                        _p(_f64(tau_s)), _p(_f64(tau_norm)), len(counts), _p(out))
+    return dict(zip(DPP_ARRAY_KEYS, out))

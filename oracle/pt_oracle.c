@@ -565,6 +565,134 @@ void or_energy_snapshots(const float* mom, int64_t chunk, int64_t nsave, const i
 }
 
 /* ------------------------------------------------------------------------
+ * Derived product arrays: the formulas that turn the accumulators into the
+ * numbers the reference writes into its HDF5 products and tables.
+ * --------------------------------------------------------------------- */
+
+/* Julia's max(0.0, x) for Float64: NaN propagates (C's fmax would drop it). */
+static inline double or_jl_max0(double x)
+{
+    if (isnan(x)) return x;
+    return x > 0.0 ? x : 0.0;
+}
+
+/* compute_dmumu_arrays_full: src/compute_delta_mu2_dmumu_full.jl:706-744.
+ * counts/sum_d/sum_d2 are Julia (n_bins, n_lags) arrays, bins fastest.  out
+ * holds seven arrays of that shape one after another: mean_delta,
+ * mean_delta2, drift_norm, dmumu_raw_norm, dmumu_centered_norm,
+ * dmumu_raw_per_s, dmumu_centered_per_s.  Cells with count < min_count stay
+ * NaN (fill(NaN, ...)). */
+void or_dmumu_arrays_full(const int64_t* counts, const double* sum_d, const double* sum_d2, const double* tau_s,
+                          const double* tau_norm, int n_lags, int n_bins, int64_t min_count, double* out)
+{
+    const int64_t cells = (int64_t)n_lags * n_bins;
+    for (int64_t i = 0; i < 7 * cells; ++i) out[i] = NAN;
+    for (int l = 0; l < n_lags; ++l) {
+        const double normalized_lag = tau_norm[l];
+        const double physical_lag = tau_s[l];
+        for (int b = 0; b < n_bins; ++b) {
+            const int64_t c = (int64_t)l * n_bins + b;
+            const int64_t count = counts[c];
+            if (!(count >= min_count)) continue;
+            const double delta_mean = sum_d[c] / (double)count;
+            const double delta2_mean = sum_d2[c] / (double)count;
+            const double centered = or_jl_max0(delta2_mean - delta_mean * delta_mean);
+            out[0 * cells + c] = delta_mean;
+            out[1 * cells + c] = delta2_mean;
+            out[2 * cells + c] = delta_mean / normalized_lag;
+            out[3 * cells + c] = delta2_mean / (2.0 * normalized_lag);
+            out[4 * cells + c] = centered / (2.0 * normalized_lag);
+            out[5 * cells + c] = delta2_mean / (2.0 * physical_lag);
+            out[6 * cells + c] = centered / (2.0 * physical_lag);
+        }
+    }
+}
+
+/* average_over_tau_full: src/compute_delta_mu2_dmumu_full.jl:746-776.
+ * values/counts are Julia (n_bins, n_lags); out_unweighted and
+ * out_count_weighted have n_bins entries (NaN where no lag qualifies). */
+void or_average_over_tau_full(const double* values, const int64_t* counts, int n_lags, int n_bins,
+                              int64_t min_count, double* out_unweighted, double* out_count_weighted)
+{
+    for (int b = 0; b < n_bins; ++b) {
+        double value_sum = 0.0, weighted_sum = 0.0;
+        int64_t valid_lags = 0, total_weight = 0;
+        for (int l = 0; l < n_lags; ++l) {
+            const double value = values[(int64_t)l * n_bins + b];
+            const int64_t count = counts[(int64_t)l * n_bins + b];
+            if (isfinite(value) && count >= min_count) {
+                value_sum += value;
+                valid_lags += 1;
+                weighted_sum += value * (double)count;
+                total_weight += count;
+            }
+        }
+        out_unweighted[b] = valid_lags > 0 ? value_sum / (double)valid_lags : NAN;
+        out_count_weighted[b] = total_weight > 0 ? weighted_sum / (double)total_weight : NAN;
+    }
+}
+
+/* sem_from_stats: src/compute_delta_mu2_curve.jl:387-393. */
+double or_sem_from_stats(int64_t count, double m2)
+{
+    if (count <= 1) return NAN;
+    const double variance = m2 / (double)(count - 1);
+    return sqrt(variance / (double)count);
+}
+
+/* The computed columns of build_output_dataframe:
+ * src/compute_delta_mu2_curve.jl:409-429.  lag_steps are offsets into the
+ * sample times t_s / t_norm (0-based here: t[lag] - t[0] is Julia's
+ * t[lag + 1] - t[1]).  out holds six n_lags arrays: tau_s, tau_norm,
+ * tau_gyroperiods (tOmega0_to_gyroperiods, src/time_units.jl:8),
+ * delta_mu2_particle_std, delta_mu2_particle_sem, delta_mu2_pair_mean. */
+void or_output_table(const int64_t* lag_steps, int n_lags, const double* t_s, const double* t_norm,
+                     const int64_t* particle_counts, const double* particle_m2s, const double* pair_sum_squares,
+                     const int64_t* pair_counts, double* out)
+{
+    const double two_pi = 2.0 * 3.141592653589793;
+    for (int l = 0; l < n_lags; ++l) {
+        const int64_t lag = lag_steps[l];
+        const double tau_norm = t_norm[lag] - t_norm[0];
+        const int64_t count = particle_counts[l];
+        out[0 * n_lags + l] = t_s[lag] - t_s[0];
+        out[1 * n_lags + l] = tau_norm;
+        out[2 * n_lags + l] = tau_norm / two_pi;
+        out[3 * n_lags + l] = count <= 1 ? NAN : sqrt(particle_m2s[l] / (double)(count - 1));
+        out[4 * n_lags + l] = or_sem_from_stats(count, particle_m2s[l]);
+        out[5 * n_lags + l] = pair_counts[l] == 0 ? NAN : pair_sum_squares[l] / (double)pair_counts[l];
+    }
+}
+
+/* compute_dpp_arrays: src/compute_dpp_full.jl:301-330.  Inputs are the five
+ * per-lag accumulators; out holds eight n_lags arrays: mean_delta_p,
+ * mean_delta_p2, mean_delta_p_norm, mean_delta_p_norm2, dpp_raw_per_s,
+ * dpp_centered_per_s, dpp_raw_norm, dpp_centered_norm (NaN where count = 0). */
+void or_dpp_arrays(const int64_t* counts, const double* sum_dp, const double* sum_dp2, const double* sum_dpn,
+                   const double* sum_dpn2, const double* tau_s, const double* tau_norm, int n_lags, double* out)
+{
+    for (int64_t i = 0; i < 8 * (int64_t)n_lags; ++i) out[i] = NAN;
+    for (int l = 0; l < n_lags; ++l) {
+        const int64_t count = counts[l];
+        if (!(count > 0)) continue;
+        const double delta_mean = sum_dp[l] / (double)count;
+        const double delta2_mean = sum_dp2[l] / (double)count;
+        const double norm_mean = sum_dpn[l] / (double)count;
+        const double norm2_mean = sum_dpn2[l] / (double)count;
+        const double centered = or_jl_max0(delta2_mean - delta_mean * delta_mean);
+        const double centered_norm = or_jl_max0(norm2_mean - norm_mean * norm_mean);
+        out[0 * n_lags + l] = delta_mean;
+        out[1 * n_lags + l] = delta2_mean;
+        out[2 * n_lags + l] = norm_mean;
+        out[3 * n_lags + l] = norm2_mean;
+        out[4 * n_lags + l] = delta2_mean / (2.0 * tau_s[l]);
+        out[5 * n_lags + l] = centered / (2.0 * tau_s[l]);
+        out[6 * n_lags + l] = norm2_mean / (2.0 * tau_norm[l]);
+        out[7 * n_lags + l] = centered_norm / (2.0 * tau_norm[l]);
+    }
+}
+
+/* ------------------------------------------------------------------------
  * Particle initialisation: init_particles / rand_unit_vector /
  * fixed_mu_unit_vector (src/phase_space_gpu_runner.jl:51-66, 170-245) over
  * the counter-based stream of the device initialiser: draw d of particle i

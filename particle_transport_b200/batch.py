@@ -343,6 +343,21 @@ def _trial(campaigns, storage, capacity, K, bps, sort_every, steps):
     return sum(len(c["state"]["x1"]) for c in campaigns) * K * epochs / el
 
 
+def check_cadences(cadences) -> None:
+    """A campaign re-sorts every (its cadence / K) epochs, where K is the
+    shortest cadence picked; that is exact only when each candidate cadence is
+    a multiple of every shorter one (16, 32, 64, 128 is; 16, 48, 64 is not:
+    48 and 64 would give K = 48 and a 64-step class sorting every epoch)."""
+    cs = sorted(set(int(c) for c in cadences))
+    if not cs or cs[0] < 1:
+        raise ValueError("cadences must be positive step counts")
+    for i, c in enumerate(cs):
+        for d in cs[:i]:
+            if c % d:
+                raise ValueError(f"cadence {c} is not a multiple of the shorter cadence {d}; each candidate cadence "
+                                 "must be a multiple of every shorter one")
+
+
 def tune_batch(campaigns, storage: str, capacity: int, cadences=(16, 32, 64, 128), blocks=(1, 2, 3),
                steps: int = 256, use_cache: bool = True) -> dict:
     """Launch shape and per-campaign sort cadence of a batch.
@@ -359,6 +374,7 @@ def tune_batch(campaigns, storage: str, capacity: int, cadences=(16, 32, 64, 128
     particle count, grid and speed classes.  Returns {"K", "blocks_per_sm",
     "sort_every" (one per campaign, in epochs), "cadence_steps" (per class),
     "timings"}."""
+    check_cadences(cadences)
     n_total = sum(len(c["state"]["x1"]) for c in campaigns)
     grid_n = max(c["field"].grid.nx for c in campaigns)
     cls = [speed_class(cells_per_step(c["field"], c["state"], c["dt"])) for c in campaigns]

@@ -188,7 +188,7 @@ extern "C" int pt_particles_init_device(pt_ctx* ctx, const pt_field* field, cons
     double* outs[6] = {d_x1, d_x2, d_x3, d_p1, d_p2, d_p3};
     for (int c = 0; c < 6; ++c) a.out[c] = outs[c];
 
-    PT_CUDA(cudaSetDevice(ctx->device));
+    PT_DEVICE_SCOPE(ctx->device);
     int* d_bad = nullptr;
     int rc = scratch_get(ctx, 3, sizeof(int), (void**)&d_bad);
     if (rc) return rc;

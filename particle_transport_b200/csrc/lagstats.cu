@@ -1096,6 +1096,7 @@ extern "C" int pt_dmumu_accumulate_device_noalloc(pt_ctx* ctx, const float* d_mu
     if (!(d_mu && d_lags && d_edges && d_counts && d_sum_d && d_sum_d2 && d_w_count && d_w_mean && d_w_m2 &&
           d_pair_ss && d_pair_n))
         return fail(PT_ERR_ARG, "null pointer");
+    PT_DEVICE_SCOPE(ctx->device);
     DmumuArgs a{d_mu, n, nsave, sp, ss, d_lags, n_lags, d_edges, n_bins, start_mode == PT_START_INJECTION, bin_abs != 0,
                 d_counts, d_sum_d, d_sum_d2, d_w_count, d_w_mean, d_w_m2, d_pair_ss, d_pair_n};
     return run_dmumu_noalloc(ctx, a, ctx->stream);

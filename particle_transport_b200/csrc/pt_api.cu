@@ -122,7 +122,7 @@ int field_create(pt_ctx* ctx, const double* const comps[6], bool on_device, cons
     if (fast_storage(storage) && !(B_ref > 0 && std::isfinite(B_ref)))
         return fail(PT_ERR_ARG, "B_ref_T must be finite and positive for the FP32-push brick storages");
     if (grid->nx > 4096 || grid->ny > 4096 || grid->nz > 4096) return fail(PT_ERR_ARG, "grid axis above 4096 nodes");
-    PT_CUDA(cudaSetDevice(ctx->device));
+    PT_DEVICE_SCOPE(ctx->device);
     pt_field* f = new (std::nothrow) pt_field();
     if (!f) return fail(PT_ERR_OOM, "host allocation failed");
     f->ctx = ctx;
@@ -381,7 +381,7 @@ int pt_ctx_create(int device, pt_ctx** out)
     cudaError_t e = cudaGetDeviceCount(&count);
     if (e != cudaSuccess) return cuda_fail(e, "cudaGetDeviceCount");
     if (device < 0 || device >= count) return fail(PT_ERR_ARG, "device index out of range");
-    PT_CUDA(cudaSetDevice(device));
+    PT_DEVICE_SCOPE(device);
     cudaDeviceProp prop;
     PT_CUDA(cudaGetDeviceProperties(&prop, device));
     if (prop.major < 10) return fail(PT_ERR_ARG, "libptb200 is built for sm_100a (B200); device is sm_" +
@@ -404,7 +404,7 @@ int pt_ctx_create(int device, pt_ctx** out)
 int pt_ctx_destroy(pt_ctx* ctx)
 {
     if (!ctx) return PT_OK;
-    cudaSetDevice(ctx->device);
+    ::pt::DeviceScope device_scope(ctx->device);
     cudaStreamSynchronize(ctx->stream);
     pt_ctx_trim(ctx);
     if (ctx->copy_stream) cudaStreamDestroy(ctx->copy_stream);
@@ -416,7 +416,7 @@ int pt_ctx_destroy(pt_ctx* ctx)
 int pt_ctx_trim(pt_ctx* ctx)
 {
     if (!ctx) return fail(PT_ERR_ARG, "ctx is null");
-    PT_CUDA(cudaSetDevice(ctx->device));
+    PT_DEVICE_SCOPE(ctx->device);
     PT_CUDA(cudaStreamSynchronize(ctx->stream));
     if (ctx->copy_stream) PT_CUDA(cudaStreamSynchronize(ctx->copy_stream));
     for (auto& b : ctx->scratch) {
@@ -478,6 +478,7 @@ int pt_push_advance_device(pt_ctx* ctx, const pt_field* f, double* d_x1, double*
                            int64_t* d_deaths)
 {
     if (!ctx || !f) return fail(PT_ERR_ARG, "null context or field");
+    PT_DEVICE_SCOPE(ctx->device);
     int rc = check_params(p, f);
     if (rc) return rc;
     if (p->precision != PT_PUSH_F64) return fail(PT_ERR_ARG, "use pt_push_advance_fast for the FP32 push");
@@ -511,6 +512,7 @@ int pt_fast_state_create(pt_ctx* ctx, const pt_field* f, const double* d_x1, con
                          int64_t n, pt_fast_state** out)
 {
     if (!ctx || !f || !out) return fail(PT_ERR_ARG, "null argument");
+    PT_DEVICE_SCOPE(ctx->device);
     if (!fast_storage(f->storage)) return fail(PT_ERR_ARG, "fast state needs an FP32-push brick field");
     if (n < 0 || n > INT32_MAX) return fail(PT_ERR_ARG, "particle count out of range");
     pt_fast_state* st = new (std::nothrow) pt_fast_state();
@@ -545,6 +547,7 @@ int pt_fast_state_export(pt_ctx* ctx, const pt_fast_state* st, double* d_x1, dou
                          double* d_p1, double* d_p2, double* d_p3, uint8_t* d_alive)
 {
     if (!ctx || !st) return fail(PT_ERR_ARG, "null argument");
+    PT_DEVICE_SCOPE(ctx->device);
     if (st->n == 0) return PT_OK;
     if (!(d_x1 && d_x2 && d_x3 && d_p1 && d_p2 && d_p3 && d_alive)) return fail(PT_ERR_ARG, "null state");
     return launch_fast_export(st, st->field, d_x1, d_x2, d_x3, d_p1, d_p2, d_p3, d_alive, ctx->stream);
@@ -571,6 +574,7 @@ int pt_fast_state_destroy(pt_fast_state* st)
 int pt_fast_state_sort(pt_ctx* ctx, pt_fast_state* st)
 {
     if (!ctx || !st) return fail(PT_ERR_ARG, "null argument");
+    PT_DEVICE_SCOPE(ctx->device);
     return fast_sort(ctx, st, st->field, ctx->stream);
 }
 
@@ -579,6 +583,7 @@ int pt_push_advance_fast(pt_ctx* ctx, const pt_field* f, pt_fast_state* st, cons
                          int64_t* d_deaths)
 {
     if (!ctx || !f || !st) return fail(PT_ERR_ARG, "null argument");
+    PT_DEVICE_SCOPE(ctx->device);
     int rc = check_params(p, f);
     if (rc) return rc;
     if (p->precision != PT_PUSH_F32) return fail(PT_ERR_ARG, "pt_push_advance_fast runs the FP32 push");
@@ -599,7 +604,7 @@ int pt_push_run(pt_ctx* ctx, const pt_field* f, double* x1, double* x2, double* 
     if (n < 0) return fail(PT_ERR_ARG, "n must be >= 0");
     if (n > 0 && !(x1 && x2 && x3 && p1 && p2 && p3 && alive)) return fail(PT_ERR_ARG, "null state");
     if (p->cache_mode != PT_CACHE_NONE && !save) return fail(PT_ERR_ARG, "a cache mode needs a save callback");
-    PT_CUDA(cudaSetDevice(ctx->device));
+    PT_DEVICE_SCOPE(ctx->device);
     cudaStream_t st = ctx->stream;
     const int64_t nsteps = p->nsteps, stride = p->stride;
     const size_t elem = p->cache_f64 ? 8 : 4;
@@ -755,6 +760,7 @@ int pt_dmumu_accumulate_device(pt_ctx* ctx, const float* d_mu, int64_t n, int64_
     if (!(d_mu && d_lags && d_edges && d_counts && d_sum_d && d_sum_d2 && d_w_count && d_w_mean && d_w_m2 &&
           d_pair_ss && d_pair_n))
         return fail(PT_ERR_ARG, "null pointer");
+    PT_DEVICE_SCOPE(ctx->device);
     DmumuArgs a{d_mu, n, nsave, sp, ss, d_lags, n_lags, d_edges, n_bins, start_mode == PT_START_INJECTION, bin_abs != 0,
                 d_counts, d_sum_d, d_sum_d2, d_w_count, d_w_mean, d_w_m2, d_pair_ss, d_pair_n};
     return run_dmumu(ctx, a, ctx->stream);
@@ -778,7 +784,7 @@ int pt_dmumu_accumulate_phase_space_device(pt_ctx* ctx, const void* d_pos, const
     if (!(d_pos && d_mom && d_bfield && d_bfield[0] && d_bfield[1] && d_bfield[2] && d_lags && d_edges &&
           d_counts && d_sum_d && d_sum_d2 && d_w_count && d_w_mean && d_w_m2 && d_pair_ss && d_pair_n))
         return fail(PT_ERR_ARG, "null pointer");
-    PT_CUDA(cudaSetDevice(ctx->device));
+    PT_DEVICE_SCOPE(ctx->device);
     DmumuArgs a{nullptr, n, nsave, 0, 0, d_lags, n_lags, d_edges, n_bins, start_mode == PT_START_INJECTION,
                 bin_abs != 0, d_counts, d_sum_d, d_sum_d2, d_w_count, d_w_mean, d_w_m2, d_pair_ss, d_pair_n};
     return run_dmumu_phase_space(ctx, a, d_pos, d_mom, row_stride, comp_stride, d_bfield, *grid, f64 != 0,
@@ -797,7 +803,7 @@ int pt_dmumu_accumulate(pt_ctx* ctx, const float* mu, int64_t n, int64_t nsave, 
         return fail(PT_ERR_ARG, "null pointer");
     int rc = check_lags_host(lags, n_lags);
     if (rc) return rc;
-    PT_CUDA(cudaSetDevice(ctx->device));
+    PT_DEVICE_SCOPE(ctx->device);
     const size_t extent = (size_t)((n - 1) * sp + (nsave - 1) * ss + 1);
     const size_t nlb = (size_t)n_lags * n_bins;
     size_t off = 0;
@@ -843,6 +849,7 @@ int pt_dpp_accumulate_device(pt_ctx* ctx, const float* d_mom, int64_t chunk, int
     if (!(std::isfinite(p0) && p0 > 0.0)) return fail(PT_ERR_ARG, "p0 must be finite and positive");
     if (chunk == 0 || n_lags == 0) return PT_OK;
     if (!(d_mom && d_lags && d_counts && d_sdp && d_sdp2 && d_sdn && d_sdn2)) return fail(PT_ERR_ARG, "null pointer");
+    PT_DEVICE_SCOPE(ctx->device);
     DppArgs a{d_mom, chunk, nsave, d_lags, n_lags, p0, d_counts, d_sdp, d_sdp2, d_sdn, d_sdn2};
     return run_dpp(ctx, a, ctx->stream);
 }
@@ -857,7 +864,7 @@ int pt_dpp_accumulate(pt_ctx* ctx, const float* mom, int64_t chunk, int64_t nsav
     if (!(mom && lags && counts && sdp && sdp2 && sdn && sdn2)) return fail(PT_ERR_ARG, "null pointer");
     int rc = check_lags_host(lags, n_lags);
     if (rc) return rc;
-    PT_CUDA(cudaSetDevice(ctx->device));
+    PT_DEVICE_SCOPE(ctx->device);
     const size_t nm = (size_t)chunk * 3 * nsave, L = (size_t)n_lags;
     size_t off = 0;
     auto take = [&](size_t b) { size_t o = off; off += (b + 255) & ~(size_t)255; return o; };
@@ -892,7 +899,7 @@ int pt_energy_snapshots(pt_ctx* ctx, const float* mom, int64_t chunk, int64_t ns
     if (!(mom && snaps && out)) return fail(PT_ERR_ARG, "null pointer");
     for (int j = 0; j < n_snap; ++j)
         if (snaps[j] < 0 || snaps[j] >= nsave) return fail(PT_ERR_ARG, "snapshot index outside [0, nsave)");
-    PT_CUDA(cudaSetDevice(ctx->device));
+    PT_DEVICE_SCOPE(ctx->device);
     const size_t nm = (size_t)chunk * 3 * nsave;
     DevBuf dm, ds, dout;
     int rc;
@@ -916,7 +923,7 @@ int pt_energy_snapshots_device(pt_ctx* ctx, const float* d_mom, int64_t chunk, i
     if (chunk < 0 || nsave < 1 || n_snap < 0 || particle_offset < 0) return fail(PT_ERR_ARG, "bad sizes");
     if (chunk == 0 || n_snap == 0) return PT_OK;
     if (!(d_mom && d_snap_steps && d_out)) return fail(PT_ERR_ARG, "null pointer");
-    PT_CUDA(cudaSetDevice(ctx->device));
+    PT_DEVICE_SCOPE(ctx->device);
     return launch_energy_snapshots(d_mom, chunk, nsave, d_snap_steps, n_snap, particle_offset, d_out, ctx->stream);
 }
 
@@ -929,6 +936,7 @@ int pt_energy_histogram_device(pt_ctx* ctx, const float* d_mom, int64_t chunk, i
     if (!(e_min > 0.0 && e_max > e_min && std::isfinite(e_max))) return fail(PT_ERR_ARG, "need 0 < e_min < e_max");
     if (chunk == 0 || n_snap == 0) return PT_OK;
     if (!(d_mom && d_snaps && d_counts)) return fail(PT_ERR_ARG, "null pointer");
+    PT_DEVICE_SCOPE(ctx->device);
     return launch_energy_histogram(d_mom, chunk, nsave, d_snaps, n_snap, e_min, e_max, n_hist, d_counts, ctx->stream);
 }
 
@@ -941,7 +949,7 @@ int pt_reconstruct_mu(pt_ctx* ctx, const void* pos, const void* mom, int64_t chu
     if (chunk < 0 || nsave < 0) return fail(PT_ERR_ARG, "bad sizes");
     if (chunk == 0 || nsave == 0) return PT_OK;
     if (!(pos && mom && mu_out && bfield && bfield[0] && bfield[1] && bfield[2])) return fail(PT_ERR_ARG, "null pointer");
-    PT_CUDA(cudaSetDevice(ctx->device));
+    PT_DEVICE_SCOPE(ctx->device);
     const size_t el = f64 ? 8 : 4;
     const size_t nps = (size_t)chunk * 3 * nsave, nf = (size_t)(grid->nx * grid->ny * grid->nz);
     DevBuf dp, dm, db, dout;

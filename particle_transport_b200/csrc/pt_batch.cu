@@ -226,7 +226,7 @@ int pt_batch_create(pt_ctx* ctx, int64_t capacity, int max_campaigns, int storag
     if (storage != PT_FIELD_BRICK_BF16 && storage != PT_FIELD_BRICK_F32 && storage != PT_FIELD_BRICK_BF16_XPAIR)
         return fail(PT_ERR_ARG, "batches run the FP32 push: storage must be a brick form");
     if (steps_per_epoch < 1) return fail(PT_ERR_ARG, "steps_per_epoch must be >= 1");
-    PT_CUDA(cudaSetDevice(ctx->device));
+    PT_DEVICE_SCOPE(ctx->device);
     pt_batch* b = new (std::nothrow) pt_batch();
     if (!b) return fail(PT_ERR_OOM, "host allocation failed");
     b->ctx = ctx;
@@ -283,6 +283,7 @@ int pt_batch_create(pt_ctx* ctx, int64_t capacity, int max_campaigns, int storag
 int pt_batch_add(pt_ctx* ctx, pt_batch* b, const pt_campaign_desc* d, int* id)
 {
     if (!ctx || !b || !d || !id) return fail(PT_ERR_ARG, "null argument");
+    PT_DEVICE_SCOPE(ctx->device);
     const pt_field* f = d->field;
     if (!f || f->storage != b->storage) return fail(PT_ERR_ARG, "campaign field must use the batch's brick storage");
     if (!(d->dt > 0 && std::isfinite(d->dt))) return fail(PT_ERR_ARG, "dt must be finite and positive");
@@ -378,6 +379,7 @@ int pt_batch_add(pt_ctx* ctx, pt_batch* b, const pt_campaign_desc* d, int* id)
 int pt_batch_remove(pt_ctx* ctx, pt_batch* b, int id)
 {
     if (!ctx || !b) return fail(PT_ERR_ARG, "null argument");
+    PT_DEVICE_SCOPE(ctx->device);
     if (id < 0 || id >= b->max_camps || !b->h_camps[id].active) return fail(PT_ERR_ARG, "no such campaign");
     BatchCampaignDev& C = b->h_camps[id];
     b->free_ranges.push_back({C.slot0, C.n});
@@ -396,6 +398,7 @@ int pt_batch_remove(pt_ctx* ctx, pt_batch* b, int id)
 int pt_batch_run(pt_ctx* ctx, pt_batch* b, int64_t epochs, int use_graph)
 {
     if (!ctx || !b) return fail(PT_ERR_ARG, "null argument");
+    PT_DEVICE_SCOPE(ctx->device);
     if (epochs < 0) return fail(PT_ERR_ARG, "epochs must be >= 0");
     cudaStream_t s = ctx->stream;
     if (use_graph) {
@@ -418,6 +421,7 @@ int pt_batch_run(pt_ctx* ctx, pt_batch* b, int64_t epochs, int use_graph)
 int pt_batch_set_running(pt_ctx* ctx, pt_batch* b, const int* ids, int n_ids)
 {
     if (!ctx || !b) return fail(PT_ERR_ARG, "null argument");
+    PT_DEVICE_SCOPE(ctx->device);
     if (n_ids > 0 && !ids) return fail(PT_ERR_ARG, "null ids");
     std::vector<char> want((size_t)b->max_camps, n_ids < 0 ? 1 : 0);
     for (int k = 0; k < n_ids; ++k) {
@@ -440,6 +444,7 @@ int pt_batch_set_running(pt_ctx* ctx, pt_batch* b, const int* ids, int n_ids)
 int pt_batch_step(pt_ctx* ctx, pt_batch* b, int id, int64_t* step)
 {
     if (!ctx || !b || !step) return fail(PT_ERR_ARG, "null argument");
+    PT_DEVICE_SCOPE(ctx->device);
     if (id < 0 || id >= b->max_camps || !b->h_camps[id].active) return fail(PT_ERR_ARG, "no such campaign");
     PT_CUDA(cudaStreamSynchronize(ctx->stream));
     PT_CUDA(cudaMemcpy(step, &b->d_camps[id].step, sizeof(int64_t), cudaMemcpyDeviceToHost));
@@ -450,6 +455,7 @@ int pt_batch_export(pt_ctx* ctx, pt_batch* b, int id, double* x1, double* x2, do
                     double* p3, uint8_t* alive)
 {
     if (!ctx || !b) return fail(PT_ERR_ARG, "null argument");
+    PT_DEVICE_SCOPE(ctx->device);
     if (id < 0 || id >= b->max_camps || !b->h_camps[id].active) return fail(PT_ERR_ARG, "no such campaign");
     if (!(x1 && x2 && x3 && p1 && p2 && p3 && alive)) return fail(PT_ERR_ARG, "null state");
     const BatchCampaignDev& C = b->h_camps[id];

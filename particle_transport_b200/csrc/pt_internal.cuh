@@ -36,6 +36,38 @@ int cuda_fail(cudaError_t e, const char* what);
         if (_e != cudaSuccess) return ::pt::cuda_fail(_e, what); \
     } while (0)
 
+// Makes a context's device current for one entry-point call and gives the
+// calling thread its own current device back on every return path, so the
+// attribute queries, occupancy queries and launches of the call all target
+// the device the context's stream and buffers belong to.
+class DeviceScope {
+public:
+    explicit DeviceScope(int device)
+    {
+        int cur = -1;
+        if (cudaGetDevice(&cur) != cudaSuccess) cur = -1;
+        if (cur == device) return;
+        err_ = cudaSetDevice(device);
+        if (err_ == cudaSuccess) prev_ = cur;
+    }
+    ~DeviceScope()
+    {
+        if (prev_ >= 0) cudaSetDevice(prev_);
+    }
+    DeviceScope(const DeviceScope&) = delete;
+    DeviceScope& operator=(const DeviceScope&) = delete;
+    cudaError_t error() const { return err_; }
+
+private:
+    int prev_ = -1;
+    cudaError_t err_ = cudaSuccess;
+};
+
+#define PT_DEVICE_SCOPE(device)                                               \
+    ::pt::DeviceScope pt_device_scope_(device);                               \
+    if (pt_device_scope_.error() != cudaSuccess)                              \
+    return ::pt::cuda_fail(pt_device_scope_.error(), "cudaSetDevice")
+
 // ---------------------------------------------------------------- context
 struct ScratchBuf {
     void* ptr = nullptr;

@@ -1,8 +1,8 @@
 # PtB200.jl -- Julia bindings of libptb200.so for the particle_transport
 # pipeline.  The functions below keep the signatures of the reference
-# functions they replace; the pipeline swaps its calls to them (see
-# INTEGRATION.md).  All arrays are the reference's own Julia arrays, passed
-# by pointer under GC.@preserve; the library never frees them.
+# functions they replace; the pipeline swaps its calls to them at those
+# seams.  All arrays are the reference's own Julia arrays, passed by pointer
+# under GC.@preserve; the library never frees them.
 module PtB200
 
 const LIB = get(ENV, "PTB200_LIB", joinpath(@__DIR__, "..", "libptb200.so"))

@@ -139,7 +139,10 @@ class CampaignServer:
         nsave = (nsteps - 1) // stride + 1
         n = spec.n_particles
         n_dpp = min(n, max(0, spec.dpp_particles))
-        return n * (2 * 49 + 49) + 4.0 * n * nsave + 12.0 * n_dpp * nsave + 64 * spec.n_lags * (spec.n_bins + 1)
+        bins = 0 if S.dmumu_noalloc_fits(nsave, spec.n_lags, spec.n_bins) else \
+            S.dmumu_scratch_bound(nsave, spec.n_lags, spec.n_bins)  # the allocating entry's scratch
+        return (n * (2 * 49 + 49) + 4.0 * n * nsave + 12.0 * n_dpp * nsave + 64 * spec.n_lags * (spec.n_bins + 1) +
+                bins)
 
     def submit(self, spec: JobSpec, arrival: float = None) -> int:
         jid = self.next_id
@@ -222,12 +225,12 @@ class CampaignServer:
             # whole device -- the epochs and every earlier job's binning.
             # All binning runs on this one side stream, so its calls never
             # overlap on the fixed scratch.  Series too long to stage on chip
-            # take the allocating entry.
-            rc = _lib.load().pt_dmumu_accumulate_device_noalloc(*args)
-            if rc == _lib.PT_ERR_ARG:
-                _lib.call("pt_dmumu_accumulate_device", *args)
+            # take the allocating entry, whose scratch job_bytes counts; any
+            # error of either entry is raised.
+            if S.dmumu_noalloc_fits(rec["nsave"], len(lags), spec.n_bins):
+                _lib.call("pt_dmumu_accumulate_device_noalloc", *args)
             else:
-                _lib.check(rc, "pt_dmumu_accumulate_device_noalloc")
+                _lib.call("pt_dmumu_accumulate_device", *args)
             dpp = None
             if rec["mom"] is not None:
                 # D_pp of the subset with p0 = 1: the kernel normalises once per

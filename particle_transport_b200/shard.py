@@ -3,8 +3,10 @@
 Particles never interact and the field is read-only, so a campaign shards
 by contiguous particle ranges with the field replicated on every GPU; the
 push and the lag statistics need no communication.  The one exchange is
-the final merge of the statistics accumulators (tens of kB): every rank
-all-gathers the others' arrays and merges them in rank order -- integer
+the final merge of the statistics accumulators (tens of kB), plus the D_pp
+normalisation p0, which belongs to the first particle and so to rank 0 and
+is broadcast before the binning.  For the merge every rank all-gathers the
+others' arrays and merges them in rank order -- integer
 counts and FP64 sums added rank by rank, per-lag Welford triples combined
 with the reference's combine_welford_stats! formula
 (src/compute_delta_mu2_dmumu_full.jl:439-455) -- so every rank holds the
@@ -82,7 +84,24 @@ def reduce_dmumu_accumulators(acc: dict, group=None) -> dict:
     return out
 
 
+def broadcast_p0(p0: float, device="cpu", group=None) -> float:
+    """The D_pp normalisation p0 = |p| of the first selected particle at the
+    first save (src/compute_dpp_full.jl:483).  With contiguous particle
+    ranges that particle is on rank 0; every rank takes rank 0's value, so
+    the per-rank sums of dp/p0 add up to the single-pass sums.  ``device``
+    is where the one-element tensor lives (a CUDA device under NCCL)."""
+    import torch
+    import torch.distributed as dist
+
+    t = torch.tensor([float(p0)], dtype=torch.float64, device=device)
+    dist.broadcast(t, src=0, group=group)
+    return float(t.item())
+
+
 def reduce_dpp_accumulators(acc: dict, group=None) -> dict:
+    """Merge per-rank D_pp accumulators (the keys of
+    stats.new_dpp_accumulators) into the job totals: counts and sums added in
+    rank order."""
     import torch
 
     gathered = {k: _gather(acc[k] if isinstance(acc[k], torch.Tensor) else torch.as_tensor(np.asarray(acc[k])), group)

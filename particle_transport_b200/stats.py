@@ -260,8 +260,57 @@ def reconstruct_mu_chunk(positions, momenta, Bx, By, Bz, grid, dtype=np.float32)
 
 
 # --------------------------------------------------------------------------
+# limits of the D_mumu entry points (the launch arithmetic of lagstats.cu)
+# --------------------------------------------------------------------------
+_DMUMU_SMEM_BUDGET = 200 * 1024  # shared memory a D_mumu CTA may use (B200 opt-in maximum is 227 KiB)
+_DMUMU_NOALLOC_BYTES = 16 << 20  # the no-alloc entry's fixed device array
+_WELFORD_PART_BYTES = 40
+
+
+def _a16(v: int) -> int:
+    return (v + 15) & ~15
+
+
+def _dmumu_shape(nsave: int, n_lags: int, n_bins: int):
+    nl_cap = min(max(32, ((_DMUMU_SMEM_BUDGET // 2) // (n_bins * 24)) // 32 * 32), 256)
+    idx = 2 if nsave <= 65535 else 4
+    slot = (_a16((nsave + 1) * 4) + _a16(nsave * idx) + _a16(4 * (8 * (n_bins + 1) + n_bins + 2)) +
+            _a16(16 * nl_cap))
+    nl = min(nl_cap, n_lags)  # the first lag batch is the widest
+    fixed = _a16(8 * (n_bins + 1)) + max(nl * n_bins * 24, _WELFORD_PART_BYTES * 1024)
+    return nl, slot, fixed
+
+
+def dmumu_noalloc_fits(nsave: int, n_lags: int, n_bins: int) -> bool:
+    """Whether pt_dmumu_accumulate_device_noalloc takes this shape: every
+    series is staged on chip, and one CTA's partials fit the fixed array."""
+    if n_lags <= 0:
+        return True
+    nl, slot, fixed = _dmumu_shape(nsave, n_lags, n_bins)
+    per_cta = nl * n_bins * 24 + _WELFORD_PART_BYTES * nl + 64
+    return fixed + slot <= _DMUMU_SMEM_BUDGET and (_DMUMU_NOALLOC_BYTES - 1024) // per_cta >= 1
+
+
+def dmumu_scratch_bound(nsave: int, n_lags: int, n_bins: int, num_sms: int = 148) -> int:
+    """Upper bound of the device scratch pt_dmumu_accumulate_device asks its
+    context for when the series are staged in global memory (1024-thread
+    CTAs, at most two per SM, eight series per CTA)."""
+    if n_lags <= 0:
+        return 0
+    nl, slot, _ = _dmumu_shape(nsave, n_lags, n_bins)
+    grid = 2 * num_sms
+    return 3 * _a16(grid * nl * n_bins * 8) + _a16(_WELFORD_PART_BYTES * grid * nl) + grid * 8 * slot
+
+
+# --------------------------------------------------------------------------
 # derived arrays (host)
 # --------------------------------------------------------------------------
+def _jl_max0(x: float) -> float:
+    """Julia's max(0.0, x) for Float64: a NaN argument gives NaN (Python's
+    max(0.0, nan) gives 0.0)."""
+    return x if (x != x or x > 0.0) else 0.0
+
+
 def compute_dmumu_arrays_full(counts, sum_delta, sum_delta2, tau_s, tau_norm, min_count_per_cell: int):
     """src/compute_delta_mu2_dmumu_full.jl:706-744; arrays are (n_lags, n_bins)."""
     counts = np.asarray(counts)
@@ -276,7 +325,7 @@ def compute_dmumu_arrays_full(counts, sum_delta, sum_delta2, tau_s, tau_norm, mi
                 continue
             dm = sum_delta[li, b] / c
             d2 = sum_delta2[li, b] / c
-            cen = max(0.0, d2 - dm * dm)
+            cen = _jl_max0(d2 - dm * dm)
             out["mean_delta"][li, b] = dm
             out["mean_delta2"][li, b] = d2
             out["drift_norm"][li, b] = dm / tn
@@ -344,7 +393,7 @@ def compute_dpp_arrays(counts, sum_delta_p, sum_delta_p2, sum_delta_p_norm, sum_
             continue
         dm, d2 = sum_delta_p[i] / c, sum_delta_p2[i] / c
         nm, n2 = sum_delta_p_norm[i] / c, sum_delta_p_norm2[i] / c
-        cen, cenn = max(0.0, d2 - dm * dm), max(0.0, n2 - nm * nm)
+        cen, cenn = _jl_max0(d2 - dm * dm), _jl_max0(n2 - nm * nm)
         out["mean_delta_p"][i], out["mean_delta_p2"][i] = dm, d2
         out["mean_delta_p_norm"][i], out["mean_delta_p_norm2"][i] = nm, n2
         out["dpp_raw_per_s"][i] = d2 / (2.0 * float(tau_s[i]))

@@ -83,6 +83,39 @@ def test_config1_fp64_bit_exact_and_dmumu(cuda, oracle, config1):
     # every save of every particle is finite with a periodic box
     assert g["pair_counts"].sum() == sum(NP * (801 - int(L)) for L in c["lags"])
 
+    # derived products of the device accumulators against the oracle's derived arrays of its own accumulators:
+    # the same cells survive the count cut, and the values agree to the summation-order differences of the sums
+    t_s = c["dt"] * STRIDE * np.arange(801, dtype=np.float64)
+    t_norm = (2 * math.pi / SPG) * STRIDE * np.arange(801, dtype=np.float64)
+    tau_s = np.array([t_s[L] - t_s[0] for L in c["lags"]])
+    tau_norm = np.array([t_norm[L] - t_norm[0] for L in c["lags"]])
+    for min_count in (1, 5000):
+        dg = S.compute_dmumu_arrays_full(g["dmumu_counts"], g["dmumu_sum_delta"], g["dmumu_sum_delta2"], tau_s,
+                                         tau_norm, min_count)
+        do = oracle.dmumu_arrays_full(o["counts"], o["sum_d"], o["sum_d2"], tau_s, tau_norm, min_count)
+        for k in oracle.DMUMU_ARRAY_KEYS:
+            assert np.array_equal(np.isnan(dg[k]), np.isnan(do[k])), k
+        ok = ~np.isnan(do["mean_delta2"])
+        assert ok.any() and (min_count == 1 or (~ok).any())
+        for k in ("mean_delta2", "dmumu_raw_norm", "dmumu_raw_per_s"):
+            assert np.allclose(dg[k][ok], do[k][ok], rtol=1e-12, atol=0), k
+        raw = do["dmumu_raw_norm"][ok]
+        assert np.all(np.abs(dg["dmumu_centered_norm"][ok] - do["dmumu_centered_norm"][ok]) <= 1e-11 * raw)
+        mscale = scale[ok] / o["counts"][ok]
+        assert np.all(np.abs(dg["mean_delta"][ok] - do["mean_delta"][ok]) <= mscale)
+        for k in ("dmumu_raw_norm", "dmumu_centered_norm"):
+            ug, wg = S.average_over_tau_full(dg[k], g["dmumu_counts"], min_count)
+            uo, wo = oracle.average_over_tau_full(do[k], o["counts"], min_count)
+            assert np.array_equal(np.isnan(ug), np.isnan(uo)) and np.array_equal(np.isnan(wg), np.isnan(wo))
+            assert np.allclose(ug, uo, rtol=1e-11, equal_nan=True) and np.allclose(wg, wo, rtol=1e-11, equal_nan=True)
+    tg = S.build_output_table(c["lags"], t_s, t_norm, g["particle_counts"], g["particle_means"], g["particle_m2s"],
+                              g["pair_sum_squares"], g["pair_counts"])
+    to = oracle.output_table(c["lags"], t_s, t_norm, o["w_count"], o["w_m2"], o["pair_ss"], o["pair_n"])
+    for k in ("tau_s", "tau_norm", "tau_gyroperiods"):
+        assert np.array_equal(tg[k], to[k]), k
+    for k in ("delta_mu2_particle_std", "delta_mu2_particle_sem", "delta_mu2_pair_mean"):
+        assert np.allclose(tg[k], to[k], rtol=1e-10, atol=0), k
+
 
 @pytest.mark.parametrize("storage", ["brick_f32", "brick_bf16"])
 def test_config1_mixed_precision(cuda, config1, storage):

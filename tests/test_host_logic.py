@@ -99,3 +99,45 @@ def test_admission_holds_later_jobs_behind_one_that_does_not_fit():
     srv.queue = [(0, big, 0.0), (1, small, 0.0)]
     assert srv.admit() == 0 and admitted == []  # FIFO: the small job does not overtake
     assert [q[0] for q in srv.queue] == [0, 1]
+
+
+def test_tune_batch_rejects_cadences_that_do_not_divide():
+    """A campaign sorts every (cadence / K) epochs with K the shortest cadence
+    picked, so each candidate must be a multiple of every shorter one."""
+    import pytest
+
+    from particle_transport_b200.batch import check_cadences, tune_batch
+
+    check_cadences((16, 32, 64, 128))
+    check_cadences((64, 16))
+    for bad in ((16, 48, 64), (32, 48), (0, 16), ()):
+        with pytest.raises(ValueError):
+            check_cadences(bad)
+    with pytest.raises(ValueError, match="multiple"):
+        tune_batch([], "brick_bf16", 1, cadences=(16, 48, 64))
+
+
+def test_dmumu_noalloc_limits_and_job_bytes():
+    """The host mirror of the no-alloc entry's limits: series of up to ~20k
+    saves at 50 bins stage on chip, 60,000 do not (that call is refused on
+    the device, tests/test_zz_no_alloc.py); a job whose series do not fit is
+    charged the allocating entry's scratch bound at admission."""
+    from particle_transport_b200 import stats as S
+    from particle_transport_b200.server import CampaignServer, JobSpec
+
+    assert S.dmumu_noalloc_fits(4001, 64, 50) and S.dmumu_noalloc_fits(20000, 64, 50)
+    assert not S.dmumu_noalloc_fits(60000, 2, 50)
+    top = max(n for n in range(15000, 30000) if S.dmumu_noalloc_fits(n, 64, 50))
+    assert 20000 < top < 22000 and not S.dmumu_noalloc_fits(top + 1, 64, 50)
+    assert S.dmumu_noalloc_fits(161, 64, 250) and not S.dmumu_noalloc_fits(401, 64, 250)
+    b = S.dmumu_scratch_bound(60000, 64, 50)
+    assert 0.5e9 < b < 2e9  # partials + 296 CTAs x 8 global staging slots of ~0.48 MB
+    short = JobSpec("256", "total", 1.0, 100_000, 500.0)
+    long = JobSpec("256", "total", 1.0, 100_000, 500.0, saves_per_gyroperiod=short.steps_per_gyroperiod)
+    nsave = int(round(long.duration_gyroperiods * long.steps_per_gyroperiod))  # + 1 sample, stride 1
+    assert not S.dmumu_noalloc_fits(nsave + 1, long.n_lags, long.n_bins)
+    extra = S.dmumu_scratch_bound(nsave + 1, long.n_lags, long.n_bins)
+    assert S.dmumu_noalloc_fits(4001, short.n_lags, short.n_bins)
+    # the long job holds 8x the mu and D_pp momentum caches of the short one and is charged the scratch bound
+    cache_diff = (4.0 * long.n_particles + 12.0 * long.dpp_particles) * (nsave + 1 - 4001)
+    assert CampaignServer.job_bytes(long) - CampaignServer.job_bytes(short) == cache_diff + extra

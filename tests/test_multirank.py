@@ -1,8 +1,10 @@
 """World-size-2 gloo test of the particle-sharded statistics merge (CPU only).
 
-Each rank accumulates its shard of a mu cache (with the oracle, standing in
-for the per-GPU kernel) and the ranks merge with
-shard.reduce_dmumu_accumulators; the merged result must equal a single pass
+Each rank accumulates its shard of a mu cache and of a momentum cache (with
+the oracle, standing in for the per-GPU kernels), takes the D_pp
+normalisation p0 from rank 0 (shard.broadcast_p0) and the ranks merge with
+shard.reduce_dmumu_accumulators / shard.reduce_dpp_accumulators, the calls
+bench.py makes under torchrun; the merged result must equal a single pass
 over all particles: counts exactly, sums and Welford moments to 1e-12."""
 import os
 import socket
@@ -11,7 +13,7 @@ import numpy as np
 import pytest
 import torch.multiprocessing as mp
 
-from helpers import random_mu_cache, zero_dmumu
+from helpers import random_mu_cache, zero_dmumu, zero_dpp
 from particle_transport_b200 import shard
 from particle_transport_b200.time_units import build_mu_edges_full, log_spaced_lag_steps
 
@@ -22,6 +24,27 @@ def _free_port():
     p = s.getsockname()[1]
     s.close()
     return p
+
+
+DPP_KEYMAP = {"counts": "counts", "sum_dp": "sum_delta_p", "sum_dp2": "sum_delta_p2", "sum_dpn": "sum_delta_p_norm",
+              "sum_dpn2": "sum_delta_p_norm2"}
+
+
+def random_momenta(n, nsave, seed=11):
+    """float32 momenta shaped (nsave, 3, n) with a slow random walk of |p|."""
+    rng = np.random.default_rng(seed)
+    p = np.abs(1.0 + 0.01 * np.cumsum(rng.normal(size=(nsave, n)), axis=0))
+    d = rng.normal(size=(nsave, 3, n))
+    d /= np.linalg.norm(d, axis=1, keepdims=True)
+    mom = (d * p[:, None, :] * 5.3e-18).astype(np.float32)
+    mom[rng.random(mom.shape) < 0.01] = np.nan
+    mom[0, :, 0] = np.abs(mom[0, :, 0])  # particle 0 is finite at the first save (it defines p0)
+    return mom
+
+
+def p0_of(mom):
+    m = mom[0, :, 0].astype(np.float64)
+    return float(np.sqrt(m[0] * m[0] + m[1] * m[1] + m[2] * m[2]))
 
 
 KEYMAP = {"counts": "dmumu_counts", "sum_d": "dmumu_sum_delta", "sum_d2": "dmumu_sum_delta2",
@@ -42,9 +65,14 @@ def _worker(rank, world, port, out_q):
     acc = zero_dmumu(len(lags), 12)
     o.dmumu_accumulate(np.ascontiguousarray(mu[a:b]), lags, edges, acc, nthreads=1)
     merged = shard.reduce_dmumu_accumulators({KEYMAP[k]: v for k, v in acc.items()})
+    mom = random_momenta(301, 90)
+    p0 = shard.broadcast_p0(p0_of(np.ascontiguousarray(mom[:, :, a:b])) if a < b else float("nan"))
+    dacc = zero_dpp(len(lags))
+    o.dpp_accumulate(np.ascontiguousarray(mom[:, :, a:b]), lags, p0, dacc, nthreads=1)
+    dmerged = shard.reduce_dpp_accumulators({DPP_KEYMAP[k]: v for k, v in dacc.items()})
     dist.barrier()
     dist.destroy_process_group()
-    out_q.put((rank, merged))
+    out_q.put((rank, (merged, dmerged, p0)))
 
 
 def test_sharded_merge_matches_single_pass(oracle):
@@ -64,8 +92,15 @@ def test_sharded_merge_matches_single_pass(oracle):
     edges, _ = build_mu_edges_full(0.0, 1.0, 12)
     ref = zero_dmumu(len(lags), 12)
     oracle.dmumu_accumulate(mu, lags, edges, ref, nthreads=1)
+    mom = random_momenta(301, 90)
+    dref = zero_dpp(len(lags))
+    oracle.dpp_accumulate(mom, lags, p0_of(mom), dref, nthreads=1)
     for r in range(world):
-        m = res[r]
+        m, d, p0 = res[r]
+        assert p0 == p0_of(mom)  # rank 1 took rank 0's p0
+        assert np.array_equal(d["counts"], dref["counts"]) and d["counts"].sum() > 0
+        for k in ("sum_dp", "sum_dp2", "sum_dpn", "sum_dpn2"):
+            assert np.allclose(d[DPP_KEYMAP[k]], dref[k], rtol=1e-12, atol=0), k
         assert np.array_equal(m["dmumu_counts"], ref["counts"])
         assert np.array_equal(m["pair_counts"], ref["pair_n"])
         assert np.array_equal(m["particle_counts"], ref["w_count"])
@@ -73,8 +108,9 @@ def test_sharded_merge_matches_single_pass(oracle):
         assert np.allclose(m["particle_means"], ref["w_mean"], rtol=1e-12, atol=0)
         assert np.allclose(m["particle_m2s"], ref["w_m2"], rtol=1e-10, atol=0)
     # both ranks hold the identical merged result
-    for k in res[0]:
-        assert np.array_equal(res[0][k], res[1][k])
+    for part in (0, 1):
+        for k in res[0][part]:
+            assert np.array_equal(res[0][part][k], res[1][part][k])
 
 
 @pytest.mark.parametrize("n,world", [(10, 3), (16_777_216, 8), (1, 2), (0, 4)])
