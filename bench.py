@@ -354,10 +354,13 @@ def run_ours(args, ws, rank, local):
     fb = FieldLibrary(fields, grid, args.storage, B_ref_T=B0)
     alive = np.ones(n, np.uint8)
     ens = R.FastEnsemble(fb, state, alive)
-    ring = torch.empty((8, n), dtype=torch.float32, device=dev)
+    # the 8 mu saves of a 64-step launch land in a time-fastest cache [n][8]:
+    # each particle's saves leave as one 32-byte store (cache_pitch = 8)
+    ring = torch.empty((n, 8), dtype=torch.float32, device=dev)
     # the sort cadence is driven here (same rule as pt_push_advance_fast's
     # sort_every) so that events can bracket the push launch alone
-    params = R.push_params(dt, NSTEPS, STRIDE, cache="mu", precision="f32", kernel_variant=args.variant)
+    params = R.push_params(dt, NSTEPS, STRIDE, cache="mu", precision="f32", kernel_variant=args.variant,
+                           cache_pitch=8)
     step_at = [0]
     last_sort = [None]
     push_ev = []
@@ -403,7 +406,7 @@ def run_ours(args, ws, rank, local):
         f32 = FieldLibrary(fields, grid, "brick_f32", B_ref_T=B0)
         ens32 = R.FastEnsemble(f32, state, alive)
         p32 = R.push_params(dt, NSTEPS, STRIDE, cache="mu", precision="f32", sort_every=args.sort_every,
-                            kernel_variant=args.variant)
+                            kernel_variant=args.variant, cache_pitch=8)
         at32 = [0]
 
         def f32_step(k):
@@ -423,6 +426,7 @@ def run_ours(args, ws, rank, local):
     # ---------------- FP64 plain push on the same particles
     fp64 = None
     if "fp64" not in skip:
+        ring = torch.empty((8, n), dtype=torch.float32, device=dev)  # the FP64 push writes mu rows [8][n]
         fr = FieldLibrary(fields, grid, "ref_f64")
         dens = R.DeviceEnsemble(fr, state, alive)
         p64 = R.push_params(dt, NSTEPS, STRIDE, cache="mu", precision="f64", steps_per_launch=64)
@@ -472,11 +476,12 @@ def run_ours(args, ws, rank, local):
         sub = {k: v[:nl] for k, v in state.items()}
         ens_l = R.FastEnsemble(fb, sub, np.ones(nl, np.uint8))
         nsave = (NSTEPS - 1) // STRIDE + 1
-        cache = torch.empty((nsave, nl), dtype=torch.float32, device=dev)
+        pitch = (nsave + 7) // 8 * 8  # time-fastest cache [nl][pitch], each particle's saves contiguous
+        cache = torch.empty((nl, pitch), dtype=torch.float32, device=dev)
         torch.cuda.synchronize()
         t0 = time.perf_counter()
         ens_l.advance(R.push_params(dt, NSTEPS, STRIDE, cache="mu", precision="f32", sort_every=args.sort_every,
-                                    kernel_variant=args.variant), 0, NSTEPS, cache, 0, nsave)
+                                    kernel_variant=args.variant, cache_pitch=pitch), 0, NSTEPS, cache, 0, nsave)
         torch.cuda.synchronize()
         push_full_s = time.perf_counter() - t0
         lags = log_spaced_lag_steps(nsave - 1, 64)
@@ -487,7 +492,7 @@ def run_ours(args, ws, rank, local):
             S.process_mu_chunk_dmumu(cache, lags, edges, acc["particle_counts"], acc["particle_means"],
                                      acc["particle_m2s"], acc["pair_sum_squares"], acc["pair_counts"],
                                      acc["dmumu_counts"], acc["dmumu_sum_delta"], acc["dmumu_sum_delta2"],
-                                     start_mode="sliding", bin_abs=True, layout="particle_fastest")
+                                     start_mode="sliding", bin_abs=True, layout="time_fastest", nsave=nsave)
             lag_pass.acc = acc
 
         lms, _ = timed(lag_pass, 2, 1, torch)
@@ -502,7 +507,7 @@ def run_ours(args, ws, rank, local):
                "campaign_push_rate": nl * (NSTEPS - 1) / push_full_s}
         if "cpu" not in skip and rank == 0:
             sys.path.insert(0, os.path.join(ROOT, "tests"))
-            mu_host = np.ascontiguousarray(cache[:, :4096].T.cpu().numpy())
+            mu_host = np.ascontiguousarray(cache[:4096, :nsave].cpu().numpy())
             lag["cpu_baseline"] = cpu_lag_rate(mu_host, lags, edges, args.cpu_seconds / 2)
         del ens_l, cache
         torch.cuda.empty_cache()
@@ -782,8 +787,11 @@ def run_batched(args, dev, rank):
     caches = []
     for c, se in zip(camps, tune["sort_every"]):
         nsave = (c["nsteps"] - 1) // c["stride"] + 1
-        caches.append(torch.empty((nsave, len(c["state"]["x1"])), dtype=torch.float32, device=dev))
-        c["id"] = b.add(c["field"], c["state"], c["dt"], c["nsteps"], c["stride"], cache=caches[-1], sort_every=se)
+        c["nsave"] = nsave
+        # time-fastest caches [n][pitch]: a particle's saves leave in 32-byte stores
+        caches.append(torch.empty((len(c["state"]["x1"]), (nsave + 7) // 8 * 8), dtype=torch.float32, device=dev))
+        c["id"] = b.add(c["field"], c["state"], c["dt"], c["nsteps"], c["stride"], cache=caches[-1], sort_every=se,
+                        time_fastest=True)
         c["sort_every"] = se
     epochs = max(math.ceil(c["nsteps"] / K) for c in camps)
     b.run(1)  # graph capture + first epoch
@@ -800,13 +808,13 @@ def run_batched(args, dev, rank):
     pairs = 0
     e0.record()
     for c, cache in zip(camps, caches):
-        nsave = cache.shape[0]
+        nsave = c["nsave"]
         lags = log_spaced_lag_steps(nsave - 1, 32)
         edges, _ = build_mu_edges_full(0.0, 1.0, 20)
         acc = S.new_dmumu_accumulators(len(lags), 20, device=dev)
         S.process_mu_chunk_dmumu(cache, lags, edges, acc["particle_counts"], acc["particle_means"],
                                  acc["particle_m2s"], acc["pair_sum_squares"], acc["pair_counts"], acc["dmumu_counts"],
-                                 acc["dmumu_sum_delta"], acc["dmumu_sum_delta2"], layout="particle_fastest")
+                                 acc["dmumu_sum_delta"], acc["dmumu_sum_delta2"], layout="time_fastest", nsave=nsave)
         c["pairs"] = acc["pair_counts"]
     e1.record()
     torch.cuda.synchronize()

@@ -95,7 +95,14 @@ typedef struct {
                                  fields: 9 = as 1 with half of the corners fetched
                                  through the texture path, 10 = as 1 with all of
                                  them, 11 = as 6 with half (same results)       */
-    int32_t reserved;
+    int32_t cache_pitch;      /* mu caches of the F32 form (pt_push_advance_fast): 0 = rows,
+                                 save row r of particle p at (r - cache_row_base) * n + p (the
+                                 reference's on-disk layout); > 0 = time-fastest, at
+                                 p * cache_pitch + (r - cache_row_base) (the Julia mu_chunk
+                                 layout, sp = cache_pitch, ss = 1 for pt_dmumu_accumulate*),
+                                 cache_pitch >= cache_rows.  A particle's saves of one call then
+                                 leave as whole 32-byte stores (32-byte aligned d_cache) instead of
+                                 one scattered 4-byte store per save.  Must be 0 elsewhere.    */
 } pt_push_params;
 
 /* Save sink for pt_push_run: called on the calling thread once per save row,
@@ -217,7 +224,8 @@ typedef struct {
     const double* d_p2;
     const double* d_p3;
     const uint8_t* d_alive;
-    void* d_cache;             /* mu rows [cache_rows][n] (NULL: no cache)                   */
+    void* d_cache;             /* mu cache of cache_rows saves (NULL: no cache), laid out as
+                                  cache_pitch says                                          */
     int64_t cache_rows;
     int32_t cache_ring;        /* 1: save row r goes to row r % cache_rows                   */
     int32_t sort_every;        /* re-sort this campaign's slots by brick before every sort_every-th
@@ -229,6 +237,9 @@ typedef struct {
                                   phase-space writer's momenta, src/phase_space_gpu_runner.jl:413-421)
                                   of particles 0 .. n_mom-1 -- the D_pp subset -- or NULL */
     int64_t n_mom;
+    int64_t cache_pitch;       /* 0: mu rows [cache_rows][n]; > 0: time-fastest, save row r of
+                                  particle p at p * cache_pitch + r (ring: r % cache_rows),
+                                  cache_pitch >= cache_rows (see pt_push_params.cache_pitch) */
 } pt_campaign_desc;
 
 /* capacity: particle slots; blocks_per_sm: resident blocks of the persistent
@@ -322,7 +333,7 @@ int pt_dmumu_accumulate_phase_space_device(pt_ctx* ctx, const void* d_pos, const
  * between calls, but calls that overlap on the GPU (two streams, two host
  * threads) race on it: serialise them.  Limits: the (lag batch x bin)
  * partials must fit in the 16 MiB array, and each particle's mu series must
- * fit on chip (about 30,000 saves at 50 bins); larger requests fail with
+ * fit on chip (about 20,000 saves at 50 bins and 64 lags); larger requests fail with
  * PT_ERR_ARG and a message naming the limit.
  */
 int pt_dmumu_accumulate_device_noalloc(pt_ctx* ctx, const float* d_mu, int64_t n, int64_t nsave, int64_t sp,

@@ -64,7 +64,7 @@ class PushParams(C.Structure):
         ("dt", C.c_double), ("nsteps", C.c_int64), ("stride", C.c_int64),
         ("periodic", C.c_int32), ("cache_mode", C.c_int32), ("cache_f64", C.c_int32), ("precision", C.c_int32),
         ("steps_per_launch", C.c_int32), ("sort_every", C.c_int32), ("kernel_variant", C.c_int32),
-        ("reserved", C.c_int32),
+        ("cache_pitch", C.c_int32),
     ]
 
 
@@ -75,7 +75,7 @@ class CampaignDesc(C.Structure):
         ("d_x1", C.c_void_p), ("d_x2", C.c_void_p), ("d_x3", C.c_void_p), ("d_p1", C.c_void_p),
         ("d_p2", C.c_void_p), ("d_p3", C.c_void_p), ("d_alive", C.c_void_p),
         ("d_cache", C.c_void_p), ("cache_rows", C.c_int64), ("cache_ring", C.c_int32), ("sort_every", C.c_int32),
-        ("d_deaths", C.c_void_p), ("d_mom_cache", C.c_void_p), ("n_mom", C.c_int64),
+        ("d_deaths", C.c_void_p), ("d_mom_cache", C.c_void_p), ("n_mom", C.c_int64), ("cache_pitch", C.c_int64),
     ]
 
 

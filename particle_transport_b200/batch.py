@@ -47,9 +47,12 @@ class Batch:
         self.campaigns = {}
 
     def add(self, field: FieldLibrary, state: dict, dt: float, nsteps: int, stride: int, periodic: bool = True,
-            cache=None, ring: bool = False, deaths=None, alive=None, mom_cache=None, sort_every: int = 1) -> int:
+            cache=None, ring: bool = False, deaths=None, alive=None, mom_cache=None, sort_every: int = 1,
+            time_fastest: bool = False) -> int:
         """Add a campaign; state: SI arrays x1..p3 (numpy or CUDA tensors);
-        cache: CUDA float32 tensor [rows][n] for the mu rows (or None);
+        cache: CUDA float tensor for the mu cache (or None), [rows][n] (the
+        reference's row layout) or, with time_fastest, [n][rows] (each
+        particle's saves contiguous: one 32-byte store per 8 saves);
         mom_cache: CUDA float32 tensor [rows][3][n_mom] that receives the
         momenta of particles 0 .. n_mom-1 at every save (needs cache);
         sort_every: re-sort the campaign by brick before every sort_every-th
@@ -61,22 +64,26 @@ class Batch:
                                  dtype=torch.float64, device=self.device).contiguous() for k in KEYS}
         al = (torch.ones(n, dtype=torch.uint8, device=self.device) if alive is None
               else torch.as_tensor(alive, dtype=torch.uint8, device=self.device).contiguous())
+        rows = pitch = 0
         if cache is not None:
-            if cache.dtype not in (torch.float32, torch.float64) or cache.shape[-1] != n or not cache.is_contiguous():
-                raise ValueError("cache must be a contiguous float tensor [rows][n]")
+            shape_ok = cache.dim() == 2 and cache.shape[0 if time_fastest else 1] == n
+            if cache.dtype not in (torch.float32, torch.float64) or not shape_ok or not cache.is_contiguous():
+                raise ValueError("cache must be a contiguous float tensor " + ("[n][rows]" if time_fastest else
+                                                                               "[rows][n]"))
+            rows = int(cache.shape[1] if time_fastest else cache.shape[0])
+            pitch = rows if time_fastest else 0
         n_mom = 0
         if mom_cache is not None:
             if (cache is None or mom_cache.dtype != torch.float32 or mom_cache.dim() != 3 or mom_cache.shape[1] != 3
-                    or mom_cache.shape[0] != cache.shape[0] or not mom_cache.is_contiguous()):
+                    or mom_cache.shape[0] != rows or not mom_cache.is_contiguous()):
                 raise ValueError("mom_cache must be a contiguous float32 tensor [rows][3][n_mom] beside the mu cache")
             n_mom = int(mom_cache.shape[2])
         d = _lib.CampaignDesc(field.handle, float(dt), int(nsteps), int(stride), int(bool(periodic)),
                               int(cache is not None and cache.dtype == torch.float64), n,
                               *[st[k].data_ptr() for k in KEYS], al.data_ptr(),
-                              cache.data_ptr() if cache is not None else None,
-                              int(cache.shape[0]) if cache is not None else 0, int(bool(ring)), int(sort_every),
-                              deaths.data_ptr() if deaths is not None else None,
-                              mom_cache.data_ptr() if mom_cache is not None else None, n_mom)
+                              cache.data_ptr() if cache is not None else None, rows, int(bool(ring)),
+                              int(sort_every), deaths.data_ptr() if deaths is not None else None,
+                              mom_cache.data_ptr() if mom_cache is not None else None, n_mom, pitch)
         cid = C.c_int()
         ctx = _lib.torch_context(self.device.index)
         _lib.call("pt_batch_add", ctx.handle, self.handle, C.byref(d), C.byref(cid))

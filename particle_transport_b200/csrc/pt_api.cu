@@ -221,6 +221,9 @@ int check_params(const pt_push_params* p, const pt_field* f)
     if (p->precision == PT_PUSH_F32 && !fast_storage(f->storage))
         return fail(PT_ERR_ARG, "the FP32 push needs a brick field (BRICK_F32 or BRICK_BF16)");
     if (p->precision != PT_PUSH_F64 && p->precision != PT_PUSH_F32) return fail(PT_ERR_ARG, "precision");
+    if (p->cache_pitch < 0) return fail(PT_ERR_ARG, "cache_pitch must be >= 0");
+    if (p->cache_pitch > 0 && (p->precision != PT_PUSH_F32 || p->cache_mode != PT_CACHE_MU))
+        return fail(PT_ERR_ARG, "cache_pitch (time-fastest layout) applies to the mu cache of the FP32 push only");
     return PT_OK;
 }
 
@@ -249,6 +252,7 @@ PushArgsFast fast_args(const pt_field* f, pt_fast_state* st, const pt_push_param
     a.variant = p->kernel_variant;
     a.ring = 0;
     a.n_cache = st->n;
+    a.pitch = p->cache_pitch;
     return a;
 }
 
@@ -342,6 +346,7 @@ static int advance_fast(pt_ctx* ctx, const pt_field* f, pt_fast_state* st, const
 {
     PushArgsFast a = fast_args(f, st, p);
     a.cache = cache; a.row_base = row_base; a.rows = rows; a.deaths = deaths;
+    a.pitch_vec = ((uintptr_t)cache & 31) == 0;
     const int64_t K = p->steps_per_launch > 0 ? p->steps_per_launch : count;
     int64_t s = s0;
     const int64_t end = s0 + count;
@@ -590,6 +595,8 @@ int pt_push_advance_fast(pt_ctx* ctx, const pt_field* f, pt_fast_state* st, cons
     if (step_begin < 0 || step_count < 0 || step_begin + step_count > p->nsteps)
         return fail(PT_ERR_ARG, "step range outside [0, nsteps)");
     if (p->cache_mode != PT_CACHE_NONE && rows > 0 && !d_cache) return fail(PT_ERR_ARG, "null cache");
+    if (p->cache_pitch > 0 && p->cache_pitch < rows)
+        return fail(PT_ERR_ARG, "cache_pitch must be at least cache_rows (the saves of one particle)");
     if (f != st->field) return fail(PT_ERR_ARG, "fast state was created against a different field");
     return advance_fast(ctx, f, st, p, step_begin, step_count, d_cache, row_base, rows, d_deaths);
 }
@@ -604,6 +611,7 @@ int pt_push_run(pt_ctx* ctx, const pt_field* f, double* x1, double* x2, double* 
     if (n < 0) return fail(PT_ERR_ARG, "n must be >= 0");
     if (n > 0 && !(x1 && x2 && x3 && p1 && p2 && p3 && alive)) return fail(PT_ERR_ARG, "null state");
     if (p->cache_mode != PT_CACHE_NONE && !save) return fail(PT_ERR_ARG, "a cache mode needs a save callback");
+    if (p->cache_pitch != 0) return fail(PT_ERR_ARG, "pt_push_run hands the save callback rows: cache_pitch must be 0");
     PT_DEVICE_SCOPE(ctx->device);
     cudaStream_t st = ctx->stream;
     const int64_t nsteps = p->nsteps, stride = p->stride;

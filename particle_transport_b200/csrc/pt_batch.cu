@@ -297,6 +297,8 @@ int pt_batch_add(pt_ctx* ctx, pt_batch* b, const pt_campaign_desc* d, int* id)
     if (d->d_mom_cache && (!d->d_cache || d->n_mom < 1 || d->n_mom > d->n))
         return fail(PT_ERR_ARG, "a momenta cache needs the mu cache and 1 <= n_mom <= n");
     if (d->sort_every < 0) return fail(PT_ERR_ARG, "sort_every must be >= 0");
+    if (d->cache_pitch < 0 || (d->d_cache && d->cache_pitch > 0 && d->cache_pitch < d->cache_rows))
+        return fail(PT_ERR_ARG, "cache_pitch must be 0 (rows) or at least cache_rows (time-fastest)");
     int c = -1;
     for (int i = 0; i < b->max_camps; ++i)
         if (!b->h_camps[i].active) {
@@ -353,6 +355,8 @@ int pt_batch_add(pt_ctx* ctx, pt_batch* b, const pt_campaign_desc* d, int* id)
     a.deaths = d->d_deaths;
     a.mom_cache = d->d_mom_cache;
     a.n_mom = d->d_mom_cache ? d->n_mom : 0;
+    a.pitch = d->d_cache ? d->cache_pitch : 0;
+    a.pitch_vec = ((uintptr_t)d->d_cache & 31) == 0;
     C.slot0 = slot0;
     C.n = d->n;
     C.step = 0;

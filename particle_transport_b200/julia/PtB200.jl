@@ -34,7 +34,7 @@ struct PtPushParams
     steps_per_launch::Int32
     sort_every::Int32
     kernel_variant::Int32
-    reserved::Int32
+    cache_pitch::Int32
 end
 
 function check(rc::Cint, where::AbstractString)

@@ -1,0 +1,171 @@
+"""The precision forms against the plain FP64 push.
+
+The FP32 push over FP32 or BF16 bricks and the FP64 push run from the same
+initial state on the same field; the transport products of each form are
+compared cell by cell with those of the FP64 push:
+
+- D_mumu(mu, tau): dmumu_raw_norm of compute_dmumu_arrays_full
+  (src/compute_delta_mu2_dmumu_full.jl:706-744) over the cells holding at
+  least ``min_count`` pairs;
+- <dmu^2>(tau): the per-lag particle mean of the Welford triple
+  (src/compute_delta_mu2_curve.jl:409-429);
+- D_pp(tau): dpp_raw_norm of compute_dpp_arrays (src/compute_dpp_full.jl:301-330)
+  over the first ``n_dpp`` particles, each form with its own p0;
+- |dgamma|/gamma at the end against the FP64 push, and |gamma_end/gamma_0 - 1|
+  of every form on the field with u = 0 (E = 0), where energy is conserved to
+  rounding.
+
+An FP64 push from positions moved by one ulp gives the floor set by chaotic
+divergence: two FP64 runs already differ by that much, so a form is as good
+as FP64 when its errors sit at that floor.
+
+The FP64 push runs over FP64 bricks with a brick sort every 64 steps; its
+results are bit-identical to the reference-layout FP64 push (the parity
+tests show this against the oracle).
+"""
+from __future__ import annotations
+
+import math
+
+import numpy as np
+
+from . import fields as F
+from . import runner as R
+from . import stats as S
+from .fields import FieldLibrary
+from .particles import energy_to_gamma, init_particles_device
+from .time_units import build_mu_edges_full, log_spaced_lag_steps, reference_Omega0
+
+FORMS = {"f32": "brick_f32", "bf16": "brick_bf16"}
+KEYS = R.KEYS
+
+
+def build_libraries(fields_si, grid, forms=("f32", "bf16"), with_e0=True):
+    """FP64-brick library plus one brick library per form, and (with_e0) the
+    same libraries of the field with u = 0.  fields_si: six CUDA float64
+    tensors (Bx, By, Bz, ux, uy, uz) in SI units."""
+    import torch
+
+    B0 = F.reference_B0_T(*fields_si[:3])
+    libs = {"f64": FieldLibrary(fields_si, grid, "brick_f64")}
+    for f in forms:
+        libs[f] = FieldLibrary(fields_si, grid, FORMS[f], B_ref_T=B0)
+    if with_e0:
+        zero = [torch.zeros_like(fields_si[0])] * 3
+        e0 = list(fields_si[:3]) + zero
+        libs["f64_e0"] = FieldLibrary(e0, grid, "brick_f64")
+        for f in forms:
+            libs[f + "_e0"] = FieldLibrary(e0, grid, FORMS[f], B_ref_T=B0)
+    return libs, B0
+
+
+def _push(lib, state, dt, nsteps, stride, cache_mode, n):
+    """Push the first n particles of `state` (dict of CUDA float64 tensors);
+    returns (cache, final state dict of CUDA tensors)."""
+    import torch
+
+    nsave = R.n_saves(nsteps, stride) if cache_mode != "none" else 0
+    sub = {k: state[k][:n].clone() for k in KEYS}
+    alive = torch.ones(n, dtype=torch.uint8, device="cuda")
+    cache = None
+    if cache_mode != "none":
+        shape = (nsave, n) if cache_mode == "mu" else (nsave, 6, n)
+        cache = torch.empty(shape, dtype=torch.float32, device="cuda")
+    if lib.storage == "brick_f64":
+        ens = R.DeviceEnsemble(lib, sub, alive)
+        ens.advance(R.push_params(dt, nsteps, stride, cache=cache_mode, precision="f64", sort_every=64), 0, nsteps,
+                    cache, 0, nsave)
+        return cache, ens.state
+    ens = R.FastEnsemble(lib, sub, alive)
+    ens.advance(R.push_params(dt, nsteps, stride, cache=cache_mode, precision="f32", sort_every=64), 0, nsteps,
+                cache, 0, nsave)
+    final, _ = ens.export()
+    ens.close()
+    return cache, final
+
+
+def _gamma(st):
+    import torch
+
+    p = torch.sqrt(st["p1"] * st["p1"] + st["p2"] * st["p2"] + st["p3"] * st["p3"])
+    return torch.sqrt(1.0 + (p / (F.M_P * F.C_LIGHT)) ** 2)
+
+
+def rel_err(a, b, mask=None):
+    """max and median |a - b| / |b| over the cells finite in both (and in mask)."""
+    a, b = np.asarray(a, np.float64), np.asarray(b, np.float64)
+    m = np.isfinite(a) & np.isfinite(b) & (np.abs(b) > 0)
+    if mask is not None:
+        m &= mask
+    if not m.any():
+        return {"max": math.nan, "median": math.nan, "cells": 0}
+    r = np.abs(a[m] - b[m]) / np.abs(b[m])
+    return {"max": float(r.max()), "median": float(np.median(r)), "cells": int(m.sum())}
+
+
+def compare_forms(libs, B0, grid, energy_GeV, n_particles, steps_per_gyroperiod=128, gyroperiods=50, stride=8,
+                  n_lags=32, n_bins=20, n_dpp=131072, min_count=100, forms=("f32", "bf16"), seed=7, mu0=0.5):
+    """Errors of each form (and of the FP64 one-ulp run) against the FP64
+    push for one energy; fixed-mu injection (mu0, random gyrophase) at
+    random positions.  Returns a dict keyed by form with the relative errors
+    of D_mumu, <dmu^2> and D_pp, |dgamma|/gamma at the end, and the E = 0
+    energy drift (when the libraries hold the u = 0 field)."""
+    import torch
+
+    g0 = energy_to_gamma(energy_GeV)
+    dt = (2 * math.pi / steps_per_gyroperiod) / reference_Omega0(B0, g0, F.Q_E, F.M_P)
+    nsteps = steps_per_gyroperiod * gyroperiods + 1
+    nsave = R.n_saves(nsteps, stride)
+    lags = log_spaced_lag_steps(nsave - 1, n_lags)
+    edges, _ = build_mu_edges_full(0.0, 1.0, n_bins)
+    tau = np.array([l * stride * 2 * math.pi / steps_per_gyroperiod for l in lags])  # t Omega0
+    n_dpp = min(n_dpp, n_particles)
+    st = init_particles_device(libs["f64"], n_particles, energy_GeV, seed=seed, injection_mode="fixed_mu", mu0=mu0)
+    st = {k: st[k].contiguous() for k in KEYS}
+    st_ulp = dict(st, x1=torch.nextafter(st["x1"], torch.full_like(st["x1"], math.inf)))
+
+    def products(lib, state):
+        mu, final = _push(lib, state, dt, nsteps, stride, "mu", n_particles)
+        acc = S.new_dmumu_accumulators(len(lags), n_bins, device="cuda")
+        S.process_mu_chunk_dmumu(mu, lags, edges, acc["particle_counts"], acc["particle_means"],
+                                 acc["particle_m2s"], acc["pair_sum_squares"], acc["pair_counts"],
+                                 acc["dmumu_counts"], acc["dmumu_sum_delta"], acc["dmumu_sum_delta2"],
+                                 layout="particle_fastest")
+        del mu
+        a = {k: v.cpu().numpy() for k, v in acc.items()}
+        d = S.compute_dmumu_arrays_full(a["dmumu_counts"], a["dmumu_sum_delta"], a["dmumu_sum_delta2"], tau, tau,
+                                        min_count)
+        ps, _ = _push(lib, state, dt, nsteps, stride, "phase_space", n_dpp)
+        mom = ps[:, 3:6, :].contiguous()
+        del ps
+        p0 = float(torch.linalg.vector_norm(mom[0, :, 0].double()).item())
+        dacc = S.new_dpp_accumulators(len(lags), device="cuda")
+        S.process_momenta_chunk_dpp(mom, lags, p0, dacc["counts"], dacc["sum_delta_p"], dacc["sum_delta_p2"],
+                                    dacc["sum_delta_p_norm"], dacc["sum_delta_p_norm2"])
+        del mom
+        b = {k: v.cpu().numpy() for k, v in dacc.items()}
+        dpp = S.compute_dpp_arrays(b["counts"], b["sum_delta_p"], b["sum_delta_p2"], b["sum_delta_p_norm"],
+                                   b["sum_delta_p_norm2"], tau, tau)
+        return dict(D=d["dmumu_raw_norm"], counts=a["dmumu_counts"], pm=a["particle_means"],
+                    Dpp=dpp["dpp_raw_norm"], gamma=_gamma(final).cpu().numpy())
+
+    ref = products(libs["f64"], st)
+    out = {"energy_GeV": energy_GeV, "particles": n_particles, "dpp_particles": n_dpp, "saves": nsave,
+           "lags": int(len(lags)), "mu_bins": n_bins, "min_count_per_cell": min_count,
+           "steps": nsteps - 1, "cells_counted": int((ref["counts"] >= min_count).sum())}
+    cells = ref["counts"] >= min_count
+    for form in ("f64_1ulp",) + tuple(forms):
+        r = products(libs["f64" if form == "f64_1ulp" else form], st_ulp if form == "f64_1ulp" else st)
+        out[form] = {"D_mumu": rel_err(r["D"], ref["D"], cells), "delta_mu2": rel_err(r["pm"], ref["pm"]),
+                     "D_pp": rel_err(r["Dpp"], ref["Dpp"]),
+                     "gamma_vs_f64_end": float(np.max(np.abs(r["gamma"] / ref["gamma"] - 1)))}
+        torch.cuda.empty_cache()
+    # E = 0: every form conserves energy to rounding
+    if "f64_e0" in libs:
+        n_e0 = min(n_particles, 65536)
+        for form in ("f64",) + tuple(forms):
+            _, final = _push(libs[form + "_e0"], st, dt, nsteps, stride, "none", n_e0)
+            g_start = _gamma({k: st[k][:n_e0] for k in KEYS})
+            drift = float(torch.max(torch.abs(_gamma(final) / g_start - 1.0)).item())
+            out.setdefault(form, {})["gamma_drift_E0"] = drift
+    return out

@@ -31,9 +31,12 @@ PRECISION = {"f64": _lib.PT_PUSH_F64, "f32": _lib.PT_PUSH_F32}
 
 def push_params(dt: float, nsteps: int, stride: int, periodic: bool = True, cache: str = "mu", cache_f64=False,
                 precision: str = "f64", steps_per_launch: int = 0, sort_every: int = 0,
-                kernel_variant: int = 0) -> _lib.PushParams:
+                kernel_variant: int = 0, cache_pitch: int = 0) -> _lib.PushParams:
+    """pt_push_params.  cache_pitch > 0 selects the time-fastest mu cache of
+    the FP32 push: save row r of particle p at p * cache_pitch + (r - row_base)."""
     return _lib.PushParams(float(dt), int(nsteps), int(stride), int(bool(periodic)), CACHE[cache], int(bool(cache_f64)),
-                           PRECISION[precision], int(steps_per_launch), int(sort_every), int(kernel_variant), 0)
+                           PRECISION[precision], int(steps_per_launch), int(sort_every), int(kernel_variant),
+                           int(cache_pitch))
 
 
 def n_saves(nsteps: int, stride: int) -> int:

@@ -161,15 +161,21 @@ class CampaignServer:
         nsave = (nsteps - 1) // stride + 1
         st = init_particles_device(fl, spec.n_particles, spec.energy_GeV, seed=spec.seed,
                                    injection_mode=spec.injection, mu0=spec.mu0)
-        cache = torch.empty((nsave, spec.n_particles), dtype=torch.float32, device=self.device)
+        # the FP32 push writes a time-fastest mu cache [n][pitch] (a particle's
+        # saves leave in 32-byte stores and the binning stages each series
+        # with coalesced reads); the FP64 push writes rows [nsave][n]
+        pitch = (nsave + 7) // 8 * 8 if self.push == "f32" else 0
+        shape = (spec.n_particles, pitch) if pitch else (nsave, spec.n_particles)
+        cache = torch.empty(shape, dtype=torch.float32, device=self.device)
         n_dpp = min(spec.n_particles, max(0, spec.dpp_particles))
         mom = torch.empty((nsave, 3, n_dpp), dtype=torch.float32, device=self.device) if n_dpp else None
         # re-sort cadence by particle speed: fast particles leave their
         # bricks within a few steps (taken from the energy: no device read)
         every = max(1, sort_cadence(cells_per_step_gamma(fl, g0, dt)) // self.K)
-        cid = self.batch.add(fl, st, dt, nsteps, stride, cache=cache, mom_cache=mom, sort_every=every)
+        extra = {"time_fastest": True} if pitch else {}
+        cid = self.batch.add(fl, st, dt, nsteps, stride, cache=cache, mom_cache=mom, sort_every=every, **extra)
         self._running_ids = None  # a new campaign runs until the next selection
-        self.active[jid] = dict(spec=spec, cid=cid, cache=cache, mom=mom, nsteps=nsteps, nsave=nsave,
+        self.active[jid] = dict(spec=spec, cid=cid, cache=cache, pitch=pitch, mom=mom, nsteps=nsteps, nsave=nsave,
                                 arrival=arrival, admitted=time.perf_counter(), bytes=self.job_bytes(spec))
         self.used += self.job_bytes(spec)
 
@@ -215,7 +221,8 @@ class CampaignServer:
             d_edges = torch.as_tensor(edges).pin_memory().to(self.device, non_blocking=True)
             self.side_ctx.use_stream(self.side)
             cache = rec["cache"]
-            args = (self.side_ctx.handle, _lib.ptr(cache), spec.n_particles, rec["nsave"], 1, spec.n_particles,
+            sp, ss = (rec["pitch"], 1) if rec["pitch"] else (1, spec.n_particles)
+            args = (self.side_ctx.handle, _lib.ptr(cache), spec.n_particles, rec["nsave"], sp, ss,
                     _lib.ptr(d_lags), len(lags), _lib.ptr(d_edges), spec.n_bins, S.START[spec.start_mode], 1,
                     *[_lib.ptr(acc[k]) for k in ("dmumu_counts", "dmumu_sum_delta", "dmumu_sum_delta2",
                                                  "particle_counts", "particle_means", "particle_m2s",
@@ -318,7 +325,11 @@ class CampaignServer:
                 # work: a copy on the main stream would wait for the epochs
                 with self.torch.cuda.stream(self.side):
                     acc = {k: v.cpu().numpy() for k, v in rec["acc"].items()}
-                    mu = rec["cache"].cpu().numpy() if self.keep_cache else None
+                    mu = None
+                    if self.keep_cache:  # the reference's row layout [nsave][n]
+                        mu = rec["cache"].cpu().numpy()
+                        if rec["pitch"]:
+                            mu = np.ascontiguousarray(mu[:, :rec["nsave"]].T)
                     dpp = self._dpp_result(rec)
                 res = JobResult(jid, spec, rec["arrival"], rec["admitted"], time.perf_counter(),
                                 spec.n_particles * (rec["nsteps"] - 1), acc, rec["lags"], rec["edges"], mu, dpp)

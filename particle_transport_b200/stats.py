@@ -63,18 +63,22 @@ def new_dmumu_accumulators(n_lags: int, n_bins: int, device=None):
 
 def process_mu_chunk_dmumu(mu_chunk, lag_steps, mu_edges, particle_counts, particle_means, particle_m2s,
                            pair_sum_squares, pair_counts, dmumu_counts, dmumu_sum_delta, dmumu_sum_delta2,
-                           start_mode="sliding", bin_abs=True, layout="time_fastest"):
+                           start_mode="sliding", bin_abs=True, layout="time_fastest", nsave=None):
     """Accumulate one chunk of mu series into the D_mumu / <dmu^2> accumulators.
 
-    mu_chunk: float32, (chunk, nsave) for layout "time_fastest" (the Julia
-    mu_chunk) or (nsave, chunk) for "particle_fastest" (the mu cache as
-    written: one row per save)."""
+    mu_chunk: float32, (chunk, pitch) for layout "time_fastest" (the Julia
+    mu_chunk, or the time-fastest cache of the FP32 push; the first nsave
+    saves of each row are used, all of them by default) or (nsave, chunk) for
+    "particle_fastest" (the mu cache as written: one row per save)."""
     start_mode = str(start_mode)
     if start_mode not in START:
         raise ValueError(f"Unknown dmumu_start_mode: {start_mode}")
     if layout == "time_fastest":
-        chunk, nsave = mu_chunk.shape
-        sp, ss = nsave, 1
+        chunk, pitch = mu_chunk.shape
+        nsave = pitch if nsave is None else int(nsave)
+        if not 1 <= nsave <= pitch:
+            raise ValueError("nsave must be in [1, mu_chunk.shape[1]]")
+        sp, ss = pitch, 1
     elif layout == "particle_fastest":
         nsave, chunk = mu_chunk.shape
         sp, ss = 1, chunk

@@ -219,3 +219,40 @@ def test_tune_batch_picks_cadences(cuda, tmp_path, monkeypatch):
     for ch, (mu_ref, _) in zip(caches, ref):
         assert np.array_equal(ch.cpu().numpy(), mu_ref, equal_nan=True)
     b.close()
+
+
+@pytest.mark.parametrize("K,every", [(64, (1, 1, 1, 1)), (16, (1, 3, 2, 5))])
+def test_batch_time_fastest_caches_bit_identical(cuda, K, every):
+    """Campaigns with time-fastest mu caches ([n][pitch]: each particle's
+    saves contiguous) hold the values of the row caches of their runs alone."""
+    torch = cuda
+    cs = campaigns(torch)
+    ref = [run_alone(torch, c) for c in cs]
+    b = Batch(5000, max_campaigns=8, steps_per_epoch=K, sort=True)
+    caches = [torch.full((len(c["state"]["x1"]), R.n_saves(c["nsteps"], c["stride"]) + 3), float("inf"),
+                         dtype=torch.float32, device="cuda") for c in cs]
+    ids = [b.add(c["field"], c["state"], c["dt"], c["nsteps"], c["stride"], cache=ch, sort_every=e, time_fastest=True)
+           for c, ch, e in zip(cs, caches, every)]
+    b.run(max(math.ceil(c["nsteps"] / K) for c in cs))
+    for c, cid, ch, (mu_ref, _) in zip(cs, ids, caches, ref):
+        assert b.step(cid) == c["nsteps"]
+        got = ch.cpu().numpy()
+        nsave = mu_ref.shape[0]
+        assert np.array_equal(got[:, :nsave].T, mu_ref, equal_nan=True)
+        assert np.all(np.isinf(got[:, nsave:]))  # the pad past the last save is left alone
+    b.close()
+
+
+def test_batch_time_fastest_ring(cuda):
+    torch = cuda
+    c = campaigns(torch)[1]
+    mu_ref, _ = run_alone(torch, c)
+    b = Batch(1000, max_campaigns=2, steps_per_epoch=64)
+    ring = torch.full((len(c["state"]["x1"]), 8), float("nan"), dtype=torch.float32, device="cuda")
+    cid = b.add(c["field"], c["state"], c["dt"], c["nsteps"], c["stride"], cache=ring, ring=True, time_fastest=True)
+    b.run(math.ceil(c["nsteps"] / 64))
+    nsave = mu_ref.shape[0]
+    got = ring.cpu().numpy()
+    for r in range(nsave - 8, nsave):
+        assert np.array_equal(got[:, r % 8], mu_ref[r], equal_nan=True)
+    b.close()

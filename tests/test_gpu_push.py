@@ -239,3 +239,58 @@ def test_push_run_context_buffers_reused(cuda, precision):
         assert np.array_equal(res[2], first[2])
     # the smaller run is the prefix of the larger one (particles are independent)
     assert np.array_equal(small[0], first[0][:, :1000], equal_nan=True)
+
+
+@pytest.mark.parametrize("pitch_pad, steps_per_launch, row_base, f64", [
+    (0, 0, 0, False),      # pitch = nsave: one call, aligned runs of 8 saves
+    (5, 0, 0, False),      # pitch not a multiple of 8: runs aligned per element, not per particle
+    (3, 24, 0, False),     # launches of 24 steps = 6 saves: runs split across launches
+    (0, 64, 3, False),     # rows from a misaligned row_base
+    (0, 40, 0, True),      # Float64 cache
+])
+def test_time_fastest_mu_cache_bit_identical_to_rows(cuda, pitch_pad, steps_per_launch, row_base, f64):
+    """cache_pitch > 0: save row r of particle p at p * pitch + (r - row_base).
+    The mu values are those of the row layout, bit for bit, under brick
+    sorts, launch splits and any pitch."""
+    torch = cuda
+    pb = small_problem(n=16, n_particles=1700, u_over_c=1e-4, energy_GeV=10.0)
+    fl = FieldLibrary(pb.fields, pb.grid, "brick_bf16")
+    nsteps, stride = 401, 4
+    nsave = R.n_saves(nsteps, stride)
+    rows = nsave - row_base
+    dt_ = torch.float64 if f64 else torch.float32
+    out = {}
+    for pitch in (0, rows + pitch_pad):
+        ens = R.FastEnsemble(fl, pb.state, np.ones(1700, np.uint8))
+        shape = (1700, pitch) if pitch else (rows, 1700)
+        cache = torch.full(shape, float("inf"), dtype=dt_, device="cuda")
+        params = R.push_params(pb.dt, nsteps, stride, cache="mu", cache_f64=f64, precision="f32", sort_every=32,
+                               steps_per_launch=steps_per_launch, cache_pitch=pitch)
+        ens.advance(params, 0, nsteps, cache, row_base, rows)
+        torch.cuda.synchronize()
+        c = cache.cpu().numpy()
+        if pitch:
+            assert np.all(np.isinf(c[:, rows:]))  # the pad past the last row is left alone
+            c = c[:, :rows].T
+        out[pitch] = c
+        ens.close()
+    a, b = out[0], out[rows + pitch_pad]
+    assert np.isfinite(a).all()
+    assert np.array_equal(a, b), np.argwhere(a != b)[:5]
+
+
+def test_time_fastest_rejected_where_it_does_not_apply(cuda):
+    from particle_transport_b200._lib import PtError
+    pb = small_problem(n=8, n_particles=64)
+    fb = FieldLibrary(pb.fields, pb.grid, "brick_bf16")
+    ens = R.FastEnsemble(fb, pb.state, np.ones(64, np.uint8))
+    torch = cuda
+    cache = torch.empty((64, 4), dtype=torch.float32, device="cuda")
+    with pytest.raises(PtError, match="at least cache_rows"):
+        ens.advance(R.push_params(pb.dt, 21, 4, cache="mu", precision="f32", cache_pitch=4), 0, 21, cache, 0, 6)
+    with pytest.raises(PtError, match="FP32 push only"):
+        ens.advance(R.push_params(pb.dt, 21, 4, cache="phase_space", precision="f32", cache_pitch=8), 0, 21, cache,
+                    0, 6)
+    with pytest.raises(PtError, match="cache_pitch must be 0"):
+        R.run_push_host(fb, copy_state(pb.state), np.ones(64, np.uint8),
+                        R.push_params(pb.dt, 21, 4, cache="mu", precision="f32", cache_pitch=8), lambda i, r: None)
