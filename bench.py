@@ -67,10 +67,16 @@ def parse():
     ap.add_argument("--e2e-gyroperiods", type=int, default=32,
                     help="T_g0 per pt_push_run call in the e2e leg (the reference pushes a whole campaign, "
                          "500 T_g0 at 512^3, per call)")
-    ap.add_argument("--skip", default="", help="comma list of legs to skip: fp32b,fp64,lag,dpp,e2e,cpu,batch,serve,config1")
+    ap.add_argument("--skip", default="",
+                    help="comma list of legs to skip: fp32b,fp64,lag,dpp,e2e,cpu,batch,serve,config1,precision")
     ap.add_argument("--cpu-seconds", type=float, default=10.0)
+    ap.add_argument("--serve-jobs", type=int, default=100, help="jobs of the serving stream")
+    ap.add_argument("--serve-cmp", type=int, default=16, help="jobs of the FP32-vs-FP64 serving comparison")
+    ap.add_argument("--serve-all", action="store_true", help="also serve the stream with every job in every epoch")
     ap.add_argument("--precision", action="store_true",
                     help="run only the plain-vs-precision study (256^3, 3 energies) and print its JSON line")
+    ap.add_argument("--precision-key-particles", type=int, default=524288,
+                    help="particles per case of the default line's precision key")
     ap.add_argument("--precision-grid", type=int, default=256)
     ap.add_argument("--precision-particles", type=int, default=1_048_576)
     ap.add_argument("--precision-gyroperiods", type=int, default=200)
@@ -505,8 +511,14 @@ def run_ours(args, ws, rank, local):
                "hbm_frac_of_compulsory": (4 * nl * nsave / lag_s / 1e9) / peaks["hbm_gbs"],
                "campaign_push_s": push_full_s,
                "campaign_push_rate": nl * (NSTEPS - 1) / push_full_s}
+        lag["roofline"] = issue_roofline("dmumu_kernel", lag["value"] / ws, clocks, dev)
+        if ws > 1:
+            # the job's products: every rank's accumulators merged in rank order
+            from particle_transport_b200 import shard
+            merged = shard.reduce_dmumu_accumulators(lag_pass.acc)
+            lag["merged"] = {"pair_counts": int(merged["pair_counts"].sum()),
+                             "particle_counts": int(merged["particle_counts"].max()), "ranks": ws}
         if "cpu" not in skip and rank == 0:
-            sys.path.insert(0, os.path.join(ROOT, "tests"))
             mu_host = np.ascontiguousarray(cache[:4096, :nsave].cpu().numpy())
             lag["cpu_baseline"] = cpu_lag_rate(mu_host, lags, edges, args.cpu_seconds / 2)
         del ens_l, cache
@@ -557,6 +569,9 @@ def run_ours(args, ws, rank, local):
         torch.cuda.empty_cache()
         lags_p = log_spaced_lag_steps(nsave - 1, 64)
         p0 = float(torch.linalg.vector_norm(mom[0, :, 0].double()).item())
+        if ws > 1:
+            from particle_transport_b200 import shard
+            p0 = shard.broadcast_p0(p0, device=dev)  # the first particle's |p| at save 1 is rank 0's
 
         def dpp_pass(_k):
             acc = S.new_dpp_accumulators(len(lags_p), device=dev)
@@ -586,6 +601,10 @@ def run_ours(args, ws, rank, local):
                                      "spacing": "log", "ms_per_pass": hms / 3,
                                      "counted": int(hist_pass.counts.sum().item()),
                                      "particles_x_snapshots": int(npp * len(snaps))}}
+        dpp["roofline"] = issue_roofline("dpp_kernel", dpp["value"] / ws, clocks, dev)
+        if ws > 1:
+            merged = shard.reduce_dpp_accumulators(dpp_pass.acc)
+            dpp["merged"] = {"counts": int(merged["counts"].sum()), "p0": p0, "ranks": ws}
         if "cpu" not in skip and rank == 0:
             dpp["cpu_baseline"] = cpu_dpp_rate(mom[:, :, :4096].cpu().numpy(), lags_p, p0, args.cpu_seconds / 2)
         del mom
@@ -635,6 +654,8 @@ def run_ours(args, ws, rank, local):
     torch.cuda.empty_cache()
     config1 = run_config1(args, rank) if ("config1" not in skip and rank == 0) else None
     torch.cuda.empty_cache()
+    precision = run_precision_key(args, dev) if ("precision" not in skip and rank == 0) else None
+    torch.cuda.empty_cache()
 
     # ---------------- CPU baseline (oracle, host cores)
     cpu = None
@@ -658,9 +679,37 @@ def run_ours(args, ws, rank, local):
                 "e2e": e2e,
                 "cpu_baseline": cpu,
                 "clocks": clocks, "gpu_launches": launches["push"] + launches["sort"], "batched": batched,
-                "job_latency": ({"p50_s": serving["p50_s"], "p99_s": serving["p99_s"]} if serving else None),
-                "serving": serving, "config1_end_to_end": config1}
+                "job_latency": ({"p50_s": serving["p50_s"], "p99_s": serving["p99_s"], "jobs": serving["jobs"]}
+                                if serving else None),
+                "serving": serving, "config1_end_to_end": config1, "precision": precision}
         print(json.dumps(line), flush=True)
+
+
+# Warp instructions per lag pair of the statistics kernels: smsp__inst_executed.sum
+# of one launch over the pairs it processed, from an ncu capture of the bench's
+# small case (profiles/dmumu_*.md, profiles/dpp_*.md).  These kernels are
+# bound by instruction issue, whose ceiling is one warp instruction per cycle
+# per SM sub-partition (4 per SM).
+WARP_INST_PER_PAIR = {"dmumu_kernel": 47.17e9 / 49.19e9}
+
+
+def issue_roofline(kernel: str, pairs_per_s: float, clocks, device) -> dict:
+    """Issue-bound roofline of a lag-statistics kernel: achieved warp
+    instructions per second (pairs/s x warp instructions per pair) over the
+    issue ceiling at the SM clock of the timed region."""
+    import torch
+
+    w = WARP_INST_PER_PAIR.get(kernel)
+    sms = torch.cuda.get_device_properties(device).multi_processor_count
+    mhz = (clocks or {}).get("sm_mhz") or (clocks or {}).get("sm_max_mhz") or 1965.0
+    peak = sms * 4 * mhz * 1e6
+    if w is None:
+        return {"kernel": kernel, "bound": "issue", "warp_inst_per_pair": None, "peak": peak / 1e9,
+                "unit": "G warp-inst/s"}
+    ach = pairs_per_s * w
+    return {"kernel": kernel, "bound": "issue", "warp_inst_per_pair": w, "achieved": ach / 1e9, "peak": peak / 1e9,
+            "unit": "G warp-inst/s", "frac": ach / peak, "sm_mhz": mhz,
+            "note": "warp instructions per pair from an ncu capture of the same kernel; peak = SMs x 4 x clock"}
 
 
 # DRAM bytes (dram__bytes_read.sum + dram__bytes_write.sum) of one 64-step
@@ -830,6 +879,52 @@ def run_batched(args, dev, rank):
                               "T_g0": (c["nsteps"] - 1) / 64, "sort_every_epochs": c["sort_every"]} for c in camps]}
 
 
+def run_precision_key(args, dev):
+    """The precision forms against the FP64 push, reduced from the
+    plain-vs-precision configuration: 128^3 (dB/B0 = 0.5 on |k| = 2..64,
+    u_rms = 1e-4 c), the total field and its alfven / fast / slow projections,
+    protons at 1, 10 and 100 GeV with fixed mu0 = 0.5, 128 steps per T_g0 for
+    50 T_g0, mu every 8 steps (801 saves), 32 log lags x 20 |mu| bins, D_pp
+    over 131,072 particles.  For each form (FP32 push over FP32 bricks and
+    over BF16 bricks) and the FP64 one-ulp floor: the largest relative error
+    of D_mumu(mu, tau) (cells with >= 100 pairs), <dmu^2>(tau) and D_pp(tau)
+    over every variant and energy, and the energy drift with E = 0."""
+    import torch
+
+    from particle_transport_b200 import fields as F
+    from particle_transport_b200 import precision as P
+
+    n, npart = 128, args.precision_key_particles
+    grid = F.build_uniform_grid((n - 1) * F.gyroradius_m(1.0, 1e-10), n, n, n)
+    t0 = time.perf_counter()
+    forms = ("f64_1ulp", "f32", "bf16")
+    worst = {f: {"D_mumu": 0.0, "delta_mu2": 0.0, "D_pp": 0.0} for f in forms}
+    drift = {"f64": 0.0, "f32": 0.0, "bf16": 0.0}
+    cases = {}
+    for mode in ("total", "alfven", "fast", "slow"):
+        fs = F.to_si(F.synthetic_mhd_fields(n, 2, n // 2, 0.5, 1.0, 1e-4, seed=5, modes=mode, device=dev))
+        libs, B0 = P.build_libraries(fs, grid)
+        del fs
+        for E in (1.0, 10.0, 100.0):
+            r = P.compare_forms(libs, B0, grid, E, npart, gyroperiods=50)
+            cases[f"{mode}/{E:g}GeV"] = {f: {k: r[f][k]["max"] for k in ("D_mumu", "delta_mu2", "D_pp")}
+                                         for f in forms}
+            for f in forms:
+                for k in worst[f]:
+                    worst[f][k] = max(worst[f][k], r[f][k]["max"])
+            for f in drift:
+                drift[f] = max(drift[f], r[f]["gamma_drift_E0"])
+        for lib in libs.values():
+            lib.close()
+        torch.cuda.empty_cache()
+    return {"max_rel_err": worst, "tolerance": 0.01, "within_tolerance": all(v <= 0.01 for f in forms
+                                                                               for v in worst[f].values()),
+            "gamma_drift_E0_max": drift, "per_case": cases, "seconds": time.perf_counter() - t0,
+            "setup": f"128^3, dB/B0=0.5, k=2..64, u_rms=1e-4 c; total/alfven/fast/slow x 1/10/100 GeV; {npart} "
+                     "protons, fixed mu0=0.5, 128 steps/T_g0, 50 T_g0, mu every 8 steps; 32 lags x 20 |mu| bins "
+                     "(cells >= 100 pairs); D_pp over 131072 particles; errors relative to the FP64 push"}
+
+
 def run_precision(args, dev):
     """Plain vs precision forms at 256^3 (total field, dB/B0 = 0.5, k = 2..128,
     u_rms = 1e-4 c): 1,048,576 protons per energy at 1, 10 and 100 GeV,
@@ -989,20 +1084,29 @@ def run_precision(args, dev):
     return out
 
 
-def run_serving(args, dev, n_jobs=16, rate=4.0, n_cmp=8):
-    """Serving (config 5): a Poisson stream (mean 4 jobs/s) of transport jobs
-    against resident 256^3 and 512^3 libraries (4 modes each), admitted
-    against a 150 GB HBM budget and continuously batched; p50/p99 job latency
-    and the aggregate particle-step rate of the FP32 push over BF16 bricks.
-    Then the FP32 push against the plain FP64 push on one smaller stream
-    (n_cmp jobs, 16k-1M particles, 10-60 T_g0) -- the FP64 server pushes every
-    job with the reference-layout kernel from FP64 libraries of the same
-    fields."""
+def run_serving(args, dev, rate=4.0):
+    """Serving (config 5).  A Poisson stream (mean 4 jobs/s) of args.serve_jobs
+    jobs drawn from the full job distribution -- 16K-8M particles, 10-300
+    T_g0, 1-300 GeV, either library, any mode, isotropic or fixed-mu -- against
+    resident 256^3 and 512^3 BF16-brick libraries (4 modes each), admitted
+    against a 150 GB HBM budget and continuously batched: p50 / p99 job
+    latency over every job and the particle-step rate over the wall clock and
+    while the device is busy.
+    Matched workload: the same campaigns in one Batch, all admitted at once,
+    with the server's steps per epoch and sort cadences and a ring mu cache;
+    its rate against the server's busy rate separates the engine's overhead
+    from the workload mix.
+    FP32 against FP64: the first args.serve_cmp jobs of the same stream (same
+    arrivals and specs) served with the FP32 push and with the FP64 push over
+    FP64 bricks (results bit-identical to the reference-layout FP64 push,
+    whose rate is the fp64 leg of the headline)."""
     import torch
 
     from particle_transport_b200 import fields as F
+    from particle_transport_b200.batch import Batch
     from particle_transport_b200.fields import FieldLibrary
-    from particle_transport_b200.server import CampaignServer, sample_jobs
+    from particle_transport_b200.particles import init_particles_device
+    from particle_transport_b200.server import CampaignServer, job_campaign, sample_jobs
 
     B0 = {}
 
@@ -1041,37 +1145,68 @@ def run_serving(args, dev, n_jobs=16, rate=4.0, n_cmp=8):
         lat = np.array([r.latency for r in srv.results])
         steps = sum(r.particle_steps for r in srv.results)
         busy = srv.device_busy_s()
-        out = {"jobs": len(specs), "p50_s": float(np.percentile(lat, 50)), "p99_s": float(np.percentile(lat, 99)),
-               "mean_s": float(lat.mean()), "wall_s": wall, "particle_steps": int(steps),
-               "aggregate_rate": steps / wall, "device_busy_s": busy, "busy_rate": steps / busy,
-               "admit_host_s": srv.admit_s, "epochs": srv.epochs}
+        out = {"jobs": len(srv.results), "p50_s": float(np.percentile(lat, 50)),
+               "p99_s": float(np.percentile(lat, 99)), "mean_s": float(lat.mean()), "max_s": float(lat.max()),
+               "wall_s": wall, "particle_steps": int(steps), "aggregate_rate": steps / wall, "device_busy_s": busy,
+               "busy_rate": steps / busy, "admit_host_s": srv.admit_s, "epochs": srv.epochs}
         srv.close()
         torch.cuda.empty_cache()
         return out
 
-    arrivals, specs = sample_jobs(n_jobs, rate, ["256", "512"], seed=2026)
+    def matched(libraries, specs, K=64):
+        """The jobs' campaigns in one Batch, every one running from the first epoch."""
+        ntot = sum(sp.n_particles for sp in specs)
+        b = Batch(ntot, max_campaigns=len(specs), storage="brick_bf16", steps_per_epoch=K)
+        rings, steps, epochs = [], 0, 0
+        for sp in specs:
+            fl, dt, nsteps, stride, every = job_campaign(sp, libraries, B0, K)
+            st = init_particles_device(fl, sp.n_particles, sp.energy_GeV, seed=sp.seed, injection_mode=sp.injection,
+                                       mu0=sp.mu0)
+            rings.append(torch.empty((sp.n_particles, 8), dtype=torch.float32, device=dev))
+            b.add(fl, st, dt, nsteps, stride, cache=rings[-1], ring=True, sort_every=every, time_fastest=True)
+            steps += sp.n_particles * (nsteps - 1)
+            epochs = max(epochs, math.ceil(nsteps / K))
+            del st
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        b.run(epochs)
+        e1.record()
+        torch.cuda.synchronize()
+        secs = e0.elapsed_time(e1) / 1e3
+        b.close()
+        del rings
+        torch.cuda.empty_cache()
+        return {"jobs": len(specs), "particles": ntot, "particle_steps": int(steps), "epochs": epochs,
+                "seconds": secs, "rate": steps / secs, "cache": "ring of 8 saves per particle (time-fastest)"}
+
+    arrivals, specs = sample_jobs(args.serve_jobs, rate, ["256", "512"], seed=2026)
     main = serve(libs, arrivals, specs, "f32")
     main.update({"rate_per_s": rate, "unit": UNIT, "push": "FP32 / BF16 bricks",
+                 "stream": f"{args.serve_jobs} jobs, Poisson {rate}/s, 16K-8M particles, 10-300 T_g0, 1-300 GeV, "
+                           "256^3 and 512^3 libraries x 4 modes, isotropic or fixed-mu",
                  "init": "on the device (pt_particles_init_device)", "hbm_budget_GB": 150,
                  "schedule": "srpt: least work left first, epochs filled to 262144 particles"})
-    every = serve(libs, arrivals, specs, "f32", schedule="all")
-    main["schedule_all"] = {k: every[k] for k in ("p50_s", "p99_s", "mean_s", "wall_s", "busy_rate", "epochs")}
-    arr_c, specs_c = sample_jobs(n_cmp, rate, ["256", "512"], seed=7, n_range=(16_384, 1_048_576),
-                                 duration_range=(10.0, 60.0))
-    cmp32 = serve(libs, arr_c, specs_c, "f32")
-    libs64 = make_libs("ref_f64")  # built after the main stream: 29 GB of FP64 fields
-    cmp64 = serve(libs64, arr_c, specs_c, "f64")
-    del libs64
+    if args.serve_all:
+        every = serve(libs, arrivals, specs, "f32", schedule="all")
+        main["schedule_all"] = {k: every[k] for k in ("p50_s", "p99_s", "mean_s", "wall_s", "busy_rate", "epochs")}
+    mt = matched(libs, specs)
+    main["matched_batch"] = dict(mt, server_busy_rate_over_batch_rate=main["busy_rate"] / mt["rate"])
+    k = min(args.serve_cmp, len(specs))
+    cmp32 = serve(libs, arrivals[:k], specs[:k], "f32")
+    del libs
     torch.cuda.empty_cache()
     libs64b = make_libs("brick_f64")  # the same fields as FP64 bricks (38 GB)
-    cmp64b = serve(libs64b, arr_c, specs_c, "f64")
+    cmp64b = serve(libs64b, arrivals[:k], specs[:k], "f64")
     del libs64b
     torch.cuda.empty_cache()
-    main["fp32_vs_fp64"] = {"stream": f"{n_cmp} jobs, Poisson {rate}/s, 16k-1M particles, 10-60 T_g0, 1-300 GeV",
-                            "fp32_bf16": cmp32, "fp64_plain": cmp64,
-                            "fp64_bricks": dict(cmp64b, note="the same FP64 push (bit-identical results) over "
-                                                              "FP64 bricks with brick-sorted slots"),
-                            "busy_rate_ratio": cmp32["busy_rate"] / cmp64["busy_rate"]}
+    main["fp32_vs_fp64"] = {"stream": f"the first {k} jobs of the same stream (same arrivals and specs)",
+                            "fp32_bf16": cmp32,
+                            "fp64_bricks": dict(cmp64b, note="the FP64 push over FP64 bricks with brick-sorted "
+                                                              "slots: results bit-identical to the reference-layout "
+                                                              "FP64 push"),
+                            "busy_rate_ratio": cmp32["busy_rate"] / cmp64b["busy_rate"],
+                            "p50_ratio": cmp64b["p50_s"] / cmp32["p50_s"]}
     return main
 
 

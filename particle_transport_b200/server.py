@@ -152,12 +152,7 @@ class CampaignServer:
 
     def _admit(self, jid, spec, arrival):
         torch = self.torch
-        fl = self.libraries[spec.library][spec.mode]
-        g0 = energy_to_gamma(spec.energy_GeV)
-        Om = reference_Omega0(self.B0[spec.library], g0, Q_E, M_P)
-        dt = (2 * math.pi / spec.steps_per_gyroperiod) / Om
-        nsteps = int(round(spec.duration_gyroperiods * spec.steps_per_gyroperiod)) + 1
-        stride = spec.steps_per_gyroperiod // spec.saves_per_gyroperiod
+        fl, dt, nsteps, stride, every = job_campaign(spec, self.libraries, self.B0, self.K)
         nsave = (nsteps - 1) // stride + 1
         st = init_particles_device(fl, spec.n_particles, spec.energy_GeV, seed=spec.seed,
                                    injection_mode=spec.injection, mu0=spec.mu0)
@@ -169,9 +164,6 @@ class CampaignServer:
         cache = torch.empty(shape, dtype=torch.float32, device=self.device)
         n_dpp = min(spec.n_particles, max(0, spec.dpp_particles))
         mom = torch.empty((nsave, 3, n_dpp), dtype=torch.float32, device=self.device) if n_dpp else None
-        # re-sort cadence by particle speed: fast particles leave their
-        # bricks within a few steps (taken from the energy: no device read)
-        every = max(1, sort_cadence(cells_per_step_gamma(fl, g0, dt)) // self.K)
         extra = {"time_fastest": True} if pitch else {}
         cid = self.batch.add(fl, st, dt, nsteps, stride, cache=cache, mom_cache=mom, sort_every=every, **extra)
         self._running_ids = None  # a new campaign runs until the next selection
@@ -365,6 +357,22 @@ class CampaignServer:
     def close(self):
         self.batch.close()
         self.side_ctx.close()
+
+
+def job_campaign(spec: JobSpec, libraries: dict, B0_ref_T: dict, steps_per_epoch: int):
+    """The campaign of a job: (field library, dt, samples, save stride,
+    re-sort cadence in epochs).  dt resolves steps_per_gyroperiod of the
+    reference gyroperiod of the library's total field at the job's energy;
+    fast particles leave their bricks within a few steps, so the cadence
+    comes from the particle speed (taken from the energy: no device read)."""
+    fl = libraries[spec.library][spec.mode]
+    g0 = energy_to_gamma(spec.energy_GeV)
+    Om = reference_Omega0(B0_ref_T[spec.library], g0, Q_E, M_P)
+    dt = (2 * math.pi / spec.steps_per_gyroperiod) / Om
+    nsteps = int(round(spec.duration_gyroperiods * spec.steps_per_gyroperiod)) + 1
+    stride = spec.steps_per_gyroperiod // spec.saves_per_gyroperiod
+    every = max(1, sort_cadence(cells_per_step_gamma(fl, g0, dt)) // steps_per_epoch)
+    return fl, dt, nsteps, stride, every
 
 
 def sample_jobs(n_jobs: int, rate_per_s: float, libraries, seed: int = 2026, n_range=(16_384, 8_388_608),
