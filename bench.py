@@ -831,8 +831,9 @@ def run_batched(args, dev, rank):
     t0 = time.perf_counter()
     tune = tune_batch(camps, "brick_f32", ntot, use_cache=False)
     tune_s = time.perf_counter() - t0
-    K, bps = tune["K"], tune["blocks_per_sm"]
-    b = Batch(ntot, max_campaigns=len(camps), storage="brick_f32", steps_per_epoch=K, blocks_per_sm=bps)
+    K, bps, thr = tune["K"], tune["blocks_per_sm"], tune["threads_per_block"]
+    b = Batch(ntot, max_campaigns=len(camps), storage="brick_f32", steps_per_epoch=K, blocks_per_sm=bps,
+              threads_per_block=thr)
     caches = []
     for c, se in zip(camps, tune["sort_every"]):
         nsave = (c["nsteps"] - 1) // c["stride"] + 1
@@ -870,7 +871,7 @@ def run_batched(args, dev, rank):
     lag_s = e0.elapsed_time(e1) / 1e3
     pairs = int(sum(int(c["pairs"].sum().item()) for c in camps))
     return {"campaigns": len(camps), "particles": ntot, "epochs": epochs, "steps_per_epoch": K,
-            "blocks_per_sm": bps,
+            "blocks_per_sm": bps, "threads_per_block": thr, "particles_per_thread": 256 // thr,
             "autotune": {"cadence_steps_by_speed_class": {str(k): v for k, v in tune["cadence_steps"].items()},
                          "trials": {k: round(v, 1) for k, v in tune["timings"].items()}, "seconds": tune_s},
             "value": steps_timed / push_s, "unit": UNIT, "push_s": push_s,

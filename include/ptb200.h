@@ -259,6 +259,13 @@ int pt_batch_run(pt_ctx* ctx, pt_batch* batch, int64_t epochs, int use_graph);
  * the least work left.  No reference counterpart (the reference has no
  * serving mode). */
 int pt_batch_set_running(pt_ctx* ctx, pt_batch* batch, const int* ids, int n_ids);
+/* Launch shape of the batch's persistent push kernel: threads_per_block
+ * (64, 128 or 256) and resident blocks per SM (1..16).  A tile holds 256
+ * particles; each thread advances 256 / threads_per_block of them, one after
+ * another.  Results do not depend on the shape.  The tuner of the Python
+ * host (batch.tune_batch) picks it with the steps per epoch and the sort
+ * cadences.  No reference counterpart. */
+int pt_batch_set_launch(pt_ctx* ctx, pt_batch* batch, int threads_per_block, int blocks_per_sm);
 /* Next step of campaign `id` (synchronises the context stream). */
 int pt_batch_step(pt_ctx* ctx, pt_batch* batch, int id, int64_t* step);
 /* Copy campaign `id`'s state back to SI device arrays (n each). */

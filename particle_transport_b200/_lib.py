@@ -33,7 +33,7 @@ EXPORTS = (
     "pt_field_upload", "pt_field_upload_device", "pt_field_destroy", "pt_field_device_bytes", "pt_push_run",
     "pt_push_advance_device", "pt_fast_state_create", "pt_fast_state_export", "pt_fast_state_destroy",
     "pt_fast_state_sort", "pt_push_advance_fast", "pt_batch_create", "pt_batch_add", "pt_batch_remove",
-    "pt_batch_run", "pt_batch_set_running", "pt_batch_step", "pt_batch_export", "pt_batch_destroy", "pt_dmumu_accumulate",
+    "pt_batch_run", "pt_batch_set_running", "pt_batch_set_launch", "pt_batch_step", "pt_batch_export", "pt_batch_destroy", "pt_dmumu_accumulate",
     "pt_dmumu_accumulate_device",
     "pt_dmumu_accumulate_device_noalloc", "pt_dmumu_accumulate_phase_space_device", "pt_dpp_accumulate",
     "pt_dpp_accumulate_device", "pt_energy_snapshots", "pt_energy_snapshots_device",
@@ -130,6 +130,7 @@ def load():
             "pt_batch_remove": (i32, [P, P, i32]),
             "pt_batch_run": (i32, [P, P, i64, i32]),
             "pt_batch_set_running": (i32, [P, P, P, i32]),
+            "pt_batch_set_launch": (i32, [P, P, i32, i32]),
             "pt_batch_step": (i32, [P, P, i32, C.POINTER(C.c_int64)]),
             "pt_batch_export": (i32, [P, P, i32, P, P, P, P, P, P, P]),
             "pt_batch_destroy": (i32, [P]),

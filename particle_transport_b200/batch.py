@@ -33,7 +33,10 @@ KEYS = ("x1", "x2", "x3", "p1", "p2", "p3")
 
 class Batch:
     def __init__(self, capacity: int, max_campaigns: int = 64, storage: str = "brick_bf16", steps_per_epoch: int = 64,
-                 sort: bool = True, blocks_per_sm: int = 0, device: int = 0):
+                 sort: bool = True, blocks_per_sm: int = 0, device: int = 0, threads_per_block: int = 256):
+        """threads_per_block (64, 128, 256) and blocks_per_sm (0: 2) set the
+        persistent push kernel's launch shape; a thread advances 256 /
+        threads_per_block particles of each 256-particle tile."""
         import torch
 
         self.storage = storage
@@ -45,6 +48,13 @@ class Batch:
                   int(bool(sort)), int(blocks_per_sm), C.byref(out))
         self.handle = out
         self.campaigns = {}
+        if threads_per_block != 256:
+            self.set_launch(threads_per_block, blocks_per_sm if blocks_per_sm > 0 else 2 * 256 // threads_per_block)
+
+    def set_launch(self, threads_per_block: int, blocks_per_sm: int) -> None:
+        """pt_batch_set_launch: launch shape of the persistent push kernel."""
+        ctx = _lib.torch_context(self.device.index)
+        _lib.call("pt_batch_set_launch", ctx.handle, self.handle, int(threads_per_block), int(blocks_per_sm))
 
     def add(self, field: FieldLibrary, state: dict, dt: float, nsteps: int, stride: int, periodic: bool = True,
             cache=None, ring: bool = False, deaths=None, alive=None, mom_cache=None, sort_every: int = 1,
@@ -330,13 +340,13 @@ def sort_cadence(cps: float) -> int:
     return 64
 
 
-def _trial(campaigns, storage, capacity, K, bps, sort_every, steps):
+def _trial(campaigns, storage, capacity, K, bps, sort_every, steps, threads=256):
     """Particle-steps/s of `steps` steps (rounded to whole epochs) of a fresh
     batch of the campaigns, after one warm-up epoch."""
     import torch
 
     b = Batch(capacity, max_campaigns=max(len(campaigns), 1), storage=storage, steps_per_epoch=K, sort=True,
-              blocks_per_sm=bps)
+              blocks_per_sm=bps, threads_per_block=threads)
     for c, se in zip(campaigns, sort_every):
         b.add(c["field"], c["state"], c["dt"], c["nsteps"], c["stride"], c.get("periodic", True), sort_every=se)
     epochs = max(1, steps // K)
@@ -365,7 +375,13 @@ def check_cadences(cadences) -> None:
                                  "must be a multiple of every shorter one")
 
 
-def tune_batch(campaigns, storage: str, capacity: int, cadences=(16, 32, 64, 128), blocks=(1, 2, 3),
+# launch shapes of the persistent push tried by tune_batch: (threads per
+# block, resident blocks per SM); a thread advances 256 / threads particles of
+# a tile, so (128, 2) holds the particles of (256, 1) with half the threads
+LAUNCH_SHAPES = ((256, 1), (256, 2), (256, 3), (128, 2), (128, 4), (128, 6))
+
+
+def tune_batch(campaigns, storage: str, capacity: int, cadences=(16, 32, 64, 128), shapes=LAUNCH_SHAPES,
                steps: int = 256, use_cache: bool = True) -> dict:
     """Launch shape and per-campaign sort cadence of a batch.
 
@@ -374,13 +390,15 @@ def tune_batch(campaigns, storage: str, capacity: int, cadences=(16, 32, 64, 128
        sort before each; the fastest is the class's cadence.
     2. The batch's steps per epoch K is the shortest cadence picked; each
        campaign re-sorts every (its class's cadence / K) epochs.
-    3. Resident blocks per SM of the persistent kernel: each of `blocks` is
-       timed on the whole batch with those cadences.
+    3. Launch shape of the persistent kernel -- threads per block, which sets
+       the particles per thread (256 / threads per tile), and resident blocks
+       per SM: each of `shapes` is timed on the whole batch with those
+       cadences.
     Every trial runs `steps` steps (whole epochs) of a fresh batch without
     caches.  The result is cached in a JSON file keyed by device, storage,
-    particle count, grid and speed classes.  Returns {"K", "blocks_per_sm",
-    "sort_every" (one per campaign, in epochs), "cadence_steps" (per class),
-    "timings"}."""
+    particle count, grid and speed classes.  Returns {"K", "threads_per_block",
+    "particles_per_thread", "blocks_per_sm", "sort_every" (one per campaign,
+    in epochs), "cadence_steps" (per class), "timings"}."""
     check_cadences(cadences)
     n_total = sum(len(c["state"]["x1"]) for c in campaigns)
     grid_n = max(c["field"].grid.nx for c in campaigns)
@@ -393,11 +411,12 @@ def tune_batch(campaigns, storage: str, capacity: int, cadences=(16, 32, 64, 128
             table = json.load(open(path))
         except Exception:
             table = {}
-    if key in table and "cadence_steps" in table[key]:
+    if key in table and "cadence_steps" in table[key] and "threads_per_block" in table[key]:
         hit = table[key]
         cad = {int(k): int(v) for k, v in hit["cadence_steps"].items()}
-        K = int(hit["K"])
-        return {"K": K, "blocks_per_sm": int(hit["blocks_per_sm"]), "sort_every": [cad[c] // K for c in cls],
+        K, thr = int(hit["K"]), int(hit["threads_per_block"])
+        return {"K": K, "threads_per_block": thr, "particles_per_thread": 256 // thr,
+                "blocks_per_sm": int(hit["blocks_per_sm"]), "sort_every": [cad[c] // K for c in cls],
                 "cadence_steps": cad, "timings": hit["timings"], "cached": True}
     timings = {}
     cad = {}
@@ -411,15 +430,15 @@ def tune_batch(campaigns, storage: str, capacity: int, cadences=(16, 32, 64, 128
     K = min(cad.values())
     sort_every = [cad[c] // K for c in cls]
     rates = {}
-    for bps in blocks:
-        rates[bps] = _trial(campaigns, storage, capacity, K, bps, sort_every, steps)
-        timings[f"all:{K}x{bps}"] = rates[bps]
-    bps = max(rates, key=rates.get)
-    table[key] = {"K": K, "blocks_per_sm": bps, "cadence_steps": {str(k): v for k, v in cad.items()},
-                  "timings": timings}
+    for thr, bps in shapes:
+        rates[(thr, bps)] = _trial(campaigns, storage, capacity, K, bps, sort_every, steps, threads=thr)
+        timings[f"all:K{K}:{thr}x{bps}"] = rates[(thr, bps)]
+    thr, bps = max(rates, key=rates.get)
+    table[key] = {"K": K, "threads_per_block": thr, "blocks_per_sm": bps,
+                  "cadence_steps": {str(k): v for k, v in cad.items()}, "timings": timings}
     try:
         json.dump(table, open(path, "w"), indent=1)
     except Exception:
         pass
-    return {"K": K, "blocks_per_sm": bps, "sort_every": sort_every, "cadence_steps": cad, "timings": timings,
-            "cached": False}
+    return {"K": K, "threads_per_block": thr, "particles_per_thread": 256 // thr, "blocks_per_sm": bps,
+            "sort_every": sort_every, "cadence_steps": cad, "timings": timings, "cached": False}

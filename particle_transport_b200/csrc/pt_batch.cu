@@ -19,6 +19,7 @@ struct pt_batch {
     int K = 64;
     int sort = 1;
     int grid = 148;
+    int threads = kBatchTile; // threads per block of the persistent push
     BatchStateDev buf[2]{};   // ping-pong state (each campaign's current buffer is its device-side par)
     int sort_grid = 1;        // blocks of the sort's tile kernels (a power of two >= the tiles, with slack)
     BatchCampaignDev* d_camps = nullptr;
@@ -190,7 +191,7 @@ int enqueue_epoch(pt_batch* b, cudaStream_t s)
         if (rc) return rc;
     }
     BatchLaunch L{b->d_camps, b->d_tiles, b->d_ntiles, b->d_counter, {b->buf[0], b->buf[1]}, b->sort,
-                  field_layout(b->storage), b->smem_words, b->grid};
+                  field_layout(b->storage), b->smem_words, b->grid, b->threads};
     int rc = launch_push_batch(L, s);
     if (rc) return rc;
     return launch_batch_epoch_end(b->d_camps, b->max_camps, b->d_counter, b->sort, s);
@@ -443,6 +444,19 @@ int pt_batch_set_running(pt_ctx* ctx, pt_batch* b, const int* ids, int n_ids)
         changed = true;
     }
     return changed ? rebuild_tables(b, -1) : PT_OK;
+}
+
+int pt_batch_set_launch(pt_ctx* ctx, pt_batch* b, int threads_per_block, int blocks_per_sm)
+{
+    if (!ctx || !b) return fail(PT_ERR_ARG, "null argument");
+    if (threads_per_block != 64 && threads_per_block != 128 && threads_per_block != kBatchTile)
+        return fail(PT_ERR_ARG, "threads_per_block must be 64, 128 or 256");
+    if (blocks_per_sm < 1 || blocks_per_sm > 16) return fail(PT_ERR_ARG, "blocks_per_sm must be in [1, 16]");
+    PT_DEVICE_SCOPE(ctx->device);
+    b->threads = threads_per_block;
+    b->grid = ctx->num_sms * blocks_per_sm;
+    drop_graphs(b);  // the next epoch captures the new shape
+    return PT_OK;
 }
 
 int pt_batch_step(pt_ctx* ctx, pt_batch* b, int id, int64_t* step)

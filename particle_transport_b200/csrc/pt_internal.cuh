@@ -306,6 +306,7 @@ struct BatchLaunch {
     int layout;        // LAYOUT_* shared by the batch's fields
     int smem_words;    // max (nx + ny + nz) over the batch's fields
     int grid;
+    int threads;       // threads per block of the push: 64, 128 or kBatchTile (particles per thread = kBatchTile / threads)
 };
 int launch_push_batch(const BatchLaunch& L, cudaStream_t s);
 int launch_batch_apply(BatchCampaignDev* camps, const BatchCampaignDev* staged, int n_camps, int fresh,

@@ -889,8 +889,10 @@ namespace {
 // campaign changes, and runs K steps of its particles from the campaign's
 // device-resident step counter.  The per-particle arithmetic is
 // advance_particle, so a particle's trajectory is the same alone or batched.
-template <int LAYOUT>
-__global__ void __launch_bounds__(256, 1) push_batch_kernel(BatchLaunch L)
+// BLOCK threads per CTA: thread i advances particles i, i + BLOCK, ... of each
+// kBatchTile-particle tile it claims, one after another.
+template <int LAYOUT, int BLOCK>
+__global__ void __launch_bounds__(BLOCK, 1) push_batch_kernel(BatchLaunch L)
 {
     extern __shared__ uint32_t s_offs[];
     __shared__ PushArgsFast s_a;
@@ -932,12 +934,12 @@ __global__ void __launch_bounds__(256, 1) push_batch_kernel(BatchLaunch L)
         }
         const int64_t sb = s_begin, se = s_end;
         if (sb >= se) continue;
-        if ((int)threadIdx.x < T.count) {
+        for (int q = threadIdx.x; q < T.count; q += BLOCK) {
             const uint32_t* ox = s_offs;
             const uint32_t* oy = s_offs + s_a.fld.nx;
             const uint32_t* oz = s_offs + s_a.fld.nx + s_a.fld.ny;
             const BatchStateDev st = s_buf ? L.st[1] : L.st[0];
-            const int64_t slot = T.begin + threadIdx.x;
+            const int64_t slot = T.begin + q;
             double x = st.x[slot], y = st.x[cap + slot], z = st.x[2 * cap + slot];
             float px = st.p[slot], py = st.p[cap + slot], pz = st.p[2 * cap + slot];
             double P2 = st.p2[slot];
@@ -1126,16 +1128,24 @@ __global__ void batch_export_kernel(BatchStateDev st0, BatchStateDev st1, const 
 
 }  // namespace
 
+template <int BLOCK>
+void* push_batch_fn(int layout)
+{
+    return layout == LAYOUT_F32 ? (void*)push_batch_kernel<LAYOUT_F32, BLOCK>
+           : (layout == LAYOUT_BF16_XPAIR ? (void*)push_batch_kernel<LAYOUT_BF16_XPAIR, BLOCK>
+                                          : (void*)push_batch_kernel<LAYOUT_BF16, BLOCK>);
+}
+
 int launch_push_batch(const BatchLaunch& L, cudaStream_t s)
 {
     const size_t smem = sizeof(uint32_t) * (size_t)std::max(L.smem_words, 1);
-    void* kfn = L.layout == LAYOUT_F32 ? (void*)push_batch_kernel<LAYOUT_F32>
-                : (L.layout == LAYOUT_BF16_XPAIR ? (void*)push_batch_kernel<LAYOUT_BF16_XPAIR>
-                                                 : (void*)push_batch_kernel<LAYOUT_BF16>);
+    void* kfn = L.threads == 64 ? push_batch_fn<64>(L.layout)
+                : (L.threads == 128 ? push_batch_fn<128>(L.layout) : push_batch_fn<kBatchTile>(L.layout));
+    const int threads = L.threads == 64 || L.threads == 128 ? L.threads : kBatchTile;
     if (smem > 48 * 1024) PT_CUDA(cudaFuncSetAttribute(kfn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-    if (L.layout == LAYOUT_F32) push_batch_kernel<LAYOUT_F32><<<L.grid, kBatchTile, smem, s>>>(L);
-    else if (L.layout == LAYOUT_BF16_XPAIR) push_batch_kernel<LAYOUT_BF16_XPAIR><<<L.grid, kBatchTile, smem, s>>>(L);
-    else push_batch_kernel<LAYOUT_BF16><<<L.grid, kBatchTile, smem, s>>>(L);
+    BatchLaunch arg = L;
+    void* args[] = {&arg};
+    PT_CUDA(cudaLaunchKernel(kfn, dim3(L.grid), dim3(threads), args, smem, s));
     PT_CHECK_LAUNCH("push_batch_kernel");
     return PT_OK;
 }

@@ -203,15 +203,17 @@ def test_tune_batch_picks_cadences(cuda, tmp_path, monkeypatch):
     torch = cuda
     monkeypatch.setenv("PTB200_TUNE_CACHE", str(tmp_path))
     cs = campaigns(torch)
-    t = tune_batch(cs, "brick_bf16", 5000, cadences=(16, 32), blocks=(1, 2), steps=64)
-    assert t["K"] in (16, 32) and t["blocks_per_sm"] in (1, 2) and not t["cached"]
+    shapes = ((256, 1), (128, 2), (64, 4))
+    t = tune_batch(cs, "brick_bf16", 5000, cadences=(16, 32), shapes=shapes, steps=64)
+    assert t["K"] in (16, 32) and (t["threads_per_block"], t["blocks_per_sm"]) in shapes and not t["cached"]
     assert len(t["sort_every"]) == len(cs) and all(v >= 1 for v in t["sort_every"])
     assert all(v in (16, 32) for v in t["cadence_steps"].values())
-    t2 = tune_batch(cs, "brick_bf16", 5000, cadences=(16, 32), blocks=(1, 2), steps=64)
+    t2 = tune_batch(cs, "brick_bf16", 5000, cadences=(16, 32), shapes=shapes, steps=64)
     assert t2["cached"] and t2["K"] == t["K"] and t2["sort_every"] == t["sort_every"]
     # the tuned batch gives every campaign the result of its run alone
     ref = [run_alone(torch, c) for c in cs]
-    b = Batch(5000, max_campaigns=8, steps_per_epoch=t["K"], blocks_per_sm=t["blocks_per_sm"])
+    b = Batch(5000, max_campaigns=8, steps_per_epoch=t["K"], blocks_per_sm=t["blocks_per_sm"],
+              threads_per_block=t["threads_per_block"])
     caches = [new_cache(torch, c) for c in cs]
     for c, ch, e in zip(cs, caches, t["sort_every"]):
         b.add(c["field"], c["state"], c["dt"], c["nsteps"], c["stride"], cache=ch, sort_every=e)
@@ -255,4 +257,30 @@ def test_batch_time_fastest_ring(cuda):
     got = ring.cpu().numpy()
     for r in range(nsave - 8, nsave):
         assert np.array_equal(got[:, r % 8], mu_ref[r], equal_nan=True)
+    b.close()
+
+
+@pytest.mark.parametrize("threads,bps", [(128, 4), (64, 8), (256, 3)])
+def test_batch_launch_shapes_bit_identical(cuda, threads, bps):
+    """Threads per block (particles per thread = 256 / threads) and blocks per
+    SM change only which thread advances a particle: caches and states are
+    those of the runs alone."""
+    torch = cuda
+    cs = campaigns(torch)
+    ref = [run_alone(torch, c) for c in cs]
+    b = Batch(5000, max_campaigns=8, steps_per_epoch=32, sort=True, blocks_per_sm=bps, threads_per_block=threads)
+    caches = [new_cache(torch, c) for c in cs]
+    ids = [b.add(c["field"], c["state"], c["dt"], c["nsteps"], c["stride"], cache=ch, sort_every=2)
+           for c, ch in zip(cs, caches)]
+    b.run(3)
+    b.set_launch(256, 2)  # a new shape between epochs: the graph is captured again
+    b.run(max(math.ceil(c["nsteps"] / 32) for c in cs))
+    for c, cid, ch, (mu_ref, st_ref) in zip(cs, ids, caches, ref):
+        assert np.array_equal(ch.cpu().numpy(), mu_ref, equal_nan=True)
+        st, _ = b.export(cid)
+        for k in st:
+            assert np.array_equal(st[k].cpu().numpy(), st_ref[k]), k
+    from particle_transport_b200._lib import PtError
+    with pytest.raises(PtError, match="threads_per_block"):
+        b.set_launch(96, 2)
     b.close()

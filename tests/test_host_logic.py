@@ -34,13 +34,13 @@ def test_tune_batch_selection_and_cache(tmp_path, monkeypatch):
     monkeypatch.setenv("PTB200_TUNE_CACHE", str(tmp_path))
     calls = []
 
-    def fake_trial(camps, storage, capacity, K, bps, sort_every, steps):
-        calls.append((len(camps), K, bps, tuple(sort_every)))
-        # slow particles prefer long cadences, fast ones short; 2 blocks per SM best
+    def fake_trial(camps, storage, capacity, K, bps, sort_every, steps, threads=256):
+        calls.append((len(camps), K, bps, tuple(sort_every), threads))
+        # slow particles prefer long cadences, fast ones short; 128 threads x 4 blocks per SM best
         cps = B.cells_per_step(camps[0]["field"], camps[0]["state"], camps[0]["dt"])
         best = 128 if cps < 0.5 else (16 if cps > 4 else 64)
         rate = 1e10 / (1 + abs(math.log2(K / best)))
-        return rate * (1.0 if bps == 2 else 0.9)
+        return rate * (1.0 if (threads, bps) == (128, 4) else 0.9)
 
     monkeypatch.setattr(B, "_trial", fake_trial)
     camps = [campaign(1.0, 1000), campaign(100.0, 2000), campaign(1.0, 500), campaign(100.0, 700)]
@@ -48,14 +48,17 @@ def test_tune_batch_selection_and_cache(tmp_path, monkeypatch):
     cls = [B.speed_class(B.cells_per_step(c["field"], c["state"], c["dt"])) for c in camps]
     assert cls[0] == cls[2] and cls[1] == cls[3] and cls[0] < cls[1]
     assert t["cadence_steps"] == {cls[0]: 128, cls[1]: 16}
-    assert t["K"] == 16 and t["blocks_per_sm"] == 2 and not t["cached"]
+    assert t["K"] == 16 and not t["cached"]
+    assert (t["threads_per_block"], t["particles_per_thread"], t["blocks_per_sm"]) == (128, 2, 4)
     assert t["sort_every"] == [8, 1, 8, 1]  # 128 / 16 and 16 / 16 epochs
-    # each class timed alone at every cadence, then the whole batch at each block count
-    assert sum(1 for c in calls if c[0] == 2) == 2 * 4 and sum(1 for c in calls if c[0] == 4) == 3
+    # each class timed alone at every cadence, then the whole batch at each launch shape
+    assert sum(1 for c in calls if c[0] == 2) == 2 * 4
+    assert sorted((c[4], c[2]) for c in calls if c[0] == 4) == sorted(B.LAUNCH_SHAPES)
     n_calls = len(calls)
     t2 = B.tune_batch(camps, "brick_f32", 10_000, use_cache=True)
     assert t2["cached"] and len(calls) == n_calls  # served from the JSON file
-    assert (t2["K"], t2["blocks_per_sm"], t2["sort_every"]) == (t["K"], t["blocks_per_sm"], t["sort_every"])
+    for k in ("K", "threads_per_block", "blocks_per_sm", "sort_every"):
+        assert t2[k] == t[k], k
 
 
 def admission_server(budget):
