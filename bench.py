@@ -75,7 +75,7 @@ def parse():
     ap.add_argument("--serve-all", action="store_true", help="also serve the stream with every job in every epoch")
     ap.add_argument("--precision", action="store_true",
                     help="run only the plain-vs-precision study (256^3, 3 energies) and print its JSON line")
-    ap.add_argument("--precision-key-particles", type=int, default=524288,
+    ap.add_argument("--precision-key-particles", type=int, default=1048576,
                     help="particles per case of the default line's precision key")
     ap.add_argument("--precision-grid", type=int, default=256)
     ap.add_argument("--precision-particles", type=int, default=1_048_576)
@@ -337,6 +337,25 @@ def run_reference(args, ws, rank):
     print(json.dumps(line), flush=True)
 
 
+def leg(name, fn, *a):
+    """Run one auxiliary leg of the line (no collectives inside);
+    a failure is recorded in the line as {"error": ...} with the traceback on
+    stderr, so the headline and the other legs still report."""
+    import traceback
+
+    import torch
+
+    t0 = time.perf_counter()
+    try:
+        out = fn(*a)
+    except Exception as e:  # noqa: BLE001 -- reported, not swallowed
+        traceback.print_exc()
+        out = {"error": f"{type(e).__name__}: {e}"}
+    torch.cuda.empty_cache()
+    print(f"[bench] {name}: {time.perf_counter() - t0:.1f} s", file=sys.stderr, flush=True)
+    return out
+
+
 def run_ours(args, ws, rank, local):
     import torch
 
@@ -405,6 +424,9 @@ def run_ours(args, ws, rank, local):
                 "traffic": TRAFFIC.get((args.storage, args.grid, n)),
                 "algorithmic_bytes_per_launch": bpl, "launch_ms": launch_ms,
                 "sort_ms_per_step": float(np.mean(steps_ms)) - launch_ms}
+    if rank == 0:
+        print(f"[bench] headline {value:.4g} {UNIT}, push launch {launch_ms:.2f} ms, frac {roofline['frac']:.3f}",
+              file=sys.stderr, flush=True)
 
     # ---------------- the same push over FP32 bricks (the field's second storage)
     fp32b = None
@@ -648,14 +670,10 @@ def run_ours(args, ws, rank, local):
     field_bytes = fb.device_bytes
     del fb
     torch.cuda.empty_cache()
-    batched = run_batched(args, dev, rank) if "batch" not in skip else None
-    torch.cuda.empty_cache()
-    serving = run_serving(args, dev) if ("serve" not in skip and ws == 1) else None
-    torch.cuda.empty_cache()
-    config1 = run_config1(args, rank) if ("config1" not in skip and rank == 0) else None
-    torch.cuda.empty_cache()
-    precision = run_precision_key(args, dev) if ("precision" not in skip and rank == 0) else None
-    torch.cuda.empty_cache()
+    batched = leg("batched", run_batched, args, dev, rank) if "batch" not in skip else None
+    serving = leg("serving", run_serving, args, dev) if ("serve" not in skip and ws == 1) else None
+    config1 = leg("config1", run_config1, args, rank) if ("config1" not in skip and rank == 0) else None
+    precision = leg("precision", run_precision_key, args, dev) if ("precision" not in skip and rank == 0) else None
 
     # ---------------- CPU baseline (oracle, host cores)
     cpu = None
@@ -887,8 +905,9 @@ def run_precision_key(args, dev):
     protons at 1, 10 and 100 GeV with fixed mu0 = 0.5, 128 steps per T_g0 for
     50 T_g0, mu every 8 steps (801 saves), 32 log lags x 20 |mu| bins, D_pp
     over 131,072 particles.  For each form (FP32 push over FP32 bricks and
-    over BF16 bricks) and the FP64 one-ulp floor: the largest relative error
-    of D_mumu(mu, tau) (cells with >= 100 pairs), <dmu^2>(tau) and D_pp(tau)
+    over BF16 bricks) and the FP64 floors (positions moved by one FP64 ulp,
+    and by one FP32 ulp of the box): the largest relative error of
+    D_mumu(mu, tau) (cells with >= 100 pairs), <dmu^2>(tau) and D_pp(tau)
     over every variant and energy, and the energy drift with E = 0."""
     import torch
 
@@ -898,18 +917,21 @@ def run_precision_key(args, dev):
     n, npart = 128, args.precision_key_particles
     grid = F.build_uniform_grid((n - 1) * F.gyroradius_m(1.0, 1e-10), n, n, n)
     t0 = time.perf_counter()
-    forms = ("f64_1ulp", "f32", "bf16")
-    worst = {f: {"D_mumu": 0.0, "delta_mu2": 0.0, "D_pp": 0.0} for f in forms}
+    forms = ("f64_1ulp", "f64_f32ulp", "f32", "bf16")
+    prods = ("D_mumu", "delta_mu2", "D_pp")
+    worst = {f: {k: 0.0 for k in prods} for f in forms}
     drift = {"f64": 0.0, "f32": 0.0, "bf16": 0.0}
     cases = {}
+    ok = True
     for mode in ("total", "alfven", "fast", "slow"):
         fs = F.to_si(F.synthetic_mhd_fields(n, 2, n // 2, 0.5, 1.0, 1e-4, seed=5, modes=mode, device=dev))
         libs, B0 = P.build_libraries(fs, grid)
         del fs
         for E in (1.0, 10.0, 100.0):
             r = P.compare_forms(libs, B0, grid, E, npart, gyroperiods=50)
-            cases[f"{mode}/{E:g}GeV"] = {f: {k: r[f][k]["max"] for k in ("D_mumu", "delta_mu2", "D_pp")}
-                                         for f in forms}
+            cases[f"{mode}/{E:g}GeV"] = {f: {k: r[f][k]["max"] for k in prods} for f in forms}
+            ok &= all(r[f][k]["max"] <= max(0.01, 2.0 * r["f64_f32ulp"][k]["max"]) for f in ("f32", "bf16")
+                      for k in prods)
             for f in forms:
                 for k in worst[f]:
                     worst[f][k] = max(worst[f][k], r[f][k]["max"])
@@ -918,12 +940,16 @@ def run_precision_key(args, dev):
         for lib in libs.values():
             lib.close()
         torch.cuda.empty_cache()
-    return {"max_rel_err": worst, "tolerance": 0.01, "within_tolerance": all(v <= 0.01 for f in forms
-                                                                               for v in worst[f].values()),
+    return {"max_rel_err": worst, "tolerance": 0.01,
+            "within_tolerance": ok,
+            "criterion": "each product of each case within 1 % of the FP64 push, or within twice the change the "
+                         "FP64 push itself shows under a one-FP32-ulp position perturbation (f64_f32ulp) where that "
+                         "exceeds 0.5 %",
             "gamma_drift_E0_max": drift, "per_case": cases, "seconds": time.perf_counter() - t0,
             "setup": f"128^3, dB/B0=0.5, k=2..64, u_rms=1e-4 c; total/alfven/fast/slow x 1/10/100 GeV; {npart} "
                      "protons, fixed mu0=0.5, 128 steps/T_g0, 50 T_g0, mu every 8 steps; 32 lags x 20 |mu| bins "
-                     "(cells >= 100 pairs); D_pp over 131072 particles; errors relative to the FP64 push"}
+                     "(cells >= 100 pairs); D_pp over 131072 particles from a Float64 phase-space cache; errors relative "
+                     "to the FP64 push"}
 
 
 def run_precision(args, dev):

@@ -80,8 +80,12 @@ class Batch:
             if cache.dtype not in (torch.float32, torch.float64) or not shape_ok or not cache.is_contiguous():
                 raise ValueError("cache must be a contiguous float tensor " + ("[n][rows]" if time_fastest else
                                                                                "[rows][n]"))
-            rows = int(cache.shape[1] if time_fastest else cache.shape[0])
-            pitch = rows if time_fastest else 0
+            if time_fastest:
+                # rows a campaign writes: every save (or the ring's length); the pitch may pad them
+                pitch = int(cache.shape[1])
+                rows = pitch if ring else min(pitch, (int(nsteps) - 1) // int(stride) + 1)
+            else:
+                rows = int(cache.shape[0])
         n_mom = 0
         if mom_cache is not None:
             if (cache is None or mom_cache.dtype != torch.float32 or mom_cache.dim() != 3 or mom_cache.shape[1] != 3
