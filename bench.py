@@ -698,7 +698,7 @@ def run_ours(args, ws, rank, local):
                 "cpu_baseline": cpu,
                 "clocks": clocks, "gpu_launches": launches["push"] + launches["sort"], "batched": batched,
                 "job_latency": ({"p50_s": serving["p50_s"], "p99_s": serving["p99_s"], "jobs": serving["jobs"]}
-                                if serving else None),
+                                if serving and "p50_s" in serving else None),
                 "serving": serving, "config1_end_to_end": config1, "precision": precision}
         print(json.dumps(line), flush=True)
 

@@ -37,7 +37,6 @@ namespace {
 
 constexpr int kWarp = 32;
 constexpr int kStageWarps = 8;  // warps of a particle slot that stage its series
-constexpr int kDmumuLagsPerLane = 1;  // default lags per lane of dmumu_kernel
 
 struct WelfordPart {
     long long count;
@@ -87,8 +86,7 @@ struct DmumuLaunch {
     int nl;                    // lags in this batch
     const double* edges;
     int n_bins, bin_abs;
-    int ppc, groups;           // particle slots per CTA, lag groups (32 x lpl lags) per slot
-    int lpl;                   // lags per lane: a lane pairs each start with lpl lags
+    int ppc, groups;           // particle slots per CTA, 32-lag groups per slot
     int parts;                 // warps splitting the bins of one (slot, lag group)
     size_t slot_bytes;
     char* gslots;              // global staging when the slots do not fit on chip
@@ -118,12 +116,8 @@ size_t dmumu_slot_bytes(int64_t nsave, size_t mu_bytes, size_t idx_bytes, int n_
            a16(sizeof(int) * (size_t)(kStageWarps * (n_bins + 1) + n_bins + 2)) + a16(16 * (size_t)nl_cap);
 }
 
-// threads per CTA at most: one lag per lane fits 64 registers at 1024 threads;
-// two lags per lane keep their accumulators in registers at 768 (85 registers)
-constexpr int dmumu_max_threads(int lpl) { return lpl == 1 ? 1024 : 768; }
-
-template <typename IdxT, bool SMEM_SLOTS, class Src, int LPL>
-__global__ void __launch_bounds__(dmumu_max_threads(LPL)) dmumu_kernel(DmumuLaunch a, Src source)
+template <typename IdxT, bool SMEM_SLOTS, class Src>
+__global__ void __launch_bounds__(1024) dmumu_kernel(DmumuLaunch a, Src source)
 {
     using MuT = typename Src::T;
     extern __shared__ __align__(16) unsigned char smem[];
@@ -148,12 +142,10 @@ __global__ void __launch_bounds__(dmumu_max_threads(LPL)) dmumu_kernel(DmumuLaun
         acc_sd2[i] = 0.0;
     }
 
-    // Lags are dealt to 32-lane groups so that lags equal modulo 32 -- which
-    // read the same shared-memory bank at every start -- fall into different
-    // groups where possible.  s_lane_lag[g*32 + lane] = lag index (-1: idle
-    // lane), s_lag_pos[lag] = g*32 + lane.  A warp owns LPL consecutive
-    // 32-lane groups: lane l pairs every start with the lags of its position
-    // in each of them.
+    // Lags are dealt to the 32-lane groups so that lags equal modulo 32 --
+    // which read the same shared-memory bank at every start -- fall into
+    // different groups where possible.  s_lane_lag[g*32 + lane] = lag index
+    // (-1: idle lane), s_lag_pos[lag] = g*32 + lane.
     __shared__ int s_lane_lag[8 * kWarp];
     __shared__ int s_lag_pos[8 * kWarp];
     __shared__ unsigned char cnt[8][kWarp];
@@ -168,7 +160,7 @@ __global__ void __launch_bounds__(dmumu_max_threads(LPL)) dmumu_kernel(DmumuLaun
         for (int i = 0; i < nl; ++i) {
             const int r = (int)(((a.lags[i] % kWarp) + kWarp) % kWarp);
             int best = -1;
-            for (int g = 0; g < a.groups * LPL; ++g) {
+            for (int g = 0; g < a.groups; ++g) {
                 if (fill[g] >= kWarp) continue;
                 if (best < 0 || cnt[g][r] < cnt[best][r] || (cnt[g][r] == cnt[best][r] && fill[g] < fill[best]))
                     best = g;
@@ -184,17 +176,10 @@ __global__ void __launch_bounds__(dmumu_max_threads(LPL)) dmumu_kernel(DmumuLaun
     const int warp = threadIdx.x / kWarp, lane = threadIdx.x % kWarp;
     const int wps = a.groups * a.parts;  // warps per particle slot
     const int slot = warp / wps, group = (warp % wps) / a.parts, part = warp % a.parts;
-    int li[LPL];
-    bool lane_on[LPL];
-    unsigned L32[LPL];  // starts, lags and nsave fit 32 bits (nsave < 2^31)
-#pragma unroll
-    for (int j = 0; j < LPL; ++j) {
-        li[j] = s_lane_lag[(group * LPL + j) * kWarp + lane];
-        lane_on[j] = li[j] >= 0;
-        int64_t L = lane_on[j] ? a.lags[li[j]] : 0;
-        if (L < 1 || L >= a.nsave) L = a.nsave;  // reference: lag >= nsteps -> skipped (valid starts: s < nsave - L)
-        L32[j] = (unsigned)L;
-    }
+    const int li = s_lane_lag[group * kWarp + lane];
+    const bool lane_on = li >= 0;
+    int64_t L = lane_on ? a.lags[li] : 0;
+    if (L < 1 || L >= a.nsave) L = a.nsave;  // reference: lag >= nsteps -> skipped (valid starts: s < nsave - L)
 
     // slot layout: series[nsave + 1] MuT | list[nsave] IdxT | whist[kStageWarps][nb+1] int
     //              | cur[nb+2] int | tot_c[nl] u64 | tot_sd2[nl] f64 (per-particle totals over the bins)
@@ -216,13 +201,8 @@ __global__ void __launch_bounds__(dmumu_max_threads(LPL)) dmumu_kernel(DmumuLaun
     const int wis = warp % wps;
     const int stagers = min(wps, kStageWarps);
 
-    long long wc[LPL], pn[LPL];
-    double wm[LPL], wm2[LPL], pss[LPL];
-#pragma unroll
-    for (int j = 0; j < LPL; ++j) {
-        wc[j] = pn[j] = 0;
-        wm[j] = wm2[j] = pss[j] = 0.0;
-    }
+    long long wc = 0, pn = 0;
+    double wm = 0.0, wm2 = 0.0, pss = 0.0;
     const int64_t scap = min(a.start_cap, a.nsave);
     const unsigned lt_mask = (1u << lane) - 1u;
 
@@ -314,18 +294,14 @@ __global__ void __launch_bounds__(dmumu_max_threads(LPL)) dmumu_kernel(DmumuLaun
         // ---- pairs: bin by bin; the `parts` warps of a (slot, lag group) take
         // bins part, part + parts, ...; every lane keeps two accumulator chains
         if (have) {
-            long long my_c[LPL];
-            double my_sd2[LPL];
-#pragma unroll
-            for (int j = 0; j < LPL; ++j) {
-                my_c[j] = 0;
-                my_sd2[j] = 0.0;
-            }
-            const unsigned n32 = (unsigned)a.nsave;
+            long long my_c = 0;
+            double my_sd2 = 0.0;
+            // starts, lags and nsave fit 32 bits (nsave < 2^31); so does a bin's count
+            const unsigned n32 = (unsigned)a.nsave, L32 = (unsigned)L;
             for (int b = part; b <= nb; b += a.parts) {
                 const int e0 = cur[b], e1 = cur[b + 1];
-                int c[LPL];
-                double sd[LPL], sq[LPL];
+                int c = 0;
+                double sd0 = 0.0, sd1 = 0.0, sq0 = 0.0, sq1 = 0.0;
                 int e = e0;
                 // Branch-free pairs.  A start in the list has a finite mu; its
                 // partner series[s + L] is NaN when the particle's mu is not
@@ -333,130 +309,66 @@ __global__ void __launch_bounds__(dmumu_max_threads(LPL)) dmumu_kernel(DmumuLaun
                 // (idle lanes have L = nsave).  An invalid partner is replaced by
                 // the start's own value, so the pair adds +0 and 0 * 0 -- the
                 // sums are bit-identical to skipping it (they are never -0).
-                if (LPL == 1) {
-                    // one lag per lane: two accumulator chains over starts 4 at a time
-                    int c0 = 0;
-                    double sd0 = 0.0, sd1 = 0.0, sq0 = 0.0, sq1 = 0.0;
-                    const unsigned Lx = L32[0];
-                    for (; e + 4 <= e1; e += 4) {
-                        MuT a_[4], v_[4];
+                for (; e + 4 <= e1; e += 4) {
+                    MuT a_[4], v_[4];
 #pragma unroll
-                        for (int k = 0; k < 4; ++k) {
-                            const unsigned s = (unsigned)list[e + k];
-                            a_[k] = series[s];
-                            v_[k] = series[min(s + Lx, n32)];
-                        }
-#pragma unroll
-                        for (int k = 0; k < 4; k += 2) {
-                            const bool ok0 = v_[k] == v_[k], ok1 = v_[k + 1] == v_[k + 1];
-                            const MuT w0 = ok0 ? v_[k] : a_[k], w1 = ok1 ? v_[k + 1] : a_[k + 1];
-                            c0 += (int)ok0 + (int)ok1;
-                            const double d0 = (double)w0 - (double)a_[k];
-                            const double d1 = (double)w1 - (double)a_[k + 1];
-                            sd0 += d0;
-                            sq0 = fma(d0, d0, sq0);
-                            sd1 += d1;
-                            sq1 = fma(d1, d1, sq1);
-                        }
+                    for (int k = 0; k < 4; ++k) {
+                        const unsigned s = (unsigned)list[e + k];
+                        a_[k] = series[s];
+                        v_[k] = series[min(s + L32, n32)];
                     }
-                    for (; e < e1; ++e) {
-                        const unsigned s = (unsigned)list[e];
-                        const MuT av = series[s];
-                        const MuT vv = series[min(s + Lx, n32)];
-                        const bool ok = vv == vv;
-                        const double d = (double)(ok ? vv : av) - (double)av;
-                        c0 += (int)ok;
-                        sd0 += d;
-                        sq0 = fma(d, d, sq0);
-                    }
-                    c[0] = c0;
-                    sd[0] = sd0 + sd1;
-                    sq[0] = sq0 + sq1;
-                } else {
-                    // LPL lags per lane: a start's index, value and its FP64
-                    // conversion serve all of them; one chain per lag
 #pragma unroll
-                    for (int j = 0; j < LPL; ++j) {
-                        c[j] = 0;
-                        sd[j] = sq[j] = 0.0;
-                    }
-                    for (; e + 2 <= e1; e += 2) {
-                        unsigned s_[2];
-                        MuT a_[2];
-                        MuT v_[2][LPL];
-#pragma unroll
-                        for (int k = 0; k < 2; ++k) {
-                            s_[k] = (unsigned)list[e + k];
-                            a_[k] = series[s_[k]];
-#pragma unroll
-                            for (int j = 0; j < LPL; ++j) v_[k][j] = series[min(s_[k] + L32[j], n32)];
-                        }
-#pragma unroll
-                        for (int k = 0; k < 2; ++k) {
-                            const double ad = (double)a_[k];
-#pragma unroll
-                            for (int j = 0; j < LPL; ++j) {
-                                const bool ok = v_[k][j] == v_[k][j];
-                                const double d = (double)(ok ? v_[k][j] : a_[k]) - ad;
-                                c[j] += (int)ok;
-                                sd[j] += d;
-                                sq[j] = fma(d, d, sq[j]);
-                            }
-                        }
-                    }
-                    for (; e < e1; ++e) {
-                        const unsigned s = (unsigned)list[e];
-                        const MuT av = series[s];
-                        const double ad = (double)av;
-#pragma unroll
-                        for (int j = 0; j < LPL; ++j) {
-                            const MuT vv = series[min(s + L32[j], n32)];
-                            const bool ok = vv == vv;
-                            const double d = (double)(ok ? vv : av) - ad;
-                            c[j] += (int)ok;
-                            sd[j] += d;
-                            sq[j] = fma(d, d, sq[j]);
-                        }
+                    for (int k = 0; k < 4; k += 2) {
+                        const bool ok0 = v_[k] == v_[k], ok1 = v_[k + 1] == v_[k + 1];
+                        const MuT w0 = ok0 ? v_[k] : a_[k], w1 = ok1 ? v_[k + 1] : a_[k + 1];
+                        c += (int)ok0 + (int)ok1;
+                        const double d0 = (double)w0 - (double)a_[k];
+                        const double d1 = (double)w1 - (double)a_[k + 1];
+                        sd0 += d0;
+                        sq0 = fma(d0, d0, sq0);
+                        sd1 += d1;
+                        sq1 = fma(d1, d1, sq1);
                     }
                 }
-#pragma unroll
-                for (int j = 0; j < LPL; ++j) {
-                    if (b < nb && c[j] > 0 && lane_on[j]) {
-                        const int ai = b * nl + li[j];  // [bin][lag]: the lanes of a flush hit consecutive words
-                        atomicAdd(&acc_cnt[ai], (unsigned long long)c[j]);
-                        atomicAdd(&acc_sd[ai], sd[j]);
-                        atomicAdd(&acc_sd2[ai], sq[j]);
-                    }
-                    my_c[j] += c[j];
-                    my_sd2[j] += sq[j];
+                for (; e < e1; ++e) {
+                    const unsigned s = (unsigned)list[e];
+                    const MuT av = series[s];
+                    const MuT vv = series[min(s + L32, n32)];
+                    const bool ok = vv == vv;
+                    const double d = (double)(ok ? vv : av) - (double)av;
+                    c += (int)ok;
+                    sd0 += d;
+                    sq0 = fma(d, d, sq0);
                 }
+                const double sd = sd0 + sd1, sd2 = sq0 + sq1;
+                if (b < nb && c > 0 && lane_on) {
+                    const int ai = b * nl + li;  // [bin][lag]: the lanes of a flush hit consecutive words
+                    atomicAdd(&acc_cnt[ai], (unsigned long long)c);
+                    atomicAdd(&acc_sd[ai], sd);
+                    atomicAdd(&acc_sd2[ai], sd2);
+                }
+                my_c += c;
+                my_sd2 += sd2;
             }
-#pragma unroll
-            for (int j = 0; j < LPL; ++j) {
-                if (lane_on[j] && my_c[j] > 0) {
-                    atomicAdd(&tot_c[li[j]], (unsigned long long)my_c[j]);
-                    atomicAdd(&tot_sd2[li[j]], my_sd2[j]);
-                }
+            if (lane_on && my_c > 0) {
+                atomicAdd(&tot_c[li], (unsigned long long)my_c);
+                atomicAdd(&tot_sd2[li], my_sd2);
             }
         }
         __syncthreads();
-        if (have && part == 0) {
-#pragma unroll
-            for (int j = 0; j < LPL; ++j) {
-                if (!lane_on[j]) continue;
-                const long long tc = (long long)tot_c[li[j]];
-                const double ts = tot_sd2[li[j]];
-                if (tc > 0) {
-                    // per-particle value: mean dmu^2 over its valid pairs (dmumu:528-537);
-                    // for the injection estimator tc == 1 and the value is dmu^2 (:625-631)
-                    const double value = ts / (double)tc;
-                    wc[j] += 1;
-                    const double delta = value - wm[j];
-                    wm[j] += delta / (double)wc[j];
-                    wm2[j] += delta * (value - wm[j]);
-                    pss[j] += ts;
-                    pn[j] += tc;
-                }
+        if (have && part == 0 && lane_on) {
+            const long long tc = (long long)tot_c[li];
+            const double ts = tot_sd2[li];
+            if (tc > 0) {
+                // per-particle value: mean dmu^2 over its valid pairs (dmumu:528-537);
+                // for the injection estimator tc == 1 and the value is dmu^2 (:625-631)
+                const double value = ts / (double)tc;
+                wc += 1;
+                const double delta = value - wm;
+                wm += delta / (double)wc;
+                wm2 += delta * (value - wm);
+                pss += ts;
+                pn += tc;
             }
         }
         __syncthreads();
@@ -474,18 +386,16 @@ __global__ void __launch_bounds__(dmumu_max_threads(LPL)) dmumu_kernel(DmumuLaun
     // reuse the accumulator region to gather per-warp Welford triples
     WelfordPart* wp = (WelfordPart*)(smem + (((size_t)(nb + 1) * sizeof(double) + 15) & ~(size_t)15));
     const int nwarps = blockDim.x / kWarp;
-#pragma unroll
-    for (int j = 0; j < LPL; ++j) wp[(warp * LPL + j) * kWarp + lane] = WelfordPart{wc[j], wm[j], wm2[j], pss[j], pn[j]};
+    wp[warp * kWarp + lane] = WelfordPart{wc, wm, wm2, pss, pn};
     __syncthreads();
     for (int l = threadIdx.x; l < nl; l += blockDim.x) {
-        const int hg = s_lag_pos[l] / kWarp, ln = s_lag_pos[l] % kWarp;
-        const int g = hg / LPL, j = hg % LPL;
+        const int g = s_lag_pos[l] / kWarp, ln = s_lag_pos[l] % kWarp;
         long long c = 0, n2 = 0;
         double m = 0.0, m2 = 0.0, ss = 0.0;
         for (int sl = 0; sl < a.ppc; ++sl) {
-            const int w = sl * wps + g * a.parts;  // the part-0 warp holds the slot's Welford triples
+            const int w = sl * wps + g * a.parts;  // the part-0 warp holds the slot's Welford triple
             if (w >= nwarps) break;
-            const WelfordPart q = wp[(w * LPL + j) * kWarp + ln];
+            const WelfordPart q = wp[w * kWarp + ln];
             welford_merge(c, m, m2, q.count, q.mean, q.m2);
             ss += q.pair_ss;
             n2 += q.pair_n;
@@ -755,33 +665,6 @@ size_t align16(size_t b) { return (b + 15) & ~(size_t)15; }
 // ------------------------------------------------------------------ host side
 namespace {
 
-// dmumu_kernel instance for the series source, start-index width, staging
-// place and lags per lane
-template <class Src, int LPL>
-void* dmumu_fn_lpl(bool small_idx, bool smem_slots)
-{
-    return small_idx ? (smem_slots ? (void*)dmumu_kernel<uint16_t, true, Src, LPL>
-                                   : (void*)dmumu_kernel<uint16_t, false, Src, LPL>)
-                     : (smem_slots ? (void*)dmumu_kernel<uint32_t, true, Src, LPL>
-                                   : (void*)dmumu_kernel<uint32_t, false, Src, LPL>);
-}
-
-template <class Src>
-void* dmumu_fn(int lpl, bool small_idx, bool smem_slots)
-{
-    return lpl == 2 ? dmumu_fn_lpl<Src, 2>(small_idx, smem_slots) : dmumu_fn_lpl<Src, 1>(small_idx, smem_slots);
-}
-
-// Lags each lane pairs with every start: 1 (two accumulator chains per lane)
-// or 2 (a start's load and FP64 conversion shared by two lags);
-// PTB200_DMUMU_LPL overrides the default.
-int dmumu_lags_per_lane()
-{
-    const char* e = getenv("PTB200_DMUMU_LPL");
-    if (e && (e[0] == '1' || e[0] == '2') && e[1] == 0) return e[0] - '0';
-    return kDmumuLagsPerLane;
-}
-
 // D_mumu over the series that `src` yields (a.mu, a.sp, a.ss are not used here)
 template <class Src>
 int run_dmumu_src(pt_ctx* ctx, const DmumuArgs& a, const Src& src, cudaStream_t s)
@@ -802,26 +685,27 @@ int run_dmumu_src(pt_ctx* ctx, const DmumuArgs& a, const Src& src, cudaStream_t 
     nl_cap = std::min(nl_cap, 32 * 8);
     const size_t slot_bytes = dmumu_slot_bytes(a.nsave, sizeof(MuT), idx_bytes, a.n_bins, nl_cap);
     const int lag_batches = (a.n_lags + nl_cap - 1) / nl_cap;
-    const int lpl = dmumu_lags_per_lane();
     for (int lb = 0; lb < lag_batches; ++lb) {
         const int lag0 = lb * nl_cap;
         const int nl = std::min(nl_cap, a.n_lags - lag0);
-        const int groups = (nl + kWarp * lpl - 1) / (kWarp * lpl);
+        const int groups = (nl + kWarp - 1) / kWarp;
         const size_t acc_bytes = (size_t)nl * a.n_bins * 24;
-        size_t fixed = edge_bytes + std::max(acc_bytes, sizeof(WelfordPart) * 1024 * lpl);
+        size_t fixed = edge_bytes + std::max(acc_bytes, sizeof(WelfordPart) * 1024);
         bool smem_slots = fixed + slot_bytes <= budget;
-        const int max_warps = dmumu_max_threads(lpl) / kWarp;
         int ppc;
-        if (smem_slots) ppc = (int)std::min<size_t>((budget - fixed) / slot_bytes, (size_t)(max_warps / groups));
-        else ppc = std::max(1, std::min(8, max_warps / groups));
+        if (smem_slots) ppc = (int)std::min<size_t>((budget - fixed) / slot_bytes, (size_t)(32 / groups));
+        else ppc = std::max(1, std::min(8, 32 / groups));
         ppc = std::max(1, ppc);
         // more warps share each staged series: split its bins over `parts` warps
-        const int parts = std::max(1, std::min(4, max_warps / (ppc * groups)));
+        const int parts = std::max(1, std::min(4, 32 / (ppc * groups)));
         const int threads = ppc * groups * parts * kWarp;
         size_t smem = fixed + (smem_slots ? (size_t)ppc * slot_bytes : 0);
         const int64_t tiles = (a.n + ppc - 1) / ppc;
         int per_sm = 1;
-        void* kfn = dmumu_fn<Src>(lpl, small_idx, smem_slots);
+        void* kfn = small_idx ? (smem_slots ? (void*)dmumu_kernel<uint16_t, true, Src>
+                                           : (void*)dmumu_kernel<uint16_t, false, Src>)
+                              : (smem_slots ? (void*)dmumu_kernel<uint32_t, true, Src>
+                                            : (void*)dmumu_kernel<uint32_t, false, Src>);
         PT_CUDA(cudaFuncSetAttribute(kfn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
         cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kfn, threads, smem);
         per_sm = std::max(1, per_sm);
@@ -838,15 +722,19 @@ int run_dmumu_src(pt_ctx* ctx, const DmumuArgs& a, const Src& src, cudaStream_t 
         L.n = a.n; L.nsave = a.nsave;
         L.start_cap = a.injection ? 1 : a.nsave;
         L.lags = a.lags + lag0; L.nl = nl; L.edges = a.edges; L.n_bins = a.n_bins; L.bin_abs = a.bin_abs;
-        L.ppc = ppc; L.groups = groups; L.lpl = lpl; L.parts = parts; L.slot_bytes = slot_bytes;
+        L.ppc = ppc; L.groups = groups; L.parts = parts; L.slot_bytes = slot_bytes;
         L.part_cnt = (unsigned long long*)base;
         L.part_sd = (double*)(base + align16(part_acc * 8));
         L.part_sd2 = (double*)(base + 2 * align16(part_acc * 8));
         L.part_w = (WelfordPart*)(base + 3 * align16(part_acc * 8));
         L.gslots = smem_slots ? nullptr : (char*)L.part_w + align16(sizeof(WelfordPart) * (size_t)grid * nl);
-        Src src_arg = src;
-        void* args[] = {&L, &src_arg};
-        PT_CUDA(cudaLaunchKernel(kfn, dim3(grid), dim3(threads), args, smem, s));
+        if (small_idx) {
+            if (smem_slots) dmumu_kernel<uint16_t, true, Src><<<grid, threads, smem, s>>>(L, src);
+            else dmumu_kernel<uint16_t, false, Src><<<grid, threads, smem, s>>>(L, src);
+        } else {
+            if (smem_slots) dmumu_kernel<uint32_t, true, Src><<<grid, threads, smem, s>>>(L, src);
+            else dmumu_kernel<uint32_t, false, Src><<<grid, threads, smem, s>>>(L, src);
+        }
         PT_CHECK_LAUNCH("dmumu_kernel");
         const int fin_threads = 256;
         const int fin_blocks = (int)((std::max(nl * a.n_bins, nl) + fin_threads - 1) / fin_threads);
@@ -1139,20 +1027,18 @@ int run_dmumu_noalloc(pt_ctx* ctx, const DmumuArgs& a, cudaStream_t s)
     nl_cap = std::min(nl_cap, 32 * 8);
     const size_t slot_bytes = dmumu_slot_bytes(a.nsave, sizeof(float), idx_bytes, a.n_bins, nl_cap);
     const CacheSource src{a.mu, a.sp, a.ss};
-    const int lpl = dmumu_lags_per_lane();
     for (int lag0 = 0; lag0 < a.n_lags; lag0 += nl_cap) {
         const int nl = std::min(nl_cap, a.n_lags - lag0);
-        const int groups = (nl + kWarp * lpl - 1) / (kWarp * lpl);
+        const int groups = (nl + kWarp - 1) / kWarp;
         const size_t acc_bytes = (size_t)nl * a.n_bins * 24;
-        const size_t fixed = edge_bytes + std::max(acc_bytes, sizeof(WelfordPart) * 1024 * lpl);
+        const size_t fixed = edge_bytes + std::max(acc_bytes, sizeof(WelfordPart) * 1024);
         if (fixed + slot_bytes > budget)
             return fail(PT_ERR_ARG, "pt_dmumu_accumulate_device_noalloc: nsave = " + std::to_string(a.nsave) +
                                         " is too long for on-chip staging with " + std::to_string(a.n_bins) +
                                         " bins; use pt_dmumu_accumulate_device");
-        const int max_warps = dmumu_max_threads(lpl) / kWarp;
-        int ppc = (int)std::min<size_t>((budget - fixed) / slot_bytes, (size_t)(max_warps / groups));
+        int ppc = (int)std::min<size_t>((budget - fixed) / slot_bytes, (size_t)(32 / groups));
         ppc = std::max(1, ppc);
-        const int parts = std::max(1, std::min(4, max_warps / (ppc * groups)));
+        const int parts = std::max(1, std::min(4, 32 / (ppc * groups)));
         const int threads = ppc * groups * parts * kWarp;
         const size_t smem = fixed + (size_t)ppc * slot_bytes;
         // per-CTA partials: counts, sum, sum^2 per (lag, bin) and a Welford triple per lag
@@ -1161,7 +1047,8 @@ int run_dmumu_noalloc(pt_ctx* ctx, const DmumuArgs& a, cudaStream_t s)
         if (cap_grid < 1)
             return fail(PT_ERR_ARG, "pt_dmumu_accumulate_device_noalloc: n_lags x n_bins too large for the " +
                                         std::to_string(kDmumuNoAllocBytes >> 20) + " MiB fixed scratch");
-        void* kfn = dmumu_fn<CacheSource>(lpl, small_idx, true);
+        void* kfn = small_idx ? (void*)dmumu_kernel<uint16_t, true, CacheSource>
+                              : (void*)dmumu_kernel<uint32_t, true, CacheSource>;
         PT_CUDA(cudaFuncSetAttribute(kfn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
         int per_sm = 1;
         cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kfn, threads, smem);
@@ -1175,7 +1062,7 @@ int run_dmumu_noalloc(pt_ctx* ctx, const DmumuArgs& a, cudaStream_t s)
         L.n = a.n; L.nsave = a.nsave;
         L.start_cap = a.injection ? 1 : a.nsave;
         L.lags = a.lags + lag0; L.nl = nl; L.edges = a.edges; L.n_bins = a.n_bins; L.bin_abs = a.bin_abs;
-        L.ppc = ppc; L.groups = groups; L.lpl = lpl; L.parts = parts; L.slot_bytes = slot_bytes;
+        L.ppc = ppc; L.groups = groups; L.parts = parts; L.slot_bytes = slot_bytes;
         L.part_cnt = (unsigned long long*)base;
         L.part_sd = (double*)(base + align16(part_acc * 8));
         L.part_sd2 = (double*)(base + 2 * align16(part_acc * 8));
@@ -1183,9 +1070,8 @@ int run_dmumu_noalloc(pt_ctx* ctx, const DmumuArgs& a, cudaStream_t s)
         L.gslots = nullptr;
         if (3 * align16(part_acc * 8) + sizeof(WelfordPart) * (size_t)grid * nl > kDmumuNoAllocBytes)
             return fail(PT_ERR_ARG, "internal: no-alloc scratch overflow");
-        CacheSource src_arg = src;
-        void* args[] = {&L, &src_arg};
-        PT_CUDA(cudaLaunchKernel(kfn, dim3(grid), dim3(threads), args, smem, s));
+        if (small_idx) dmumu_kernel<uint16_t, true, CacheSource><<<grid, threads, smem, s>>>(L, src);
+        else dmumu_kernel<uint32_t, true, CacheSource><<<grid, threads, smem, s>>>(L, src);
         PT_CHECK_LAUNCH("dmumu_kernel (no-alloc)");
         const int fin_blocks = (int)((std::max(nl * a.n_bins, nl) + 255) / 256);
         dmumu_finalize_kernel<<<fin_blocks, 256, 0, s>>>(L.part_cnt, L.part_sd, L.part_sd2, L.part_w, grid, nl,

@@ -87,8 +87,46 @@ def _wavenumbers(n: int, torch, device):
     return kx, ky, kz
 
 
+# c_s^2 / v_A^2 of the finite-beta mode decomposition of the synthetic variants
+MODE_ALPHA = 1.0
+
+
+def _mode_basis(kx, ky, kz, alpha, torch):
+    """Unit vectors per wave vector (B0 along z; k_perp > 0):
+    e_A = k x z / |k x z| (Alfven), e_P = k^ x e_A (the second polarisation
+    perpendicular to k, in the k-z plane), and the fast and slow MHD
+    displacement directions of Cho & Lazarian (2003, MNRAS 345, 325, eq. 5-6)
+    for alpha = c_s^2 / v_A^2:
+        xi_f ~ (-1 + alpha + sqrt(D)) k_par z^ + (1 + alpha + sqrt(D)) k_perp k_perp^,
+        D = (1 + alpha)^2 - 4 alpha cos^2(theta),
+    and xi_s, the direction orthogonal to it in the (k_perp^, z) plane
+    (their eq. 6 with the minus sign); with e_A they form an orthonormal basis.  Returns (e_A, e_P, xi_f, xi_s)
+    as tuples of three tensors, and each mode's magnetic response
+    |xi . k_perp^| (the field a displacement xi bends: k x (xi x z) has
+    magnitude k |xi . k_perp^|)."""
+    kp = torch.sqrt(kx * kx + ky * ky).clamp_min(1e-30)
+    kk = torch.sqrt(kx * kx + ky * ky + kz * kz).clamp_min(1e-30)
+    cos, sin = kz / kk, kp / kk
+    zero, one = torch.zeros_like(kx), torch.ones_like(kx)
+    e_a = (ky / kp, -kx / kp, zero)
+    kph = (kx / kp, ky / kp, zero)
+    e_p = (cos * kph[0], cos * kph[1], -sin)
+    sq = torch.sqrt(((1 + alpha) ** 2 - 4 * alpha * cos * cos).clamp_min(0.0))
+    f_par = (-1 + alpha + sq) * cos
+    f_perp = (1 + alpha + sq) * sin  # > 0 whenever k_perp > 0
+    nrm = torch.sqrt(f_par * f_par + f_perp * f_perp).clamp_min(1e-30)
+    f_par, f_perp = f_par / nrm, f_perp / nrm
+    # xi_s is xi_f turned by 90 degrees in the (k_perp^, z) plane: the same
+    # direction as the formula's slow vector, which vanishes (0/0) at
+    # perpendicular propagation, where its limit is z
+    s_par, s_perp = f_perp, -f_par
+    xi_f = (f_perp * kph[0], f_perp * kph[1], f_par * one)
+    xi_s = (s_perp * kph[0], s_perp * kph[1], s_par * one)
+    return e_a, e_p, xi_f, xi_s, f_perp.abs(), s_perp.abs()
+
+
 def solenoidal_field(n: int, kmin: float, kmax: float, rms: float, seed: int, spectrum: str = "isotropic",
-                     device="cpu", modes: str = "total"):
+                     device="cpu", modes: str = "total", kind: str = "magnetic"):
     """Seeded divergence-free Gaussian random vector field on an n^3 grid.
 
     spectrum "isotropic": |A(k)|^2 ~ |k|^(-11/3) for kmin <= |k| <= kmax
@@ -96,8 +134,22 @@ def solenoidal_field(n: int, kmin: float, kmax: float, rms: float, seed: int, sp
     spectrum "gs": Goldreich-Sridhar-like anisotropy about z: |A|^2 ~
     k_perp^(-10/3) for kmin <= k_perp <= kmax and |k_par| <= k_perp^(2/3) kmin^(1/3)
     (E(k_perp) ~ k_perp^(-5/3)).
-    modes: "total", or the per-k projection "alfven" (e_A = k x z / |k x z|),
-    "fast" (k_perp / |k_perp|) or "slow" (z) of the total field.
+    modes: "total", or one MHD mode family of the total field, with B0
+    along z (the reference reads such variants from an MHD mode
+    decomposition; these are their synthetic stand-ins):
+      - "alfven": the projection on e_A = k x z / |k x z|, for either kind;
+      - kind "velocity": the projection on the fast or slow displacement
+        direction xi_f, xi_s of a finite-beta plasma (c_s^2 / v_A^2 =
+        MODE_ALPHA); e_A, xi_f, xi_s are orthonormal, so the three variants
+        add up to the total velocity field, and fast / slow carry the
+        compressive parts;
+      - kind "magnetic": the component along e_P, the polarisation
+        perpendicular to k in the k-z plane (divergence-free), split between
+        fast and slow by their magnetic responses |xi . k_perp^| (power
+        preserving: |dB_f|^2 + |dB_s|^2 = |dB . e_P|^2).
+    Wave vectors along z (k_perp = 0) go to the Alfven variant.  Every
+    variant then bends the field lines and has a motional electric field
+    E = -u x B.
     Returns three float64 torch tensors of shape (n, n, n) (z, y, x) scaled to
     sqrt(<|A|^2>) = rms over the grid (before any mode projection).
     """
@@ -134,21 +186,26 @@ def solenoidal_field(n: int, kmin: float, kmax: float, rms: float, seed: int, sp
     fields = [torch.fft.irfftn(c, s=(n, n, n)) for c in (ax, ay, az)]
     scale = rms / math.sqrt(float(sum((f * f).mean() for f in fields)))
     if modes != "total":
-        spec = [torch.fft.rfftn(f) for f in fields]
-        kp = kperp.clamp_min(1e-30)
-        zero = torch.zeros_like(spec[0])
-        if modes == "alfven":
-            e = (ky / kp, -kx / kp, torch.zeros_like(kx))
-            along_z = (spec[0], spec[1], zero)
-        elif modes == "fast":
-            e = (kx / kp, ky / kp, torch.zeros_like(kx))
-            along_z = (zero, zero, zero)
-        elif modes == "slow":
-            e = (torch.zeros_like(kx), torch.zeros_like(kx), torch.ones_like(kx))
-            along_z = (zero, zero, spec[2])
-        else:
+        if modes not in ("alfven", "fast", "slow"):
             raise ValueError("modes must be total, alfven, fast or slow")
-        dot = e[0] * spec[0] + e[1] * spec[1] + e[2] * spec[2]
+        if kind not in ("magnetic", "velocity"):
+            raise ValueError("kind must be magnetic or velocity")
+        spec = [torch.fft.rfftn(f) for f in fields]
+        zero = torch.zeros_like(spec[0])
+        e_a, e_p, xi_f, xi_s, bf, bs = _mode_basis(kx, ky, kz, MODE_ALPHA, torch)
+        weight = torch.ones_like(kx)
+        if modes == "alfven":
+            e = e_a
+            along_z = (spec[0], spec[1], spec[2])
+        else:
+            along_z = (zero, zero, zero)
+            if kind == "velocity":
+                e = xi_f if modes == "fast" else xi_s
+            else:
+                e = e_p
+                b = bf if modes == "fast" else bs
+                weight = b / torch.sqrt(bf * bf + bs * bs).clamp_min(1e-30)
+        dot = (e[0] * spec[0] + e[1] * spec[1] + e[2] * spec[2]) * weight
         par = kperp < 1e-12  # k along z: no k x z direction
         proj = [torch.where(par, az_, dot * ei) for az_, ei in zip(along_z, e)]
         fields = [torch.fft.irfftn(c, s=(n, n, n)) for c in proj]
@@ -163,10 +220,11 @@ def synthetic_mhd_fields(n: int, kmin: float, kmax: float, dB_over_B0: float, B0
     u_rms_over_c * c (zero when u_rms_over_c == 0)."""
     import torch
 
-    dB = solenoidal_field(n, kmin, kmax, dB_over_B0 * B0_uG, seed, spectrum, device, modes)
+    dB = solenoidal_field(n, kmin, kmax, dB_over_B0 * B0_uG, seed, spectrum, device, modes, kind="magnetic")
     dB[2] = dB[2] + B0_uG
     if u_rms_over_c > 0:
-        u = solenoidal_field(n, kmin, kmax, u_rms_over_c * C_LIGHT / KMPS_TO_MPS, seed + 7919, spectrum, device, modes)
+        u = solenoidal_field(n, kmin, kmax, u_rms_over_c * C_LIGHT / KMPS_TO_MPS, seed + 7919, spectrum, device, modes,
+                             kind="velocity")
     else:
         u = [torch.zeros((n, n, n), dtype=torch.float64, device=device) for _ in range(3)]
     return dB + u

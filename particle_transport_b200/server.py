@@ -126,6 +126,7 @@ class CampaignServer:
         self.binning = {}    # job_id -> record (lag pairs running on the side stream)
         self.results = []
         self.used = 0.0
+        self.reserve_bytes = float(2 << 30)  # kept free for the kernels' scratch and torch's workspaces
         self.next_id = 0
         self.epochs = 0
         self.admit_s = 0.0   # host seconds spent admitting jobs
@@ -178,12 +179,23 @@ class CampaignServer:
         finally:
             self.admit_s += time.perf_counter() - t0
 
+    def device_room(self) -> float:
+        """Bytes a new job can still take on the device: free memory plus
+        what torch holds cached but unused, less a reserve for workspaces.
+        The HBM budget counts the jobs only; the field libraries, the slot
+        arena and the scratch of the kernels live beside them, so admission
+        checks both."""
+        torch = self.torch
+        free, _ = torch.cuda.mem_get_info(self.device)
+        cached = torch.cuda.memory_reserved(self.device) - torch.cuda.memory_allocated(self.device)
+        return float(free + cached) - self.reserve_bytes
+
     def _admit_waiting(self) -> int:
         n = 0
         keep = []
         for jid, spec, arrival in self.queue:
             need = self.job_bytes(spec)
-            if not keep and self.used + need <= self.budget:
+            if not keep and self.used + need <= self.budget and need <= self.device_room():
                 try:
                     self._admit(jid, spec, arrival)
                     n += 1
@@ -191,6 +203,8 @@ class CampaignServer:
                 except _lib.PtError as e:  # no slot range free yet
                     if e.code not in (-3, -6):
                         raise
+                except self.torch.OutOfMemoryError:  # the device is fuller than it looked: wait for a job to end
+                    self.torch.cuda.empty_cache()
             keep.append((jid, spec, arrival))
         self.queue = keep
         return n

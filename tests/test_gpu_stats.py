@@ -67,19 +67,6 @@ def test_dmumu_matches_oracle(cuda, oracle, n, nsave, n_lags, n_bins, bin_abs, n
     check_dmumu(g, o)
 
 
-@pytest.mark.parametrize("n,nsave,n_lags,n_bins,bin_abs,nan_frac,mode", CASES)
-def test_dmumu_two_lags_per_lane_matches_oracle(cuda, oracle, monkeypatch, n, nsave, n_lags, n_bins, bin_abs,
-                                                nan_frac, mode):
-    """The pair loop with two lags per lane (PTB200_DMUMU_LPL=2) against the oracle."""
-    monkeypatch.setenv("PTB200_DMUMU_LPL", "2")
-    mu = random_mu_cache(n, nsave, seed=n + nsave, nan_frac=nan_frac)
-    lags = log_spaced_lag_steps(nsave - 1, n_lags) if n_lags < nsave else np.arange(1, n_lags + 1)
-    edges, _ = build_mu_edges_full(0.0, 1.0, n_bins, bin_abs=bin_abs)
-    o = zero_dmumu(len(lags), n_bins)
-    oracle.dmumu_accumulate(mu, lags, edges, o, injection=mode == "injection", bin_abs=bin_abs)
-    check_dmumu(gpu_dmumu(mu, lags, edges, start_mode=mode, bin_abs=bin_abs), o)
-
-
 @pytest.mark.parametrize("bin_abs", [True, False])
 def test_dmumu_non_uniform_edges(cuda, oracle, bin_abs):
     """Edges that are not a uniform range (the bin lookup starts from a

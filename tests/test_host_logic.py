@@ -61,9 +61,11 @@ def test_tune_batch_selection_and_cache(tmp_path, monkeypatch):
         assert t2[k] == t[k], k
 
 
-def admission_server(budget):
+def admission_server(budget, room=float("inf")):
     srv = CampaignServer.__new__(CampaignServer)
     srv.budget = budget
+    srv.room = room
+    srv.device_room = lambda: srv.room - srv.used
     srv.used = 0.0
     srv.queue = []
     srv.active = {}
@@ -144,3 +146,17 @@ def test_dmumu_noalloc_limits_and_job_bytes():
     # the long job holds 8x the mu and D_pp momentum caches of the short one and is charged the scratch bound
     cache_diff = (4.0 * long.n_particles + 12.0 * long.dpp_particles) * (nsave + 1 - 4001)
     assert CampaignServer.job_bytes(long) - CampaignServer.job_bytes(short) == cache_diff + extra
+
+
+def test_admission_also_needs_room_on_the_device():
+    """The budget counts the jobs; the device also holds the libraries, the
+    arena and scratch.  A job the budget admits waits while the device has
+    no room for it, then goes in once a job ends."""
+    small = JobSpec("256", "total", 1.0, 10_000, 10.0)
+    big = JobSpec("256", "total", 1.0, 4_000_000, 300.0)
+    s_b, b_b = CampaignServer.job_bytes(small), CampaignServer.job_bytes(big)
+    srv, admitted = admission_server(budget=10 * b_b, room=b_b + 0.5 * s_b)
+    srv.queue = [(0, big, 0.0), (1, small, 0.0), (2, small, 0.0)]
+    assert srv.admit() == 1 and admitted == [0]  # the budget has room; the device does not
+    srv.used -= b_b  # the big job ends
+    assert srv.admit() == 2 and admitted == [0, 1, 2]
