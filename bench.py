@@ -380,7 +380,7 @@ def run_ours(args, ws, rank, local):
     alive = np.ones(n, np.uint8)
     ens = R.FastEnsemble(fb, state, alive)
     # the 8 mu saves of a 64-step launch land in a time-fastest cache [n][8]:
-    # each particle's saves leave as one 32-byte store (cache_pitch = 8)
+    # each particle's saves side by side (cache_pitch = 8), merged by L2 into whole sectors
     ring = torch.empty((n, 8), dtype=torch.float32, device=dev)
     # the sort cadence is driven here (same rule as pt_push_advance_fast's
     # sort_every) so that events can bracket the push launch alone
@@ -856,7 +856,7 @@ def run_batched(args, dev, rank):
     for c, se in zip(camps, tune["sort_every"]):
         nsave = (c["nsteps"] - 1) // c["stride"] + 1
         c["nsave"] = nsave
-        # time-fastest caches [n][pitch]: a particle's saves leave in 32-byte stores
+        # time-fastest caches [n][pitch]: a particle's saves side by side reach DRAM as whole sectors
         caches.append(torch.empty((len(c["state"]["x1"]), (nsave + 7) // 8 * 8), dtype=torch.float32, device=dev))
         c["id"] = b.add(c["field"], c["state"], c["dt"], c["nsteps"], c["stride"], cache=caches[-1], sort_every=se,
                         time_fastest=True)
@@ -906,9 +906,11 @@ def run_precision_key(args, dev):
     50 T_g0, mu every 8 steps (801 saves), 32 log lags x 20 |mu| bins, D_pp
     over 131,072 particles.  For each form (FP32 push over FP32 bricks and
     over BF16 bricks) and the FP64 floors (positions moved by one FP64 ulp,
-    and by one FP32 ulp of the box): the largest relative error of
-    D_mumu(mu, tau) (cells with >= 100 pairs), <dmu^2>(tau) and D_pp(tau)
-    over every variant and energy, and the energy drift with E = 0."""
+    by one FP32 ulp of the box, and an independent sample): the largest
+    relative error of D_mumu(mu, tau) (cells with >= 100 pairs), <dmu^2>(tau)
+    and D_pp(tau) over every variant and energy, over all cells and over the
+    cells both FP64 floors reproduce within 0.5 %, and the energy drift with
+    E = 0."""
     import torch
 
     from particle_transport_b200 import fields as F
@@ -917,9 +919,11 @@ def run_precision_key(args, dev):
     n, npart = 128, args.precision_key_particles
     grid = F.build_uniform_grid((n - 1) * F.gyroradius_m(1.0, 1e-10), n, n, n)
     t0 = time.perf_counter()
-    forms = ("f64_1ulp", "f64_f32ulp", "f32", "bf16")
-    prods = ("D_mumu", "delta_mu2", "D_pp")
+    forms = ("f64_1ulp", "f64_f32ulp", "f64_resample", "f32", "bf16")
+    prods = P.PRODUCTS
     worst = {f: {k: 0.0 for k in prods} for f in forms}
+    worst_resolved = {f: {k: 0.0 for k in prods} for f in ("f32", "bf16")}
+    failures = {}
     drift = {"f64": 0.0, "f32": 0.0, "bf16": 0.0}
     cases = {}
     ok = True
@@ -929,22 +933,29 @@ def run_precision_key(args, dev):
         del fs
         for E in (1.0, 10.0, 100.0):
             r = P.compare_forms(libs, B0, grid, E, npart, gyroperiods=50)
-            cases[f"{mode}/{E:g}GeV"] = {f: {k: r[f][k]["max"] for k in prods} for f in forms}
-            ok &= all(r[f][k]["max"] <= max(0.01, 2.0 * r["f64_f32ulp"][k]["max"]) for f in ("f32", "bf16")
-                      for k in prods)
+            case = f"{mode}/{E:g}GeV"
+            cases[case] = {f: {k: r[f][k]["max"] for k in prods} for f in forms}
+            cases[case]["resolved"] = {f: {k: r[f][k].get("max_resolved") for k in prods} for f in ("f32", "bf16")}
+            bad = P.check_forms(r, ("f32", "bf16"), 0.01)
+            if bad:
+                failures[case] = [list(map(str, b)) for b in bad]
+            ok &= not bad
             for f in forms:
                 for k in worst[f]:
                     worst[f][k] = max(worst[f][k], r[f][k]["max"])
+            for f in worst_resolved:
+                for k in prods:
+                    worst_resolved[f][k] = max(worst_resolved[f][k], r[f][k].get("max_resolved", 0.0))
             for f in drift:
                 drift[f] = max(drift[f], r[f]["gamma_drift_E0"])
         for lib in libs.values():
             lib.close()
         torch.cuda.empty_cache()
-    return {"max_rel_err": worst, "tolerance": 0.01,
-            "within_tolerance": ok,
-            "criterion": "each product of each case within 1 % of the FP64 push, or within twice the change the "
-                         "FP64 push itself shows under a one-FP32-ulp position perturbation (f64_f32ulp) where that "
-                         "exceeds 0.5 %",
+    return {"max_rel_err": worst, "max_rel_err_resolved": worst_resolved, "tolerance": 0.01,
+            "within_tolerance": ok, "failures": failures,
+            "criterion": "per cell against the FP64 push: every cell that both FP64 floors (one FP32 ulp of the box, "
+                         "an independent sample) reproduce within 0.5 % is within 1 %; every other cell within 1 %, or "
+                         "within twice the larger floor where the statistic itself moves by more",
             "gamma_drift_E0_max": drift, "per_case": cases, "seconds": time.perf_counter() - t0,
             "setup": f"128^3, dB/B0=0.5, k=2..64, u_rms=1e-4 c; total/alfven/fast/slow x 1/10/100 GeV; {npart} "
                      "protons, fixed mu0=0.5, 128 steps/T_g0, 50 T_g0, mu every 8 steps; 32 lags x 20 |mu| bins "

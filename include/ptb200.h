@@ -100,9 +100,11 @@ typedef struct {
                                  reference's on-disk layout); > 0 = time-fastest, at
                                  p * cache_pitch + (r - cache_row_base) (the Julia mu_chunk
                                  layout, sp = cache_pitch, ss = 1 for pt_dmumu_accumulate*),
-                                 cache_pitch >= cache_rows.  A particle's saves of one call then
-                                 leave as whole 32-byte stores (32-byte aligned d_cache) instead of
-                                 one scattered 4-byte store per save.  Must be 0 elsewhere.    */
+                                 cache_pitch >= cache_rows.  The saves of a particle then sit side
+                                 by side and are written by one thread within microseconds, so L2
+                                 merges them into whole 32-byte DRAM sectors, where rows (the
+                                 particles in brick order) cost a sector per 4-byte save.  Must
+                                 be 0 elsewhere.                                                */
 } pt_push_params;
 
 /* Save sink for pt_push_run: called on the calling thread once per save row,

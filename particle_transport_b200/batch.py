@@ -62,7 +62,7 @@ class Batch:
         """Add a campaign; state: SI arrays x1..p3 (numpy or CUDA tensors);
         cache: CUDA float tensor for the mu cache (or None), [rows][n] (the
         reference's row layout) or, with time_fastest, [n][rows] (each
-        particle's saves contiguous: one 32-byte store per 8 saves);
+        particle's saves contiguous, so they reach DRAM as whole sectors);
         mom_cache: CUDA float32 tensor [rows][3][n_mom] that receives the
         momenta of particles 0 .. n_mom-1 at every save (needs cache);
         sort_every: re-sort the campaign by brick before every sort_every-th

@@ -346,7 +346,6 @@ static int advance_fast(pt_ctx* ctx, const pt_field* f, pt_fast_state* st, const
 {
     PushArgsFast a = fast_args(f, st, p);
     a.cache = cache; a.row_base = row_base; a.rows = rows; a.deaths = deaths;
-    a.pitch_vec = ((uintptr_t)cache & 31) == 0;
     const int64_t K = p->steps_per_launch > 0 ? p->steps_per_launch : count;
     int64_t s = s0;
     const int64_t end = s0 + count;

@@ -357,7 +357,6 @@ int pt_batch_add(pt_ctx* ctx, pt_batch* b, const pt_campaign_desc* d, int* id)
     a.mom_cache = d->d_mom_cache;
     a.n_mom = d->d_mom_cache ? d->n_mom : 0;
     a.pitch = d->d_cache ? d->cache_pitch : 0;
-    a.pitch_vec = ((uintptr_t)d->d_cache & 31) == 0;
     C.slot0 = slot0;
     C.n = d->n;
     C.step = 0;

@@ -252,8 +252,6 @@ struct PushArgsFast {
     float* mom_cache;      // with a mu cache: momenta rows [rows][3][n_mom] of particles pid < n_mom, or null
     int64_t n_mom;
     int64_t pitch;         // mu cache: 0 = rows [r][n_cache]; > 0 = time-fastest, element r of pid at pid * pitch + r
-    int pitch_vec;         // time-fastest Float32 cache 32-byte aligned: aligned runs of 8 saves leave as one store
-    int pad0_;
 };
 int launch_push_fast(const PushArgsFast& a, cudaStream_t s);
 

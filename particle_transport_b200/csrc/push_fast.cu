@@ -144,59 +144,6 @@ __device__ __forceinline__ double wrap_cells(double x, double w)
     return x;
 }
 
-// 32-byte store (sm_100 256-bit vector store; the address is 32-byte aligned)
-__device__ __forceinline__ void stg256(float* p, const float v[8])
-{
-    asm volatile("st.global.v8.f32 [%0], {%1, %2, %3, %4, %5, %6, %7, %8};"
-                 :: "l"(p), "f"(v[0]), "f"(v[1]), "f"(v[2]), "f"(v[3]), "f"(v[4]), "f"(v[5]), "f"(v[6]), "f"(v[7])
-                 : "memory");
-}
-
-// Saves of one particle bound for a time-fastest mu cache (element q of
-// particle pid at pid * pitch + q).  Consecutive saves collect in registers
-// (v[8 - n .. 7], oldest first, the newest at element e_last) and leave when
-// an aligned group of 8 elements is complete, when the run breaks, or at the
-// end of the launch: a full aligned group is one 32-byte store, so the saves
-// of a particle fill whole DRAM sectors whatever the order of the slots.
-struct MuRun {
-    float v[8];
-    int n;
-    int64_t e_last;
-};
-
-__device__ __forceinline__ void mu_run_flush(MuRun& m, const PushArgsFast& a)
-{
-    if (m.n == 0) return;
-    const int64_t e0 = m.e_last - 7;  // element of v[0]
-    if (a.cache_f64) {
-        double* C = (double*)a.cache;
-#pragma unroll
-        for (int j = 0; j < 8; ++j)
-            if (j >= 8 - m.n) C[e0 + j] = (double)m.v[j];
-    } else {
-        float* C = (float*)a.cache;
-        if (m.n == 8 && a.pitch_vec) {
-            stg256(C + e0, m.v);
-        } else {
-#pragma unroll
-            for (int j = 0; j < 8; ++j)
-                if (j >= 8 - m.n) C[e0 + j] = m.v[j];
-        }
-    }
-    m.n = 0;
-}
-
-__device__ __forceinline__ void mu_run_push(MuRun& m, float mu, int64_t e, const PushArgsFast& a)
-{
-    if (m.n > 0 && e != m.e_last + 1) mu_run_flush(m, a);
-#pragma unroll
-    for (int j = 0; j < 7; ++j) m.v[j] = m.v[j + 1];
-    m.v[7] = mu;
-    m.n += 1;
-    m.e_last = e;
-    if ((e & 7) == 7) mu_run_flush(m, a);  // an aligned group ends here (n == 8: the whole group)
-}
-
 // K steps of one particle held in registers.  State is (x, y, z) in cells
 // (FP64), p/(mc) (FP32) and |p/(mc)|^2 (FP64); pid indexes the cache row.
 // Cache rows of a.n_cache particles: row r at (r - a.row_base) or, with
@@ -210,9 +157,6 @@ __device__ __forceinline__ void advance_particle(double& x, double& y, double& z
     const int nx = (int)a.fld.nx, ny = (int)a.fld.ny, nz = (int)a.fld.nz;
     const float hB = a.hB;
     const int64_t n = a.n_cache;
-    MuRun run;
-    run.n = 0;
-    run.e_last = -2;
     {
         int64_t next_save = ((s_begin + a.stride - 1) / a.stride) * a.stride;
         for (int64_t s = s_begin; s < s_end; ++s) {
@@ -236,9 +180,13 @@ __device__ __forceinline__ void advance_particle(double& x, double& y, double& z
                     float mu = NAN;
                     if (al && x >= 0.0 && x <= a.wx && y >= 0.0 && y <= a.wy && z >= 0.0 && z <= a.wz)
                         mu = mu_f32(px, py, pz, f[0], f[1], f[2]);
-                    if (a.pitch > 0) mu_run_push(run, mu, pid * a.pitch + r, a);
-                    else if (a.cache_f64) ((double*)a.cache)[r * n + pid] = (double)mu;
-                    else ((float*)a.cache)[r * n + pid] = mu;
+                    // rows: save r of every particle in one row; time-fastest
+                    // (pitch > 0): a particle's saves side by side, so the 8
+                    // saves of a launch, written by this thread within a few
+                    // microseconds, merge in L2 into one whole DRAM sector
+                    const int64_t at = a.pitch > 0 ? pid * a.pitch + r : r * n + pid;
+                    if (a.cache_f64) ((double*)a.cache)[at] = (double)mu;
+                    else ((float*)a.cache)[at] = mu;
                     if (pid < a.n_mom) {
                         // momenta of the D_pp subset, as the phase-space writer stores them
                         const double pm = sqrt(P2) / sqrt((double)px * px + (double)py * py + (double)pz * pz) *
@@ -307,7 +255,6 @@ __device__ __forceinline__ void advance_particle(double& x, double& y, double& z
             }
         }
     }
-    mu_run_flush(run, a);
 }
 
 template <int LAYOUT, int BLOCK, int MINB, int TEXC = 0>

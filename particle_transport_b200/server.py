@@ -158,7 +158,7 @@ class CampaignServer:
         st = init_particles_device(fl, spec.n_particles, spec.energy_GeV, seed=spec.seed,
                                    injection_mode=spec.injection, mu0=spec.mu0)
         # the FP32 push writes a time-fastest mu cache [n][pitch] (a particle's
-        # saves leave in 32-byte stores and the binning stages each series
+        # saves sit side by side and reach DRAM as whole sectors, and the binning stages each series
         # with coalesced reads); the FP64 push writes rows [nsave][n]
         pitch = (nsave + 7) // 8 * 8 if self.push == "f32" else 0
         shape = (spec.n_particles, pitch) if pitch else (nsave, spec.n_particles)

@@ -10,14 +10,17 @@ every 8 steps (801 saves), 32 log lags x 20 |mu| bins, D_pp over the first
 
 For the FP32 push over FP32 bricks and over BF16 bricks, D_mumu(mu, tau)
 over the cells holding at least MIN_COUNT pairs, <dmu^2>(tau) and D_pp(tau)
-must each be within 1 % (relative, every cell) of the FP64 push from the
-same initial state -- or, where the statistic itself is not converged at
-1 %, within twice the floor: the largest change the FP64 push shows when
-its positions move by one FP32 ulp of the box, a perturbation the size of
-the FP32 push's own rounding.  In the compressive ("slow") field a few
-particles cross a mirror separatrix and carry most of <dmu^2>, so any
-perturbation of that size moves the sums by several per cent.  On the same
-field with u = 0 (E = 0) every form conserves gamma to rounding."""
+are compared cell by cell with the FP64 push from the same initial state.
+Two FP64 floors say which cells FP64 itself resolves: the same push with
+positions moved by one FP32 ulp of the box (a perturbation the size of the
+FP32 push's own rounding) and the same push from an independent sample.
+Every cell both floors reproduce within 0.5 % must be within 1 % in each
+form; every other cell within 1 %, or within twice the larger floor where
+the statistic itself moves by more (in the compressive "slow" field at
+100 GeV a few particles cross a mirror separatrix and carry most of
+<dmu^2>, so any perturbation of that size moves the sums by tens of per
+cent).  On the same field with u = 0 (E = 0) every form conserves gamma to
+rounding."""
 import math
 
 import pytest
@@ -56,12 +59,9 @@ def test_precision_forms_within_one_percent(cuda, mode, energy):
     libs, B0, grid = libraries(mode)
     r = P.compare_forms(libs, B0, grid, energy, N_PARTICLES, gyroperiods=GYROPERIODS, min_count=MIN_COUNT)
     assert r["cells_counted"] >= 0.8 * r["lags"] * r["mu_bins"], r["cells_counted"]
-    for product in ("D_mumu", "delta_mu2", "D_pp"):
-        floor = r["f64_f32ulp"][product]["max"]
-        for form in ("f32", "bf16"):
-            e = r[form][product]
-            assert e["cells"] > 0, (form, product)
-            assert e["max"] <= max(TOL, 2.0 * floor), (mode, energy, form, product, e, floor)
+    assert r["f32"]["D_mumu"]["resolved_cells"] >= 0.25 * r["cells_counted"], r["f32"]["D_mumu"]
+    failures = P.check_forms(r, ("f32", "bf16"), TOL)
+    assert not failures, (mode, energy, failures)
     # E = 0: energy conserved to rounding (FP32 forms carry |p|^2 in FP64 and change it only in the E kicks)
     assert r["f64"]["gamma_drift_E0"] < 1e-12, r["f64"]
     for form in ("f32", "bf16"):
