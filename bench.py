@@ -733,7 +733,7 @@ def issue_roofline(kernel: str, pairs_per_s: float, clocks, device) -> dict:
 # DRAM bytes (dram__bytes_read.sum + dram__bytes_write.sum) of one 64-step
 # push_fast_kernel launch of this workload, from a 1-pass ncu capture of the
 # same command; keyed by (storage, grid, particles)
-TRAFFIC = {("brick_bf16", 512, 16_777_216): 12.89e9 + 5.02e9}
+TRAFFIC = {("brick_bf16", 512, 16_777_216): 6.63e9 + 1.44e9}
 
 
 def run_config1(args, rank):
@@ -902,15 +902,16 @@ def run_precision_key(args, dev):
     """The precision forms against the FP64 push, reduced from the
     plain-vs-precision configuration: 128^3 (dB/B0 = 0.5 on |k| = 2..64,
     u_rms = 1e-4 c), the total field and its alfven / fast / slow projections,
-    protons at 1, 10 and 100 GeV with fixed mu0 = 0.5, 128 steps per T_g0 for
+    protons at 1, 10 and 100 GeV with fixed mu0 = 0.525, 128 steps per T_g0 for
     50 T_g0, mu every 8 steps (801 saves), 32 log lags x 20 |mu| bins, D_pp
     over 131,072 particles.  For each form (FP32 push over FP32 bricks and
     over BF16 bricks) and the FP64 floors (positions moved by one FP64 ulp,
     by one FP32 ulp of the box, and an independent sample): the largest
     relative error of D_mumu(mu, tau) (cells with >= 100 pairs), <dmu^2>(tau)
     and D_pp(tau) over every variant and energy, over all cells and over the
-    cells both FP64 floors reproduce within 0.5 %, and the energy drift with
-    E = 0."""
+    cells the particle count resolves to 1 % (FP64 standard error by batch
+    means), the largest error in FP64 standard errors, and the energy drift
+    with E = 0."""
     import torch
 
     from particle_transport_b200 import fields as F
@@ -936,7 +937,8 @@ def run_precision_key(args, dev):
             case = f"{mode}/{E:g}GeV"
             cases[case] = {f: {k: r[f][k]["max"] for k in prods} for f in forms}
             cases[case]["resolved"] = {f: {k: r[f][k].get("max_resolved") for k in prods} for f in ("f32", "bf16")}
-            bad = P.check_forms(r, ("f32", "bf16"), 0.01)
+            cases[case]["max_z"] = {f: {k: r[f][k].get("max_z") for k in prods} for f in forms}
+            bad = P.check_forms(r, ("f32", "bf16"))
             if bad:
                 failures[case] = [list(map(str, b)) for b in bad]
             ok &= not bad
@@ -953,12 +955,12 @@ def run_precision_key(args, dev):
         torch.cuda.empty_cache()
     return {"max_rel_err": worst, "max_rel_err_resolved": worst_resolved, "tolerance": 0.01,
             "within_tolerance": ok, "failures": failures,
-            "criterion": "per cell against the FP64 push: every cell that both FP64 floors (one FP32 ulp of the box, "
-                         "an independent sample) reproduce within 0.5 % is within 1 %; every other cell within 1 %, or "
-                         "within twice the larger floor where the statistic itself moves by more",
+            "criterion": "per cell against the FP64 push: within 1 %, or within 5 standard errors of the difference "
+                         "of two runs where the FP64 statistic is not resolved to 1 % (standard errors by batch means "
+                         "over 16 particle batches); the three FP64 floor runs pass the same test",
             "gamma_drift_E0_max": drift, "per_case": cases, "seconds": time.perf_counter() - t0,
             "setup": f"128^3, dB/B0=0.5, k=2..64, u_rms=1e-4 c; total/alfven/fast/slow x 1/10/100 GeV; {npart} "
-                     "protons, fixed mu0=0.5, 128 steps/T_g0, 50 T_g0, mu every 8 steps; 32 lags x 20 |mu| bins "
+                     "protons, fixed mu0=0.525, 128 steps/T_g0, 50 T_g0, mu every 8 steps; 32 lags x 20 |mu| bins "
                      "(cells >= 100 pairs); D_pp over 131072 particles from a Float64 phase-space cache; errors relative "
                      "to the FP64 push"}
 

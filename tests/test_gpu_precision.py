@@ -3,24 +3,25 @@
 A reduced form of the plain-vs-precision configuration: a 128³ box
 (one cell = the 1 GeV gyroradius in B0 = 1 uG), dB/B0 = 0.5 on |k| = 2..64
 with u_rms = 1e-4 c, as the total field and its alfven / fast / slow
-projections; protons at 1, 10 and 100 GeV with fixed mu0 = 0.5 and random
-gyrophase; 1,048,576 protons, 128 steps per T_g0 for 50 T_g0, mu cache
-every 8 steps (801 saves), 32 log lags x 20 |mu| bins, D_pp over the first
-131,072 particles (from a Float64 phase-space cache).
+projections; protons at 1, 10 and 100 GeV with fixed mu0 = 0.525 (the
+centre of a |mu| bin) and random gyrophase; 1,048,576 protons, 128 steps
+per T_g0 for 50 T_g0, mu cache every 8 steps (801 saves), 32 log lags x
+20 |mu| bins, D_pp over the first 131,072 particles (from a Float64
+phase-space cache).
 
 For the FP32 push over FP32 bricks and over BF16 bricks, D_mumu(mu, tau)
 over the cells holding at least MIN_COUNT pairs, <dmu^2>(tau) and D_pp(tau)
 are compared cell by cell with the FP64 push from the same initial state.
-Two FP64 floors say which cells FP64 itself resolves: the same push with
-positions moved by one FP32 ulp of the box (a perturbation the size of the
-FP32 push's own rounding) and the same push from an independent sample.
-Every cell both floors reproduce within 0.5 % must be within 1 % in each
-form; every other cell within 1 %, or within twice the larger floor where
-the statistic itself moves by more (in the compressive "slow" field at
-100 GeV a few particles cross a mirror separatrix and carry most of
-<dmu^2>, so any perturbation of that size moves the sums by tens of per
-cent).  On the same field with u = 0 (E = 0) every form conserves gamma to
-rounding."""
+Each FP64 statistic has a sampling error of its own, measured by batch
+means over 16 independent batches of particles.  A cell passes when the
+form is within 1 % of the FP64 value, or -- where the statistic is not
+resolved to 1 % by the particle count -- within 5 standard errors of the
+difference of two runs (in the compressive "slow" field at 100 GeV a few
+particles cross a mirror separatrix and carry most of some cells).  The
+FP64 push from positions moved by one FP64 ulp, by one FP32 ulp of the box
+and from an independent sample must pass the same test, which checks the
+test itself; most cells must be resolved to 1 %.  On the same field with
+u = 0 (E = 0) every form conserves gamma to rounding."""
 import math
 
 import pytest
@@ -59,8 +60,10 @@ def test_precision_forms_within_one_percent(cuda, mode, energy):
     libs, B0, grid = libraries(mode)
     r = P.compare_forms(libs, B0, grid, energy, N_PARTICLES, gyroperiods=GYROPERIODS, min_count=MIN_COUNT)
     assert r["cells_counted"] >= 0.8 * r["lags"] * r["mu_bins"], r["cells_counted"]
-    assert r["f32"]["D_mumu"]["resolved_cells"] >= 0.25 * r["cells_counted"], r["f32"]["D_mumu"]
-    failures = P.check_forms(r, ("f32", "bf16"), TOL)
+    for product in ("D_mumu", "delta_mu2", "D_pp"):
+        e = r["f32"][product]
+        assert e["resolved_cells"] >= 0.5 * e["cells"], (product, e["resolved_cells"], e["cells"])
+    failures = P.check_forms(r, ("f32", "bf16"))
     assert not failures, (mode, energy, failures)
     # E = 0: energy conserved to rounding (FP32 forms carry |p|^2 in FP64 and change it only in the E kicks)
     assert r["f64"]["gamma_drift_E0"] < 1e-12, r["f64"]
