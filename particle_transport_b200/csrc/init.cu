@@ -43,6 +43,7 @@ struct InitArgs {
     const double* B[3];   // PT_FIELD_REF_F64
     const void* nodes;    // brick forms
     const uint32_t* offs;
+    float boff[3];        // BF16 forms: the mean field the nodes are stored less
     pt_grid g;
     double* out[6];
     int* bad;
@@ -57,7 +58,7 @@ __device__ inline double node_B(const InitArgs& a, int64_t i, int64_t j, int64_t
     if (a.storage == PT_FIELD_BRICK_F32) return (double)((const float*)a.nodes)[8 * (size_t)node + c];
     const size_t words = a.storage == PT_FIELD_BRICK_BF16 ? 4 : 8;  // 16 B records or 32 B x-pair records
     const uint32_t w = ((const uint32_t*)a.nodes)[words * node + (c >> 1)];
-    return (double)__uint_as_float((c & 1) ? (w & 0xFFFF0000u) : (w << 16));
+    return (double)__uint_as_float((c & 1) ? (w & 0xFFFF0000u) : (w << 16)) + (double)a.boff[c];
 }
 
 // trilinear_sample, src/phase_space_gpu_runner.jl:247-276 (x, then y, then z lerps)
@@ -184,6 +185,7 @@ extern "C" int pt_particles_init_device(pt_ctx* ctx, const pt_field* field, cons
     for (int c = 0; c < 3; ++c) a.B[c] = field->comp[c];
     a.nodes = field->nodes;
     a.offs = field->offs;
+    for (int c = 0; c < 3; ++c) a.boff[c] = field->boff[c];
     a.g = g;
     double* outs[6] = {d_x1, d_x2, d_x3, d_p1, d_p2, d_p3};
     for (int c = 0; c < 6; ++c) a.out[c] = outs[c];

@@ -181,7 +181,19 @@ int field_create(pt_ctx* ctx, const double* const comps[6], bool on_device, cons
     }
     const double* src[6];
     for (int c = 0; c < 6; ++c) src[c] = on_device ? comps[c] : tmp[c];
-    rc = launch_brick_convert(src, *grid, B_ref, field_layout(storage), f->nodes, f->offs, f->n_nodes, s);
+    if (field_layout(storage) == LAYOUT_BF16 || field_layout(storage) == LAYOUT_BF16_XPAIR) {
+        // BF16 keeps 8 significant bits: B stored as B - <B> (|B - <B>| ~ dB
+        // instead of ~ B0) rounds with the spacing of the fluctuation, which
+        // for a mean field above the fluctuation is several times finer
+        double mean[3];
+        rc = field_means(ctx, src, nn, mean, s);
+        if (rc) {
+            for (int c = 0; c < 6; ++c) if (tmp[c]) cudaFree(tmp[c]);
+            return cleanup(rc);
+        }
+        for (int c = 0; c < 3; ++c) f->boff[c] = (float)(mean[c] / B_ref);
+    }
+    rc = launch_brick_convert(src, *grid, B_ref, field_layout(storage), f->nodes, f->offs, f->n_nodes, f->boff, s);
     e = cudaStreamSynchronize(s);
     for (int c = 0; c < 6; ++c) if (tmp[c]) cudaFree(tmp[c]);
     if (rc) return cleanup(rc);
@@ -237,6 +249,7 @@ PushArgsFast fast_args(const pt_field* f, pt_fast_state* st, const pt_push_param
     a.fld.bf16 = f->storage != PT_FIELD_BRICK_F32;
     a.fld.layout = field_layout(f->storage);
     a.fld.tex = f->tex;
+    for (int c = 0; c < 3; ++c) a.fld.boff[c] = f->boff[c];
     a.wx = (g.xmax - g.xmin) / g.dx;
     a.wy = (g.ymax - g.ymin) / g.dy;
     a.wz = (g.zmax - g.zmin) / g.dz;

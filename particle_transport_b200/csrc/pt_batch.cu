@@ -333,6 +333,7 @@ int pt_batch_add(pt_ctx* ctx, pt_batch* b, const pt_campaign_desc* d, int* id)
     a.fld.bf16 = f->storage != PT_FIELD_BRICK_F32;
     a.fld.layout = field_layout(f->storage);
     a.fld.tex = f->tex;
+    for (int k = 0; k < 3; ++k) a.fld.boff[k] = f->boff[k];
     a.wx = (g.xmax - g.xmin) / g.dx;
     a.wy = (g.ymax - g.ymin) / g.dy;
     a.wz = (g.zmax - g.zmin) / g.dz;

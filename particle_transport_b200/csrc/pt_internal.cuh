@@ -100,6 +100,9 @@ struct pt_field {
     uint32_t* offs = nullptr;  // [nx + ny + nz]: offx, offy, offz
     int64_t bytes = 0;
     cudaTextureObject_t tex = 0;  // brick forms: node records as uint4 texels (0 if over the texture limit)
+    // BF16 forms: the mean of B / B_ref per component, subtracted before the
+    // rounding to BF16 and added back after the interpolation (0 otherwise)
+    float boff[3] = {0.0f, 0.0f, 0.0f};
 };
 
 struct pt_fast_state {
@@ -227,6 +230,7 @@ struct FieldArgsBrick {
     int bf16;    // 1 for the BF16 forms
     int layout;  // LAYOUT_*
     cudaTextureObject_t tex;  // the node records as a linear uint4 texture (0: none)
+    float boff[3];            // BF16 forms: mean field added back after the interpolation
 };
 struct PushArgsFast {
     FieldArgsBrick fld;
@@ -332,7 +336,10 @@ int launch_fast_export(const pt_fast_state* st, const pt_field* f, double* x1, d
 int fast_sort(pt_ctx* ctx, pt_fast_state* st, const pt_field* f, cudaStream_t s);
 
 int launch_brick_convert(const double* const comps[6], const pt_grid& g, double B_ref, int layout, void* nodes,
-                         const uint32_t* offs, int64_t n_nodes, cudaStream_t s);
+                         const uint32_t* offs, int64_t n_nodes, const float boff[3], cudaStream_t s);
+// mean of the three B components (device arrays of nn values), summed in a
+// fixed order (the same bits on every call); waits for the stream
+int field_means(pt_ctx* ctx, const double* const comps[6], int64_t nn, double mean[3], cudaStream_t s);
 
 struct DmumuArgs {
     const float* mu;

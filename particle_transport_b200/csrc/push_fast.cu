@@ -173,6 +173,12 @@ __device__ __forceinline__ void advance_particle(double& x, double& y, double& z
             if (al && (do_push || (is_save && a.cache_mode == PT_CACHE_MU))) {
                 Corners c = locate_brick(x, y, z, ox, oy, oz, nx, ny, nz);
                 gather6<LAYOUT, TEXC>(a.fld.nodes, a.fld.tex, c, f);
+                if (LAYOUT == LAYOUT_BF16 || LAYOUT == LAYOUT_BF16_XPAIR) {
+                    // the BF16 nodes hold B - <B>: the weights sum to 1, so the mean adds back once
+                    f[0] += a.fld.boff[0];
+                    f[1] += a.fld.boff[1];
+                    f[2] += a.fld.boff[2];
+                }
             }
             if (is_save) {
                 const int64_t r = a.ring ? row % a.rows : row - a.row_base;
@@ -288,11 +294,14 @@ __global__ void brick_convert_kernel(const double* __restrict__ bx, const double
                                      const double* __restrict__ bz, const double* __restrict__ ux,
                                      const double* __restrict__ uy, const double* __restrict__ uz, int64_t nx,
                                      int64_t ny, int64_t nz, double inv_b, double inv_c, int layout, void* nodes,
-                                     const uint32_t* __restrict__ offs, int64_t n_nodes)
+                                     const uint32_t* __restrict__ offs, int64_t n_nodes, float o0, float o1, float o2)
 {
     const int64_t total = nx * ny * nz;
+    // B / B_ref less the stored mean-field offset (0 but for the BF16 forms)
     auto comps = [&](int64_t t, float v[6]) {
-        v[0] = (float)(bx[t] * inv_b); v[1] = (float)(by[t] * inv_b); v[2] = (float)(bz[t] * inv_b);
+        v[0] = (float)(bx[t] * inv_b - (double)o0);
+        v[1] = (float)(by[t] * inv_b - (double)o1);
+        v[2] = (float)(bz[t] * inv_b - (double)o2);
         v[3] = (float)(ux[t] * inv_c); v[4] = (float)(uy[t] * inv_c); v[5] = (float)(uz[t] * inv_c);
     };
     auto pack3 = [](const float v[6], uint32_t w[3]) {
@@ -680,15 +689,77 @@ int launch_push_fast(const PushArgsFast& a, cudaStream_t s)
 }
 
 int launch_brick_convert(const double* const comps[6], const pt_grid& g, double B_ref, int layout, void* nodes,
-                         const uint32_t* offs, int64_t n_nodes, cudaStream_t s)
+                         const uint32_t* offs, int64_t n_nodes, const float boff[3], cudaStream_t s)
 {
     const int64_t total = g.nx * g.ny * g.nz;
     const int threads = 256;
     int blocks = (int)std::min<int64_t>((total + threads - 1) / threads, 148 * 32);
     brick_convert_kernel<<<blocks, threads, 0, s>>>(comps[0], comps[1], comps[2], comps[3], comps[4], comps[5],
                                                     g.nx, g.ny, g.nz, 1.0 / B_ref, 1.0 / C_LIGHT, layout, nodes, offs,
-                                                    n_nodes);
+                                                    n_nodes, boff[0], boff[1], boff[2]);
     PT_CHECK_LAUNCH("brick_convert_kernel");
+    return PT_OK;
+}
+
+// Sums of Bx, By, Bz: kMeanBlocks blocks each add a contiguous range (a
+// strided sum per thread, then a tree over the block), and one thread adds
+// the block sums in block order -- a fixed order, so the same bits each time.
+constexpr int kMeanBlocks = 256, kMeanThreads = 256;
+__global__ void __launch_bounds__(kMeanThreads) component_sum_kernel(const double* __restrict__ bx,
+                                                                     const double* __restrict__ by,
+                                                                     const double* __restrict__ bz, int64_t nn,
+                                                                     double* __restrict__ partial)
+{
+    __shared__ double sh[3][kMeanThreads];
+    const int64_t per = (nn + gridDim.x - 1) / gridDim.x;
+    const int64_t lo = (int64_t)blockIdx.x * per, hi = min(nn, lo + per);
+    double s0 = 0.0, s1 = 0.0, s2 = 0.0;
+    for (int64_t t = lo + threadIdx.x; t < hi; t += blockDim.x) {
+        s0 += bx[t];
+        s1 += by[t];
+        s2 += bz[t];
+    }
+    sh[0][threadIdx.x] = s0;
+    sh[1][threadIdx.x] = s1;
+    sh[2][threadIdx.x] = s2;
+    __syncthreads();
+    for (int w = kMeanThreads / 2; w > 0; w >>= 1) {
+        if (threadIdx.x < w)
+            for (int c = 0; c < 3; ++c) sh[c][threadIdx.x] += sh[c][threadIdx.x + w];
+        __syncthreads();
+    }
+    if (threadIdx.x == 0)
+        for (int c = 0; c < 3; ++c) partial[3 * blockIdx.x + c] = sh[c][0];
+}
+
+__global__ void partial_sum_kernel(const double* __restrict__ partial, int blocks, double* __restrict__ out)
+{
+    if (threadIdx.x != 0 || blockIdx.x != 0) return;
+    double s[3] = {0.0, 0.0, 0.0};
+    for (int b = 0; b < blocks; ++b)
+        for (int c = 0; c < 3; ++c) s[c] += partial[3 * b + c];
+    for (int c = 0; c < 3; ++c) out[c] = s[c];
+}
+
+int field_means(pt_ctx* ctx, const double* const comps[6], int64_t nn, double mean[3], cudaStream_t s)
+{
+    (void)ctx;
+    if (nn <= 0) return fail(PT_ERR_ARG, "empty field");
+    double* d = nullptr;
+    cudaError_t e = cudaMalloc(&d, sizeof(double) * (3 * kMeanBlocks + 3));
+    if (e != cudaSuccess) {
+        cudaGetLastError();
+        return fail(PT_ERR_OOM, "field mean scratch allocation failed");
+    }
+    component_sum_kernel<<<kMeanBlocks, kMeanThreads, 0, s>>>(comps[0], comps[1], comps[2], nn, d);
+    partial_sum_kernel<<<1, 32, 0, s>>>(d, kMeanBlocks, d + 3 * kMeanBlocks);
+    double sums[3] = {0.0, 0.0, 0.0};
+    e = cudaGetLastError();
+    if (e == cudaSuccess) e = cudaMemcpyAsync(sums, d + 3 * kMeanBlocks, sizeof(sums), cudaMemcpyDeviceToHost, s);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+    cudaFree(d);
+    if (e != cudaSuccess) return cuda_fail(e, "field means");
+    for (int c = 0; c < 3; ++c) mean[c] = sums[c] / (double)nn;
     return PT_OK;
 }
 
