@@ -1188,7 +1188,8 @@ def run_serving(args, dev, rate=4.0):
         out = {"jobs": len(srv.results), "p50_s": float(np.percentile(lat, 50)),
                "p99_s": float(np.percentile(lat, 99)), "mean_s": float(lat.mean()), "max_s": float(lat.max()),
                "wall_s": wall, "particle_steps": int(steps), "aggregate_rate": steps / wall, "device_busy_s": busy,
-               "busy_rate": steps / busy, "admit_host_s": srv.admit_s, "epochs": srv.epochs}
+               "busy_rate": steps / busy, "admit_host_s": srv.admit_s, "admission": dict(srv.admit_stats),
+               "epochs": srv.epochs}
         srv.close()
         torch.cuda.empty_cache()
         return out

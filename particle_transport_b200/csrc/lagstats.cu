@@ -291,18 +291,26 @@ __global__ void __launch_bounds__(1024) dmumu_kernel(DmumuLaunch a, Src source)
             }
         }
         __syncthreads();
-        // ---- pairs: bin by bin; the `parts` warps of a (slot, lag group) take
-        // bins part, part + parts, ...; every lane keeps two accumulator chains
+        // ---- pairs: the `parts` warps of a (slot, lag group) split the
+        // bin-sorted start list into equal shares (a bin may straddle two
+        // shares; each flushes its part of it), so they reach the barrier
+        // together whatever the particle's bin counts; every lane keeps two
+        // accumulator chains
         if (have) {
             long long my_c = 0;
             double my_sd2 = 0.0;
             // starts, lags and nsave fit 32 bits (nsave < 2^31); so does a bin's count
             const unsigned n32 = (unsigned)a.nsave, L32 = (unsigned)L;
-            for (int b = part; b <= nb; b += a.parts) {
-                const int e0 = cur[b], e1 = cur[b + 1];
+            const int total = cur[nb + 1];
+            const int r0 = (int)(((long long)total * part) / a.parts);
+            const int r1 = (int)(((long long)total * (part + 1)) / a.parts);
+            int b = 0;
+            if (r0 < r1)
+                while (cur[b + 1] <= r0) ++b;  // the bin holding entry r0 (r0 < total = cur[nb + 1])
+            for (int e = r0; e < r1; ++b) {
+                const int e1 = min(cur[b + 1], r1);
                 int c = 0;
                 double sd0 = 0.0, sd1 = 0.0, sq0 = 0.0, sq1 = 0.0;
-                int e = e0;
                 // Branch-free pairs.  A start in the list has a finite mu; its
                 // partner series[s + L] is NaN when the particle's mu is not
                 // finite there, and s + L past the series end reads the NaN pad
@@ -349,6 +357,7 @@ __global__ void __launch_bounds__(1024) dmumu_kernel(DmumuLaunch a, Src source)
                 }
                 my_c += c;
                 my_sd2 += sd2;
+                e = e1;
             }
             if (lane_on && my_c > 0) {
                 atomicAdd(&tot_c[li], (unsigned long long)my_c);

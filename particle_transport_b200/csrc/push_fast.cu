@@ -78,8 +78,7 @@ template <int LAYOUT, int TEXC = 0>
 __device__ __forceinline__ void gather6(const void* __restrict__ nodes, cudaTextureObject_t tex, const Corners& c,
                                         float f[6])
 {
-#pragma unroll
-    for (int k = 0; k < 6; ++k) f[k] = 0.0f;
+    // adds the weighted corners to f (which holds 0, or the BF16 forms' mean field)
     if (LAYOUT == LAYOUT_F32) {
         const char* N = (const char*)nodes;
         uint32_t v[8][8];
@@ -172,13 +171,14 @@ __device__ __forceinline__ void advance_particle(double& x, double& y, double& z
             float f[6] = {0, 0, 0, 0, 0, 0};
             if (al && (do_push || (is_save && a.cache_mode == PT_CACHE_MU))) {
                 Corners c = locate_brick(x, y, z, ox, oy, oz, nx, ny, nz);
-                gather6<LAYOUT, TEXC>(a.fld.nodes, a.fld.tex, c, f);
                 if (LAYOUT == LAYOUT_BF16 || LAYOUT == LAYOUT_BF16_XPAIR) {
-                    // the BF16 nodes hold B - <B>: the weights sum to 1, so the mean adds back once
-                    f[0] += a.fld.boff[0];
-                    f[1] += a.fld.boff[1];
-                    f[2] += a.fld.boff[2];
+                    // the BF16 nodes hold B - <B>: the weights sum to 1, so the
+                    // mean enters once, as the start of the weighted sum
+                    f[0] = a.fld.boff[0];
+                    f[1] = a.fld.boff[1];
+                    f[2] = a.fld.boff[2];
                 }
+                gather6<LAYOUT, TEXC>(a.fld.nodes, a.fld.tex, c, f);
             }
             if (is_save) {
                 const int64_t r = a.ring ? row % a.rows : row - a.row_base;

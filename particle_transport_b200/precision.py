@@ -128,6 +128,7 @@ def _gamma(st):
 
 
 K_SIGMA = 5.0  # sampling band: k standard errors of the difference of two runs
+SE_CAP = 0.05  # cells whose FP64 standard error exceeds this are not measured by the sample
 
 
 def rel(a, b):
@@ -156,18 +157,23 @@ def ratio_se(S, C):
     return out
 
 
-def rel_err(a, b, se, mask=None, tol=0.01, k=K_SIGMA):
+def rel_err(a, b, se, mask=None, tol=0.01, k=K_SIGMA, se_cap=SE_CAP):
     """Relative errors |a - b| / |b| over the cells finite in both (and in
     mask), judged against the reference's own relative standard error `se`
     per cell: a cell passes when its error is within tol, or within
     k * sqrt(2) * se where the statistic is not resolved to tol (two runs
-    each carry the sampling error).  Returns the max and median error, the
-    max over the resolved cells (k sqrt(2) se <= tol), the largest
-    z = error / (sqrt(2) se), and the failing cells."""
+    each carry the sampling error).  Cells whose standard error exceeds
+    se_cap are held by a handful of particles (a few mirror crossings carry
+    the sum); their spread is not Gaussian and they are counted, not judged.
+    Returns the max and median error, the max over the resolved cells
+    (k sqrt(2) se <= tol), the largest z = error / (sqrt(2) se), and the
+    failing cells."""
     r = rel(a, b)
     m = np.isfinite(r) & np.isfinite(se)
     if mask is not None:
         m &= mask
+    unmeasured = int((m & (se > se_cap)).sum())
+    m &= se <= se_cap
     if not m.any():
         return {"max": math.nan, "median": math.nan, "cells": 0, "failing": []}
     band = k * math.sqrt(2.0) * se
@@ -175,7 +181,7 @@ def rel_err(a, b, se, mask=None, tol=0.01, k=K_SIGMA):
     z = np.where(m, r / (math.sqrt(2.0) * np.maximum(se, 1e-300)), 0.0)
     fail = m & (r > np.maximum(tol, band))
     out = {"max": float(r[m].max()), "median": float(np.median(r[m])), "cells": int(m.sum()),
-           "resolved_cells": int(resolved.sum()),
+           "unmeasured_cells": unmeasured, "resolved_cells": int(resolved.sum()),
            "max_resolved": float(r[resolved].max()) if resolved.any() else 0.0,
            "max_z": float(z.max()), "median_se": float(np.median(se[m])),
            "failing": [[int(v) for v in np.atleast_1d(i)] for i in zip(*np.nonzero(fail))][:8]}

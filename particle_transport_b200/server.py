@@ -130,9 +130,17 @@ class CampaignServer:
         self.next_id = 0
         self.epochs = 0
         self.admit_s = 0.0   # host seconds spent admitting jobs
+        # where admission time goes: jobs admitted and the seconds of their
+        # setup; attempts the device refused (out of memory, no slot range)
+        self.admit_stats = self.new_admit_stats()
         self._epoch_events = []
 
     # ------------------------------------------------------------ admission
+    @staticmethod
+    def new_admit_stats() -> dict:
+        return {"admitted": 0, "admit_setup_s": 0.0, "refused_oom": 0, "refused_slots": 0, "refused_s": 0.0,
+                "room_checks": 0, "room_s": 0.0}
+
     @staticmethod
     def job_bytes(spec: JobSpec) -> float:
         nsteps = int(round(spec.duration_gyroperiods * spec.steps_per_gyroperiod)) + 1
@@ -193,18 +201,31 @@ class CampaignServer:
     def _admit_waiting(self) -> int:
         n = 0
         keep = []
+        st = self.admit_stats
         for jid, spec, arrival in self.queue:
             need = self.job_bytes(spec)
-            if not keep and self.used + need <= self.budget and need <= self.device_room():
+            fits = False
+            if not keep and self.used + need <= self.budget:
+                t0 = time.perf_counter()
+                fits = need <= self.device_room()
+                st["room_checks"] += 1
+                st["room_s"] += time.perf_counter() - t0
+            if fits:
+                t0 = time.perf_counter()
                 try:
                     self._admit(jid, spec, arrival)
                     n += 1
+                    st["admitted"] += 1
+                    st["admit_setup_s"] += time.perf_counter() - t0
                     continue
                 except _lib.PtError as e:  # no slot range free yet
                     if e.code not in (-3, -6):
                         raise
+                    st["refused_slots"] += 1
                 except self.torch.OutOfMemoryError:  # the device is fuller than it looked: wait for a job to end
                     self.torch.cuda.empty_cache()
+                    st["refused_oom"] += 1
+                st["refused_s"] += time.perf_counter() - t0
             keep.append((jid, spec, arrival))
         self.queue = keep
         return n

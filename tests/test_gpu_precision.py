@@ -16,8 +16,10 @@ Each FP64 statistic has a sampling error of its own, measured by batch
 means over 16 independent batches of particles.  A cell passes when the
 form is within 1 % of the FP64 value, or -- where the statistic is not
 resolved to 1 % by the particle count -- within 5 standard errors of the
-difference of two runs (in the compressive "slow" field at 100 GeV a few
-particles cross a mirror separatrix and carry most of some cells).  The
+difference of two runs.  Cells whose standard error exceeds 5 % are held by
+a handful of particles (in the compressive "slow" field at 100 GeV a few
+particles cross a mirror separatrix and carry most of some cells) and are
+counted, not judged.  The
 FP64 push from positions moved by one FP64 ulp, by one FP32 ulp of the box
 and from an independent sample must pass the same test, which checks the
 test itself; at least a third of the cells of each product must be

@@ -112,14 +112,23 @@ def _fast_mu(pb, storage, nsteps, stride, sort_every=0, u=True, variant=0):
     return cache.cpu().numpy(), {k: v.cpu().numpy() for k, v in st.items()}, fl
 
 
-@pytest.mark.parametrize("storage,tol_max,tol_med", [("brick_f32", 2e-3, 1e-4), ("brick_bf16", 0.2, 0.02)])
-def test_fast_push_close_over_one_gyroperiod(cuda, storage, tol_max, tol_med):
+@pytest.mark.parametrize("storage,tol_particle,share,tol_med", [("brick_f32", 2e-3, 1.0, 1e-4),
+                                                                ("brick_bf16", 0.05, 0.99, 0.02)])
+def test_fast_push_close_over_one_gyroperiod(cuda, storage, tol_particle, share, tol_med):
+    """mu of the FP32 push against the FP64 push over one gyroperiod: every
+    particle within tol_particle over FP32 bricks.  Over BF16 bricks (B
+    stored less its mean, 8 significant bits) a particle that passes a
+    weak-field node sees a field error of ~2^-9 of the mean field there and
+    can leave on another non-adiabatic branch, so the bound holds for 99 %
+    of the particles, and the median sample error stays small."""
     pb = small_problem(n=16, n_particles=1000, u_over_c=1e-4)
     (mu_o, _, _, _), _ = run_both(pb, 65, 4, "mu")
     mu_f, _, _ = _fast_mu(pb, storage, 65, 4)
     d = np.abs(mu_f - mu_o)
     assert np.all(np.isfinite(mu_f))
-    assert d.max() < tol_max and np.median(d) < tol_med, (d.max(), np.median(d))
+    per_particle = d.max(axis=0)
+    assert np.mean(per_particle < tol_particle) >= share, np.sort(per_particle)[-12:]
+    assert np.median(d) < tol_med, np.median(d)
 
 
 def test_xpair_layout_bit_identical_to_bf16(cuda):

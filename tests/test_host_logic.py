@@ -70,6 +70,7 @@ def admission_server(budget, room=float("inf")):
     srv.queue = []
     srv.active = {}
     srv.admit_s = 0.0
+    srv.admit_stats = CampaignServer.new_admit_stats()
     admitted = []
 
     def fake_admit(jid, spec, arrival):
@@ -160,3 +161,4 @@ def test_admission_also_needs_room_on_the_device():
     assert srv.admit() == 1 and admitted == [0]  # the budget has room; the device does not
     srv.used -= b_b  # the big job ends
     assert srv.admit() == 2 and admitted == [0, 1, 2]
+    assert srv.admit_stats["admitted"] == 3 and srv.admit_stats["room_checks"] == 4

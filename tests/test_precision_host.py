@@ -48,6 +48,9 @@ def test_cell_test_resolved_and_unresolved():
     # cells outside the mask or without a standard error are not judged
     e2 = P.rel_err(form, ref, np.array([[1e-4, np.nan, 0.01, 0.01]]), mask=np.array([[True, True, True, False]]))
     assert e2["cells"] == 2 and e2["failing"] == []
+    # nor are cells the sample does not measure (standard error above the cap): counted apart
+    e3 = P.rel_err(np.array([1.0, 3.0]), np.array([1.0, 1.0]), np.array([1e-4, 2 * P.SE_CAP]))
+    assert e3["cells"] == 1 and e3["unmeasured_cells"] == 1 and e3["failing"] == []
 
 
 def test_check_forms_reports_forms_and_floors():
