@@ -630,9 +630,15 @@ int pt_push_run(pt_ctx* ctx, const pt_field* f, double* x1, double* x2, double* 
     const size_t elem = p->cache_f64 ? 8 : 4;
     const int64_t row_elems = p->cache_mode == PT_CACHE_MU ? n : 6 * n;
     const size_t row_bytes = p->cache_mode == PT_CACHE_NONE ? 0 : elem * (size_t)row_elems;
+    // The FP32 push writes its mu saves time-fastest, [n][8] (a particle's
+    // saves of a chunk side by side, merged by L2 into whole sectors), and a
+    // transpose turns each chunk into the rows the callback receives.
+    const bool tf = p->precision == PT_PUSH_F32 && p->cache_mode == PT_CACHE_MU && !p->cache_f64 && n > 0;
+    const int tf_pitch = 8;
     // rows per egress chunk: enough steps per launch, bounded staging memory
-    int64_t R = std::max<int64_t>(1, (256 + stride - 1) / stride);
-    if (row_bytes > 0) R = std::max<int64_t>(1, std::min<int64_t>(R, (int64_t)((256u << 20) / row_bytes)));
+    int64_t R = tf ? tf_pitch : std::max<int64_t>(1, (256 + stride - 1) / stride);
+    const size_t slot_cap = tf ? (512u << 20) : (256u << 20);
+    if (row_bytes > 0) R = std::max<int64_t>(1, std::min<int64_t>(R, (int64_t)(slot_cap / row_bytes)));
     const int64_t chunk_steps = R * stride;
 
     // device: state [6][m] doubles + alive [m] + deaths [nsteps] + two egress slots
@@ -642,14 +648,17 @@ int pt_push_run(pt_ctx* ctx, const pt_field* f, double* x1, double* x2, double* 
     const size_t state_bytes = align_up(sizeof(double) * 6 * m + m, 256);
     const size_t deaths_bytes = align_up(sizeof(int64_t) * (size_t)nsteps, 256);
     const size_t slots_bytes = row_bytes ? 2 * (size_t)R * row_bytes : 0;
+    const size_t tf_bytes = tf ? align_up(sizeof(float) * tf_pitch * m, 256) + 256 : 0;
     const size_t stage_chunk = 32u << 20;
     const int stage_nbuf = 3;
     void* dbase = nullptr;
     void* hbase = nullptr;
-    if ((rc = scratch_get(ctx, 2, state_bytes + deaths_bytes + slots_bytes, &dbase))) return rc;
+    if ((rc = scratch_get(ctx, 2, state_bytes + deaths_bytes + slots_bytes + tf_bytes, &dbase))) return rc;
     if ((rc = pinned_get(ctx, slots_bytes + stage_chunk * stage_nbuf, &hbase))) return rc;
     char* stage = (char*)hbase + slots_bytes;
     char* dslot_base = (char*)dbase + state_bytes + deaths_bytes;  // [2][R] device egress rows
+    // [n][8] time-fastest saves of a chunk, 32-byte records on 256-byte-aligned storage
+    float* dtf = tf ? (float*)(dslot_base + align_up(slots_bytes, 256)) : nullptr;
     char* hslot_base = (char*)hbase;                                // [2][R] pinned egress rows
     int64_t* d_deaths = (int64_t*)((char*)dbase + state_bytes);
     double* d[6];
@@ -724,6 +733,11 @@ int pt_push_run(pt_ctx* ctx, const pt_field* f, double* x1, double* x2, double* 
             pt_push_params q = *p;
             rc = pt_push_advance_device(ctx, f, d[0], d[1], d[2], d[3], d[4], d[5], dal, n, &q, s0, steps, dslot,
                                         row_base, rows, d_deaths);
+        } else if (tf) {
+            pt_push_params q = *p;
+            q.cache_pitch = tf_pitch;
+            rc = advance_fast(ctx, f, fs, &q, s0, steps, dtf, row_base, rows, d_deaths);
+            if (!rc) rc = launch_tf_to_rows(dtf, n, tf_pitch, (int)rows, (float*)dslot, st);
         } else {
             rc = advance_fast(ctx, f, fs, p, s0, steps, dslot, row_base, rows, d_deaths);
         }

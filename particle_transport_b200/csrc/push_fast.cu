@@ -701,6 +701,26 @@ int launch_brick_convert(const double* const comps[6], const pt_grid& g, double 
     return PT_OK;
 }
 
+// One thread per particle: its `rows` saves (contiguous, one 32-byte record
+// at pitch 8) out to `rows` coalesced rows.
+__global__ void tf_to_rows_kernel(const float* __restrict__ tf, int64_t n, int pitch, int rows,
+                                  float* __restrict__ out)
+{
+    for (int64_t p = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; p < n; p += (int64_t)gridDim.x * blockDim.x) {
+        const float* rec = tf + p * pitch;
+        for (int r = 0; r < rows; ++r) out[(int64_t)r * n + p] = rec[r];
+    }
+}
+
+int launch_tf_to_rows(const float* tf, int64_t n, int pitch, int rows, float* out, cudaStream_t s)
+{
+    if (n <= 0 || rows <= 0) return PT_OK;
+    const int blocks = (int)std::min<int64_t>((n + 255) / 256, (int64_t)148 * 64);
+    tf_to_rows_kernel<<<blocks, 256, 0, s>>>(tf, n, pitch, rows, out);
+    PT_CHECK_LAUNCH("tf_to_rows_kernel");
+    return PT_OK;
+}
+
 // Sums of Bx, By, Bz: kMeanBlocks blocks each add a contiguous range (a
 // strided sum per thread, then a tree over the block), and one thread adds
 // the block sums in block order -- a fixed order, so the same bits each time.

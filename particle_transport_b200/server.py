@@ -133,6 +133,9 @@ class CampaignServer:
         # where admission time goes: jobs admitted and the seconds of their
         # setup; attempts the device refused (out of memory, no slot range)
         self.admit_stats = self.new_admit_stats()
+        self._need = {}               # job id -> bytes charged (job_bytes, computed once)
+        self._blocked_at = None       # self.used when the head job last did not fit
+        self._blocked_t = 0.0
         self._epoch_events = []
 
     # ------------------------------------------------------------ admission
@@ -198,14 +201,32 @@ class CampaignServer:
         cached = torch.cuda.memory_reserved(self.device) - torch.cuda.memory_allocated(self.device)
         return float(free + cached) - self.reserve_bytes
 
+    # a head job that did not fit is tried again once a job has released
+    # its bytes (self.used fell), or after this many seconds: the budget and
+    # the device's room change only when jobs end, and each refused attempt
+    # costs a device-memory query or a failed allocation
+    retry_s = 0.25
+
     def _admit_waiting(self) -> int:
+        if not self.queue:
+            return 0
+        if self._blocked_at is not None:
+            if self.used >= self._blocked_at and time.perf_counter() - self._blocked_t < self.retry_s:
+                return 0
+            self._blocked_at = None
         n = 0
         keep = []
         st = self.admit_stats
+        need_of = self.__dict__.setdefault("_need", {})
         for jid, spec, arrival in self.queue:
-            need = self.job_bytes(spec)
+            if keep:  # arrival order: every later job waits behind the first that does not fit
+                keep.append((jid, spec, arrival))
+                continue
+            need = need_of.get(jid)
+            if need is None:
+                need = need_of[jid] = self.job_bytes(spec)
             fits = False
-            if not keep and self.used + need <= self.budget:
+            if self.used + need <= self.budget:
                 t0 = time.perf_counter()
                 fits = need <= self.device_room()
                 st["room_checks"] += 1
@@ -227,6 +248,7 @@ class CampaignServer:
                     st["refused_oom"] += 1
                 st["refused_s"] += time.perf_counter() - t0
             keep.append((jid, spec, arrival))
+            self._blocked_at, self._blocked_t = self.used, time.perf_counter()
         self.queue = keep
         return n
 

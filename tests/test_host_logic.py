@@ -71,6 +71,7 @@ def admission_server(budget, room=float("inf")):
     srv.active = {}
     srv.admit_s = 0.0
     srv.admit_stats = CampaignServer.new_admit_stats()
+    srv._need, srv._blocked_at, srv._blocked_t = {}, None, 0.0
     admitted = []
 
     def fake_admit(jid, spec, arrival):
@@ -158,7 +159,10 @@ def test_admission_also_needs_room_on_the_device():
     s_b, b_b = CampaignServer.job_bytes(small), CampaignServer.job_bytes(big)
     srv, admitted = admission_server(budget=10 * b_b, room=b_b + 0.5 * s_b)
     srv.queue = [(0, big, 0.0), (1, small, 0.0), (2, small, 0.0)]
+    srv.retry_s = 1e9
     assert srv.admit() == 1 and admitted == [0]  # the budget has room; the device does not
+    checks = srv.admit_stats["room_checks"]
+    assert srv.admit() == 0 and srv.admit_stats["room_checks"] == checks  # no retry before a job ends
     srv.used -= b_b  # the big job ends
     assert srv.admit() == 2 and admitted == [0, 1, 2]
     assert srv.admit_stats["admitted"] == 3 and srv.admit_stats["room_checks"] == 4
