@@ -154,7 +154,10 @@ int64_t pt_field_device_bytes(const pt_field* field);
  * The state crosses the link through the context's pinned staging chunks
  * (host threads copy while the DMA engine moves the previous chunk); the
  * device state, staging and the FP32-push state stay in the context for the
- * next call (pt_ctx_trim releases them).
+ * next call (pt_ctx_trim releases them).  The FP32 push with a Float32 mu
+ * cache writes each 64-step chunk's saves time-fastest on the device and
+ * transposes them to rows before the egress (two slots of up to 8 rows of
+ * n floats, device and pinned, plus the [n][8] buffer).
  */
 int pt_push_run(pt_ctx* ctx, const pt_field* field, double* x1, double* x2, double* x3, double* p1, double* p2,
                 double* p3, uint8_t* alive, int64_t n, const pt_push_params* params, pt_save_fn save, void* user,
