@@ -498,41 +498,118 @@ __global__ void __launch_bounds__(1024) sort_scan_top_kernel(uint32_t* tile_off,
     }
 }
 
-// The whole state of a particle is loaded (and its bucket recomputed from
-// it) before the cursor atomic, so the loads overlap the atomic's round trip.
-__global__ void sort_scatter_kernel(uint32_t* cursor, const uint32_t* __restrict__ tile_off, int64_t n,
-                                    const uint32_t* __restrict__ offs, int nx, int ny, int nz, uint32_t dead_key,
-                                    const double* __restrict__ xs, const float* __restrict__ ps,
-                                    const double* __restrict__ p2s, const int32_t* __restrict__ pids,
-                                    const uint8_t* __restrict__ as, double* __restrict__ xd, float* __restrict__ pd,
-                                    double* __restrict__ p2d, int32_t* __restrict__ pidd, uint8_t* __restrict__ ad)
+// Block-local scatter.  A CTA takes 256 slots, sorts their (key, thread)
+// pairs (bitonic: partners within a warp by shuffle, across warps through
+// shared memory), reserves one cursor range per run of equal keys -- one
+// atomic per run instead of one per warp and key -- and writes the particles
+// in key order, so that a run's particles go to consecutive slots from
+// consecutive threads.  The particle data is staged in shared memory by
+// thread and read back by sorted position.
+constexpr int kScatterBlock = 256;
+constexpr uint32_t kPastEnd = 0xFFFFFFFFu;  // key of a thread without a particle: sorts last, written nowhere
+static_assert(kScatterBlock == kBatchTile, "the batch scatter runs one tile per block");
+
+struct RunScratch {
+    unsigned long long v[kScatterBlock];
+    uint32_t key[kScatterBlock], base[kScatterBlock];
+    int wmax[kScatterBlock / 32];
+};
+// the FP32-push state of a block's particles
+struct ScatterStage {
+    double x[3][kScatterBlock], p2[kScatterBlock];
+    float p[3][kScatterBlock];
+    int32_t pid[kScatterBlock];
+    uint8_t alive[kScatterBlock];
+    RunScratch run;
+};
+// the FP64 SI state of a block's particles
+struct ExactStage {
+    double v[6][kScatterBlock];
+    int32_t pid[kScatterBlock];
+    uint8_t alive[kScatterBlock];
+    RunScratch run;
+};
+
+struct BlockRun {
+    int src;      // thread whose particle leaves from this sorted position
+    int64_t dest; // its slot relative to the bucket's cursor base; -1: nothing to write
+};
+
+// Called by every thread of the block, with its key (kPastEnd without a
+// particle); its barriers also publish the staged particle data.
+__device__ __forceinline__ BlockRun block_runs(uint32_t key, uint32_t* cursor, const uint32_t* __restrict__ tile_off,
+                                               RunScratch& sh)
 {
-    const int lane = threadIdx.x & 31;
-    const unsigned lt = (1u << lane) - 1u;
-    const int64_t stride = (int64_t)gridDim.x * blockDim.x;
-    for (int64_t base = (int64_t)blockIdx.x * blockDim.x + (threadIdx.x & ~31); base < n; base += stride) {
-        const int64_t i = base + lane;
-        const bool valid = i < n;
-        const unsigned act = __ballot_sync(0xffffffffu, valid);
-        if (!valid) continue;
-        const double x0 = xs[i], x1 = xs[n + i], x2 = xs[2 * n + i];
-        const float q0 = ps[i], q1 = ps[n + i], q2 = ps[2 * n + i];
-        const double pp = p2s[i];
-        const int32_t id = pids[i];
-        const uint8_t al = as[i];
-        const uint32_t key = brick_key(x0, x1, x2, al, offs, nx, ny, nz, dead_key);
-        const unsigned same = __match_any_sync(act, key);
-        const int leader = __ffs(same) - 1;
-        uint32_t first = 0;
-        if (lane == leader) first = atomicAdd(&cursor[key], (uint32_t)__popc(same)) + tile_off[key / kScanTile];
-        first = __shfl_sync(same, first, leader);
-        const int64_t d = (int64_t)first + __popc(same & lt);
-        xd[d] = x0; xd[n + d] = x1; xd[2 * n + d] = x2;
-        pd[d] = q0; pd[n + d] = q1; pd[2 * n + d] = q2;
-        p2d[d] = pp;
-        pidd[d] = id;
-        ad[d] = al;
+    const int t = threadIdx.x, lane = t & 31, w = t >> 5;
+    unsigned long long v = ((unsigned long long)key << 32) | (unsigned)t;
+    for (int k = 2; k <= kScatterBlock; k <<= 1) {
+        for (int j = k >> 1; j > 0; j >>= 1) {
+            unsigned long long o;
+            if (j >= 32) {
+                sh.v[t] = v;
+                __syncthreads();
+                o = sh.v[t ^ j];
+                __syncthreads();
+            } else {
+                o = __shfl_xor_sync(0xffffffffu, v, j);
+            }
+            const bool up = (t & k) == 0, lower = (t & j) == 0;
+            v = (lower == up) ? (v < o ? v : o) : (v > o ? v : o);
+        }
     }
+    const uint32_t k_t = (uint32_t)(v >> 32);
+    sh.key[t] = k_t;
+    __syncthreads();
+    const bool head = t == 0 || sh.key[t - 1] != k_t;
+    const bool tail = t == kScatterBlock - 1 || sh.key[t + 1] != k_t;
+    // start of this position's run: inclusive max-scan of (head ? t : 0)
+    int rs = head ? t : 0;
+    for (int d = 1; d < 32; d <<= 1) {
+        const int y = __shfl_up_sync(0xffffffffu, rs, d);
+        if (lane >= d) rs = max(rs, y);
+    }
+    if (lane == 31) sh.wmax[w] = rs;
+    __syncthreads();
+    for (int q = 0; q < w; ++q) rs = max(rs, sh.wmax[q]);
+    if (tail && k_t != kPastEnd)
+        sh.base[rs] = atomicAdd(&cursor[k_t], (uint32_t)(t - rs + 1)) + tile_off[k_t / kScanTile];
+    __syncthreads();
+    BlockRun r;
+    r.src = (int)(v & 0xFFFFFFFFu);
+    r.dest = k_t == kPastEnd ? -1 : (int64_t)sh.base[rs] + (t - rs);
+    return r;
+}
+
+__global__ void __launch_bounds__(kScatterBlock) sort_scatter_block_kernel(
+    uint32_t* cursor, const uint32_t* __restrict__ tile_off, int64_t n, const uint32_t* __restrict__ offs, int nx,
+    int ny, int nz, uint32_t dead_key, const double* __restrict__ xs, const float* __restrict__ ps,
+    const double* __restrict__ p2s, const int32_t* __restrict__ pids, const uint8_t* __restrict__ as,
+    double* __restrict__ xd, float* __restrict__ pd, double* __restrict__ p2d, int32_t* __restrict__ pidd,
+    uint8_t* __restrict__ ad)
+{
+    __shared__ ScatterStage sh;
+    const int t = threadIdx.x;
+    const int64_t i = (int64_t)blockIdx.x * kScatterBlock + t;
+    uint32_t key = kPastEnd;
+    if (i < n) {
+        const double x0 = xs[i], x1 = xs[n + i], x2 = xs[2 * n + i];
+        const uint8_t al = as[i];
+        sh.x[0][t] = x0; sh.x[1][t] = x1; sh.x[2][t] = x2;
+        sh.p[0][t] = ps[i]; sh.p[1][t] = ps[n + i]; sh.p[2][t] = ps[2 * n + i];
+        sh.p2[t] = p2s[i];
+        sh.pid[t] = pids[i];
+        sh.alive[t] = al;
+        key = brick_key(x0, x1, x2, al, offs, nx, ny, nz, dead_key);
+    }
+    const BlockRun r = block_runs(key, cursor, tile_off, sh.run);
+    if (r.dest < 0) return;
+    const int64_t d = r.dest;
+    const int q = r.src;
+    xd[d] = sh.x[0][q]; xd[n + d] = sh.x[1][q]; xd[2 * n + d] = sh.x[2][q];
+    pd[d] = sh.p[0][q]; pd[n + d] = sh.p[1][q]; pd[2 * n + d] = sh.p[2][q];
+    p2d[d] = sh.p2[q];
+    pidd[d] = sh.pid[q];
+    ad[d] = sh.alive[q];
 }
 
 // ---- brick sort of an FP64 SI state (the FP64 push over BRICK_F64 fields):
@@ -565,35 +642,32 @@ __global__ void exact_key_kernel(const double* __restrict__ xs, const uint8_t* _
     }
 }
 
-__global__ void exact_scatter_kernel(uint32_t* cursor, const uint32_t* __restrict__ tile_off, int64_t n, double x0,
-                                     double y0, double z0, double idx, double idy, double idz,
-                                     const uint32_t* __restrict__ offs, int nx, int ny, int nz, uint32_t dead_key,
-                                     const double* __restrict__ xs, const int32_t* __restrict__ pids,
-                                     const uint8_t* __restrict__ as, double* __restrict__ xd,
-                                     int32_t* __restrict__ pidd, uint8_t* __restrict__ ad)
+__global__ void __launch_bounds__(kScatterBlock) exact_scatter_kernel(
+    uint32_t* cursor, const uint32_t* __restrict__ tile_off, int64_t n, double x0, double y0, double z0, double idx,
+    double idy, double idz, const uint32_t* __restrict__ offs, int nx, int ny, int nz, uint32_t dead_key,
+    const double* __restrict__ xs, const int32_t* __restrict__ pids, const uint8_t* __restrict__ as,
+    double* __restrict__ xd, int32_t* __restrict__ pidd, uint8_t* __restrict__ ad)
 {
-    const int lane = threadIdx.x & 31;
-    const unsigned lt = (1u << lane) - 1u;
-    const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-    const bool valid = i < n;
-    const unsigned act = __ballot_sync(0xffffffffu, valid);
-    if (!valid) return;
-    double v[6];
+    // block-local runs as in sort_scatter_block_kernel
+    __shared__ ExactStage sh;
+    const int t = threadIdx.x;
+    const int64_t i = (int64_t)blockIdx.x * kScatterBlock + t;
+    uint32_t key = kPastEnd;
+    if (i < n) {
 #pragma unroll
-    for (int k = 0; k < 6; ++k) v[k] = xs[k * n + i];
-    const int32_t id = pids[i];
-    const uint8_t al = as[i];
-    const uint32_t key = exact_brick_key(xs, n, i, al, x0, y0, z0, idx, idy, idz, offs, nx, ny, nz, dead_key);
-    const unsigned same = __match_any_sync(act, key);
-    const int leader = __ffs(same) - 1;
-    uint32_t first = 0;
-    if (lane == leader) first = atomicAdd(&cursor[key], (uint32_t)__popc(same)) + tile_off[key / kScanTile];
-    first = __shfl_sync(same, first, leader);
-    const int64_t d = (int64_t)first + __popc(same & lt);
+        for (int k = 0; k < 6; ++k) sh.v[k][t] = xs[k * n + i];
+        const uint8_t al = as[i];
+        sh.pid[t] = pids[i];
+        sh.alive[t] = al;
+        key = exact_brick_key(xs, n, i, al, x0, y0, z0, idx, idy, idz, offs, nx, ny, nz, dead_key);
+    }
+    const BlockRun r = block_runs(key, cursor, tile_off, sh.run);
+    if (r.dest < 0) return;
+    const int64_t d = r.dest;
 #pragma unroll
-    for (int k = 0; k < 6; ++k) xd[k * n + d] = v[k];
-    pidd[d] = id;
-    ad[d] = al;
+    for (int k = 0; k < 6; ++k) xd[k * n + d] = sh.v[k][r.src];
+    pidd[d] = sh.pid[r.src];
+    ad[d] = sh.alive[r.src];
 }
 
 __global__ void exact_import_kernel(const double* __restrict__ s0, const double* __restrict__ s1,
@@ -859,9 +933,10 @@ int fast_sort(pt_ctx* ctx, pt_fast_state* st, const pt_field* f, cudaStream_t s)
     PT_CHECK_LAUNCH("sort_scan_tiles_kernel");
     sort_scan_top_kernel<<<1, 1024, 0, s>>>(tile_off, tiles, nullptr);
     PT_CHECK_LAUNCH("sort_scan_top_kernel");
-    sort_scatter_kernel<<<gb, 256, 0, s>>>(cur, tile_off, n, f->offs, nx, ny, nz, nb, st->x, st->p, st->p2, st->pid,
-                                           st->alive, st->x_alt, st->p_alt, st->p2_alt, st->pid_alt, st->alive_alt);
-    PT_CHECK_LAUNCH("sort_scatter_kernel");
+    sort_scatter_block_kernel<<<(unsigned)((n + kScatterBlock - 1) / kScatterBlock), kScatterBlock, 0, s>>>(
+        cur, tile_off, n, f->offs, nx, ny, nz, nb, st->x, st->p, st->p2, st->pid, st->alive, st->x_alt, st->p_alt,
+        st->p2_alt, st->pid_alt, st->alive_alt);
+    PT_CHECK_LAUNCH("sort_scatter_block_kernel");
     std::swap(st->x, st->x_alt);
     std::swap(st->p, st->p_alt);
     std::swap(st->p2, st->p2_alt);
@@ -891,8 +966,9 @@ int launch_exact_sort(const double* xs, const int32_t* pids, const uint8_t* as, 
     PT_CHECK_LAUNCH("sort_scan_tiles_kernel");
     sort_scan_top_kernel<<<1, 1024, 0, s>>>(tile_off, tiles, nullptr);
     PT_CHECK_LAUNCH("sort_scan_top_kernel");
-    exact_scatter_kernel<<<gb, 256, 0, s>>>(cursor, tile_off, n, g.xmin, g.ymin, g.zmin, idx, idy, idz, f->offs, nx, ny,
-                                            nz, nb, xs, pids, as, xd, pidd, ad);
+    exact_scatter_kernel<<<(unsigned)((n + kScatterBlock - 1) / kScatterBlock), kScatterBlock, 0, s>>>(
+        cursor, tile_off, n, g.xmin, g.ymin, g.zmin, idx, idy, idz, f->offs, nx, ny, nz, nb, xs, pids, as, xd, pidd,
+        ad);
     PT_CHECK_LAUNCH("exact_scatter_kernel");
     (void)num_sms;
     return PT_OK;
@@ -1092,32 +1168,37 @@ __global__ void __launch_bounds__(kBatchTile) batch_scatter_kernel(const uint32_
                                                                    const int* __restrict__ n_tiles,
                                                                    BatchStateDev st0, BatchStateDev st1)
 {
-    const int lane = threadIdx.x & 31;
-    const unsigned lt = (1u << lane) - 1u;
+    // one tile per block at a time, scattered as in sort_scatter_block_kernel
+    __shared__ ScatterStage sh;
     const int64_t cap = st0.cap;
     const int nt = *n_tiles;
-    for (int t = blockIdx.x; t < nt; t += gridDim.x) {
-        const BatchTile T = tiles[t];
+    const int t = threadIdx.x;
+    for (int tl = blockIdx.x; tl < nt; tl += gridDim.x) {
+        const BatchTile T = tiles[tl];
         const BatchCampaignDev& C = camps[T.campaign];
         if (!batch_sort_due(C)) continue;  // uniform over the block
         const BatchStateDev from = C.par ? st1 : st0, to = C.par ? st0 : st1;
-        const int64_t base = C.slot0 - C.dense_base;
-        const bool valid = (int)threadIdx.x < T.count;
-        const unsigned act = __ballot_sync(0xffffffffu, valid);
-        if (!valid) continue;
-        const int64_t i = T.begin + threadIdx.x;
-        const uint32_t key = keys[i];
-        const unsigned same = __match_any_sync(act, key);
-        const int leader = __ffs(same) - 1;
-        uint32_t first = 0;
-        if (lane == leader) first = atomicAdd(&cursor[key], (uint32_t)__popc(same)) + tile_off[key / kScanTile];
-        first = __shfl_sync(same, first, leader);
-        const int64_t d = (int64_t)first + __popc(same & lt) + base;
-        to.x[d] = from.x[i]; to.x[cap + d] = from.x[cap + i]; to.x[2 * cap + d] = from.x[2 * cap + i];
-        to.p[d] = from.p[i]; to.p[cap + d] = from.p[cap + i]; to.p[2 * cap + d] = from.p[2 * cap + i];
-        to.p2[d] = from.p2[i];
-        to.pid[d] = from.pid[i];
-        to.alive[d] = from.alive[i];
+        uint32_t key = kPastEnd;
+        if (t < T.count) {
+            const int64_t i = T.begin + t;
+            key = keys[i];
+            sh.x[0][t] = from.x[i]; sh.x[1][t] = from.x[cap + i]; sh.x[2][t] = from.x[2 * cap + i];
+            sh.p[0][t] = from.p[i]; sh.p[1][t] = from.p[cap + i]; sh.p[2][t] = from.p[2 * cap + i];
+            sh.p2[t] = from.p2[i];
+            sh.pid[t] = from.pid[i];
+            sh.alive[t] = from.alive[i];
+        }
+        const BlockRun r = block_runs(key, cursor, tile_off, sh.run);
+        if (r.dest >= 0) {
+            const int64_t d = r.dest + C.slot0 - C.dense_base;
+            const int q = r.src;
+            to.x[d] = sh.x[0][q]; to.x[cap + d] = sh.x[1][q]; to.x[2 * cap + d] = sh.x[2][q];
+            to.p[d] = sh.p[0][q]; to.p[cap + d] = sh.p[1][q]; to.p[2 * cap + d] = sh.p[2][q];
+            to.p2[d] = sh.p2[q];
+            to.pid[d] = sh.pid[q];
+            to.alive[d] = sh.alive[q];
+        }
+        __syncthreads();  // the next tile's staging overwrites sh
     }
 }
 
