@@ -977,10 +977,15 @@ def run_precision(args, dev):
     D_mumu(mu, tau) and <dmu^2>(tau) (32 log lags x 20 |mu| bins, cells with
     >= 100 pairs) and D_pp(tau) (same lags, all particles).  An FP64 run from
     positions moved by one ulp gives the floor set by chaotic divergence: the
-    statistics of two FP64 runs differ by that much already."""
+    statistics of two FP64 runs differ by that much already.  Each product is
+    also judged cell by cell against the FP64 statistic's own standard error
+    (batch means over 16 particle batches; precision.rel_err).  mu0 = 0.5 is
+    an edge of the 20 |mu| bins, so the cells a form's first saves fill can
+    differ from the FP64 ones (the test of the forms injects at 0.525)."""
     import torch
 
     from particle_transport_b200 import fields as F
+    from particle_transport_b200 import precision as P
     from particle_transport_b200 import runner as R
     from particle_transport_b200 import stats as S
     from particle_transport_b200.fields import FieldLibrary
@@ -1034,21 +1039,41 @@ def run_precision(args, dev):
             ens.close()
         return cache, final, time.perf_counter() - t0
 
-    def dmumu(mu):
+    batches = 16  # independent particle batches for the FP64 statistics' standard errors
+    sub = npart // batches
+
+    def dmumu_acc(mu):
         acc = S.new_dmumu_accumulators(len(lags), 20, device=dev)
         S.process_mu_chunk_dmumu(mu, lags, edges, acc["particle_counts"], acc["particle_means"],
                                  acc["particle_m2s"], acc["pair_sum_squares"], acc["pair_counts"],
                                  acc["dmumu_counts"], acc["dmumu_sum_delta"], acc["dmumu_sum_delta2"],
                                  layout="particle_fastest")
-        a = {k: v.cpu().numpy() for k, v in acc.items()}
-        d = S.compute_dmumu_arrays_full(a["dmumu_counts"], a["dmumu_sum_delta"], a["dmumu_sum_delta2"], tau, tau, 100)
-        return d["dmumu_raw_norm"], a["particle_means"], a["dmumu_counts"]
+        return {k: v.cpu().numpy() for k, v in acc.items()}
 
-    def phase_space(form, st, dt, p0):
+    def dmumu(mu, with_se=False):
+        a = dmumu_acc(mu)
+        d = S.compute_dmumu_arrays_full(a["dmumu_counts"], a["dmumu_sum_delta"], a["dmumu_sum_delta2"], tau, tau, 100)
+        se = None
+        if with_se:
+            parts = [dmumu_acc(mu[:, g * sub:(g + 1) * sub].contiguous()) for g in range(batches)]
+            n_p = a["particle_counts"].astype(np.float64)
+            with np.errstate(divide="ignore", invalid="ignore"):
+                se_pm = np.sqrt(a["particle_m2s"] / (n_p - 1.0) / n_p) / np.abs(a["particle_means"])
+            se = {"D": P.ratio_se([q["dmumu_sum_delta2"] for q in parts], [q["dmumu_counts"] for q in parts]),
+                  "pm": se_pm}
+        return d["dmumu_raw_norm"], a["particle_means"], a["dmumu_counts"], se
+
+    def dpp_add(acc, mom, p0):
+        S.process_momenta_chunk_dpp(mom, lags, p0, acc["counts"], acc["sum_delta_p"], acc["sum_delta_p2"],
+                                    acc["sum_delta_p_norm"], acc["sum_delta_p_norm2"])
+
+    def phase_space(form, st, dt, p0, with_se=False):
         """D_pp over all particles from phase-space caches of ps_chunk
         particles (add-into accumulators, p0 fixed across chunks), plus the
-        positions of the first nsub particles at 1 and 10 T_g0."""
+        positions of the first nsub particles at 1 and 10 T_g0; with_se, the
+        relative standard error of each lag from the particle batches."""
         acc = S.new_dpp_accumulators(len(lags), device=dev)
+        parts = []
         rows = {}
         for c0 in range(0, npart, ps_chunk):
             ps, _, _ = run(form, st, dt, "phase_space", c0, min(npart, c0 + ps_chunk))
@@ -1059,13 +1084,18 @@ def run_precision(args, dev):
                     rows[t] = ps[t * spg // stride, 0:3, :nsub].double().cpu().numpy()
             mom = ps[:, 3:6, :].contiguous()
             del ps
-            S.process_momenta_chunk_dpp(mom, lags, p0, acc["counts"], acc["sum_delta_p"], acc["sum_delta_p2"],
-                                        acc["sum_delta_p_norm"], acc["sum_delta_p_norm2"])
+            dpp_add(acc, mom, p0)
+            if with_se:
+                for b0 in range(0, mom.shape[2], sub):
+                    q = S.new_dpp_accumulators(len(lags), device=dev)
+                    dpp_add(q, mom[:, :, b0:b0 + sub].contiguous(), p0)
+                    parts.append({k: v.cpu().numpy() for k, v in q.items()})
             del mom
         a = {k: v.cpu().numpy() for k, v in acc.items()}
         d = S.compute_dpp_arrays(a["counts"], a["sum_delta_p"], a["sum_delta_p2"], a["sum_delta_p_norm"],
                                  a["sum_delta_p_norm2"], tau, tau)
-        return d["dpp_raw_norm"], rows, p0
+        se = P.ratio_se([q["sum_delta_p_norm2"] for q in parts], [q["counts"] for q in parts]) if with_se else None
+        return d["dpp_raw_norm"], rows, p0, se
 
     def rel(a, b, w=None):
         m = np.isfinite(a) & np.isfinite(b) & (np.abs(b) > 0)
@@ -1092,15 +1122,18 @@ def run_precision(args, dev):
         p0 = None
         for form in ("f64", "f64_1ulp", "f32", "bf16"):
             mu, final, secs = run(form, st_pert if form == "f64_1ulp" else st, dt, "mu", 0, npart)
-            D, pmean, counts = dmumu(mu)
+            D, pmean, counts, se = dmumu(mu, with_se=form == "f64")
             mu10 = mu[10 * spg // stride].cpu().numpy()
             del mu
             torch.cuda.empty_cache()
-            Dpp, rows, p0 = phase_space(form, st_pert if form == "f64_1ulp" else st, dt, p0)
+            Dpp, rows, p0, se_pp = phase_space(form, st_pert if form == "f64_1ulp" else st, dt, p0,
+                                               with_se=form == "f64")
+            if se is not None:
+                se["Dpp"] = se_pp
             p = np.stack([final[k] for k in ("p1", "p2", "p3")])
             gam = np.sqrt(1 + (np.linalg.norm(p, axis=0) / (F.M_P * F.C_LIGHT)) ** 2)
             res[form] = dict(D=D, pm=pmean, counts=counts, Dpp=Dpp, rows=rows, gam=gam, mu10=mu10,
-                             rate=npart * (nsteps - 1) / secs, secs=secs)
+                             rate=npart * (nsteps - 1) / secs, secs=secs, se=se)
             torch.cuda.empty_cache()
         ref = res["f64"]
         e = {"f64_particle_steps_per_s": ref["rate"], "f64_s": ref["secs"],
@@ -1117,7 +1150,12 @@ def run_precision(args, dev):
                                              "max": float(np.max(np.abs(r["gam"] / ref["gam"] - 1)))},
                        "D_mumu_raw_norm_rel_err": rel(r["D"], ref["D"], ref["counts"].astype(np.float64)),
                        "delta_mu2_particle_mean_rel_err": rel(r["pm"], ref["pm"]),
-                       "D_pp_raw_norm_rel_err": rel(r["Dpp"], ref["Dpp"])}
+                       "D_pp_raw_norm_rel_err": rel(r["Dpp"], ref["Dpp"]),
+                       # the per-cell test of the precision forms against the FP64 sampling error
+                       "against_sampling_error": {
+                           "D_mumu": P.rel_err(r["D"], ref["D"], ref["se"]["D"], ref["counts"] >= 100),
+                           "delta_mu2": P.rel_err(r["pm"], ref["pm"], ref["se"]["pm"]),
+                           "D_pp": P.rel_err(r["Dpp"], ref["Dpp"], ref["se"]["Dpp"])}}
         out["energies"][f"{E:g}"] = e
         print(json.dumps({"precision_energy_GeV": E, **e}), flush=True)
         torch.cuda.empty_cache()

@@ -131,6 +131,24 @@ def test_fast_push_close_over_one_gyroperiod(cuda, storage, tol_particle, share,
     assert np.median(d) < tol_med, np.median(d)
 
 
+def test_bf16_mean_field_offset_off_axis(cuda):
+    """BF16 bricks store B less its per-component mean and add the mean back
+    after the interpolation.  With a uniform B0 added to Bx the mean field
+    points between x and z, so all three offsets are in play; the BF16 push
+    stays as close to the FP64 push over one gyroperiod as in the test above,
+    and the FP32-brick push (no offset) stays within its own bound."""
+    pb = small_problem(n=16, n_particles=1000, u_over_c=1e-4)
+    pb.fields = [pb.fields[0] + pb.B0, *pb.fields[1:]]
+    (mu_o, _, _, _), _ = run_both(pb, 65, 4, "mu")
+    for storage, tol_particle, share in (("brick_f32", 2e-3, 0.99), ("brick_bf16", 0.05, 0.99)):
+        mu_f, _, _ = _fast_mu(pb, storage, 65, 4)
+        d = np.abs(mu_f - mu_o)
+        assert np.all(np.isfinite(mu_f)), storage
+        per_particle = d.max(axis=0)
+        assert np.mean(per_particle < tol_particle) >= share, (storage, np.sort(per_particle)[-12:])
+        assert np.median(d) < 0.02, (storage, np.median(d))
+
+
 def test_xpair_layout_bit_identical_to_bf16(cuda):
     """The x-pair records hold the same BF16 values and the gather adds the
     corners in the same order: identical trajectories."""
