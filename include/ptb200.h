@@ -47,7 +47,9 @@ enum {
 enum {
     PT_FIELD_REF_F64 = 0, /* six column-major Float64 arrays, SI units (parity form)        */
     PT_FIELD_BRICK_F32 = 1, /* Morton 8^3 bricks, 6 comps interleaved per node, Float32      */
-    PT_FIELD_BRICK_BF16 = 2, /* Morton 8^3 bricks, 6 comps interleaved per node, bfloat16     */
+    PT_FIELD_BRICK_BF16 = 2, /* Morton 8^3 bricks, 6 comps interleaved per node, bfloat16;
+                                B is stored less its grid mean per component (computed at
+                                upload), which the push adds back after the interpolation */
     PT_FIELD_BRICK_BF16_XPAIR = 3, /* as BF16, each 32-byte record holds a node and its +x neighbour:
                                       the 8 corners of a cell are 4 x 32-byte loads          */
     PT_FIELD_BRICK_F64 = 4 /* Morton 8^3 bricks of Float64 SI values in two planes: (Bx, By, Bz, ux)
@@ -413,7 +415,7 @@ int pt_reconstruct_mu(pt_ctx* ctx, const void* pos, const void* mom, int64_t chu
  * position (random mode); draw 3: z (isotropic) or phi (fixed mu); draw 4:
  * phi (isotropic).  For fixed mu, B at the position is the trilinear sample
  * of the field's own values (FP64 for PT_FIELD_REF_F64; the stored FP32/BF16
- * values for bricks).  Positions are exact; momenta agree with a host
+ * values for bricks, with the BF16 forms' mean field added back).  Positions are exact; momenta agree with a host
  * restatement to the last bits of cos/sin.  Synchronous: returns PT_ERR_ARG
  * ("cannot use fixed-mu injection where local B is zero or non-finite", as
  * the reference) after the kernel if any particle met such a field.
