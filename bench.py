@@ -73,6 +73,9 @@ def parse():
     ap.add_argument("--serve-jobs", type=int, default=100, help="jobs of the serving stream")
     ap.add_argument("--serve-cmp", type=int, default=16, help="jobs of the FP32-vs-FP64 serving comparison")
     ap.add_argument("--serve-all", action="store_true", help="also serve the stream with every job in every epoch")
+    ap.add_argument("--serve-fill", type=int, default=1 << 18, help="particles the server's epochs are filled to")
+    ap.add_argument("--serve-fill-sweep", default="",
+                    help="comma list of epoch fills to serve the same stream with (reported as fill_sweep)")
     ap.add_argument("--precision", action="store_true",
                     help="run only the plain-vs-precision study (256^3, 3 energies) and print its JSON line")
     ap.add_argument("--precision-key-particles", type=int, default=1048576,
@@ -1207,9 +1210,9 @@ def run_serving(args, dev, rate=4.0):
 
     libs = make_libs("brick_bf16")
 
-    def serve(libraries, arrivals, specs, push, schedule="srpt"):
+    def serve(libraries, arrivals, specs, push, schedule="srpt", fill=args.serve_fill):
         srv = CampaignServer(libraries, B0, hbm_budget_bytes=150e9, capacity=1 << 27, max_jobs=len(specs), push=push,
-                             schedule=schedule)
+                             schedule=schedule, fill_particles=fill)
         torch.cuda.synchronize()
         t_start = time.perf_counter()
         nxt = 0
@@ -1265,7 +1268,13 @@ def run_serving(args, dev, rate=4.0):
                  "stream": f"{args.serve_jobs} jobs, Poisson {rate}/s, 16K-8M particles, 10-300 T_g0, 1-300 GeV, "
                            "256^3 and 512^3 libraries x 4 modes, isotropic or fixed-mu",
                  "init": "on the device (pt_particles_init_device)", "hbm_budget_GB": 150,
-                 "schedule": "srpt: least work left first, epochs filled to 262144 particles"})
+                 "schedule": f"srpt: least work left first, epochs filled to {args.serve_fill} particles"})
+    if args.serve_fill_sweep:
+        main["fill_sweep"] = {}
+        for fill in (int(v) for v in args.serve_fill_sweep.split(",") if v):
+            r = serve(libs, arrivals, specs, "f32", fill=fill)
+            main["fill_sweep"][str(fill)] = {k: r[k] for k in ("p50_s", "p99_s", "mean_s", "wall_s", "busy_rate",
+                                                               "aggregate_rate", "epochs")}
     if args.serve_all:
         every = serve(libs, arrivals, specs, "f32", schedule="all")
         main["schedule_all"] = {k: every[k] for k in ("p50_s", "p99_s", "mean_s", "wall_s", "busy_rate", "epochs")}
