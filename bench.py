@@ -46,8 +46,8 @@ PEAKS_FALLBACK = {"hbm_gbs": 6650.0, "source": "fallback"}
 # components x 2 B.  Per launch each particle also reads and writes its
 # state (x 24 B, p 12 B, |p|^2 8 B, id 4 B, alive 1 B) and writes one 4-byte
 # mu per save row.
-GATHER_BYTES = {"brick_bf16": 96, "brick_f32": 192, "ref_f64": 384}
-STATE_BYTES = {"brick_bf16": 49, "brick_f32": 49, "ref_f64": 49}
+GATHER_BYTES = {"brick_bf16": 96, "brick_bf16x": 96, "brick_f32": 192, "ref_f64": 384}
+STATE_BYTES = {"brick_bf16": 49, "brick_bf16x": 49, "brick_f32": 49, "ref_f64": 49}
 
 
 def parse():
