@@ -340,8 +340,9 @@ int launch_brick_convert(const double* const comps[6], const pt_grid& g, double 
 // rows [rows][n] of a time-fastest mu cache [n][pitch] (save r of particle p
 // at p * pitch + r), for the row-by-row egress of pt_push_run
 int launch_tf_to_rows(const float* tf, int64_t n, int pitch, int rows, float* out, cudaStream_t s);
-// mean of the three B components (device arrays of nn values), summed in a
-// fixed order (the same bits on every call); waits for the stream
+// mean of the finite values of each of the three B components (device
+// arrays of nn values; 0 when none is finite), summed in a fixed order (the
+// same bits on every call); waits for the stream
 int field_means(pt_ctx* ctx, const double* const comps[6], int64_t nn, double mean[3], cudaStream_t s);
 
 struct DmumuArgs {

@@ -795,44 +795,50 @@ int launch_tf_to_rows(const float* tf, int64_t n, int pitch, int rows, float* ou
     return PT_OK;
 }
 
-// Sums of Bx, By, Bz: kMeanBlocks blocks each add a contiguous range (a
-// strided sum per thread, then a tree over the block), and one thread adds
-// the block sums in block order -- a fixed order, so the same bits each time.
+// Sums and counts of the finite values of Bx, By, Bz: kMeanBlocks blocks
+// each add a contiguous range (a strided sum per thread, then a tree over the
+// block), and one thread adds the block sums in block order -- a fixed order,
+// so the same bits each time.  A non-finite node is left out of the mean
+// (it stays non-finite in the bricks, where only its own cells see it).
 constexpr int kMeanBlocks = 256, kMeanThreads = 256;
 __global__ void __launch_bounds__(kMeanThreads) component_sum_kernel(const double* __restrict__ bx,
                                                                      const double* __restrict__ by,
                                                                      const double* __restrict__ bz, int64_t nn,
                                                                      double* __restrict__ partial)
 {
-    __shared__ double sh[3][kMeanThreads];
+    __shared__ double sh[6][kMeanThreads];
     const int64_t per = (nn + gridDim.x - 1) / gridDim.x;
     const int64_t lo = (int64_t)blockIdx.x * per, hi = min(nn, lo + per);
-    double s0 = 0.0, s1 = 0.0, s2 = 0.0;
+    double s[3] = {0.0, 0.0, 0.0}, k[3] = {0.0, 0.0, 0.0};
     for (int64_t t = lo + threadIdx.x; t < hi; t += blockDim.x) {
-        s0 += bx[t];
-        s1 += by[t];
-        s2 += bz[t];
+        const double v[3] = {bx[t], by[t], bz[t]};
+        for (int c = 0; c < 3; ++c)
+            if (isfinite(v[c])) {
+                s[c] += v[c];
+                k[c] += 1.0;
+            }
     }
-    sh[0][threadIdx.x] = s0;
-    sh[1][threadIdx.x] = s1;
-    sh[2][threadIdx.x] = s2;
+    for (int c = 0; c < 3; ++c) {
+        sh[c][threadIdx.x] = s[c];
+        sh[3 + c][threadIdx.x] = k[c];
+    }
     __syncthreads();
     for (int w = kMeanThreads / 2; w > 0; w >>= 1) {
         if (threadIdx.x < w)
-            for (int c = 0; c < 3; ++c) sh[c][threadIdx.x] += sh[c][threadIdx.x + w];
+            for (int c = 0; c < 6; ++c) sh[c][threadIdx.x] += sh[c][threadIdx.x + w];
         __syncthreads();
     }
     if (threadIdx.x == 0)
-        for (int c = 0; c < 3; ++c) partial[3 * blockIdx.x + c] = sh[c][0];
+        for (int c = 0; c < 6; ++c) partial[6 * blockIdx.x + c] = sh[c][0];
 }
 
 __global__ void partial_sum_kernel(const double* __restrict__ partial, int blocks, double* __restrict__ out)
 {
     if (threadIdx.x != 0 || blockIdx.x != 0) return;
-    double s[3] = {0.0, 0.0, 0.0};
+    double s[6] = {0.0, 0.0, 0.0, 0.0, 0.0, 0.0};
     for (int b = 0; b < blocks; ++b)
-        for (int c = 0; c < 3; ++c) s[c] += partial[3 * b + c];
-    for (int c = 0; c < 3; ++c) out[c] = s[c];
+        for (int c = 0; c < 6; ++c) s[c] += partial[6 * b + c];
+    for (int c = 0; c < 6; ++c) out[c] = s[c];
 }
 
 int field_means(pt_ctx* ctx, const double* const comps[6], int64_t nn, double mean[3], cudaStream_t s)
@@ -840,20 +846,20 @@ int field_means(pt_ctx* ctx, const double* const comps[6], int64_t nn, double me
     (void)ctx;
     if (nn <= 0) return fail(PT_ERR_ARG, "empty field");
     double* d = nullptr;
-    cudaError_t e = cudaMalloc(&d, sizeof(double) * (3 * kMeanBlocks + 3));
+    cudaError_t e = cudaMalloc(&d, sizeof(double) * (6 * kMeanBlocks + 6));
     if (e != cudaSuccess) {
         cudaGetLastError();
         return fail(PT_ERR_OOM, "field mean scratch allocation failed");
     }
     component_sum_kernel<<<kMeanBlocks, kMeanThreads, 0, s>>>(comps[0], comps[1], comps[2], nn, d);
-    partial_sum_kernel<<<1, 32, 0, s>>>(d, kMeanBlocks, d + 3 * kMeanBlocks);
-    double sums[3] = {0.0, 0.0, 0.0};
+    partial_sum_kernel<<<1, 32, 0, s>>>(d, kMeanBlocks, d + 6 * kMeanBlocks);
+    double sums[6] = {0.0, 0.0, 0.0, 0.0, 0.0, 0.0};
     e = cudaGetLastError();
-    if (e == cudaSuccess) e = cudaMemcpyAsync(sums, d + 3 * kMeanBlocks, sizeof(sums), cudaMemcpyDeviceToHost, s);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(sums, d + 6 * kMeanBlocks, sizeof(sums), cudaMemcpyDeviceToHost, s);
     if (e == cudaSuccess) e = cudaStreamSynchronize(s);
     cudaFree(d);
     if (e != cudaSuccess) return cuda_fail(e, "field means");
-    for (int c = 0; c < 3; ++c) mean[c] = sums[c] / (double)nn;
+    for (int c = 0; c < 3; ++c) mean[c] = sums[3 + c] > 0.0 ? sums[c] / sums[3 + c] : 0.0;
     return PT_OK;
 }
 

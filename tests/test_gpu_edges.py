@@ -132,3 +132,18 @@ def test_all_dead_particles_push(cuda, oracle):
     ac2 = R.run_push_host(flb, copy_state(pb.state), alive.copy(),
                           R.push_params(pb.dt, 40, 4, cache="mu", precision="f32", sort_every=8), col2)
     assert np.all(np.isnan(col2.mu)) and np.all(ac2 == 0)
+
+
+def test_bf16_field_with_a_nan_node(cuda):
+    """A non-finite node stays local in the BF16 bricks: their mean field is
+    taken over the finite nodes only, so only the particles whose cells
+    touch that node see NaN (all of them would, through the mean)."""
+    pb = small_problem(n=16, n_particles=500)
+    fields = [np.array(a, copy=True) for a in pb.fields]
+    fields[2].reshape(-1)[1234] = np.nan
+    flb = FieldLibrary(fields, pb.grid, "brick_bf16", B_ref_T=pb.B0)  # mean |B| of the field is NaN now
+    col = R.CacheCollector(500, R.n_saves(40, 4), "mu")
+    R.run_push_host(flb, copy_state(pb.state), np.ones(500, np.uint8),
+                    R.push_params(pb.dt, 40, 4, cache="mu", precision="f32"), col)
+    finite = np.isfinite(col.mu).all(axis=0)
+    assert 0.9 < finite.mean() <= 1.0, finite.mean()
