@@ -188,8 +188,9 @@ __device__ __forceinline__ void advance_particle(double& x, double& y, double& z
                         mu = mu_f32(px, py, pz, f[0], f[1], f[2]);
                     // rows: save r of every particle in one row; time-fastest
                     // (pitch > 0): a particle's saves side by side, so the 8
-                    // saves of a launch, written by this thread within a few
-                    // microseconds, merge in L2 into one whole DRAM sector
+                    // saves of a launch, written by this thread while it holds
+                    // the particle (~0.1 ms of a 64-step launch at 16.7M
+                    // particles), merge in L2 into one whole DRAM sector
                     const int64_t at = a.pitch > 0 ? pid * a.pitch + r : r * n + pid;
                     if (a.cache_f64) ((double*)a.cache)[at] = (double)mu;
                     else ((float*)a.cache)[at] = mu;
