@@ -306,7 +306,7 @@ def run_reference(args, ws, rank):
     ff = [np.asfortranarray(f.T) for f in fields_host]
     nthreads = host_threads()
     # size one step (a sample of the particles over 64 pushes) at ~3 s
-    n = 4096
+    n = min(4096, args.particles)
     while True:
         st = {k: np.ascontiguousarray(v[:n]).copy() for k, v in state.items()}
         t0 = time.perf_counter()
