@@ -64,9 +64,9 @@ def parse():
     ap.add_argument("--variant", type=int, default=1, help="push launch shape (pt_push_params.kernel_variant)")
     ap.add_argument("--lag-particles", type=int, default=1_048_576)
     ap.add_argument("--dpp-particles", type=int, default=262_144)
-    ap.add_argument("--e2e-gyroperiods", type=int, default=32,
-                    help="T_g0 per pt_push_run call in the e2e leg (the reference pushes a whole campaign, "
-                         "500 T_g0 at 512^3, per call)")
+    ap.add_argument("--e2e-gyroperiods", type=int, default=500,
+                    help="T_g0 per pt_push_run call in the e2e leg: the whole 512^3 campaign (500 T_g0), as the "
+                         "reference pushes a campaign per run_mu_cache_ensemble call")
     ap.add_argument("--skip", default="",
                     help="comma list of legs to skip: fp32b,fp64,lag,dpp,e2e,cpu,batch,serve,config1,precision")
     ap.add_argument("--cpu-seconds", type=float, default=10.0)
@@ -656,7 +656,7 @@ def run_ours(args, ws, rank, local):
             e2e_call(-1)
         dist_barrier(ws)
         t0 = time.perf_counter()
-        ncall = max(1, min(3, K // 3))
+        ncall = max(1, min(3 if G <= 100 else 2, K // 3))
         for _ in range(ncall):
             e2e_call(0)
         el = time.perf_counter() - t0
