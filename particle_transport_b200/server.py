@@ -217,7 +217,7 @@ class CampaignServer:
         n = 0
         keep = []
         st = self.admit_stats
-        need_of = self.__dict__.setdefault("_need", {})
+        need_of = self._need
         for jid, spec, arrival in self.queue:
             if keep:  # arrival order: every later job waits behind the first that does not fit
                 keep.append((jid, spec, arrival))
@@ -235,6 +235,7 @@ class CampaignServer:
                 t0 = time.perf_counter()
                 try:
                     self._admit(jid, spec, arrival)
+                    need_of.pop(jid, None)
                     n += 1
                     st["admitted"] += 1
                     st["admit_setup_s"] += time.perf_counter() - t0
