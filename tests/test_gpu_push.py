@@ -221,6 +221,20 @@ def test_host_run_fast_matches_device(cuda):
     assert np.array_equal(col.mu, mu_dev, equal_nan=True)
 
 
+def test_host_run_fast_matches_device_many_particles(cuda):
+    """pt_push_run with more particles than 8 rows of the 512 MB egress slot
+    hold (17M: 7 rows, i.e. 28-step chunks that do not line up with the
+    64-step sort cadence) gives the same mu cache as the device entry point:
+    the time-fastest chunks and their transpose to rows lose nothing."""
+    n, nsteps, stride = 17_000_000, 100, 4
+    pb = small_problem(n=16, n_particles=n, u_over_c=1e-4)
+    mu_dev, _, fl = _fast_mu(pb, "brick_bf16", nsteps, stride, sort_every=64)
+    col = R.CacheCollector(n, R.n_saves(nsteps, stride), "mu")
+    R.run_push_host(fl, copy_state(pb.state), np.ones(n, np.uint8),
+                    R.push_params(pb.dt, nsteps, stride, cache="mu", precision="f32", sort_every=64), col)
+    assert np.array_equal(col.mu, mu_dev, equal_nan=True)
+
+
 def test_errors_raise(cuda):
     from particle_transport_b200._lib import PtError
     pb = small_problem(n=8, n_particles=4)
