@@ -669,6 +669,26 @@ __global__ void energy_hist_kernel(const float* __restrict__ mom, int64_t chunk,
 
 size_t align16(size_t b) { return (b + 15) & ~(size_t)15; }
 
+// Particle slots per CTA (ppc <= max_ppc) and warps per (slot, lag group)
+// (parts): the most warps per CTA (at most 32), the larger ppc among equals.
+// With 55 lags (two groups) and room for five slots this gives 4 slots x 4
+// parts, 32 warps: 8.58e11 lag-pairs/s against 8.28e11 for 5 x 3 (30 warps).
+constexpr int kMaxParts = 8;
+void dmumu_shape(int max_ppc, int groups, int& ppc, int& parts)
+{
+    int best = 0;
+    ppc = 1;
+    parts = 1;
+    for (int c = 1; c <= std::max(1, max_ppc) && c * groups <= 32; ++c) {
+        const int pt = std::max(1, std::min(kMaxParts, 32 / (c * groups)));
+        if (c * groups * pt >= best) {
+            best = c * groups * pt;
+            ppc = c;
+            parts = pt;
+        }
+    }
+}
+
 }  // namespace
 
 // ------------------------------------------------------------------ host side
@@ -701,12 +721,9 @@ int run_dmumu_src(pt_ctx* ctx, const DmumuArgs& a, const Src& src, cudaStream_t 
         const size_t acc_bytes = (size_t)nl * a.n_bins * 24;
         size_t fixed = edge_bytes + std::max(acc_bytes, sizeof(WelfordPart) * 1024);
         bool smem_slots = fixed + slot_bytes <= budget;
-        int ppc;
-        if (smem_slots) ppc = (int)std::min<size_t>((budget - fixed) / slot_bytes, (size_t)(32 / groups));
-        else ppc = std::max(1, std::min(8, 32 / groups));
-        ppc = std::max(1, ppc);
-        // more warps share each staged series: split its bins over `parts` warps
-        const int parts = std::max(1, std::min(4, 32 / (ppc * groups)));
+        // more warps share each staged series: its start list is split over `parts` warps
+        int ppc, parts;
+        dmumu_shape(smem_slots ? (int)std::min<size_t>((budget - fixed) / slot_bytes, 32) : 8, groups, ppc, parts);
         const int threads = ppc * groups * parts * kWarp;
         size_t smem = fixed + (smem_slots ? (size_t)ppc * slot_bytes : 0);
         const int64_t tiles = (a.n + ppc - 1) / ppc;
@@ -1045,9 +1062,8 @@ int run_dmumu_noalloc(pt_ctx* ctx, const DmumuArgs& a, cudaStream_t s)
             return fail(PT_ERR_ARG, "pt_dmumu_accumulate_device_noalloc: nsave = " + std::to_string(a.nsave) +
                                         " is too long for on-chip staging with " + std::to_string(a.n_bins) +
                                         " bins; use pt_dmumu_accumulate_device");
-        int ppc = (int)std::min<size_t>((budget - fixed) / slot_bytes, (size_t)(32 / groups));
-        ppc = std::max(1, ppc);
-        const int parts = std::max(1, std::min(4, 32 / (ppc * groups)));
+        int ppc, parts;
+        dmumu_shape((int)std::min<size_t>((budget - fixed) / slot_bytes, 32), groups, ppc, parts);
         const int threads = ppc * groups * parts * kWarp;
         const size_t smem = fixed + (size_t)ppc * slot_bytes;
         // per-CTA partials: counts, sum, sum^2 per (lag, bin) and a Welford triple per lag
