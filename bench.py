@@ -711,7 +711,7 @@ def run_ours(args, ws, rank, local):
 # small case (profiles/dmumu_*.md, profiles/dpp_*.md).  These kernels are
 # bound by instruction issue, whose ceiling is one warp instruction per cycle
 # per SM sub-partition (4 per SM).
-WARP_INST_PER_PAIR = {"dmumu_kernel": 47.257e9 / 49.193e9, "dpp_kernel": 6.663e9 / 12.298e9}
+WARP_INST_PER_PAIR = {"dmumu_kernel": 47.59e9 / 49.193e9, "dpp_kernel": 6.663e9 / 12.298e9}
 
 
 def issue_roofline(kernel: str, pairs_per_s: float, clocks, device) -> dict:
